@@ -1,0 +1,179 @@
+/*
+ * velox_b200.h — C ABI of the B200 (sm_100a) rigid-body contact pipeline.
+ *
+ * The library replaces the reference engine's CUDA backend
+ * (src/backend_cuda.cu, class CudaBackend) behind its Backend interface
+ * (include/velox/backend.h:111-172). Every entry point takes plain pointers
+ * and sizes, returns a status code (never throws), and operates on one
+ * vxb_context = one backend instance = one CUDA stream on one device.
+ * Records crossing the ABI use the reference's host layouts
+ * (velox_b200_types.h), so the reference-side adapter passes
+ * `std::vector<Body>::data()` straight through.
+ *
+ * Status codes map onto the reference's error model
+ * (src/backend_cuda.cu:24-40, include/velox/backend.h:95-106):
+ *   VXB_ERR_OOM          -> BackendFailure(MemoryAllocation)
+ *   VXB_ERR_DEVICE_LOST  -> BackendFailure(DeviceLost)
+ *   VXB_ERR_TIMEOUT      -> BackendFailure(DeviceLost) (a bounded device wait gave up)
+ *   VXB_ERR_CAPACITY     -> VeloxCapacityExceeded(ContactCountOverflow)
+ *   VXB_ERR_NO_DEVICE    -> createCudaBackend() returning nullptr
+ *   others               -> VeloxRuntimeError(BackendUnavailable)
+ * Threading matches the reference backend: one owner thread per context.
+ */
+#ifndef VELOX_B200_H
+#define VELOX_B200_H
+
+#include "velox_b200_types.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Every declaration below is exported from libvelox_b200.so (the library is
+ * otherwise built with hidden visibility). */
+#pragma GCC visibility push(default)
+
+#define VXB_OK 0
+#define VXB_ERR_INVALID 1
+#define VXB_ERR_NO_DEVICE 2
+#define VXB_ERR_OOM 3
+#define VXB_ERR_DEVICE_LOST 4
+#define VXB_ERR_CAPACITY 5
+#define VXB_ERR_UNSUPPORTED 6
+#define VXB_ERR_TIMEOUT 7
+
+typedef struct vxb_context vxb_context;
+
+/* Per-step configuration of the device-resident world (World::step's inputs:
+ * include/velox/world.h:434-438 gravity/substeps, SolverOptions). */
+typedef struct vxb_step_config {
+    float dt;
+    vx_vec3 gravity;
+    int32_t substeps;
+    vx_solver_options solver;
+} vxb_step_config;
+
+/* Counters of the last device step (subset of velox::StepStats,
+ * include/velox/world.h:175-208, plus pipeline internals). */
+typedef struct vxb_step_stats {
+    uint32_t candidatePairs;     /* broad-phase pairs (narrowPhaseTests) */
+    uint32_t contacts;           /* generatedContacts */
+    uint32_t colors;             /* largest colour count of any island */
+    uint32_t islands;            /* contact islands solved */
+    uint32_t largestIsland;      /* contacts in the largest island */
+    uint32_t rewinds;            /* conservative-advancement rewinds */
+    uint32_t velocityIterations; /* sweeps per step (2*velocityIterations*substeps) */
+    uint32_t warmStarted;        /* contacts that inherited impulses */
+} vxb_step_stats;
+
+/* ---- library / context ------------------------------------------------ */
+
+const char* vxb_version(void);
+const char* vxb_status_string(int status);
+
+/* Creates a backend instance on `device` (createCudaBackend(),
+ * src/backend_cuda.cu:352-356 and :1020). Returns VXB_ERR_NO_DEVICE when no
+ * CUDA device is present (the reference returns nullptr). */
+int vxb_context_create(int device, vxb_context** out);
+/* Drains the stream and releases every device buffer (~CudaBackend,
+ * src/backend_cuda.cu:358-388). Never fails. */
+void vxb_context_destroy(vxb_context* ctx);
+/* Message of the last failure on this context ("" when none). */
+const char* vxb_context_last_error(const vxb_context* ctx);
+/* Launch subsequent work on `stream` (a cudaStream_t); null restores the
+ * context's own stream. */
+int vxb_context_set_stream(vxb_context* ctx, void* stream);
+/* Number of kernel launches this context issued since it was created. */
+uint64_t vxb_context_launch_count(const vxb_context* ctx);
+
+/* ---- Backend interface over host arrays ------------------------------- */
+
+/* Backend::integrate (backend.h:116; CudaBackend::integrate,
+ * src/backend_cuda.cu:393-403): first-substep velocity integration. */
+int vxb_backend_integrate(vxb_context* ctx, vx_body* bodies, uint32_t n, vx_vec3 gravity,
+                          float dt);
+/* Backend::findContacts (backend.h:125-127; src/backend_cuda.cu:405-567):
+ * speculative contacts of every candidate pair for a step of `dt`. Contacts
+ * stay device-resident; *count receives their number, copy them with
+ * vxb_backend_copy_contacts. Hull geometry comes from `soup`. */
+int vxb_backend_find_contacts(vxb_context* ctx, const vx_body* bodies, uint32_t n,
+                              const vx_soup* soup, float dt, uint32_t* count);
+/* Copies the contacts of the last find (sorted by (a, b, point)). */
+int vxb_backend_copy_contacts(vxb_context* ctx, vx_contact* out, uint32_t cap);
+/* Backend::solveVelocities (backend.h:132-135; src/backend_cuda.cu:569-689).
+ * With warmStart != 0 the contacts are sorted, coloured and written back in
+ * colour order, exactly as the reference writes back its colour-sorted copy. */
+int vxb_backend_solve_velocities(vxb_context* ctx, vx_body* bodies, uint32_t n,
+                                 vx_contact* contacts, uint32_t m, float dt, int warmStart,
+                                 const vx_solver_options* options, uint32_t* iterations);
+/* Backend::advanceSubsteps (backend.h:139-144; src/backend_cuda.cu:691-761).
+ * *advanced = 0 when the request needs the host path (iteration policy
+ * Adaptive), matching the reference's `return false`. */
+int vxb_backend_advance_substeps(vxb_context* ctx, vx_body* bodies, uint32_t n,
+                                 vx_contact* contacts, uint32_t m, vx_vec3 gravity, float h,
+                                 int substeps, const vx_solver_options* options, int* advanced,
+                                 uint32_t* iterations);
+/* Backend::fetchImpulses (backend.h:148; src/backend_cuda.cu:763-768). */
+int vxb_backend_fetch_impulses(vxb_context* ctx, vx_contact* contacts, uint32_t m);
+/* Backend::invalidateCaches (backend.h:150; src/backend_cuda.cu:770-784). */
+int vxb_backend_invalidate(vxb_context* ctx);
+
+/* ---- device-resident world: the whole World::step on the GPU --------------
+ * One call runs src/world.cpp:3830-4521's contact pipeline for every world
+ * of the batch without host round trips: orientation normalisation,
+ * first-substep gravity, broad phase, narrow phase, warm-start matching,
+ * colouring, the substep loop, the conservative-advancement rewind,
+ * split-impulse position correction and the previous-contact cache.
+ * Batches: `worldOfBody` (nullable = one world) assigns each body to a world;
+ * bodies of one world must be contiguous and worlds never interact. */
+int vxb_world_load(vxb_context* ctx, const vx_body* bodies, uint32_t n, const vx_soup* soup,
+                   const uint32_t* worldOfBody);
+int vxb_world_configure(vxb_context* ctx, const vxb_step_config* config);
+int vxb_world_step(vxb_context* ctx, int steps);
+int vxb_world_read_bodies(vxb_context* ctx, vx_body* out, uint32_t n);
+/* position xyz + orientation xyzw per body (7 floats). */
+int vxb_world_read_poses(vxb_context* ctx, float* out, uint32_t n);
+/* force xyz + torque xyz per body (6 floats), consumed and cleared by the
+ * next step like Body::force/torque. */
+int vxb_world_write_forces(vxb_context* ctx, const float* in, uint32_t n);
+int vxb_world_read_contacts(vxb_context* ctx, vx_contact* out, uint32_t cap, uint32_t* count);
+int vxb_world_stats(vxb_context* ctx, vxb_step_stats* out);
+
+/* ---- individual stages (parity testing) --------------------------------- */
+
+/* Candidate pairs (i<j) of the sorted-grid broad phase, returned sorted
+ * ascending as (i<<32)|j: the pair set of gridPairsKernel/oversizePairsKernel
+ * and allPairsContactsKernel (src/backend_cuda.cu:174-299). */
+int vxb_stage_pairs(vxb_context* ctx, const vx_body* bodies, uint32_t n, float dt,
+                    uint64_t* out, uint32_t cap, uint32_t* count);
+/* collidePair (src/narrowphase.h:678-714) for each listed pair; contacts are
+ * returned grouped in pair order, counts[p] per pair, *total overall. */
+int vxb_stage_collide(vxb_context* ctx, const vx_body* bodies, uint32_t n, const vx_soup* soup,
+                      const uint64_t* pairs, uint32_t npairs, float dt, vx_contact* out,
+                      uint32_t cap, uint32_t* counts, uint32_t* total);
+/* Greedy first-free-bit colouring (src/backend_cuda.cu:603-630) of contacts
+ * already in (a, b, point) order. */
+int vxb_stage_color(vxb_context* ctx, const vx_body* bodies, uint32_t n,
+                    const vx_contact* contacts, uint32_t m, int32_t* colorOf,
+                    uint32_t* numColors);
+
+/* ---- scene construction (host only) ------------------------------------- */
+
+/* Shape-level specs of a benchmark workload (1..5); `size` overrides its
+ * count (lattice side, bodies, pyramids or worlds; 0 = full size). */
+int vxb_scene_generate(int config, uint64_t seed, uint32_t size, vx_shape_spec* specs,
+                       uint32_t cap, uint32_t* count, vx_vec3* pool, uint32_t poolCap,
+                       uint32_t* poolCount);
+/* Bodies + hull soup from specs, following World::add* (src/world.cpp:646-985). */
+int vxb_bodies_from_specs(const vx_shape_spec* specs, uint32_t n, const vx_vec3* pool,
+                          vx_body* bodies, vx_vec3* hullPoints, uint32_t hullCap,
+                          uint32_t* hullCount, uint32_t* faceIndices, uint32_t faceCap,
+                          uint32_t* faceIndexCount);
+
+#pragma GCC visibility pop
+
+#ifdef __cplusplus
+}  /* extern "C" */
+#endif
+
+#endif /* VELOX_B200_H */

@@ -1,0 +1,210 @@
+/*
+ * velox_b200_types.h — plain-C data layouts shared by the B200 contact
+ * pipeline's C ABI, its CPU oracle and its tests.
+ *
+ * The records are byte-compatible with the reference engine's host arrays so
+ * a `std::vector<velox::Body>` / `std::vector<velox::Contact>` can be handed
+ * across the ABI as a raw pointer without repacking:
+ *
+ *   vx_body     <-> velox::Body     include/velox/body.h:128-345   (320 B, align 64)
+ *   vx_contact  <-> velox::Contact  include/velox/backend.h:63-83  (128 B, align 64)
+ *   vx_solver_options <-> velox::SolverOptions include/velox/solver.h:23-35 (24 B)
+ *   vx_ccd_tuning <-> velox::BodyCcdTuning include/velox/ccd.h:89-96 (52 B)
+ *
+ * Field order, widths and padding follow the reference exactly (the offsets
+ * are asserted at compile time below and against the reference headers by
+ * the reference-side adapter).
+ */
+#ifndef VELOX_B200_TYPES_H
+#define VELOX_B200_TYPES_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VX_ALIGN64 __attribute__((aligned(64)))
+
+typedef struct vx_vec3 { float x, y, z; } vx_vec3;
+typedef struct vx_quat { float x, y, z, w; } vx_quat;
+
+/* velox::ShapeType (include/velox/body.h:59-62) */
+enum {
+    VX_SHAPE_SPHERE = 0, VX_SHAPE_PLANE = 1, VX_SHAPE_BOX = 2, VX_SHAPE_CAPSULE = 3,
+    VX_SHAPE_MESH = 4, VX_SHAPE_HULL = 5, VX_SHAPE_COMPOUND = 6, VX_SHAPE_CYLINDER = 7,
+    VX_SHAPE_CONE = 8, VX_SHAPE_ROUNDED_BOX = 9, VX_SHAPE_ELLIPSOID = 10
+};
+/* velox::MotionType (body.h:65-69) */
+enum { VX_MOTION_STATIC = 0, VX_MOTION_KINEMATIC = 1, VX_MOTION_DYNAMIC = 2 };
+/* velox::MotionQuality (ccd.h) */
+enum { VX_QUALITY_LOW = 0, VX_QUALITY_MEDIUM = 1, VX_QUALITY_HIGH = 2, VX_QUALITY_LOCKED = 3 };
+/* velox::GeometryQuality (body.h:77) */
+enum { VX_GEOM_NORMAL = 0, VX_GEOM_ROBUST = 1, VX_GEOM_PARANOID = 2 };
+/* velox::MaterialCombineMode (body.h:84-86) */
+enum { VX_COMBINE_AVERAGE = 0, VX_COMBINE_GEOMETRIC_MEAN = 1, VX_COMBINE_MINIMUM = 2,
+       VX_COMBINE_MULTIPLY = 3, VX_COMBINE_MAXIMUM = 4 };
+/* velox::FrictionModel (solver.h:11-14) */
+enum { VX_FRICTION_TWO_AXIS = 0, VX_FRICTION_CONE_BLOCK = 1 };
+
+typedef struct vx_ccd_settings {
+    uint8_t quality;
+    uint8_t pad0[3];
+    uint32_t maxAdvancementIterations;
+    uint32_t maxRootFindIterations;
+    float distanceTolerance;
+    float timeTolerance;
+    uint8_t enableRotationalCcd;
+    uint8_t enableCompoundCcd;
+    uint8_t useBrentRootFinder;
+    uint8_t pad1;
+    uint32_t meshBvhMaxDepth;
+    float speculativeMargin;
+} vx_ccd_settings;
+
+typedef struct vx_ccd_tuning {
+    uint8_t quality;
+    uint8_t pad0[3];
+    float collisionMargin;
+    float speculativeDistance;
+    uint8_t enableContinuous;
+    uint8_t pad1[3];
+    float minVelocityForCCD;
+    vx_ccd_settings ccdSettings;
+} vx_ccd_tuning;
+
+typedef struct VX_ALIGN64 vx_body {
+    vx_vec3 position;
+    vx_quat orientation;
+    vx_vec3 velocity;
+    vx_vec3 angularVelocity;
+    vx_vec3 force;
+    vx_vec3 torque;
+    float invMass;
+    vx_vec3 invInertia;
+    vx_quat inertiaOrientation;
+    float restitution;
+    float friction;
+    vx_vec3 frictionScale;
+    float rollingFriction;
+    float spinningFriction;
+    uint8_t frictionCombine;
+    uint8_t restitutionCombine;
+    uint8_t pad0[2];
+    float linearDamping;
+    float angularDamping;
+    float gravityScale;
+    uint8_t motionType;
+    uint8_t pad1[3];
+    vx_ccd_tuning ccdTuning;
+    uint8_t geometryQuality;
+    uint8_t pad2[3];
+    uint32_t categoryBits;
+    uint32_t maskBits;
+    int32_t groupIndex;
+    uint8_t sensor;
+    uint8_t enableSleep;
+    uint8_t fixedRotation;
+    uint8_t asleep;
+    float sleepTimer;
+    uint8_t shape;
+    uint8_t pad3[3];
+    float radius;
+    vx_vec3 halfExtents;
+    float capsuleHalfHeight;
+    vx_vec3 planeNormal;
+    float planeOffset;
+    uint32_t meshIndex;
+    uint32_t hullFirst, hullCount;
+    uint32_t hullFaceFirst, hullFaceCount;
+    uint32_t compoundFirst, compoundCount;
+} vx_body;
+
+typedef struct VX_ALIGN64 vx_contact {
+    uint32_t a, b;
+    uint64_t featureKey;
+    vx_vec3 normal;        /* from b towards a */
+    vx_vec3 point;
+    vx_vec3 localAnchorA;
+    vx_vec3 localAnchorB;
+    float gap;
+    float bias0;
+    float vn0;
+    float restitution;
+    float friction1, friction2;
+    float rollingFriction, spinningFriction;
+    float normalImpulse;
+    float tangentImpulse1;
+    float tangentImpulse2;
+    float rollingImpulse1, rollingImpulse2;
+    float spinningImpulse;
+} vx_contact;
+
+typedef struct vx_solver_options {
+    float impulseThreshold;
+    float stackStiffness;
+    float stackDamping;
+    int32_t velocityIterations;
+    int32_t positionIterations;
+    uint8_t frictionModel;
+    uint8_t iterationPolicy;
+    uint8_t enableStackStabilization;
+    uint8_t reserved;
+} vx_solver_options;
+
+/* Static convex-hull geometry: the hull slice of velox::MeshSoup
+ * (include/velox/backend.h:13-22). Bodies index it through
+ * hullFirst/hullCount (points) and hullFaceFirst/hullFaceCount (triangles,
+ * three point indices each, local to the body's point range). */
+typedef struct vx_soup {
+    const vx_vec3* hullPoints;
+    uint32_t hullPointCount;
+    const uint32_t* hullFaceIndices;
+    uint32_t hullFaceIndexCount;
+} vx_soup;
+
+/* One body of a synthetic scene, described at the level of the reference's
+ * World::add* calls (include/velox/world.h:459-470: addSphere, addBox,
+ * addCapsule, addCylinder, addConvexHull, addStaticPlane). Mass properties,
+ * hull topology and centring are derived from it by whichever engine builds
+ * the scene, so the same spec list drives the reference and this library. */
+typedef struct vx_shape_spec {
+    uint8_t shape;         /* VX_SHAPE_SPHERE/BOX/CAPSULE/CYLINDER/HULL/PLANE */
+    uint8_t enableSleep;   /* copied into Body::enableSleep */
+    uint8_t pad[2];
+    uint32_t world;        /* batch world id; 0 for single-world scenes */
+    float mass;            /* > 0 dynamic, 0 static */
+    float radius;          /* sphere / capsule / cylinder radius */
+    float halfHeight;      /* capsule / cylinder half height */
+    vx_vec3 halfExtents;   /* box half extents */
+    vx_vec3 position;      /* requested position (hulls: before centring) */
+    vx_quat orientation;
+    vx_vec3 velocity;
+    vx_vec3 angularVelocity;
+    float friction;
+    float restitution;
+    vx_vec3 planeNormal;   /* planes only */
+    float planeOffset;     /* planes only */
+    uint32_t hullFirst;    /* hulls: first raw point in the scene's point pool */
+    uint32_t hullCount;    /* hulls: number of raw points */
+} vx_shape_spec;
+
+#ifdef __cplusplus
+}  /* extern "C" */
+#define VX_STATIC_ASSERT(c, m) static_assert(c, m)
+#else
+#define VX_STATIC_ASSERT(c, m) _Static_assert(c, m)
+#endif
+
+VX_STATIC_ASSERT(sizeof(vx_ccd_settings) == 32, "vx_ccd_settings layout");
+VX_STATIC_ASSERT(sizeof(vx_ccd_tuning) == 52, "vx_ccd_tuning layout");
+VX_STATIC_ASSERT(sizeof(vx_body) == 320, "vx_body must match velox::Body (320 B)");
+VX_STATIC_ASSERT(offsetof(vx_body, ccdTuning) == 156, "vx_body.ccdTuning offset");
+VX_STATIC_ASSERT(offsetof(vx_body, shape) == 232, "vx_body.shape offset");
+VX_STATIC_ASSERT(offsetof(vx_body, compoundCount) == 296, "vx_body.compoundCount offset");
+VX_STATIC_ASSERT(sizeof(vx_contact) == 128, "vx_contact must match velox::Contact (128 B)");
+VX_STATIC_ASSERT(offsetof(vx_contact, normalImpulse) == 96, "vx_contact.normalImpulse offset");
+VX_STATIC_ASSERT(sizeof(vx_solver_options) == 24, "vx_solver_options layout");
+
+#endif /* VELOX_B200_TYPES_H */

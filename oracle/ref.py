@@ -1,0 +1,241 @@
+"""Test infrastructure: ctypes binding of the reference engine built from its
+sources by oracle/Makefile (oracle/_ref/libvelox_ref_*.so, see ref_shim.cpp).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this
+module, as the checker / baseline — never as the product path.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_DIR = os.path.join(HERE, "_ref")
+STRICT = os.path.join(REF_DIR, "libvelox_ref_strict.so")
+FAST = os.path.join(REF_DIR, "libvelox_ref_fast.so")
+
+BACKEND_CPU = 1
+BACKEND_CUDA_EMULATED = 2
+
+
+def available(strict=True):
+    return os.path.exists(STRICT if strict else FAST)
+
+
+_libs = {}
+
+
+def lib(strict=True):
+    path = STRICT if strict else FAST
+    if path in _libs:
+        return _libs[path]
+    if not os.path.exists(path):
+        raise RuntimeError(f"reference build missing: {path} (run `make -C oracle ref`)")
+    L = ctypes.CDLL(path)
+    vp, u32, i32, f32 = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_int, ctypes.c_float
+    sig = {
+        "ref_last_error": ([], ctypes.c_char_p),
+        "ref_is_strict": ([], i32),
+        "ref_world_new": ([i32], vp),
+        "ref_world_free": ([vp], None),
+        "ref_world_backend_name": ([vp], ctypes.c_char_p),
+        "ref_world_build": ([vp, vp, u32, vp], i32),
+        "ref_world_body_count": ([vp], u32),
+        "ref_world_get_bodies": ([vp, vp], None),
+        "ref_world_set_bodies": ([vp, vp], None),
+        "ref_world_soup": ([vp, vp, vp, ctypes.POINTER(u32)], u32),
+        "ref_world_captured_soup": ([vp, vp, vp, ctypes.POINTER(u32)], u32),
+        "ref_world_configure": ([vp, f32, f32, f32, i32, vp, i32], None),
+        "ref_world_worker_count": ([vp], u32),
+        "ref_world_step": ([vp, f32, i32], i32),
+        "ref_world_last_call_ms": ([vp], ctypes.c_double),
+        "ref_world_stats": ([vp, vp], None),
+        "ref_world_contacts": ([vp, vp, u32], u32),
+        "ref_world_found_contacts": ([vp, vp, u32], u32),
+        "ref_candidate_pairs": ([vp, u32, f32, vp, u32], u32),
+        "ref_body_aabb": ([vp, f32, vp], None),
+        "ref_collide_pairs": ([vp, vp, vp, u32, f32, vp, u32, vp], u32),
+        "ref_gjk": ([vp, vp, vp, vp], None),
+        "ref_sort_contacts": ([vp, u32], None),
+        "ref_color_contacts": ([vp, u32, vp, u32, vp], u32),
+        "ref_solve_sequence": ([vp, vp, u32, f32, vp, i32, i32], None),
+        "ref_integrate_velocities": ([vp, u32, f32, f32, f32, f32], None),
+        "ref_integrate_transforms": ([vp, u32, f32], None),
+    }
+    for name, (args, res) in sig.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = res
+    _libs[path] = L
+    return L
+
+
+def _p(a):
+    return ctypes.c_void_p(a.ctypes.data) if a is not None and a.size else ctypes.c_void_p(0)
+
+
+class RefWorld:
+    """A reference World built from shape specs (dense index == spec index)."""
+
+    def __init__(self, specs, pool, backend=BACKEND_CUDA_EMULATED, strict=True):
+        from velox_b200.binding import BODY  # record layout only
+        self._BODY = BODY
+        self.L = lib(strict)
+        self.h = self.L.ref_world_new(backend)
+        if not self.h:
+            raise RuntimeError(self.L.ref_last_error().decode())
+        pool = np.ascontiguousarray(pool, np.float32)
+        if self.L.ref_world_build(self.h, _p(specs), len(specs), _p(pool)) != 0:
+            raise RuntimeError(self.L.ref_last_error().decode())
+        self.n = len(specs)
+
+    def close(self):
+        if self.h:
+            self.L.ref_world_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def configure(self, gravity=(0.0, -9.81, 0.0), substeps=4, solver=None, workers=1):
+        self.L.ref_world_configure(self.h, gravity[0], gravity[1], gravity[2], substeps,
+                                   ctypes.byref(solver) if solver is not None else None, workers)
+
+    def bodies(self):
+        out = np.zeros(self.n, self._BODY)
+        self.L.ref_world_get_bodies(self.h, _p(out))
+        return out
+
+    def set_bodies(self, b):
+        self.L.ref_world_set_bodies(self.h, _p(np.ascontiguousarray(b)))
+
+    def soup(self):
+        nf = ctypes.c_uint32()
+        npts = self.L.ref_world_soup(self.h, None, None, ctypes.byref(nf))
+        pts = np.zeros((max(npts, 1), 3), np.float32)
+        faces = np.zeros(max(nf.value, 1), np.uint32)
+        self.L.ref_world_soup(self.h, _p(pts), _p(faces), ctypes.byref(nf))
+        return pts[:npts], faces[:nf.value]
+
+    def step(self, dt=1.0 / 60.0, steps=1):
+        if self.L.ref_world_step(self.h, dt, steps) != 0:
+            raise RuntimeError(self.L.ref_last_error().decode())
+        return self.L.ref_world_last_call_ms(self.h)
+
+    def stats(self):
+        out = np.zeros(5, np.uint64)
+        self.L.ref_world_stats(self.h, _p(out))
+        return dict(zip(["generated", "solved", "iterations", "deviceSubsteps", "awake"], out.tolist()))
+
+    def contacts(self):
+        from velox_b200.binding import CONTACT
+        m = self.L.ref_world_contacts(self.h, None, 0)
+        out = np.zeros(m, CONTACT)
+        self.L.ref_world_contacts(self.h, _p(out), m)
+        return out
+
+
+def candidate_pairs(bodies, dt, strict=True):
+    L = lib(strict)
+    n = L.ref_candidate_pairs(_p(bodies), len(bodies), dt, None, 0)
+    out = np.zeros(max(n, 1), np.uint64)
+    L.ref_candidate_pairs(_p(bodies), len(bodies), dt, _p(out), n)
+    return out[:n]
+
+
+def collide_pairs(bodies, soup, pairs, dt, strict=True):
+    from velox_b200.binding import CONTACT
+    L = lib(strict)
+    pairs = np.ascontiguousarray(pairs, np.uint64)
+    cap = 12 * max(len(pairs), 1)
+    out = np.zeros(cap, CONTACT)
+    counts = np.zeros(max(len(pairs), 1), np.uint32)
+    total = L.ref_collide_pairs(_p(bodies), ctypes.byref(soup), _p(pairs), len(pairs), dt, _p(out), cap,
+                                _p(counts))
+    return out[:total], counts[:len(pairs)]
+
+
+def sort_contacts(contacts, strict=True):
+    c = np.ascontiguousarray(contacts).copy()
+    lib(strict).ref_sort_contacts(_p(c), len(c))
+    return c
+
+
+def color_contacts(bodies, contacts, strict=True):
+    colors = np.zeros(max(len(contacts), 1), np.int32)
+    nc = lib(strict).ref_color_contacts(_p(bodies), len(bodies), _p(contacts), len(contacts), _p(colors))
+    return colors[:len(contacts)], nc
+
+
+def solve_sequence(bodies, contacts, dt, solver, warm_start=True, sweeps=16, strict=True):
+    b = np.ascontiguousarray(bodies).copy()
+    c = np.ascontiguousarray(contacts).copy()
+    lib(strict).ref_solve_sequence(_p(b), _p(c), len(c), dt, ctypes.byref(solver), int(warm_start), sweeps)
+    return b, c
+
+
+# ---- the C restatement (oracle/velox_oracle.c) -------------------------------
+
+ORACLE = os.path.join(HERE, "_build", "libvelox_oracle.so")
+_oracle = None
+
+
+def oracle():
+    global _oracle
+    if _oracle is not None:
+        return _oracle
+    if not os.path.exists(ORACLE):
+        raise RuntimeError(f"oracle restatement missing: {ORACLE} (run `make -C oracle oracle`)")
+    L = ctypes.CDLL(ORACLE)
+    vp, u32 = ctypes.c_void_p, ctypes.c_uint32
+    for name, args, res in [
+        ("vxo_candidate_pairs", [vp, u32, ctypes.c_float, vp, u32], u32),
+        ("vxo_sort_contacts", [vp, u32], None),
+        ("vxo_color_contacts", [vp, u32, vp, u32, vp], u32),
+        ("vxo_color_order", [vp, u32, u32, vp, vp], None),
+        ("vxo_warm_start_match", [vp, u32, vp, u32], u32),
+        ("vxo_body_aabb", [vp, ctypes.c_float, vp, vp], None),
+    ]:
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = res
+    _oracle = L
+    return L
+
+
+def oracle_pairs(bodies, dt):
+    L = oracle()
+    n = L.vxo_candidate_pairs(_p(bodies), len(bodies), dt, None, 0)
+    out = np.zeros(max(n, 1), np.uint64)
+    L.vxo_candidate_pairs(_p(bodies), len(bodies), dt, _p(out), n)
+    return out[:n]
+
+
+def oracle_sort(contacts):
+    c = np.ascontiguousarray(contacts).copy()
+    oracle().vxo_sort_contacts(_p(c), len(c))
+    return c
+
+
+def oracle_color(bodies, contacts):
+    colors = np.zeros(max(len(contacts), 1), np.int32)
+    nc = oracle().vxo_color_contacts(_p(bodies), len(bodies), _p(contacts), len(contacts), _p(colors))
+    return colors[:len(contacts)], nc
+
+
+def oracle_color_order(colors, num_colors):
+    colors = np.ascontiguousarray(colors, np.int32)
+    order = np.zeros(max(len(colors), 1), np.uint32)
+    starts = np.zeros(num_colors + 1, np.uint32)
+    oracle().vxo_color_order(_p(colors), len(colors), num_colors, _p(order), _p(starts))
+    return order[:len(colors)], starts
+
+
+def oracle_warm_start(cur, prev):
+    c = np.ascontiguousarray(cur).copy()
+    p = np.ascontiguousarray(prev)
+    warm = oracle().vxo_warm_start_match(_p(c), len(c), _p(p), len(p))
+    return c, warm

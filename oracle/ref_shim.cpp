@@ -1,0 +1,574 @@
+// Test infrastructure: a C adapter over the reference engine, compiled from the
+// reference sources by oracle/Makefile into oracle/_ref/. Nothing in the
+// product links or loads it; only tests and bench.py's CPU-baseline leg do.
+//
+// It provides
+//   * createCudaBackend(): a CPU emulation of the reference CUDA backend's
+//     algorithm (src/backend_cuda.cu:390-768) built from the reference's own
+//     VELOX_HD routines — all-pairs/grid candidate set, collidePair, host
+//     contact sort, greedy first-free-bit colouring, counting sort into colour
+//     order, per-colour warm start and 2*velocityIterations coloured sweeps,
+//     the advanceSubsteps loop and fetchImpulses. Running World(BackendType::Cuda)
+//     against it reproduces the reference CUDA backend's step on the CPU
+//     (colour order makes the parallel solve equal to this sequential one).
+//   * extern "C" entry points for scene building, stepping and the
+//     individual stages (pair set, narrow phase, colouring, coloured solve).
+#include "velox/world.h"
+#include "velox/backend.h"
+#include "velox/sleep.h"
+#include "narrowphase.h"
+#include "mass_properties.h"
+#include "velox_b200_types.h"
+
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+static_assert(sizeof(velox::Body) == sizeof(vx_body), "Body layout");
+static_assert(offsetof(velox::Body, ccdTuning) == offsetof(vx_body, ccdTuning), "Body.ccdTuning");
+static_assert(offsetof(velox::Body, shape) == offsetof(vx_body, shape), "Body.shape");
+static_assert(offsetof(velox::Body, hullFaceCount) == offsetof(vx_body, hullFaceCount), "Body.hullFaceCount");
+static_assert(offsetof(velox::Body, sleepTimer) == offsetof(vx_body, sleepTimer), "Body.sleepTimer");
+static_assert(sizeof(velox::Contact) == sizeof(vx_contact), "Contact layout");
+static_assert(offsetof(velox::Contact, spinningImpulse) == offsetof(vx_contact, spinningImpulse), "Contact tail");
+static_assert(sizeof(velox::SolverOptions) == sizeof(vx_solver_options), "SolverOptions layout");
+
+namespace velox {
+namespace {
+
+thread_local std::string g_error;
+
+inline bool inert(const Body& b) { return b.isStatic() || isFullyAsleep(b.asleep); }
+
+struct BoxLH { Vec3 lo, hi; };
+
+// Candidate pair set of the reference CUDA backend: allPairsContactsKernel
+// (backend_cuda.cu:272-299) below 4096 bodies, the grid (:174-250) above. Both
+// enumerate exactly the pairs i<j whose compact AABBs overlap (planes are
+// unbounded), that are not both inert and that pass canCollideWith. Returned
+// sorted ascending as (i<<32)|j.
+std::vector<uint64_t> candidatePairs(const std::vector<Body>& bodies, float dt) {
+    const size_t n = bodies.size();
+    std::vector<BoxLH> boxes(n);
+    std::vector<uint32_t> order;
+    std::vector<uint32_t> planes;
+    for (uint32_t i = 0; i < n; ++i) {
+        const Body& b = bodies[i];
+        if (b.shape == ShapeType::Plane) {
+            boxes[i] = {{-1e30f, -1e30f, -1e30f}, {1e30f, 1e30f, 1e30f}};
+            planes.push_back(i);
+        } else {
+            bodyAabb(b, dt, boxes[i].lo, boxes[i].hi);
+            order.push_back(i);
+        }
+    }
+    std::vector<uint64_t> pairs;
+    auto consider = [&](uint32_t i, uint32_t j) {
+        uint32_t lo = i < j ? i : j, hi = i < j ? j : i;
+        if (!aabbOverlap(boxes[lo].lo, boxes[lo].hi, boxes[hi].lo, boxes[hi].hi)) return;
+        if (inert(bodies[lo]) && inert(bodies[hi])) return;
+        if (!bodies[lo].canCollideWith(bodies[hi])) return;
+        pairs.push_back((uint64_t(lo) << 32) | hi);
+    };
+    for (size_t p = 0; p < planes.size(); ++p) {
+        for (uint32_t i : order) consider(planes[p], i);
+        for (size_t q = p + 1; q < planes.size(); ++q) consider(planes[p], planes[q]);
+    }
+    std::sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
+        return boxes[a].lo.x < boxes[b].lo.x || (boxes[a].lo.x == boxes[b].lo.x && a < b);
+    });
+    for (size_t s = 0; s < order.size(); ++s) {
+        uint32_t i = order[s];
+        for (size_t t = s + 1; t < order.size(); ++t) {
+            uint32_t j = order[t];
+            if (boxes[j].lo.x > boxes[i].hi.x) break;
+            consider(i, j);
+        }
+    }
+    std::sort(pairs.begin(), pairs.end());
+    return pairs;
+}
+
+bool contactLess(const Contact& x, const Contact& y) {
+    uint64_t kx = (uint64_t)x.a << 32 | x.b;
+    uint64_t ky = (uint64_t)y.a << 32 | y.b;
+    if (kx != ky) return kx < ky;
+    if (x.point.x != y.point.x) return x.point.x < y.point.x;
+    if (x.point.y != y.point.y) return x.point.y < y.point.y;
+    return x.point.z < y.point.z;
+}
+
+// Greedy first-free-bit colouring exactly as backend_cuda.cu:603-630.
+int greedyColor(const std::vector<Body>& bodies, const Contact* contacts, int m,
+                int* colorOf) {
+    const size_t n = bodies.size();
+    std::vector<uint64_t> mask(n, 0);
+    std::vector<int> nextColor(n, 64);
+    int numColors = 0;
+    for (int k = 0; k < m; ++k) {
+        const Contact& c = contacts[k];
+        bool sensor = bodies[c.a].isSensor() || bodies[c.b].isSensor();
+        bool sa = sensor || !bodies[c.a].isDynamic();
+        bool sb = sensor || !bodies[c.b].isDynamic();
+        uint64_t used = (sa ? 0 : mask[c.a]) | (sb ? 0 : mask[c.b]);
+        int color;
+        if (~used) {
+            color = 0;
+            while (used & (1ull << color)) ++color;
+        } else {
+            int na = sa ? 64 : nextColor[c.a];
+            int nb = sb ? 64 : nextColor[c.b];
+            color = na > nb ? na : nb;
+            if (!sa) nextColor[c.a] = color + 1;
+            if (!sb) nextColor[c.b] = color + 1;
+        }
+        if (color < 64) {
+            if (!sa) mask[c.a] |= 1ull << color;
+            if (!sb) mask[c.b] |= 1ull << color;
+        }
+        colorOf[k] = color;
+        if (color + 1 > numColors) numColors = color + 1;
+    }
+    return numColors;
+}
+
+void integrateVelocities(std::vector<Body>& bodies, const Vec3& gravity, float dt) {
+    for (Body& b : bodies) {  // integrateKernel, backend_cuda.cu:80-89
+        if (!b.isDynamic() || b.isLocked() || isFullyAsleep(b.asleep)) continue;
+        b.velocity += (gravity * b.gravityScale + b.force * b.solverInvMass()) * dt;
+        b.angularVelocity += b.invInertiaMul(b.torque) * dt;
+        b.velocity *= 1.0f / (1.0f + b.linearDamping * dt);
+        b.angularVelocity *= 1.0f / (1.0f + b.angularDamping * dt);
+    }
+}
+
+void integrateTransforms(std::vector<Body>& bodies, float dt) {
+    for (Body& b : bodies) {  // integrateTransformsKernel, backend_cuda.cu:91-97
+        if (b.isStatic() || b.isLocked() || isFullyAsleep(b.asleep)) continue;
+        b.advanceTransform(dt);
+    }
+}
+
+class ColoredCpuBackend final : public Backend {
+public:
+    const char* name() const override { return "cuda"; }
+    uint32_t lastVelocityIterations() const override { return lastIterations_; }
+
+    void integrate(std::vector<Body>& bodies, const Vec3& gravity, float dt) override {
+        integrateVelocities(bodies, gravity, dt);
+    }
+
+    void findContacts(const std::vector<Body>& bodies, const MeshSoup& meshes, float dt,
+                      const std::vector<uint64_t>*, std::vector<Contact>& out) override {
+        out.clear();
+        soupPoints = meshes.hullPoints;
+        soupFaces = meshes.hullFaceIndices;
+        if (bodies.size() < 2) return;
+        const MeshSoupView soup = view(meshes);
+        lastPairs = candidatePairs(bodies, dt);
+        Contact buf[kMaxContactsPerPair];
+        for (uint64_t p : lastPairs) {
+            BodyIndex i = BodyIndex(p >> 32), j = BodyIndex(p);
+            int count = collidePair(bodies[i], bodies[j], i, j, soup, dt, buf,
+                                    kMaxContactsPerPair);
+            out.insert(out.end(), buf, buf + count);
+        }
+        lastFound = out;
+    }
+
+    void solveVelocities(std::vector<Body>& bodies, std::vector<Contact>& contacts,
+                         float dt, bool warmStart, const SolverOptions& options) override {
+        lastIterations_ = 0;
+        const int m = (int)contacts.size();
+        if (m == 0) return;
+        if (warmStart) {
+            std::sort(contacts.begin(), contacts.end(), contactLess);
+            colorOf_.resize(m);
+            numColors_ = greedyColor(bodies, contacts.data(), m, colorOf_.data());
+            colorStart_.assign(numColors_ + 1, 0);
+            for (int k = 0; k < m; ++k) ++colorStart_[colorOf_[k] + 1];
+            for (int c = 0; c < numColors_; ++c) colorStart_[c + 1] += colorStart_[c];
+            std::vector<int> fill = colorStart_;
+            solve_.resize(m);
+            for (int k = 0; k < m; ++k) solve_[fill[colorOf_[k]]++] = contacts[k];
+            contacts = solve_;
+            for (Contact& c : solve_)
+                if (!bodies[c.a].isSensor() && !bodies[c.b].isSensor())
+                    warmStartContact(bodies[c.a], bodies[c.b], c);
+        }
+        sweeps_ = 2 * options.velocityIterations;
+        lastIterations_ = (uint32_t)sweeps_;
+        runSweeps(bodies, dt, options);
+    }
+
+    bool advanceSubsteps(std::vector<Body>& bodies, std::vector<Contact>& contacts,
+                         std::vector<Joint>& joints, const Vec3& gravity, float dt,
+                         int substeps, const SolverOptions& options) override {
+        if (!joints.empty()) return false;
+        if (options.iterationPolicy == IterationPolicy::Adaptive) return false;
+        const bool hasContacts = !contacts.empty();
+        solveVelocities(bodies, contacts, dt, true, options);
+        for (int s = 0; s < substeps; ++s) {
+            if (s > 0) {
+                integrateVelocities(bodies, gravity, dt);
+                if (hasContacts) runSweeps(bodies, dt, options);
+            }
+            integrateTransforms(bodies, dt);
+        }
+        lastIterations_ *= (uint32_t)substeps;
+        return true;
+    }
+
+    void fetchImpulses(std::vector<Contact>& contacts) override {
+        if (solve_.empty() || contacts.size() != solve_.size()) return;
+        contacts = solve_;
+    }
+
+    void invalidateCaches() override { solve_.clear(); }
+
+    std::vector<Contact> solve_;
+    std::vector<Contact> lastFound;
+    std::vector<uint64_t> lastPairs;
+    std::vector<Vec3> soupPoints;
+    std::vector<uint32_t> soupFaces;
+
+private:
+    void runSweeps(std::vector<Body>& bodies, float dt, const SolverOptions& options) {
+        for (int it = 0; it < sweeps_; ++it)
+            for (Contact& c : solve_)
+                if (!bodies[c.a].isSensor() && !bodies[c.b].isSensor())
+                    solveContact(bodies[c.a], bodies[c.b], c, dt, options);
+    }
+    std::vector<int> colorOf_, colorStart_;
+    int numColors_ = 0;
+    int sweeps_ = 0;
+    uint32_t lastIterations_ = 0;
+};
+
+thread_local ColoredCpuBackend* g_lastEmulated = nullptr;
+
+}  // namespace
+
+Backend* createCudaBackend() {
+    auto* backend = new ColoredCpuBackend();
+    g_lastEmulated = backend;
+    return backend;
+}
+
+}  // namespace velox
+
+using namespace velox;
+
+namespace {
+
+struct RefWorld {
+    std::unique_ptr<World> world;
+    ColoredCpuBackend* emulated = nullptr;
+    std::vector<BodyId> ids;
+    std::vector<Vec3> soupPoints;
+    std::vector<uint32_t> soupFaces;
+    double lastStepMs = 0.0;
+};
+
+Vec3 V(const vx_vec3& v) { return {v.x, v.y, v.z}; }
+Quat Q(const vx_quat& q) { return {q.x, q.y, q.z, q.w}; }
+
+MeshSoupView soupView(const vx_soup* s) {
+    MeshSoupView v{};
+    if (s) {
+        v.hullPoints = reinterpret_cast<const Vec3*>(s->hullPoints);
+        v.hullFaceIndices = s->hullFaceIndices;
+    }
+    return v;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* ref_last_error(void) { return g_error.c_str(); }
+
+int ref_is_strict(void) { return VELOX_STRICT_FLOATING_POINT ? 1 : 0; }
+
+// backend: 1 = the reference CPU backend, 2 = World(BackendType::Cuda) served
+// by the CPU emulation of the CUDA backend above.
+void* ref_world_new(int backend) {
+    try {
+        auto* w = new RefWorld();
+        g_lastEmulated = nullptr;
+        w->world.reset(new World(backend == 2 ? BackendType::Cuda : BackendType::Cpu));
+        if (backend == 2) w->emulated = g_lastEmulated;
+        return w;
+    } catch (const std::exception& e) {
+        g_error = e.what();
+        return nullptr;
+    }
+}
+
+void ref_world_free(void* handle) { delete static_cast<RefWorld*>(handle); }
+
+const char* ref_world_backend_name(void* handle) {
+    return static_cast<RefWorld*>(handle)->world->backendName();
+}
+
+// Adds the bodies of a scene through World::add* in spec order, so dense
+// index == spec index. Hull points are centred exactly as addConvexHull does
+// (src/world.cpp:909-985); the resulting hull soup is mirrored for export.
+int ref_world_build(void* handle, const vx_shape_spec* specs, uint32_t n,
+                    const vx_vec3* pool) {
+    auto* w = static_cast<RefWorld*>(handle);
+    try {
+        for (uint32_t k = 0; k < n; ++k) {
+            const vx_shape_spec& s = specs[k];
+            BodyId id;
+            switch (s.shape) {
+            case VX_SHAPE_SPHERE: id = w->world->addSphere(V(s.position), s.radius, s.mass); break;
+            case VX_SHAPE_BOX: id = w->world->addBox(V(s.position), V(s.halfExtents), s.mass); break;
+            case VX_SHAPE_CAPSULE:
+                id = w->world->addCapsule(V(s.position), s.radius, s.halfHeight, s.mass); break;
+            case VX_SHAPE_CYLINDER:
+                id = w->world->addCylinder(V(s.position), s.radius, s.halfHeight, s.mass); break;
+            case VX_SHAPE_PLANE:
+                id = w->world->addStaticPlane(V(s.planeNormal), s.planeOffset); break;
+            case VX_SHAPE_HULL: {
+                std::vector<Vec3> pts;
+                for (uint32_t i = 0; i < s.hullCount; ++i) pts.push_back(V(pool[s.hullFirst + i]));
+                id = w->world->addConvexHull(V(s.position), pts, s.mass);
+                mass_properties::ConvexMassProperties props = mass_properties::convex(pts);
+                if (s.mass > 0.0f)
+                    for (Vec3& p : pts) p -= props.center;
+                w->soupPoints.insert(w->soupPoints.end(), pts.begin(), pts.end());
+                for (const auto& t : props.triangles)
+                    w->soupFaces.insert(w->soupFaces.end(), t.begin(), t.end());
+                break;
+            }
+            default:
+                g_error = "unsupported shape in spec";
+                return -1;
+            }
+            w->ids.push_back(id);
+            if (s.shape != VX_SHAPE_PLANE) {
+                Body& b = w->world->body(id);
+                b.orientation = Q(s.orientation);
+                b.velocity = V(s.velocity);
+                b.angularVelocity = V(s.angularVelocity);
+                b.friction = s.friction;
+                b.restitution = s.restitution;
+                b.enableSleep = s.enableSleep;
+            }
+        }
+        return 0;
+    } catch (const std::exception& e) {
+        g_error = e.what();
+        return -1;
+    }
+}
+
+uint32_t ref_world_body_count(void* handle) {
+    return (uint32_t)static_cast<RefWorld*>(handle)->ids.size();
+}
+
+void ref_world_get_bodies(void* handle, vx_body* out) {
+    auto* w = static_cast<RefWorld*>(handle);
+    for (size_t i = 0; i < w->ids.size(); ++i) {
+        Body b = w->world->bodyState(w->ids[i]);
+        std::memcpy(&out[i], &b, sizeof(Body));
+    }
+}
+
+void ref_world_set_bodies(void* handle, const vx_body* in) {
+    auto* w = static_cast<RefWorld*>(handle);
+    for (size_t i = 0; i < w->ids.size(); ++i)
+        std::memcpy(&w->world->body(w->ids[i]), &in[i], sizeof(Body));
+}
+
+// Copies the hull soup; returns the number of points, writes the number of
+// face indices to *faceIndexCount. Pass null buffers to query sizes.
+uint32_t ref_world_soup(void* handle, vx_vec3* points, uint32_t* faces,
+                        uint32_t* faceIndexCount) {
+    auto* w = static_cast<RefWorld*>(handle);
+    if (points) std::memcpy(points, w->soupPoints.data(), w->soupPoints.size() * sizeof(Vec3));
+    if (faces) std::memcpy(faces, w->soupFaces.data(), w->soupFaces.size() * sizeof(uint32_t));
+    if (faceIndexCount) *faceIndexCount = (uint32_t)w->soupFaces.size();
+    return (uint32_t)w->soupPoints.size();
+}
+
+// Hull soup as the emulated backend last received it from World::step.
+uint32_t ref_world_captured_soup(void* handle, vx_vec3* points, uint32_t* faces,
+                                 uint32_t* faceIndexCount) {
+    auto* w = static_cast<RefWorld*>(handle);
+    if (!w->emulated) return 0;
+    const auto& P = w->emulated->soupPoints;
+    const auto& F = w->emulated->soupFaces;
+    if (points) std::memcpy(points, P.data(), P.size() * sizeof(Vec3));
+    if (faces) std::memcpy(faces, F.data(), F.size() * sizeof(uint32_t));
+    if (faceIndexCount) *faceIndexCount = (uint32_t)F.size();
+    return (uint32_t)P.size();
+}
+
+void ref_world_configure(void* handle, float gx, float gy, float gz, int substeps,
+                         const vx_solver_options* options, int workers) {
+    auto* w = static_cast<RefWorld*>(handle);
+    w->world->gravity = {gx, gy, gz};
+    w->world->substeps = substeps;
+    if (options) {
+        SolverOptions o;
+        std::memcpy(&o, options, sizeof(o));
+        w->world->setSolverOptions(o);
+    }
+    if (workers >= 0) w->world->setWorkerCount((uint32_t)workers);
+}
+
+uint32_t ref_world_worker_count(void* handle) {
+    return static_cast<RefWorld*>(handle)->world->workerCount();
+}
+
+int ref_world_step(void* handle, float dt, int steps) {
+    auto* w = static_cast<RefWorld*>(handle);
+    try {
+        auto t0 = std::chrono::steady_clock::now();
+        for (int s = 0; s < steps; ++s) w->world->step(dt);
+        auto t1 = std::chrono::steady_clock::now();
+        w->lastStepMs = std::chrono::duration<double, std::milli>(t1 - t0).count();
+        return 0;
+    } catch (const std::exception& e) {
+        g_error = e.what();
+        return -1;
+    }
+}
+
+double ref_world_last_call_ms(void* handle) { return static_cast<RefWorld*>(handle)->lastStepMs; }
+
+// StepStats subset: [generatedContacts, solvedContacts, velocityIterations,
+// deviceSubsteps, awakeDynamicBodies].
+void ref_world_stats(void* handle, uint64_t* out5) {
+    const StepStats& s = static_cast<RefWorld*>(handle)->world->lastStepStats();
+    out5[0] = s.generatedContacts;
+    out5[1] = s.solvedContacts;
+    out5[2] = s.velocityIterations;
+    out5[3] = s.deviceSubsteps ? 1 : 0;
+    out5[4] = s.awakeDynamicBodies;
+}
+
+// Contacts held by the emulated CUDA backend after the last step: colour order,
+// impulses and points as fetchImpulses returns them (World::contacts_).
+uint32_t ref_world_contacts(void* handle, vx_contact* out, uint32_t cap) {
+    auto* w = static_cast<RefWorld*>(handle);
+    if (!w->emulated) return 0;
+    const auto& c = w->emulated->solve_;
+    uint32_t m = (uint32_t)c.size();
+    if (out) std::memcpy(out, c.data(), std::min(m, cap) * sizeof(Contact));
+    return m;
+}
+
+// Contacts as the emulated backend's findContacts produced them in the last
+// step (pair order, before warm-start matching).
+uint32_t ref_world_found_contacts(void* handle, vx_contact* out, uint32_t cap) {
+    auto* w = static_cast<RefWorld*>(handle);
+    if (!w->emulated) return 0;
+    const auto& c = w->emulated->lastFound;
+    uint32_t m = (uint32_t)c.size();
+    if (out) std::memcpy(out, c.data(), std::min(m, cap) * sizeof(Contact));
+    return m;
+}
+
+// ---- stage-level entry points over raw arrays ---------------------------
+
+uint32_t ref_candidate_pairs(const vx_body* bodies, uint32_t n, float dt, uint64_t* out,
+                             uint32_t cap) {
+    std::vector<Body> v(reinterpret_cast<const Body*>(bodies),
+                        reinterpret_cast<const Body*>(bodies) + n);
+    std::vector<uint64_t> pairs = candidatePairs(v, dt);
+    if (out) std::memcpy(out, pairs.data(), std::min<size_t>(pairs.size(), cap) * 8);
+    return (uint32_t)pairs.size();
+}
+
+void ref_body_aabb(const vx_body* body, float dt, float* out6) {
+    Vec3 lo, hi;
+    bodyAabb(*reinterpret_cast<const Body*>(body), dt, lo, hi);
+    out6[0] = lo.x; out6[1] = lo.y; out6[2] = lo.z;
+    out6[3] = hi.x; out6[4] = hi.y; out6[5] = hi.z;
+}
+
+// collidePair over a list of pairs; contacts are appended in pair order and
+// counts[p] receives each pair's count. Returns the total (may exceed cap).
+uint32_t ref_collide_pairs(const vx_body* bodies, const vx_soup* soup, const uint64_t* pairs,
+                           uint32_t npairs, float dt, vx_contact* out, uint32_t cap,
+                           uint32_t* counts) {
+    const Body* b = reinterpret_cast<const Body*>(bodies);
+    MeshSoupView sv = soupView(soup);
+    Contact buf[kMaxContactsPerPair];
+    uint32_t total = 0;
+    for (uint32_t p = 0; p < npairs; ++p) {
+        BodyIndex i = BodyIndex(pairs[p] >> 32), j = BodyIndex(pairs[p]);
+        int count = collidePair(b[i], b[j], i, j, sv, dt, buf, kMaxContactsPerPair);
+        if (counts) counts[p] = (uint32_t)count;
+        for (int c = 0; c < count; ++c) {
+            if (total < cap) std::memcpy(&out[total], &buf[c], sizeof(Contact));
+            ++total;
+        }
+    }
+    return total;
+}
+
+// gjkDistance(makeConvex(a), makeConvex(b)); out = distance, normal[3],
+// pointA[3], pointB[3], overlapping.
+void ref_gjk(const vx_body* a, const vx_body* b, const vx_soup* soup, float* out11) {
+    MeshSoupView sv = soupView(soup);
+    GjkResult r = gjkDistance(makeConvex(*reinterpret_cast<const Body*>(a), sv),
+                              makeConvex(*reinterpret_cast<const Body*>(b), sv));
+    out11[0] = r.distance;
+    out11[1] = r.normal.x; out11[2] = r.normal.y; out11[3] = r.normal.z;
+    out11[4] = r.pointA.x; out11[5] = r.pointA.y; out11[6] = r.pointA.z;
+    out11[7] = r.pointB.x; out11[8] = r.pointB.y; out11[9] = r.pointB.z;
+    out11[10] = r.overlapping ? 1.0f : 0.0f;
+}
+
+void ref_sort_contacts(vx_contact* contacts, uint32_t m) {
+    Contact* c = reinterpret_cast<Contact*>(contacts);
+    std::stable_sort(c, c + m, contactLess);
+}
+
+uint32_t ref_color_contacts(const vx_body* bodies, uint32_t n, const vx_contact* contacts,
+                            uint32_t m, int32_t* colorOf) {
+    std::vector<Body> v(reinterpret_cast<const Body*>(bodies),
+                        reinterpret_cast<const Body*>(bodies) + n);
+    return (uint32_t)greedyColor(v, reinterpret_cast<const Contact*>(contacts), (int)m,
+                                 colorOf);
+}
+
+// Warm start (optional) then `sweeps` passes of solveContact over the contacts
+// in the given order (colour order reproduces the coloured parallel solve).
+void ref_solve_sequence(vx_body* bodies, vx_contact* contacts, uint32_t m, float dt,
+                        const vx_solver_options* options, int warmStart, int sweeps) {
+    Body* b = reinterpret_cast<Body*>(bodies);
+    Contact* c = reinterpret_cast<Contact*>(contacts);
+    SolverOptions o;
+    std::memcpy(&o, options, sizeof(o));
+    if (warmStart)
+        for (uint32_t k = 0; k < m; ++k)
+            if (!b[c[k].a].isSensor() && !b[c[k].b].isSensor())
+                warmStartContact(b[c[k].a], b[c[k].b], c[k]);
+    for (int it = 0; it < sweeps; ++it)
+        for (uint32_t k = 0; k < m; ++k)
+            if (!b[c[k].a].isSensor() && !b[c[k].b].isSensor())
+                solveContact(b[c[k].a], b[c[k].b], c[k], dt, o);
+}
+
+void ref_integrate_velocities(vx_body* bodies, uint32_t n, float gx, float gy, float gz,
+                              float dt) {
+    std::vector<Body> v(reinterpret_cast<Body*>(bodies), reinterpret_cast<Body*>(bodies) + n);
+    integrateVelocities(v, {gx, gy, gz}, dt);
+    std::memcpy(bodies, v.data(), n * sizeof(Body));
+}
+
+void ref_integrate_transforms(vx_body* bodies, uint32_t n, float dt) {
+    std::vector<Body> v(reinterpret_cast<Body*>(bodies), reinterpret_cast<Body*>(bodies) + n);
+    integrateTransforms(v, dt);
+    std::memcpy(bodies, v.data(), n * sizeof(Body));
+}
+
+}  // extern "C"

@@ -1,0 +1,340 @@
+"""ctypes binding of libvelox_b200.so and numpy views of its records.
+
+The records mirror include/velox_b200_types.h (and through it the reference
+engine's velox::Body / velox::Contact host layouts).
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libvelox_b200.so")
+
+VXB_OK = 0
+STATUS = {0: "ok", 1: "invalid", 2: "no device", 3: "out of memory", 4: "device lost",
+          5: "capacity", 6: "unsupported", 7: "timeout"}
+
+SHAPE = dict(sphere=0, plane=1, box=2, capsule=3, mesh=4, hull=5, compound=6, cylinder=7,
+             cone=8, rounded_box=9, ellipsoid=10)
+
+_v3 = (np.float32, 3)
+_q4 = (np.float32, 4)
+
+CCD_SETTINGS = np.dtype({
+    "names": ["quality", "maxAdvancementIterations", "maxRootFindIterations", "distanceTolerance",
+              "timeTolerance", "enableRotationalCcd", "enableCompoundCcd", "useBrentRootFinder",
+              "meshBvhMaxDepth", "speculativeMargin"],
+    "formats": [np.uint8, np.uint32, np.uint32, np.float32, np.float32, np.uint8, np.uint8, np.uint8,
+                np.uint32, np.float32],
+    "offsets": [0, 4, 8, 12, 16, 20, 21, 22, 24, 28],
+    "itemsize": 32})
+
+CCD_TUNING = np.dtype({
+    "names": ["quality", "collisionMargin", "speculativeDistance", "enableContinuous",
+              "minVelocityForCCD", "ccdSettings"],
+    "formats": [np.uint8, np.float32, np.float32, np.uint8, np.float32, CCD_SETTINGS],
+    "offsets": [0, 4, 8, 12, 16, 20],
+    "itemsize": 52})
+
+BODY = np.dtype({
+    "names": ["position", "orientation", "velocity", "angularVelocity", "force", "torque", "invMass",
+              "invInertia", "inertiaOrientation", "restitution", "friction", "frictionScale",
+              "rollingFriction", "spinningFriction", "frictionCombine", "restitutionCombine",
+              "linearDamping", "angularDamping", "gravityScale", "motionType", "ccdTuning",
+              "geometryQuality", "categoryBits", "maskBits", "groupIndex", "sensor", "enableSleep",
+              "fixedRotation", "asleep", "sleepTimer", "shape", "radius", "halfExtents",
+              "capsuleHalfHeight", "planeNormal", "planeOffset", "meshIndex", "hullFirst", "hullCount",
+              "hullFaceFirst", "hullFaceCount", "compoundFirst", "compoundCount"],
+    "formats": [_v3, _q4, _v3, _v3, _v3, _v3, np.float32, _v3, _q4, np.float32, np.float32, _v3,
+                np.float32, np.float32, np.uint8, np.uint8, np.float32, np.float32, np.float32, np.uint8,
+                CCD_TUNING, np.uint8, np.uint32, np.uint32, np.int32, np.uint8, np.uint8, np.uint8,
+                np.uint8, np.float32, np.uint8, np.float32, _v3, np.float32, _v3, np.float32, np.uint32,
+                np.uint32, np.uint32, np.uint32, np.uint32, np.uint32, np.uint32],
+    "offsets": [0, 12, 28, 40, 52, 64, 76, 80, 92, 108, 112, 116, 128, 132, 136, 137, 140, 144, 148,
+                152, 156, 208, 212, 216, 220, 224, 225, 226, 227, 228, 232, 236, 240, 252, 256, 268,
+                272, 276, 280, 284, 288, 292, 296],
+    "itemsize": 320})
+
+CONTACT = np.dtype({
+    "names": ["a", "b", "featureKey", "normal", "point", "localAnchorA", "localAnchorB", "gap", "bias0",
+              "vn0", "restitution", "friction1", "friction2", "rollingFriction", "spinningFriction",
+              "normalImpulse", "tangentImpulse1", "tangentImpulse2", "rollingImpulse1",
+              "rollingImpulse2", "spinningImpulse"],
+    "formats": [np.uint32, np.uint32, np.uint64, _v3, _v3, _v3, _v3] + [np.float32] * 14,
+    "offsets": [0, 4, 8, 16, 28, 40, 52] + [64 + 4 * k for k in range(14)],
+    "itemsize": 128})
+
+SPEC = np.dtype({
+    "names": ["shape", "enableSleep", "world", "mass", "radius", "halfHeight", "halfExtents",
+              "position", "orientation", "velocity", "angularVelocity", "friction", "restitution",
+              "planeNormal", "planeOffset", "hullFirst", "hullCount"],
+    "formats": [np.uint8, np.uint8, np.uint32, np.float32, np.float32, np.float32, _v3, _v3, _q4, _v3,
+                _v3, np.float32, np.float32, _v3, np.float32, np.uint32, np.uint32],
+    "offsets": [0, 1, 4, 8, 12, 16, 20, 32, 44, 60, 72, 84, 88, 92, 104, 108, 112],
+    "itemsize": 116})
+
+# Contact fields that carry physics (padding bytes excluded).
+CONTACT_FLOAT_FIELDS = ["normal", "point", "localAnchorA", "localAnchorB", "gap", "bias0", "vn0",
+                        "restitution", "friction1", "friction2", "rollingFriction", "spinningFriction",
+                        "normalImpulse", "tangentImpulse1", "tangentImpulse2", "rollingImpulse1",
+                        "rollingImpulse2", "spinningImpulse"]
+
+
+class SolverOptions(ctypes.Structure):
+    _fields_ = [("impulseThreshold", ctypes.c_float), ("stackStiffness", ctypes.c_float),
+                ("stackDamping", ctypes.c_float), ("velocityIterations", ctypes.c_int32),
+                ("positionIterations", ctypes.c_int32), ("frictionModel", ctypes.c_uint8),
+                ("iterationPolicy", ctypes.c_uint8), ("enableStackStabilization", ctypes.c_uint8),
+                ("reserved", ctypes.c_uint8)]
+
+    @classmethod
+    def default(cls, **kw):
+        o = cls(1e-5, 1000.0, 10.0, 8, 3, 0, 0, 0, 0)
+        for k, v in kw.items():
+            setattr(o, k, v)
+        return o
+
+
+class Vec3(ctypes.Structure):
+    _fields_ = [("x", ctypes.c_float), ("y", ctypes.c_float), ("z", ctypes.c_float)]
+
+
+class Soup(ctypes.Structure):
+    _fields_ = [("hullPoints", ctypes.c_void_p), ("hullPointCount", ctypes.c_uint32),
+                ("hullFaceIndices", ctypes.c_void_p), ("hullFaceIndexCount", ctypes.c_uint32)]
+
+
+class StepConfig(ctypes.Structure):
+    _fields_ = [("dt", ctypes.c_float), ("gravity", Vec3), ("substeps", ctypes.c_int32),
+                ("solver", SolverOptions)]
+
+
+class StepStats(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint32) for n in ("candidatePairs", "contacts", "colors", "islands",
+                                               "largestIsland", "rewinds", "velocityIterations",
+                                               "warmStarted")]
+
+
+def ptr(a):
+    return ctypes.c_void_p(a.ctypes.data) if a is not None and a.size else ctypes.c_void_p(0)
+
+
+_lib = None
+
+
+def lib(path=LIB_PATH):
+    """Loads the library (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(f"velox_b200: {path} is missing; run `python -m velox_b200.build`")
+    L = ctypes.CDLL(path)
+    vp, u32, i32, f32 = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_int, ctypes.c_float
+    p_u32 = ctypes.POINTER(ctypes.c_uint32)
+    sig = {
+        "vxb_version": ([], ctypes.c_char_p),
+        "vxb_status_string": ([i32], ctypes.c_char_p),
+        "vxb_context_create": ([i32, ctypes.POINTER(vp)], i32),
+        "vxb_context_destroy": ([vp], None),
+        "vxb_context_last_error": ([vp], ctypes.c_char_p),
+        "vxb_context_set_stream": ([vp, vp], i32),
+        "vxb_context_launch_count": ([vp], ctypes.c_uint64),
+        "vxb_backend_integrate": ([vp, vp, u32, Vec3, f32], i32),
+        "vxb_backend_find_contacts": ([vp, vp, u32, ctypes.POINTER(Soup), f32, p_u32], i32),
+        "vxb_backend_copy_contacts": ([vp, vp, u32], i32),
+        "vxb_backend_solve_velocities": ([vp, vp, u32, vp, u32, f32, i32, ctypes.POINTER(SolverOptions),
+                                          p_u32], i32),
+        "vxb_backend_advance_substeps": ([vp, vp, u32, vp, u32, Vec3, f32, i32,
+                                          ctypes.POINTER(SolverOptions), ctypes.POINTER(ctypes.c_int),
+                                          p_u32], i32),
+        "vxb_backend_fetch_impulses": ([vp, vp, u32], i32),
+        "vxb_backend_invalidate": ([vp], i32),
+        "vxb_world_load": ([vp, vp, u32, ctypes.POINTER(Soup), vp], i32),
+        "vxb_world_configure": ([vp, ctypes.POINTER(StepConfig)], i32),
+        "vxb_world_step": ([vp, i32], i32),
+        "vxb_world_read_bodies": ([vp, vp, u32], i32),
+        "vxb_world_read_poses": ([vp, vp, u32], i32),
+        "vxb_world_write_forces": ([vp, vp, u32], i32),
+        "vxb_world_read_contacts": ([vp, vp, u32, p_u32], i32),
+        "vxb_world_stats": ([vp, ctypes.POINTER(StepStats)], i32),
+        "vxb_stage_pairs": ([vp, vp, u32, f32, vp, u32, p_u32], i32),
+        "vxb_stage_collide": ([vp, vp, u32, ctypes.POINTER(Soup), vp, u32, f32, vp, u32, vp, p_u32], i32),
+        "vxb_stage_color": ([vp, vp, u32, vp, u32, vp, p_u32], i32),
+        "vxb_scene_generate": ([i32, ctypes.c_uint64, u32, vp, u32, p_u32, vp, u32, p_u32], i32),
+        "vxb_bodies_from_specs": ([vp, u32, vp, vp, vp, u32, p_u32, vp, u32, p_u32], i32),
+    }
+    for name, (args, res) in sig.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = res
+    _lib = L
+    return L
+
+
+class VeloxError(RuntimeError):
+    def __init__(self, status, message=""):
+        super().__init__(f"velox_b200 status {status} ({STATUS.get(status, '?')}): {message}")
+        self.status = status
+
+
+def check(status, ctx=None):
+    if status != VXB_OK:
+        msg = lib().vxb_context_last_error(ctx).decode() if ctx else ""
+        raise VeloxError(status, msg)
+
+
+def generate_scene(config, seed=None, size=0):
+    """Specs + raw hull point pool of a benchmark workload (1..5)."""
+    L = lib()
+    seed = config if seed is None else seed
+    count, pool = ctypes.c_uint32(), ctypes.c_uint32()
+    check(L.vxb_scene_generate(config, seed, size, None, 0, ctypes.byref(count), None, 0, ctypes.byref(pool)))
+    specs = np.zeros(count.value, SPEC)
+    pts = np.zeros((max(pool.value, 1), 3), np.float32)
+    check(L.vxb_scene_generate(config, seed, size, ptr(specs), count.value, ctypes.byref(count), ptr(pts),
+                               pool.value, ctypes.byref(pool)))
+    return specs, pts[:pool.value]
+
+
+def bodies_from_specs(specs, pool):
+    L = lib()
+    n = len(specs)
+    hc, fc = ctypes.c_uint32(), ctypes.c_uint32()
+    check(L.vxb_bodies_from_specs(ptr(specs), n, ptr(pool), None, None, 0, ctypes.byref(hc), None, 0,
+                                  ctypes.byref(fc)))
+    bodies = np.zeros(n, BODY)
+    hull = np.zeros((max(hc.value, 1), 3), np.float32)
+    faces = np.zeros(max(fc.value, 1), np.uint32)
+    check(L.vxb_bodies_from_specs(ptr(specs), n, ptr(pool), ptr(bodies), ptr(hull), hc.value,
+                                  ctypes.byref(hc), ptr(faces), fc.value, ctypes.byref(fc)))
+    return bodies, hull[:hc.value], faces[:fc.value]
+
+
+def make_soup(hull, faces):
+    hull = np.ascontiguousarray(hull, np.float32)
+    faces = np.ascontiguousarray(faces, np.uint32)
+    s = Soup(ptr(hull), len(hull), ptr(faces), len(faces))
+    s._keep = (hull, faces)
+    return s
+
+
+class Context:
+    """One pipeline instance (one CUDA stream on one device)."""
+
+    def __init__(self, device=0):
+        self.L = lib()
+        h = ctypes.c_void_p()
+        check(self.L.vxb_context_create(device, ctypes.byref(h)))
+        self.h = h
+
+    def close(self):
+        if self.h:
+            self.L.vxb_context_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, status):
+        check(status, self.h)
+
+    @property
+    def launches(self):
+        return int(self.L.vxb_context_launch_count(self.h))
+
+    def set_stream(self, stream_handle):
+        self._check(self.L.vxb_context_set_stream(self.h, ctypes.c_void_p(stream_handle)))
+
+    # ---- device world
+    def load(self, bodies, soup, world_of=None):
+        self.bodies_n = len(bodies)
+        wo = None if world_of is None else np.ascontiguousarray(world_of, np.uint32)
+        self._check(self.L.vxb_world_load(self.h, ptr(bodies), len(bodies), ctypes.byref(soup), ptr(wo)))
+
+    def configure(self, dt=1.0 / 60.0, substeps=4, gravity=(0.0, -9.81, 0.0), solver=None):
+        cfg = StepConfig(dt, Vec3(*gravity), substeps, solver or SolverOptions.default())
+        self._check(self.L.vxb_world_configure(self.h, ctypes.byref(cfg)))
+
+    def step(self, steps=1):
+        self._check(self.L.vxb_world_step(self.h, steps))
+
+    def read_bodies(self):
+        out = np.zeros(self.bodies_n, BODY)
+        self._check(self.L.vxb_world_read_bodies(self.h, ptr(out), self.bodies_n))
+        return out
+
+    def read_poses(self, out=None):
+        if out is None:
+            out = np.zeros((self.bodies_n, 7), np.float32)
+        self._check(self.L.vxb_world_read_poses(self.h, ptr(out), self.bodies_n))
+        return out
+
+    def write_forces(self, ft):
+        self._check(self.L.vxb_world_write_forces(self.h, ptr(ft), self.bodies_n))
+
+    def read_contacts(self):
+        cnt = ctypes.c_uint32()
+        self._check(self.L.vxb_world_read_contacts(self.h, None, 0, ctypes.byref(cnt)))
+        out = np.zeros(cnt.value, CONTACT)
+        self._check(self.L.vxb_world_read_contacts(self.h, ptr(out), cnt.value, ctypes.byref(cnt)))
+        return out
+
+    def stats(self):
+        s = StepStats()
+        self._check(self.L.vxb_world_stats(self.h, ctypes.byref(s)))
+        return {k: getattr(s, k) for k, _ in StepStats._fields_}
+
+    # ---- stages
+    def pairs(self, bodies, dt):
+        cnt = ctypes.c_uint32()
+        self._check(self.L.vxb_stage_pairs(self.h, ptr(bodies), len(bodies), dt, None, 0, ctypes.byref(cnt)))
+        out = np.zeros(max(cnt.value, 1), np.uint64)
+        self._check(self.L.vxb_stage_pairs(self.h, ptr(bodies), len(bodies), dt, ptr(out), cnt.value,
+                                           ctypes.byref(cnt)))
+        return out[:cnt.value]
+
+    def collide(self, bodies, soup, pairs, dt, cap=None):
+        pairs = np.ascontiguousarray(pairs, np.uint64)
+        cap = cap or max(12 * len(pairs), 1)
+        out = np.zeros(cap, CONTACT)
+        counts = np.zeros(max(len(pairs), 1), np.uint32)
+        total = ctypes.c_uint32()
+        self._check(self.L.vxb_stage_collide(self.h, ptr(bodies), len(bodies), ctypes.byref(soup), ptr(pairs),
+                                             len(pairs), dt, ptr(out), cap, ptr(counts), ctypes.byref(total)))
+        return out[:total.value], counts[:len(pairs)]
+
+    def color(self, bodies, contacts):
+        colors = np.zeros(max(len(contacts), 1), np.int32)
+        nc = ctypes.c_uint32()
+        self._check(self.L.vxb_stage_color(self.h, ptr(bodies), len(bodies), ptr(contacts), len(contacts),
+                                           ptr(colors), ctypes.byref(nc)))
+        return colors[:len(contacts)], nc.value
+
+    # ---- Backend interface
+    def backend_integrate(self, bodies, gravity, dt):
+        self._check(self.L.vxb_backend_integrate(self.h, ptr(bodies), len(bodies), Vec3(*gravity), dt))
+
+    def backend_find_contacts(self, bodies, soup, dt):
+        cnt = ctypes.c_uint32()
+        self._check(self.L.vxb_backend_find_contacts(self.h, ptr(bodies), len(bodies), ctypes.byref(soup), dt,
+                                                     ctypes.byref(cnt)))
+        out = np.zeros(cnt.value, CONTACT)
+        self._check(self.L.vxb_backend_copy_contacts(self.h, ptr(out), cnt.value))
+        return out
+
+    def backend_advance_substeps(self, bodies, contacts, gravity, h, substeps, solver=None):
+        adv = ctypes.c_int()
+        it = ctypes.c_uint32()
+        opts = solver or SolverOptions.default()
+        self._check(self.L.vxb_backend_advance_substeps(self.h, ptr(bodies), len(bodies), ptr(contacts),
+                                                        len(contacts), Vec3(*gravity), h, substeps,
+                                                        ctypes.byref(opts), ctypes.byref(adv), ctypes.byref(it)))
+        return bool(adv.value), it.value
+
+    def backend_fetch_impulses(self, contacts):
+        self._check(self.L.vxb_backend_fetch_impulses(self.h, ptr(contacts), len(contacts)))

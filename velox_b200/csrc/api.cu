@@ -1,0 +1,305 @@
+// extern "C" entry points (include/velox_b200.h). Every function validates
+// its arguments, never throws, and maps failures to status codes.
+#include <cstring>
+#include <new>
+
+#include "context.cuh"
+
+using vxb::Context;
+
+struct vxb_context {
+    Context impl;
+};
+
+namespace {
+
+int guardContext(vxb_context* ctx) {
+    if (!ctx) return VXB_ERR_INVALID;
+    cudaError_t e = cudaSetDevice(ctx->impl.device);
+    if (e != cudaSuccess) return vxb::cudaStatus(ctx->impl, e, "cudaSetDevice");
+    return VXB_OK;
+}
+
+#define GUARD(ctx)                          \
+    do {                                    \
+        int g_ = guardContext(ctx);         \
+        if (g_ != VXB_OK) return g_;        \
+    } while (0)
+
+#define TRY(expr)                          \
+    do {                                   \
+        int s_ = (expr);                   \
+        if (s_ != VXB_OK) return s_;       \
+    } while (0)
+
+int ensureCounters(Context& c) {
+    TRY(vxb::ensure(c, c.countersBuf, sizeof(vxb::Counters)));
+    c.dCounters = reinterpret_cast<vxb::Counters*>(c.countersBuf.ptr);
+    return VXB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* vxb_version(void) { return "velox_b200 0.1 (sm_100a)"; }
+
+const char* vxb_status_string(int status) {
+    switch (status) {
+    case VXB_OK: return "ok";
+    case VXB_ERR_INVALID: return "invalid argument or state";
+    case VXB_ERR_NO_DEVICE: return "no CUDA device";
+    case VXB_ERR_OOM: return "device memory allocation failed";
+    case VXB_ERR_DEVICE_LOST: return "device lost";
+    case VXB_ERR_CAPACITY: return "caller buffer too small";
+    case VXB_ERR_UNSUPPORTED: return "unsupported input";
+    case VXB_ERR_TIMEOUT: return "bounded device wait timed out";
+    default: return "unknown status";
+    }
+}
+
+int vxb_context_create(int device, vxb_context** out) {
+    if (!out) return VXB_ERR_INVALID;
+    *out = nullptr;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+        cudaGetLastError();
+        return VXB_ERR_NO_DEVICE;
+    }
+    if (device < 0 || device >= count) return VXB_ERR_INVALID;
+    if (cudaSetDevice(device) != cudaSuccess) return VXB_ERR_NO_DEVICE;
+    auto* ctx = new (std::nothrow) vxb_context();
+    if (!ctx) return VXB_ERR_OOM;
+    Context& c = ctx->impl;
+    c.device = device;
+    cudaDeviceGetAttribute(&c.smCount, cudaDevAttrMultiProcessorCount, device);
+    if (cudaStreamCreateWithFlags(&c.ownStream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete ctx;
+        return VXB_ERR_DEVICE_LOST;
+    }
+    c.stream = c.ownStream;
+    if (ensureCounters(c) != VXB_OK) {
+        cudaStreamDestroy(c.ownStream);
+        delete ctx;
+        return VXB_ERR_OOM;
+    }
+    *out = ctx;
+    return VXB_OK;
+}
+
+void vxb_context_destroy(vxb_context* ctx) {
+    if (!ctx) return;
+    Context& c = ctx->impl;
+    cudaSetDevice(c.device);
+    if (c.stream) cudaStreamSynchronize(c.stream);
+    vxb::DevBuf* bufs[] = {&c.bodyBuf, &c.aosBuf, &c.worldOfBuf, &c.planeStartBuf, &c.planeListBuf, &c.prevPoseBuf,
+                           &c.snapBuf, &c.hullPtsBuf, &c.facesBuf, &c.aabbBuf, &c.cellKeyBuf, &c.cellValBuf,
+                           &c.sortKeysAlt, &c.sortValsAlt, &c.sortHist, &c.hashKeyBuf, &c.hashValBuf, &c.pairBuf,
+                           &c.contactTmpBuf, &c.recKeyBuf, &c.recValBuf, &c.recInfoBuf, &c.recCountBuf,
+                           &c.contactBuf[0], &c.contactBuf[1], &c.prevKeyBuf, &c.pairKeyBuf, &c.recOffsetBuf,
+                           &c.parentBuf, &c.islandOfBodyBuf, &c.islandKeyBuf, &c.islandValBuf, &c.colorBuf,
+                           &c.colorKeyBuf, &c.maskBuf, &c.nextColorBuf, &c.islandStartBuf, &c.islandInfoBuf,
+                           &c.flagBuf, &c.scanBuf, &c.scanTmp, &c.segStartBuf, &c.islandSegBuf, &c.bodyKeyBuf,
+                           &c.bodyValBuf, &c.islandBodyStartBuf, &c.caFlagBuf, &c.caBodyMarkBuf, &c.caCandBuf,
+                           &c.countersBuf};
+    for (vxb::DevBuf* b : bufs)
+        if (b->ptr) cudaFree(b->ptr);
+    if (c.ownStream) cudaStreamDestroy(c.ownStream);
+    delete ctx;
+}
+
+const char* vxb_context_last_error(const vxb_context* ctx) {
+    return ctx ? ctx->impl.lastError.c_str() : "null context";
+}
+
+int vxb_context_set_stream(vxb_context* ctx, void* stream) {
+    GUARD(ctx);
+    ctx->impl.stream = stream ? reinterpret_cast<cudaStream_t>(stream) : ctx->impl.ownStream;
+    return VXB_OK;
+}
+
+uint64_t vxb_context_launch_count(const vxb_context* ctx) { return ctx ? ctx->impl.launches : 0; }
+
+// ---- Backend interface ---------------------------------------------------
+
+int vxb_backend_integrate(vxb_context* ctx, vx_body* bodies, uint32_t n, vx_vec3 gravity, float dt) {
+    GUARD(ctx);
+    if (n == 0) return VXB_OK;
+    if (!bodies) return VXB_ERR_INVALID;
+    Context& c = ctx->impl;
+    TRY(ensureCounters(c));
+    TRY(vxb::loadBodies(c, bodies, n, nullptr));
+    TRY(vxb::backendIntegrate(c, gravity, dt));
+    return vxb::readBodies(c, bodies, n);
+}
+
+int vxb_backend_find_contacts(vxb_context* ctx, const vx_body* bodies, uint32_t n, const vx_soup* soup, float dt,
+                              uint32_t* count) {
+    GUARD(ctx);
+    if (!count) return VXB_ERR_INVALID;
+    *count = 0;
+    Context& c = ctx->impl;
+    c.backendContacts = 0;
+    if (n < 2) return VXB_OK;
+    if (!bodies) return VXB_ERR_INVALID;
+    TRY(ensureCounters(c));
+    TRY(vxb::loadBodies(c, bodies, n, nullptr));
+    TRY(vxb::loadSoup(c, soup));
+    return vxb::backendFindContacts(c, dt, count);
+}
+
+int vxb_backend_copy_contacts(vxb_context* ctx, vx_contact* out, uint32_t cap) {
+    GUARD(ctx);
+    if (!out && ctx->impl.backendContacts) return VXB_ERR_INVALID;
+    return vxb::backendCopyContacts(ctx->impl, out, cap);
+}
+
+int vxb_backend_solve_velocities(vxb_context* ctx, vx_body* bodies, uint32_t n, vx_contact* contacts, uint32_t m,
+                                 float dt, int warmStart, const vx_solver_options* options, uint32_t* iterations) {
+    GUARD(ctx);
+    if (iterations) *iterations = 0;
+    if (m == 0) return VXB_OK;
+    if (!bodies || !contacts || !options || n == 0) return VXB_ERR_INVALID;
+    Context& c = ctx->impl;
+    if (!warmStart && (!c.backendColored || c.backendContacts != m))
+        return vxb::fail(c, VXB_ERR_INVALID, "solve without warm start needs the resident coloured contacts");
+    TRY(ensureCounters(c));
+    TRY(vxb::loadBodies(c, bodies, n, nullptr));
+    TRY(vxb::backendSolve(c, contacts, m, dt, warmStart != 0, *options, vx_vec3{0, 0, 0}, 1, false));
+    if (iterations) *iterations = (uint32_t)(2 * options->velocityIterations);
+    return vxb::readBodies(c, bodies, n);
+}
+
+int vxb_backend_advance_substeps(vxb_context* ctx, vx_body* bodies, uint32_t n, vx_contact* contacts, uint32_t m,
+                                 vx_vec3 gravity, float h, int substeps, const vx_solver_options* options,
+                                 int* advanced, uint32_t* iterations) {
+    GUARD(ctx);
+    if (!advanced || !options) return VXB_ERR_INVALID;
+    *advanced = 0;
+    if (iterations) *iterations = 0;
+    if (options->iterationPolicy != 0) return VXB_OK;  // Adaptive: host path, like the reference
+    if (n == 0) { *advanced = 1; return VXB_OK; }
+    if (!bodies || (m && !contacts) || substeps <= 0) return VXB_ERR_INVALID;
+    Context& c = ctx->impl;
+    TRY(ensureCounters(c));
+    TRY(vxb::loadBodies(c, bodies, n, nullptr));
+    TRY(vxb::backendSolve(c, contacts, m, h, true, *options, gravity, substeps, true));
+    TRY(vxb::readBodies(c, bodies, n));
+    *advanced = 1;
+    if (iterations) *iterations = m ? (uint32_t)(2 * options->velocityIterations * substeps) : 0u;
+    return VXB_OK;
+}
+
+int vxb_backend_fetch_impulses(vxb_context* ctx, vx_contact* contacts, uint32_t m) {
+    GUARD(ctx);
+    if (m && !contacts) return VXB_ERR_INVALID;
+    return vxb::backendFetchImpulses(ctx->impl, contacts, m);
+}
+
+int vxb_backend_invalidate(vxb_context* ctx) {
+    GUARD(ctx);
+    ctx->impl.backendColored = false;
+    ctx->impl.backendContacts = 0;
+    ctx->impl.prevCount = 0;
+    return VXB_OK;
+}
+
+// ---- device-resident world -------------------------------------------------
+
+int vxb_world_load(vxb_context* ctx, const vx_body* bodies, uint32_t n, const vx_soup* soup,
+                   const uint32_t* worldOfBody) {
+    GUARD(ctx);
+    if (!bodies || n == 0) return VXB_ERR_INVALID;
+    Context& c = ctx->impl;
+    TRY(ensureCounters(c));
+    TRY(vxb::loadBodies(c, bodies, n, worldOfBody));
+    TRY(vxb::loadSoup(c, soup));
+    cudaError_t e = cudaStreamSynchronize(c.stream);
+    return vxb::cudaStatus(c, e, "world load");
+}
+
+int vxb_world_configure(vxb_context* ctx, const vxb_step_config* config) {
+    GUARD(ctx);
+    if (!config || !(config->dt >= 0.0f) || config->substeps <= 0) return VXB_ERR_INVALID;
+    if (config->solver.iterationPolicy != 0)
+        return vxb::fail(ctx->impl, VXB_ERR_UNSUPPORTED, "the adaptive iteration policy runs on the host");
+    ctx->impl.config = *config;
+    ctx->impl.configured = true;
+    return VXB_OK;
+}
+
+int vxb_world_step(vxb_context* ctx, int steps) {
+    GUARD(ctx);
+    if (steps < 0) return VXB_ERR_INVALID;
+    if (ctx->impl.config.dt == 0.0f) return VXB_OK;
+    return vxb::worldStep(ctx->impl, steps);
+}
+
+int vxb_world_read_bodies(vxb_context* ctx, vx_body* out, uint32_t n) {
+    GUARD(ctx);
+    if (!out) return VXB_ERR_INVALID;
+    return vxb::readBodies(ctx->impl, out, n);
+}
+
+int vxb_world_read_poses(vxb_context* ctx, float* out, uint32_t n) {
+    GUARD(ctx);
+    if (!out) return VXB_ERR_INVALID;
+    return vxb::readPoses(ctx->impl, out, n);
+}
+
+int vxb_world_write_forces(vxb_context* ctx, const float* in, uint32_t n) {
+    GUARD(ctx);
+    if (!in) return VXB_ERR_INVALID;
+    return vxb::writeForces(ctx->impl, in, n);
+}
+
+int vxb_world_read_contacts(vxb_context* ctx, vx_contact* out, uint32_t cap, uint32_t* count) {
+    GUARD(ctx);
+    return vxb::readContacts(ctx->impl, out, cap, count);
+}
+
+int vxb_world_stats(vxb_context* ctx, vxb_step_stats* out) {
+    if (!ctx || !out) return VXB_ERR_INVALID;
+    *out = ctx->impl.stats;
+    return VXB_OK;
+}
+
+// ---- stages ----------------------------------------------------------------
+
+int vxb_stage_pairs(vxb_context* ctx, const vx_body* bodies, uint32_t n, float dt, uint64_t* out, uint32_t cap,
+                    uint32_t* count) {
+    GUARD(ctx);
+    if (!bodies || !count || n == 0) return VXB_ERR_INVALID;
+    Context& c = ctx->impl;
+    TRY(ensureCounters(c));
+    TRY(vxb::loadBodies(c, bodies, n, nullptr));
+    return vxb::stagePairs(c, dt, out, cap, count);
+}
+
+int vxb_stage_collide(vxb_context* ctx, const vx_body* bodies, uint32_t n, const vx_soup* soup,
+                      const uint64_t* pairs, uint32_t npairs, float dt, vx_contact* out, uint32_t cap,
+                      uint32_t* counts, uint32_t* total) {
+    GUARD(ctx);
+    if (!bodies || !total || n == 0 || (npairs && !pairs)) return VXB_ERR_INVALID;
+    Context& c = ctx->impl;
+    for (uint32_t p = 0; p < npairs; ++p)
+        if ((uint32_t)(pairs[p] >> 32) >= n || (uint32_t)pairs[p] >= n) return VXB_ERR_INVALID;
+    TRY(ensureCounters(c));
+    TRY(vxb::loadBodies(c, bodies, n, nullptr));
+    TRY(vxb::loadSoup(c, soup));
+    return vxb::stageCollide(c, pairs, npairs, dt, out, cap, counts, total);
+}
+
+int vxb_stage_color(vxb_context* ctx, const vx_body* bodies, uint32_t n, const vx_contact* contacts, uint32_t m,
+                    int32_t* colorOf, uint32_t* numColors) {
+    GUARD(ctx);
+    if (!bodies || !numColors || n == 0 || (m && (!contacts || !colorOf))) return VXB_ERR_INVALID;
+    Context& c = ctx->impl;
+    for (uint32_t k = 0; k < m; ++k)
+        if (contacts[k].a >= n || contacts[k].b >= n) return VXB_ERR_INVALID;
+    TRY(ensureCounters(c));
+    TRY(vxb::loadBodies(c, bodies, n, nullptr));
+    return vxb::stageColor(c, contacts, m, colorOf, numColors);
+}
+
+}  // extern "C"

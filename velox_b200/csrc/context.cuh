@@ -1,0 +1,159 @@
+// Backend context: device buffers and the step orchestration of one
+// pipeline instance (the role of class CudaBackend, src/backend_cuda.cu:350-1017,
+// re-planned for the device: SoA body state, device-side counts, no host
+// round trips inside a step).
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "geom.cuh"
+#include "radix_sort.cuh"
+#include "velox_b200.h"
+
+namespace vxb {
+
+// Island decomposition of one step's contacts.
+struct IslandPlan {
+    uint32_t islands = 0;      // including the null island when present
+    uint32_t realIslands = 0;  // islands with a dynamic body
+    uint32_t segments = 0;     // (island, colour) runs
+    uint32_t freeFrom = 0, freeTo = 0;  // contact-free bodies (range in the island-sorted body order)
+};
+
+// Grow-only device allocation.
+struct DevBuf {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+};
+
+// Device-side counters and flags (one small allocation, read back once per call).
+struct Counters {
+    uint32_t pairs;          // candidate pairs emitted (may exceed capacity)
+    uint32_t contactsTmp;    // contacts appended by the narrow phase
+    uint32_t records;        // pairs with at least one contact
+    uint32_t contacts;       // contacts after placement (== contactsTmp when no overflow)
+    uint32_t islands;        // contact islands
+    uint32_t segments;       // (island, colour) segments
+    uint32_t maxColors;      // largest colour count of an island
+    uint32_t largestIsland;  // contacts in the largest island
+    uint32_t caCandidates;   // pairs visited by the serial rewind pass
+    uint32_t rewinds;        // conservative-advancement rewinds
+    uint32_t caOverflow;     // rewind cascade left the 1-hop candidate set
+    uint32_t warmStarted;    // contacts that inherited impulses
+    uint32_t overflow;       // bit 0 pairs, bit 1 contacts, bit 2 records
+    uint32_t timeout;        // a bounded device wait gave up
+    uint32_t cellMinBits[3]; // ordered-int encodings of the minimum AABB centre
+    uint32_t cellMaxBits[3]; // ordered-int encodings of the maximum AABB centre
+    uint32_t extentBits;     // float bits of the largest non-plane AABB extent
+    uint32_t worldBits;      // bits of the world id in cell keys
+    uint32_t pad[8];
+};
+
+struct Context {
+    int device = 0;
+    int smCount = 148;
+    cudaStream_t ownStream = nullptr;
+    cudaStream_t stream = nullptr;
+    std::string lastError;
+    uint64_t launches = 0;
+
+    // ---- bodies ----
+    uint32_t n = 0;
+    uint32_t worlds = 1;
+    DevBuf bodyBuf;     // all SoA arrays in one allocation
+    BodyArrays B{};
+    DevBuf aosBuf;      // vx_body staging (upload / download)
+    DevBuf worldOfBuf;  // uint32 world id per body
+    DevBuf planeStartBuf, planeListBuf;  // per-world plane CSR
+    DevBuf prevPoseBuf;                  // float4 prevPos[n], prevRot[n]
+    DevBuf snapBuf;                      // call-start snapshot of the mutable state
+    std::vector<uint32_t> hostWorldOf;
+    bool hasKinematic = false;
+
+    // ---- soup ----
+    DevBuf hullPtsBuf, facesBuf;
+    size_t hullPointCount = 0, faceIndexCount = 0;
+
+    // ---- broad phase ----
+    DevBuf aabbBuf;      // float4 lo[n], hi[n]
+    DevBuf cellKeyBuf, cellValBuf;
+    RadixScratch sortScratch;
+    DevBuf sortKeysAlt, sortValsAlt, sortHist;
+    DevBuf hashKeyBuf, hashValBuf;
+    uint32_t hashCap = 0;
+    DevBuf pairBuf;
+    uint32_t pairCap = 0;
+
+    // ---- narrow phase ----
+    DevBuf contactTmpBuf;
+    uint32_t contactCap = 0;
+    DevBuf recKeyBuf, recValBuf, recInfoBuf, recCountBuf;
+    uint32_t recCap = 0;
+    DevBuf contactBuf[2];  // key-sorted contacts: current / previous step
+    int cur = 0;
+    uint32_t prevCount = 0;     // contacts held in contactBuf[cur ^ 1]
+    DevBuf prevKeyBuf;          // (a<<32|b) of the previous contacts
+    DevBuf pairKeyBuf;          // (a<<32|b) per record in sorted order (CA pairs)
+    DevBuf recOffsetBuf;        // first contact of each sorted record
+
+    // ---- islands / colouring ----
+    DevBuf parentBuf, islandOfBodyBuf;
+    DevBuf islandKeyBuf, islandValBuf;  // per contact
+    DevBuf colorBuf;                    // colour per contact (key-sorted index)
+    DevBuf colorKeyBuf;                 // (island << 16 | colour) in island order
+    DevBuf maskBuf, nextColorBuf;       // per body
+    DevBuf islandStartBuf, islandInfoBuf;  // per island
+    DevBuf flagBuf, scanBuf, scanTmp;
+    DevBuf segStartBuf, islandSegBuf;
+    DevBuf bodyKeyBuf, bodyValBuf, islandBodyStartBuf;
+    DevBuf caFlagBuf, caBodyMarkBuf, caCandBuf;
+
+    DevBuf countersBuf;
+    Counters* dCounters = nullptr;
+    Counters hostCounters{};
+
+    // ---- configuration ----
+    vxb_step_config config{};
+    bool configured = false;
+    vxb_step_stats stats{};
+
+    // ---- Backend-interface mode ----
+    uint32_t backendContacts = 0;   // contacts resident after a find / solve
+    bool backendColored = false;
+    int backendSweeps = 0;
+    vx_solver_options backendOptions{};
+    std::vector<vx_contact> hostSorted;
+    IslandPlan backendPlan;
+
+    cudaError_t err = cudaSuccess;
+};
+
+// Records a failure on the context; returns the mapped status.
+int fail(Context& c, int status, const std::string& message);
+int cudaStatus(Context& c, cudaError_t e, const char* what);
+
+// Grow-only device allocation helper; returns VXB_OK or VXB_ERR_OOM.
+int ensure(Context& c, DevBuf& b, size_t bytes);
+
+// Pipeline entry points (pipeline.cu).
+int loadBodies(Context& c, const vx_body* bodies, uint32_t n, const uint32_t* worldOf);
+int loadSoup(Context& c, const vx_soup* soup);
+int readBodies(Context& c, vx_body* out, uint32_t n);
+int worldStep(Context& c, int steps);
+int stagePairs(Context& c, float dt, uint64_t* out, uint32_t cap, uint32_t* count);
+int stageCollide(Context& c, const uint64_t* pairs, uint32_t npairs, float dt, vx_contact* out,
+                 uint32_t cap, uint32_t* counts, uint32_t* total);
+int stageColor(Context& c, const vx_contact* contacts, uint32_t m, int32_t* colorOf, uint32_t* numColors);
+int backendIntegrate(Context& c, vx_vec3 gravity, float dt);
+int backendFindContacts(Context& c, float dt, uint32_t* count);
+int backendCopyContacts(Context& c, vx_contact* out, uint32_t cap);
+int backendSolve(Context& c, vx_contact* contacts, uint32_t m, float h, bool warmStart,
+                 const vx_solver_options& options, vx_vec3 gravity, int substeps, bool fullSubsteps);
+int backendFetchImpulses(Context& c, vx_contact* contacts, uint32_t m);
+int readPoses(Context& c, float* out, uint32_t n);
+int writeForces(Context& c, const float* in, uint32_t n);
+int readContacts(Context& c, vx_contact* out, uint32_t cap, uint32_t* count);
+
+}  // namespace vxb

@@ -1,0 +1,1812 @@
+// The per-step contact pipeline on the device.
+//
+// Step structure (src/world.cpp:3830-4521 with the CUDA backend's
+// advanceSubsteps, src/backend_cuda.cu:691-761):
+//   prepare      orientation normalisation, first-substep gravity, pre-solve poses
+//   broad phase  swept AABBs, cell keys (world id in the high bits), radix sort,
+//                cell hash table, 27-cell pair emission + per-world plane pairs
+//   narrow phase collidePair per candidate pair, contacts sorted by (a, b, point)
+//   warm start   impulse matching against the previous step's contacts
+//   islands      union-find over dynamic-dynamic contacts; contacts grouped by
+//                island keep their global order, so island-local greedy
+//                colouring equals the reference's global greedy colouring and
+//                island-local colour order equals its global colour order
+//   solve        one launch runs every island's whole substep loop
+//                (integration, warm start, 2*velocityIterations coloured
+//                sweeps, transform integration); tiny islands run one thread
+//                each, larger ones a block with a barrier between colours
+//   rewind       conservative advancement for deep end-of-step overlaps
+//   correction   split-impulse position correction, coloured per island
+#include <algorithm>
+#include <cstring>
+
+#include "context.cuh"
+
+namespace vxb {
+
+// ---------------------------------------------------------------------------
+// host helpers
+// ---------------------------------------------------------------------------
+
+int fail(Context& c, int status, const std::string& message) {
+    c.lastError = message;
+    return status;
+}
+
+int cudaStatus(Context& c, cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return VXB_OK;
+    std::string msg = std::string("velox_b200 CUDA failure: ") + cudaGetErrorString(e) + " (" + what + ")";
+    if (e == cudaErrorMemoryAllocation) return fail(c, VXB_ERR_OOM, msg);
+    if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return fail(c, VXB_ERR_NO_DEVICE, msg);
+    if (e == cudaErrorLaunchFailure || e == cudaErrorLaunchTimeout || e == cudaErrorUnknown ||
+        e == cudaErrorIllegalAddress || e == cudaErrorDevicesUnavailable)
+        return fail(c, VXB_ERR_DEVICE_LOST, msg);
+    return fail(c, VXB_ERR_INVALID, msg);
+}
+
+int ensure(Context& c, DevBuf& b, size_t bytes) {
+    if (bytes <= b.bytes && b.ptr) return VXB_OK;
+    if (b.ptr) cudaFree(b.ptr);
+    b.ptr = nullptr;
+    b.bytes = 0;
+    size_t want = bytes + bytes / 2 + 256;
+    cudaError_t e = cudaMalloc(&b.ptr, want);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return cudaStatus(c, e, "cudaMalloc");
+    }
+    b.bytes = want;
+    return VXB_OK;
+}
+
+template <class T> T* P(DevBuf& b) { return reinterpret_cast<T*>(b.ptr); }
+
+#define VXB_TRY(expr)                  \
+    do {                               \
+        int s_ = (expr);               \
+        if (s_ != VXB_OK) return s_;   \
+    } while (0)
+
+#define VXB_CUDA(c, expr)                                             \
+    do {                                                              \
+        cudaError_t e_ = (expr);                                      \
+        if (e_ != cudaSuccess) return cudaStatus((c), e_, #expr);     \
+    } while (0)
+
+static inline uint32_t blocksFor(uint64_t items, int threads, uint32_t cap = 65535u * 16u) {
+    uint64_t b = (items + threads - 1) / threads;
+    if (b == 0) b = 1;
+    return (uint32_t)std::min<uint64_t>(b, cap);
+}
+
+static inline int bitsFor(uint64_t maxValue) { return keyBits(maxValue); }
+
+#define LAUNCH(c, kernel, grid, block, ...)                                  \
+    do {                                                                     \
+        kernel<<<(grid), (block), 0, (c).stream>>>(__VA_ARGS__);            \
+        ++(c).launches;                                                      \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+// device helpers
+// ---------------------------------------------------------------------------
+
+VXD uint32_t orderedBits(float f) {
+    const uint32_t u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+VXD float fromOrdered(uint32_t u) {
+    return __uint_as_float((u & 0x80000000u) ? (u & 0x7fffffffu) : ~u);
+}
+VXD uint64_t mix64(uint64_t k) {
+    k ^= k >> 33; k *= 0xff51afd7ed558ccdull; k ^= k >> 33; k *= 0xc4ceb9fe1a85ec53ull; k ^= k >> 33;
+    return k;
+}
+VXD unsigned laneMaskLt() {
+    unsigned m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+// Warp-aggregated slot reservation for the currently active lanes.
+VXD uint32_t aggregatedSlot(uint32_t* counter) {
+    const unsigned active = __activemask();
+    const int leader = __ffs(active) - 1;
+    const int lane = threadIdx.x & 31;
+    uint32_t base = 0;
+    if (lane == leader) base = atomicAdd(counter, (uint32_t)__popc(active));
+    base = __shfl_sync(active, base, leader);
+    return base + __popc(active & laneMaskLt());
+}
+
+VXD Mass loadMass(const BodyArrays& B, uint32_t i) {
+    const float4 in = B.inertia[i];
+    Mass m;
+    m.invI = V3{in.x, in.y, in.z};
+    m.invMass = in.w;
+    m.iq = q4(B.iq[i]);
+    m.flags = B.filt[i].x;
+    return m;
+}
+
+VXD SolverBody loadSolverBody(const BodyArrays& B, uint32_t i) {
+    SolverBody s;
+    s.p = f3(B.pos[i]);
+    s.q = q4(B.rot[i]);
+    s.v = f3(B.vel[i]);
+    s.w = f3(B.ang[i]);
+    s.m = loadMass(B, i);
+    s.sphere = shapeOf(s.m.flags) == kSphere;
+    return s;
+}
+
+VXD void loadRow(const vx_contact& c, RowContact& r) {
+    r.normal = V3{c.normal.x, c.normal.y, c.normal.z};
+    r.point = V3{c.point.x, c.point.y, c.point.z};
+    r.la = V3{c.localAnchorA.x, c.localAnchorA.y, c.localAnchorA.z};
+    r.lb = V3{c.localAnchorB.x, c.localAnchorB.y, c.localAnchorB.z};
+    r.bias0 = c.bias0; r.vn0 = c.vn0; r.restitution = c.restitution;
+    r.friction1 = c.friction1; r.friction2 = c.friction2;
+    r.rolling = c.rollingFriction; r.spinning = c.spinningFriction;
+    r.nImp = c.normalImpulse; r.t1Imp = c.tangentImpulse1; r.t2Imp = c.tangentImpulse2;
+    r.r1Imp = c.rollingImpulse1; r.r2Imp = c.rollingImpulse2; r.sImp = c.spinningImpulse;
+}
+VXD void storeRow(vx_contact& c, const RowContact& r) {
+    c.point = vx_vec3{r.point.x, r.point.y, r.point.z};
+    c.normalImpulse = r.nImp; c.tangentImpulse1 = r.t1Imp; c.tangentImpulse2 = r.t2Imp;
+    c.rollingImpulse1 = r.r1Imp; c.rollingImpulse2 = r.r2Imp; c.spinningImpulse = r.sImp;
+}
+
+// integrateKernel semantics (src/backend_cuda.cu:80-89) for body i.
+VXD void integrateVelocity(const BodyArrays& B, uint32_t i, const V3& g, float dt) {
+    const Mass m = loadMass(B, i);
+    if (!isDynamic(m.flags) || isLocked(m.flags) || isAsleep(m.flags)) return;
+    const Q4 q = q4(B.rot[i]);
+    V3 v = f3(B.vel[i]);
+    V3 w = f3(B.ang[i]);
+    const V3 F = f3(B.force[i]);
+    const V3 T = f3(B.torque[i]);
+    const float4 ex = B.extra[i];
+    v += (g * ex.y + F * solverInvMass(m)) * dt;
+    w += invInertiaMulAt(m, T, q) * dt;
+    v *= 1.0f / (1.0f + ex.z * dt);
+    w *= 1.0f / (1.0f + ex.w * dt);
+    B.vel[i] = pack(v, 0.0f);
+    B.ang[i] = pack(w, 0.0f);
+}
+
+// integrateTransformsKernel semantics (src/backend_cuda.cu:91-97).
+VXD void integrateTransform(const BodyArrays& B, uint32_t i, float dt) {
+    const Mass m = loadMass(B, i);
+    if (isStaticBody(m.flags) || isLocked(m.flags) || isAsleep(m.flags)) return;
+    V3 p = f3(B.pos[i]);
+    Q4 q = q4(B.rot[i]);
+    const V3 v = f3(B.vel[i]);
+    V3 w = f3(B.ang[i]);
+    advanceTransform(m, p, q, v, w, dt);
+    B.pos[i] = pack(p, 0.0f);
+    B.rot[i] = pack(q);
+    B.ang[i] = pack(w, 0.0f);
+}
+
+// ---------------------------------------------------------------------------
+// body packing
+// ---------------------------------------------------------------------------
+
+__global__ void packBodiesKernel(const vx_body* __restrict__ in, uint32_t n, BodyArrays B) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const vx_body& b = in[i];
+        B.pos[i] = make_float4(b.position.x, b.position.y, b.position.z, 0.0f);
+        B.rot[i] = make_float4(b.orientation.x, b.orientation.y, b.orientation.z, b.orientation.w);
+        B.vel[i] = make_float4(b.velocity.x, b.velocity.y, b.velocity.z, 0.0f);
+        B.ang[i] = make_float4(b.angularVelocity.x, b.angularVelocity.y, b.angularVelocity.z, 0.0f);
+        B.inertia[i] = make_float4(b.invInertia.x, b.invInertia.y, b.invInertia.z, b.invMass);
+        B.iq[i] = make_float4(b.inertiaOrientation.x, b.inertiaOrientation.y, b.inertiaOrientation.z,
+                              b.inertiaOrientation.w);
+        B.dims[i] = make_float4(b.halfExtents.x, b.halfExtents.y, b.halfExtents.z, b.radius);
+        B.extra[i] = make_float4(b.capsuleHalfHeight, b.gravityScale, b.linearDamping, b.angularDamping);
+        B.mat[i] = make_float4(b.friction, b.restitution, b.rollingFriction, b.spinningFriction);
+        B.fscale[i] = make_float4(b.frictionScale.x, b.frictionScale.y, b.frictionScale.z,
+                                  b.ccdTuning.speculativeDistance);
+        B.ccd[i] = make_float4(b.ccdTuning.collisionMargin, b.ccdTuning.minVelocityForCCD, 0.0f, 0.0f);
+        B.plane[i] = make_float4(b.planeNormal.x, b.planeNormal.y, b.planeNormal.z, b.planeOffset);
+        B.hull[i] = make_uint4(b.hullFirst, b.hullCount, b.hullFaceFirst, b.hullFaceCount);
+        const uint32_t flags = (uint32_t)(b.shape & 15u) | ((uint32_t)(b.motionType & 3u) << kMotionShift) |
+                               ((uint32_t)(b.ccdTuning.quality & 3u) << kQualityShift) |
+                               (b.ccdTuning.enableContinuous ? kContinuousBit : 0u) |
+                               (b.sensor ? kSensorBit : 0u) | (b.fixedRotation ? kFixedRotationBit : 0u) |
+                               (b.asleep == 1 ? kAsleepBit : 0u) |
+                               ((uint32_t)(b.frictionCombine & 7u) << kFrictionCombineShift) |
+                               ((uint32_t)(b.restitutionCombine & 7u) << kRestitutionCombineShift) |
+                               ((uint32_t)(b.geometryQuality & 3u) << kGeomQualityShift);
+        B.filt[i] = make_uint4(flags, b.categoryBits, b.maskBits, (uint32_t)b.groupIndex);
+        B.force[i] = make_float4(b.force.x, b.force.y, b.force.z, 0.0f);
+        B.torque[i] = make_float4(b.torque.x, b.torque.y, b.torque.z, 0.0f);
+    }
+}
+
+__global__ void unpackBodiesKernel(vx_body* __restrict__ out, uint32_t n, BodyArrays B) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        vx_body& b = out[i];
+        float4 t = B.pos[i]; b.position = vx_vec3{t.x, t.y, t.z};
+        t = B.rot[i]; b.orientation = vx_quat{t.x, t.y, t.z, t.w};
+        t = B.vel[i]; b.velocity = vx_vec3{t.x, t.y, t.z};
+        t = B.ang[i]; b.angularVelocity = vx_vec3{t.x, t.y, t.z};
+        t = B.force[i]; b.force = vx_vec3{t.x, t.y, t.z};
+        t = B.torque[i]; b.torque = vx_vec3{t.x, t.y, t.z};
+    }
+}
+
+__global__ void posesKernel(float* __restrict__ out, uint32_t n, BodyArrays B) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float4 p = B.pos[i], q = B.rot[i];
+        float* o = out + 7 * (size_t)i;
+        o[0] = p.x; o[1] = p.y; o[2] = p.z; o[3] = q.x; o[4] = q.y; o[5] = q.z; o[6] = q.w;
+    }
+}
+
+__global__ void forcesKernel(const float* __restrict__ in, uint32_t n, BodyArrays B) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float* f = in + 6 * (size_t)i;
+        B.force[i] = make_float4(f[0], f[1], f[2], 0.0f);
+        B.torque[i] = make_float4(f[3], f[4], f[5], 0.0f);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// prepare: World::stepImpl orientation normalisation (world.cpp:3930),
+// first-substep gravity (world.cpp:4014) and the pre-solve poses (:4186-4188)
+// ---------------------------------------------------------------------------
+
+__global__ void prepareKernel(BodyArrays B, uint32_t n, V3 g, float h, float4* prevPos, float4* prevRot,
+                              int normalizeOrientation) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        if (normalizeOrientation) B.rot[i] = pack(qnormalize(q4(B.rot[i])));
+        integrateVelocity(B, i, g, h);
+        if (prevPos) {
+            prevPos[i] = B.pos[i];
+            prevRot[i] = B.rot[i];
+        }
+    }
+}
+
+__global__ void integrateKernel(BodyArrays B, uint32_t n, V3 g, float h) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        integrateVelocity(B, i, g, h);
+}
+
+// ---------------------------------------------------------------------------
+// broad phase
+// ---------------------------------------------------------------------------
+
+constexpr int kCellBits = 10;  // per axis; coordinates wrap modulo 1024 (exactness kept by the AABB test)
+constexpr uint32_t kCellMask = (1u << kCellBits) - 1u;
+constexpr uint64_t kEmptySlot = ~0ull;
+
+__global__ void aabbKernel(BodyArrays B, uint32_t n, float dt, float4* lo, float4* hi, Counters* C) {
+    float ext = 0.0f;
+    float mn[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, mx[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t flags = B.filt[i].x;
+        if (shapeOf(flags) == kPlane) {
+            lo[i] = make_float4(-1e30f, -1e30f, -1e30f, 0.0f);
+            hi[i] = make_float4(1e30f, 1e30f, 1e30f, 0.0f);
+            continue;
+        }
+        const V3 p = f3(B.pos[i]);
+        const float4 d = B.dims[i];
+        const float reach = aabbReach(flags, V3{d.x, d.y, d.z}, d.w, B.extra[i].x, B.ccd[i].x,
+                                      f3(B.vel[i]), f3(B.ang[i]), dt);
+        const V3 L = p - V3{reach, reach, reach};
+        const V3 H = p + V3{reach, reach, reach};
+        lo[i] = pack(L, 0.0f);
+        hi[i] = pack(H, 0.0f);
+        const float e = fmaxf(H.x - L.x, fmaxf(H.y - L.y, H.z - L.z));
+        if (e < 1e6f) ext = fmaxf(ext, e);
+        const float c[3] = {(L.x + H.x) * 0.5f, (L.y + H.y) * 0.5f, (L.z + H.z) * 0.5f};
+        for (int a = 0; a < 3; ++a) { mn[a] = fminf(mn[a], c[a]); mx[a] = fmaxf(mx[a], c[a]); }
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+        ext = fmaxf(ext, __shfl_xor_sync(0xffffffffu, ext, off));
+        for (int a = 0; a < 3; ++a) {
+            mn[a] = fminf(mn[a], __shfl_xor_sync(0xffffffffu, mn[a], off));
+            mx[a] = fmaxf(mx[a], __shfl_xor_sync(0xffffffffu, mx[a], off));
+        }
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (ext > 0.0f) atomicMax(&C->extentBits, __float_as_uint(ext));
+        for (int a = 0; a < 3; ++a)
+            if (mn[a] <= mx[a]) {
+                atomicMin(&C->cellMinBits[a], orderedBits(mn[a]));
+                atomicMax(&C->cellMaxBits[a], orderedBits(mx[a]));
+            }
+    }
+}
+
+VXD float cellSizeOf(const Counters* C) {
+    float s = __uint_as_float(C->extentBits);
+    return s > 0.0f ? s : 1.0f;
+}
+VXD int cellCoord(float centre, float inv, float minCentre) {
+    float f = floorf(centre * inv) - floorf(minCentre * inv);
+    f = fminf(fmaxf(f, -1.0e9f), 1.0e9f);
+    return (int)f;
+}
+
+__global__ void keyKernel(BodyArrays B, uint32_t n, const uint32_t* worldOf, const float4* lo, const float4* hi,
+                          const Counters* C, uint64_t* keys, uint32_t* vals, uint64_t planeKey) {
+    const float cs = cellSizeOf(C);
+    const float inv = 1.0f / cs;
+    const float m0 = fromOrdered(C->cellMinBits[0]), m1 = fromOrdered(C->cellMinBits[1]),
+                m2 = fromOrdered(C->cellMinBits[2]);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        vals[i] = i;
+        if (shapeOf(B.filt[i].x) == kPlane) { keys[i] = planeKey; continue; }
+        const float4 L = lo[i], H = hi[i];
+        const int cx = cellCoord((L.x + H.x) * 0.5f, inv, m0);
+        const int cy = cellCoord((L.y + H.y) * 0.5f, inv, m1);
+        const int cz = cellCoord((L.z + H.z) * 0.5f, inv, m2);
+        const uint64_t w = worldOf ? worldOf[i] : 0u;
+        keys[i] = (w << (3 * kCellBits)) | ((uint64_t)((uint32_t)cz & kCellMask) << (2 * kCellBits)) |
+                  ((uint64_t)((uint32_t)cy & kCellMask) << kCellBits) | (uint64_t)((uint32_t)cx & kCellMask);
+    }
+}
+
+__global__ void cellTableKernel(const uint64_t* keys, uint32_t n, uint64_t planeKey, uint64_t* hk, uint32_t* hv,
+                                uint32_t mask) {
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+        const uint64_t key = keys[s];
+        if (key == planeKey) continue;
+        if (s > 0 && keys[s - 1] == key) continue;
+        uint32_t slot = (uint32_t)mix64(key) & mask;
+        for (uint32_t probe = 0; probe <= mask; ++probe) {
+            const unsigned long long prev = atomicCAS((unsigned long long*)&hk[slot], (unsigned long long)kEmptySlot,
+                                                      (unsigned long long)key);
+            if (prev == kEmptySlot) { hv[slot] = s; break; }
+            slot = (slot + 1) & mask;
+        }
+    }
+}
+
+VXD uint32_t cellLookup(const uint64_t* hk, const uint32_t* hv, uint32_t mask, uint64_t key) {
+    uint32_t slot = (uint32_t)mix64(key) & mask;
+    for (uint32_t probe = 0; probe <= mask; ++probe) {
+        const uint64_t k = hk[slot];
+        if (k == key) return hv[slot];
+        if (k == kEmptySlot) return 0xffffffffu;
+        slot = (slot + 1) & mask;
+    }
+    return 0xffffffffu;
+}
+
+VXD void emitPair(uint64_t pair, uint64_t* pairs, uint32_t cap, Counters* C) {
+    const uint32_t slot = aggregatedSlot(&C->pairs);
+    if (slot < cap) pairs[slot] = pair;
+    else atomicOr(&C->overflow, 1u);
+}
+
+// Candidate pairs (src/backend_cuda.cu:174-250): the 27 neighbouring cells of
+// each body's cell (same world), pairs i<j discovered from i's side, plus the
+// planes of the body's world.
+__global__ void pairKernel(BodyArrays B, uint32_t n, const uint64_t* keys, const uint32_t* vals, const float4* lo,
+                           const float4* hi, const uint64_t* hk, const uint32_t* hv, uint32_t mask, uint64_t planeKey,
+                           const uint32_t* worldOf, const uint32_t* planeStart, const uint32_t* planeList,
+                           uint64_t* pairs, uint32_t cap, Counters* C) {
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+        const uint64_t key = keys[s];
+        if (key == planeKey) continue;
+        const uint32_t i = vals[s];
+        const uint4 fi = B.filt[i];
+        const V3 Li = f3(lo[i]), Hi = f3(hi[i]);
+        const int cx = (int)(key & kCellMask), cy = (int)((key >> kCellBits) & kCellMask),
+                  cz = (int)((key >> (2 * kCellBits)) & kCellMask);
+        const uint64_t wbits = key >> (3 * kCellBits);
+        for (int dz = -1; dz <= 1; ++dz)
+            for (int dy = -1; dy <= 1; ++dy)
+                for (int dx = -1; dx <= 1; ++dx) {
+                    const uint64_t nk = (wbits << (3 * kCellBits)) |
+                                        ((uint64_t)((uint32_t)(cz + dz) & kCellMask) << (2 * kCellBits)) |
+                                        ((uint64_t)((uint32_t)(cy + dy) & kCellMask) << kCellBits) |
+                                        (uint64_t)((uint32_t)(cx + dx) & kCellMask);
+                    const uint32_t start = cellLookup(hk, hv, mask, nk);
+                    if (start == 0xffffffffu) continue;
+                    for (uint32_t t = start; t < n && keys[t] == nk; ++t) {
+                        const uint32_t j = vals[t];
+                        if (j <= i) continue;
+                        if (!aabbOverlap(Li, Hi, f3(lo[j]), f3(hi[j]))) continue;
+                        const uint4 fj = B.filt[j];
+                        if (inert(fi.x) && inert(fj.x)) continue;
+                        if (!canCollide(fi.y, fi.z, (int32_t)fi.w, fj.y, fj.z, (int32_t)fj.w)) continue;
+                        emitPair(((uint64_t)i << 32) | j, pairs, cap, C);
+                    }
+                }
+        const uint32_t w = worldOf ? worldOf[i] : 0u;
+        for (uint32_t k = planeStart[w]; k < planeStart[w + 1]; ++k) {
+            const uint32_t p = planeList[k];
+            const uint4 fp = B.filt[p];
+            if (inert(fi.x) && inert(fp.x)) continue;
+            const uint32_t a = i < p ? i : p, b = i < p ? p : i;
+            const uint4 fa = a == i ? fi : fp, fb = a == i ? fp : fi;
+            if (!canCollide(fa.y, fa.z, (int32_t)fa.w, fb.y, fb.z, (int32_t)fb.w)) continue;
+            emitPair(((uint64_t)a << 32) | b, pairs, cap, C);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// narrow phase
+// ---------------------------------------------------------------------------
+
+VXD bool pointLess(const vx_contact& x, const vx_contact& y) {
+    if (x.point.x != y.point.x) return x.point.x < y.point.x;
+    if (x.point.y != y.point.y) return x.point.y < y.point.y;
+    return x.point.z < y.point.z;
+}
+
+// One thread per candidate pair: collidePair into a local buffer, order the
+// pair's contacts by point (the host sort of src/backend_cuda.cu:587-595
+// within one (a, b) key), append them and a record keyed for the global sort.
+// mode 0: key = (a << bodyBits) | b; mode 1: key = pair index, emission order kept.
+__global__ void __launch_bounds__(128) collideKernel(BodyArrays B, Soup soup, const uint64_t* pairs,
+                                                     uint32_t npairs, float dt, int mode, int bodyBits,
+                                                     vx_contact* tmp, uint32_t contactCap, uint64_t* recKeys,
+                                                     uint32_t* recVals, uint2* recInfo, uint32_t recCap,
+                                                     Counters* C) {
+    const uint32_t stride = gridDim.x * blockDim.x;
+    const uint32_t rounded = (npairs + 31u) & ~31u;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < rounded; base += stride) {
+        const uint32_t p = base + threadIdx.x;
+        vx_contact buf[kMaxContactsPerPair];
+        int count = 0;
+        if (p < npairs) {
+            const uint64_t pr = pairs[p];
+            const uint32_t i = (uint32_t)(pr >> 32), j = (uint32_t)pr;
+            const BodyView a = loadView(B, i);
+            const BodyView b = loadView(B, j);
+            count = collidePair(a, b, i, j, soup, dt, buf, kMaxContactsPerPair);
+            if (mode == 0)
+                for (int x = 1; x < count; ++x) {
+                    vx_contact key = buf[x];
+                    int y = x - 1;
+                    while (y >= 0 && pointLess(key, buf[y])) { buf[y + 1] = buf[y]; --y; }
+                    buf[y + 1] = key;
+                }
+        }
+        // Warp-wide exclusive scan of the counts, one atomic per warp.
+        const int lane = threadIdx.x & 31;
+        uint32_t incl = (uint32_t)count;
+        for (int off = 1; off < 32; off <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, off);
+            if (lane >= off) incl += y;
+        }
+        const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+        const unsigned hasMask = __ballot_sync(0xffffffffu, count > 0);
+        uint32_t cbase = 0, rbase = 0;
+        if (lane == 0 && total) {
+            cbase = atomicAdd(&C->contactsTmp, total);
+            rbase = atomicAdd(&C->records, (uint32_t)__popc(hasMask));
+        }
+        cbase = __shfl_sync(0xffffffffu, cbase, 0);
+        rbase = __shfl_sync(0xffffffffu, rbase, 0);
+        if (count > 0) {
+            const uint32_t off = cbase + incl - (uint32_t)count;
+            const uint32_t rec = rbase + __popc(hasMask & laneMaskLt());
+            if (off + (uint32_t)count > contactCap || rec >= recCap) {
+                atomicOr(&C->overflow, 2u);
+            } else {
+                for (int x = 0; x < count; ++x) tmp[off + x] = buf[x];
+                recKeys[rec] = mode == 0 ? (((uint64_t)buf[0].a << bodyBits) | buf[0].b) : (uint64_t)p;
+                recVals[rec] = rec;
+                recInfo[rec] = make_uint2(off, (uint32_t)count);
+            }
+        }
+    }
+}
+
+__global__ void gatherCountsKernel(const uint32_t* recVals, const uint2* recInfo, uint32_t nrec, uint32_t* counts) {
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < nrec; k += gridDim.x * blockDim.x)
+        counts[k] = recInfo[recVals[k]].y;
+}
+
+// Copies each record's contacts to their sorted position.
+__global__ void placeKernel(const uint32_t* recVals, const uint2* recInfo, const uint32_t* offsets, uint32_t nrec,
+                            const vx_contact* tmp, vx_contact* out, uint64_t* contactKeys, uint64_t* pairKeys,
+                            uint32_t* recOffset) {
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < nrec; k += gridDim.x * blockDim.x) {
+        const uint2 info = recInfo[recVals[k]];
+        const uint32_t dst = offsets[k];
+        const float4* src = reinterpret_cast<const float4*>(tmp + info.x);
+        float4* d = reinterpret_cast<float4*>(out + dst);
+        for (uint32_t x = 0; x < info.y * 8u; ++x) d[x] = src[x];
+        const uint64_t key = ((uint64_t)tmp[info.x].a << 32) | tmp[info.x].b;
+        if (contactKeys)
+            for (uint32_t x = 0; x < info.y; ++x) contactKeys[dst + x] = key;
+        if (pairKeys) pairKeys[k] = key;
+        if (recOffset) recOffset[k] = dst;
+    }
+}
+
+// Multi-block exclusive scan: per-block sums, a single-block scan of the sums,
+// then per-block scans with the carried offsets.
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 8;
+constexpr uint32_t kScanTile = kScanThreads * kScanItems;
+
+__device__ uint32_t blockExclusiveScan(uint32_t v, uint32_t* warpSums, uint32_t* total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t x = v;
+    for (int off = 1; off < 32; off <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, off);
+        if (lane >= off) x += y;
+    }
+    if (lane == 31) warpSums[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        const int nw = blockDim.x >> 5;
+        uint32_t w = lane < nw ? warpSums[lane] : 0u;
+        for (int off = 1; off < 32; off <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, w, off);
+            if (lane >= off) w += y;
+        }
+        warpSums[lane] = w;
+    }
+    __syncthreads();
+    const uint32_t r = x - v + (warp > 0 ? warpSums[warp - 1] : 0u);
+    if (total) *total = warpSums[(blockDim.x >> 5) - 1];
+    __syncthreads();
+    return r;
+}
+
+__global__ void scanReduceKernel(const uint32_t* in, uint32_t n, uint32_t* blockSums) {
+    __shared__ uint32_t ws[32];
+    const uint32_t base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
+    uint32_t s = 0;
+    for (int k = 0; k < kScanItems; ++k)
+        if (base + k < n) s += in[base + k];
+    uint32_t total;
+    blockExclusiveScan(s, ws, &total);
+    if (threadIdx.x == 0) blockSums[blockIdx.x] = total;
+}
+
+__global__ void scanSumsKernel(uint32_t* sums, uint32_t len) {
+    __shared__ uint32_t ws[32];
+    __shared__ uint32_t carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (uint32_t start = 0; start < len; start += blockDim.x) {
+        const uint32_t i = start + threadIdx.x;
+        const uint32_t v = i < len ? sums[i] : 0u;
+        uint32_t total;
+        const uint32_t ex = blockExclusiveScan(v, ws, &total);
+        if (i < len) sums[i] = carry + ex;
+        __syncthreads();
+        if (threadIdx.x == 0) carry += total;
+        __syncthreads();
+    }
+}
+
+__global__ void scanApplyKernel(const uint32_t* in, uint32_t n, const uint32_t* blockSums, uint32_t* out,
+                                uint32_t* grandTotal) {
+    __shared__ uint32_t ws[32];
+    const uint32_t base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
+    uint32_t v[kScanItems];
+    uint32_t s = 0;
+    for (int k = 0; k < kScanItems; ++k) {
+        v[k] = base + k < n ? in[base + k] : 0u;
+        s += v[k];
+    }
+    uint32_t total;
+    uint32_t ex = blockExclusiveScan(s, ws, &total) + blockSums[blockIdx.x];
+    for (int k = 0; k < kScanItems; ++k) {
+        if (base + k < n) out[base + k] = ex;
+        ex += v[k];
+    }
+    if (grandTotal && blockIdx.x == gridDim.x - 1 && threadIdx.x == blockDim.x - 1) *grandTotal = ex;
+}
+
+static int exclusiveScan(Context& c, const uint32_t* in, uint32_t* out, uint32_t n, uint32_t* grandTotal) {
+    if (n == 0) return VXB_OK;
+    const uint32_t blocks = (n + kScanTile - 1) / kScanTile;
+    VXB_TRY(ensure(c, c.scanTmp, (size_t)blocks * 4 + 16));
+    uint32_t* sums = P<uint32_t>(c.scanTmp);
+    LAUNCH(c, scanReduceKernel, blocks, kScanThreads, in, n, sums);
+    LAUNCH(c, scanSumsKernel, 1, 1024, sums, blocks);
+    LAUNCH(c, scanApplyKernel, blocks, kScanThreads, in, n, sums, out, grandTotal);
+    return VXB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// warm-start matching (src/world.cpp:4133-4184)
+// ---------------------------------------------------------------------------
+
+__global__ void matchKernel(vx_contact* cur, uint32_t m, const vx_contact* prev, const uint64_t* prevKeys,
+                            uint32_t mPrev, Counters* C) {
+    uint32_t warm = 0;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < m; k += gridDim.x * blockDim.x) {
+        vx_contact c = cur[k];
+        const uint64_t key = ((uint64_t)c.a << 32) | c.b;
+        uint32_t lo = 0, hi = mPrev;
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (prevKeys[mid] < key) lo = mid + 1;
+            else hi = mid;
+        }
+        bool copied = false;
+        bool matched = false;
+        if (c.featureKey != 0) {
+            for (uint32_t it = lo; it < mPrev && prevKeys[it] == key; ++it) {
+                const vx_contact& p = prev[it];
+                if (p.featureKey == c.featureKey) {
+                    c.normalImpulse = p.normalImpulse; c.tangentImpulse1 = p.tangentImpulse1;
+                    c.tangentImpulse2 = p.tangentImpulse2; c.rollingImpulse1 = p.rollingImpulse1;
+                    c.rollingImpulse2 = p.rollingImpulse2; c.spinningImpulse = p.spinningImpulse;
+                    if (c.vn0 < -1.0f && p.vn0 < c.vn0) c.vn0 = p.vn0;
+                    matched = copied = true;
+                    break;
+                }
+            }
+        }
+        if (!matched) {
+            if (c.vn0 < -1.0f)
+                for (uint32_t it = lo; it < mPrev && prevKeys[it] == key; ++it)
+                    if (prev[it].vn0 < c.vn0) c.vn0 = prev[it].vn0;
+            float best = 2.5e-3f;
+            for (uint32_t it = lo; it < mPrev && prevKeys[it] == key; ++it) {
+                const vx_contact& p = prev[it];
+                const V3 d{p.point.x - c.point.x, p.point.y - c.point.y, p.point.z - c.point.z};
+                const float ds = lengthSq(d);
+                if (ds < best) {
+                    best = ds;
+                    c.normalImpulse = p.normalImpulse; c.tangentImpulse1 = p.tangentImpulse1;
+                    c.tangentImpulse2 = p.tangentImpulse2; c.rollingImpulse1 = p.rollingImpulse1;
+                    c.rollingImpulse2 = p.rollingImpulse2; c.spinningImpulse = p.spinningImpulse;
+                    copied = true;
+                }
+            }
+        }
+        if (copied) ++warm;
+        cur[k] = c;
+    }
+    for (int off = 16; off > 0; off >>= 1) warm += __shfl_xor_sync(0xffffffffu, warm, off);
+    if ((threadIdx.x & 31) == 0 && warm) atomicAdd(&C->warmStarted, warm);
+}
+
+// ---------------------------------------------------------------------------
+// islands and colouring
+// ---------------------------------------------------------------------------
+
+__global__ void iotaKernel(uint32_t* a, uint32_t n) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) a[i] = i;
+}
+
+VXD uint32_t ufFind(uint32_t* parent, uint32_t x) {
+    uint32_t p = parent[x];
+    while (p != x) {
+        const uint32_t gp = parent[p];
+        if (gp != p) parent[x] = gp;  // path halving (benign race: any ancestor is valid)
+        x = p;
+        p = gp;
+    }
+    return x;
+}
+
+VXD bool solvedContact(uint32_t fa, uint32_t fb) { return !isSensor(fa) && !isSensor(fb); }
+
+__global__ void unionKernel(const vx_contact* cs, uint32_t m, const BodyArrays B, uint32_t* parent) {
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < m; k += gridDim.x * blockDim.x) {
+        const uint32_t a = cs[k].a, b = cs[k].b;
+        const uint32_t fa = B.filt[a].x, fb = B.filt[b].x;
+        if (!solvedContact(fa, fb) || !isDynamic(fa) || !isDynamic(fb)) continue;
+        for (int guard = 0; guard < 1 << 20; ++guard) {
+            uint32_t ra = ufFind(parent, a), rb = ufFind(parent, b);
+            if (ra == rb) break;
+            if (ra < rb) { const uint32_t t = ra; ra = rb; rb = t; }
+            if (atomicCAS(&parent[ra], ra, rb) == ra) break;
+        }
+    }
+}
+
+__global__ void compressKernel(uint32_t* parent, uint32_t n) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        parent[i] = ufFind(parent, i);
+}
+
+// Island key of each contact: the root of its dynamic endpoint; contacts with
+// no dynamic endpoint (or a sensor) go to the "null" island keyed n.
+__global__ void islandKeyKernel(const vx_contact* cs, uint32_t m, const BodyArrays B, const uint32_t* root, uint32_t n,
+                                uint64_t* keys, uint32_t* vals) {
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < m; k += gridDim.x * blockDim.x) {
+        const uint32_t a = cs[k].a, b = cs[k].b;
+        const uint32_t fa = B.filt[a].x, fb = B.filt[b].x;
+        uint32_t key = n;
+        if (solvedContact(fa, fb)) {
+            if (isDynamic(fa)) key = root[a];
+            else if (isDynamic(fb)) key = root[b];
+        }
+        keys[k] = key;
+        vals[k] = k;
+    }
+}
+
+__global__ void runFlagKernel(const uint64_t* keys, uint32_t m, uint32_t* flags) {
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < m; k += gridDim.x * blockDim.x)
+        flags[k] = (k == 0 || keys[k] != keys[k - 1]) ? 1u : 0u;
+}
+
+// starts[index[k]] = k for run heads; also starts[runs] = m.
+__global__ void runStartKernel(const uint32_t* flags, const uint32_t* index, uint32_t m, uint32_t* starts) {
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < m; k += gridDim.x * blockDim.x) {
+        if (flags[k]) starts[index[k]] = k;
+        if (k == m - 1) starts[index[k] + flags[k]] = m;
+    }
+}
+
+// Greedy first-free-bit colouring (src/backend_cuda.cu:603-630), one thread
+// per island, contacts in their global (a, b, point) order. Static,
+// kinematic and sensor endpoints do not constrain colours; past 64 colours
+// each body continues from its own spill counter.
+__global__ void colorKernel(const vx_contact* cs, const uint32_t* order, const uint32_t* islandStart,
+                            uint32_t islands, const BodyArrays B, unsigned long long* mask, uint32_t* nextColor,
+                            uint32_t* colorOf, uint64_t* colorKeys, Counters* C) {
+    for (uint32_t isl = blockIdx.x * blockDim.x + threadIdx.x; isl < islands; isl += gridDim.x * blockDim.x) {
+        const uint32_t s0 = islandStart[isl], s1 = islandStart[isl + 1];
+        for (uint32_t k = s0; k < s1; ++k) {
+            const vx_contact& c = cs[order[k]];
+            mask[c.a] = 0ull; mask[c.b] = 0ull;
+            nextColor[c.a] = 64u; nextColor[c.b] = 64u;
+        }
+        uint32_t colors = 0;
+        for (uint32_t k = s0; k < s1; ++k) {
+            const uint32_t ci = order[k];
+            const vx_contact& c = cs[ci];
+            const uint32_t fa = B.filt[c.a].x, fb = B.filt[c.b].x;
+            const bool sensor = isSensor(fa) || isSensor(fb);
+            const bool sa = sensor || !isDynamic(fa);
+            const bool sb = sensor || !isDynamic(fb);
+            const unsigned long long used = (sa ? 0ull : mask[c.a]) | (sb ? 0ull : mask[c.b]);
+            uint32_t color;
+            if (~used) {
+                color = (uint32_t)(__ffsll((long long)~used) - 1);
+            } else {
+                const uint32_t na = sa ? 64u : nextColor[c.a];
+                const uint32_t nb = sb ? 64u : nextColor[c.b];
+                color = na > nb ? na : nb;
+                if (!sa) nextColor[c.a] = color + 1;
+                if (!sb) nextColor[c.b] = color + 1;
+            }
+            if (color < 64) {
+                if (!sa) mask[c.a] |= 1ull << color;
+                if (!sb) mask[c.b] |= 1ull << color;
+            }
+            colorOf[ci] = color;
+            colorKeys[k] = ((uint64_t)isl << 16) | (color < 65535u ? color : 65535u);
+            if (color + 1 > colors) colors = color + 1;
+        }
+        atomicMax(&C->maxColors, colors);
+        atomicMax(&C->largestIsland, s1 - s0);
+    }
+}
+
+__global__ void islandBodyKernel(const vx_contact* cs, const uint32_t* order, const uint32_t* islandStart,
+                                 uint32_t realIslands, const BodyArrays B, uint32_t* islandOfBody) {
+    for (uint32_t isl = blockIdx.x; isl < realIslands; isl += gridDim.x) {
+        const uint32_t s0 = islandStart[isl], s1 = islandStart[isl + 1];
+        for (uint32_t k = s0 + threadIdx.x; k < s1; k += blockDim.x) {
+            const vx_contact& c = cs[order[k]];
+            if (isDynamic(B.filt[c.a].x)) islandOfBody[c.a] = isl;
+            if (isDynamic(B.filt[c.b].x)) islandOfBody[c.b] = isl;
+        }
+    }
+}
+
+__global__ void bodyKeyKernel(const uint32_t* islandOfBody, uint32_t n, uint32_t freeKey, uint64_t* keys,
+                              uint32_t* vals) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t isl = islandOfBody[i];
+        keys[i] = isl == 0xffffffffu ? freeKey : isl;
+        vals[i] = i;
+    }
+}
+
+// bodyStart[key] for each run of sorted body keys; bodyStart has islands+2 entries.
+__global__ void bodyStartKernel(const uint64_t* keys, uint32_t n, uint32_t* bodyStart, uint32_t entries) {
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const uint64_t key = keys[k];
+        const uint64_t prevKey = k == 0 ? ~0ull : keys[k - 1];
+        if (key != prevKey) {
+            // every key in (prevKey, key] starts at k (empty islands get empty ranges)
+            const uint64_t from = k == 0 ? 0 : prevKey + 1;
+            for (uint64_t x = from; x <= key && x < entries; ++x) bodyStart[x] = k;
+        }
+        if (k == n - 1)
+            for (uint64_t x = key + 1; x < entries; ++x) bodyStart[x] = n;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// island solve (src/backend_cuda.cu:569-761 semantics)
+// ---------------------------------------------------------------------------
+
+struct SolveArgs {
+    BodyArrays B;
+    vx_contact* contacts;        // key-sorted storage
+    const uint32_t* order;       // solve order -> contact index
+    const uint32_t* islandStart; // islands + 1 (solve-order ranges)
+    const uint32_t* segStart;    // segments + 1
+    const uint32_t* islandSeg;   // islands + 1 (first segment)
+    const uint32_t* bodyOrder;   // bodies sorted by island
+    const uint32_t* bodyStart;   // islands + 2
+    uint32_t islands;
+    uint32_t realIslands;  // islands >= realIslands (the null island) own no bodies
+    V3 gravity;
+    float h;
+    int substeps;
+    int sweeps;
+    int warmStart;     // warm start on the first substep
+    int integrate;     // integrate velocities (s > 0) and transforms each substep
+    int coneBlock;
+    uint32_t tinyLimit;
+    int positionIterations;  // position-correction mode when > 0
+    int stackStabilization;
+    float stackStiffness, stackDamping;
+};
+
+VXD void warmRow(const SolveArgs& A, uint32_t ci) {
+    vx_contact& cc = A.contacts[ci];
+    const uint32_t fa = A.B.filt[cc.a].x, fb = A.B.filt[cc.b].x;
+    if (!solvedContact(fa, fb)) return;
+    RowContact r;
+    loadRow(cc, r);
+    SolverBody a = loadSolverBody(A.B, cc.a), b = loadSolverBody(A.B, cc.b);
+    warmStartRow(a, b, r);
+    if (isDynamic(fa)) { A.B.vel[cc.a] = pack(a.v, 0.0f); A.B.ang[cc.a] = pack(a.w, 0.0f); }
+    if (isDynamic(fb)) { A.B.vel[cc.b] = pack(b.v, 0.0f); A.B.ang[cc.b] = pack(b.w, 0.0f); }
+    storeRow(cc, r);
+}
+
+VXD void solveRowAt(const SolveArgs& A, uint32_t ci) {
+    vx_contact& cc = A.contacts[ci];
+    const uint32_t fa = A.B.filt[cc.a].x, fb = A.B.filt[cc.b].x;
+    if (!solvedContact(fa, fb)) return;
+    RowContact r;
+    loadRow(cc, r);
+    SolverBody a = loadSolverBody(A.B, cc.a), b = loadSolverBody(A.B, cc.b);
+    solveRow(a, b, r, A.h, A.coneBlock != 0);
+    if (isDynamic(fa)) { A.B.vel[cc.a] = pack(a.v, 0.0f); A.B.ang[cc.a] = pack(a.w, 0.0f); }
+    if (isDynamic(fb)) { A.B.vel[cc.b] = pack(b.v, 0.0f); A.B.ang[cc.b] = pack(b.w, 0.0f); }
+    storeRow(cc, r);
+}
+
+// Split-impulse position correction row (src/world.cpp:4370-4397).
+VXD void positionRow(const SolveArgs& A, uint32_t ci) {
+    const vx_contact& cc = A.contacts[ci];
+    const uint32_t fa = A.B.filt[cc.a].x, fb = A.B.filt[cc.b].x;
+    if (!solvedContact(fa, fb)) return;
+    const Mass ma = loadMass(A.B, cc.a), mb = loadMass(A.B, cc.b);
+    const float ima = solverInvMass(ma), imb = solverInvMass(mb);
+    const float invMassSum = ima + imb;
+    if (invMassSum <= 0.0f) return;
+    V3 pa = f3(A.B.pos[cc.a]), pb = f3(A.B.pos[cc.b]);
+    const Q4 qa = q4(A.B.rot[cc.a]), qb = q4(A.B.rot[cc.b]);
+    const V3 n{cc.normal.x, cc.normal.y, cc.normal.z};
+    const V3 wa = anchorWorld(shapeOf(fa) == kSphere, pa, qa, V3{cc.localAnchorA.x, cc.localAnchorA.y, cc.localAnchorA.z});
+    const V3 wb = anchorWorld(shapeOf(fb) == kSphere, pb, qb, V3{cc.localAnchorB.x, cc.localAnchorB.y, cc.localAnchorB.z});
+    const float g = cc.bias0 + dot(n, wa - wb);
+    const float slop = 1e-3f;
+    if (g >= -slop) return;
+    float resolve = 0.6f;
+    if (A.stackStabilization) {
+        const V3 rv = f3(A.B.vel[cc.a]) - f3(A.B.vel[cc.b]);
+        if (lengthSq(rv) < 1e-4f) {
+            const float stiffness = A.stackStiffness / 1000.0f;
+            const float damping = 1.0f + A.stackDamping * A.h;
+            resolve += 0.2f * stiffness / damping;
+        }
+    }
+    const float push = -resolve * (g + slop) / invMassSum;
+    if (isDynamic(fa) && !isAsleep(fa)) { pa += n * (push * ima); A.B.pos[cc.a] = pack(pa, 0.0f); }
+    if (isDynamic(fb) && !isAsleep(fb)) { pb -= n * (push * imb); A.B.pos[cc.b] = pack(pb, 0.0f); }
+}
+
+VXD uint32_t islandSize(const SolveArgs& A, uint32_t isl) { return A.islandStart[isl + 1] - A.islandStart[isl]; }
+
+// Sequential island processing (one thread).
+VXD void solveIslandSerial(const SolveArgs& A, uint32_t isl) {
+    const uint32_t s0 = A.islandStart[isl], s1 = A.islandStart[isl + 1];
+    if (A.positionIterations > 0) {
+        for (int it = 0; it < A.positionIterations; ++it)
+            for (uint32_t k = s0; k < s1; ++k) positionRow(A, A.order[k]);
+        return;
+    }
+    const uint32_t b0 = isl < A.realIslands ? A.bodyStart[isl] : 0u;
+    const uint32_t b1 = isl < A.realIslands ? A.bodyStart[isl + 1] : 0u;
+    for (int s = 0; s < A.substeps; ++s) {
+        if (A.integrate && s > 0)
+            for (uint32_t k = b0; k < b1; ++k) integrateVelocity(A.B, A.bodyOrder[k], A.gravity, A.h);
+        if (A.warmStart && s == 0)
+            for (uint32_t k = s0; k < s1; ++k) warmRow(A, A.order[k]);
+        for (int it = 0; it < A.sweeps; ++it)
+            for (uint32_t k = s0; k < s1; ++k) solveRowAt(A, A.order[k]);
+        if (A.integrate)
+            for (uint32_t k = b0; k < b1; ++k) integrateTransform(A.B, A.bodyOrder[k], A.h);
+    }
+}
+
+__global__ void __launch_bounds__(128) solveTinyKernel(SolveArgs A) {
+    for (uint32_t isl = blockIdx.x * blockDim.x + threadIdx.x; isl < A.islands; isl += gridDim.x * blockDim.x)
+        if (islandSize(A, isl) <= A.tinyLimit) solveIslandSerial(A, isl);
+}
+
+// Block-cooperative island processing: contacts of one colour in parallel,
+// a block barrier between colours.
+__global__ void __launch_bounds__(256) solveBlockKernel(SolveArgs A) {
+    for (uint32_t isl = blockIdx.x; isl < A.islands; isl += gridDim.x) {
+        if (islandSize(A, isl) <= A.tinyLimit) continue;
+        const uint32_t g0 = A.islandSeg[isl], g1 = A.islandSeg[isl + 1];
+        if (A.positionIterations > 0) {
+            for (int it = 0; it < A.positionIterations; ++it)
+                for (uint32_t g = g0; g < g1; ++g) {
+                    for (uint32_t k = A.segStart[g] + threadIdx.x; k < A.segStart[g + 1]; k += blockDim.x)
+                        positionRow(A, A.order[k]);
+                    __syncthreads();
+                }
+            continue;
+        }
+        const uint32_t b0 = isl < A.realIslands ? A.bodyStart[isl] : 0u;
+        const uint32_t b1 = isl < A.realIslands ? A.bodyStart[isl + 1] : 0u;
+        for (int s = 0; s < A.substeps; ++s) {
+            if (A.integrate && s > 0) {
+                for (uint32_t k = b0 + threadIdx.x; k < b1; k += blockDim.x)
+                    integrateVelocity(A.B, A.bodyOrder[k], A.gravity, A.h);
+                __syncthreads();
+            }
+            if (A.warmStart && s == 0)
+                for (uint32_t g = g0; g < g1; ++g) {
+                    for (uint32_t k = A.segStart[g] + threadIdx.x; k < A.segStart[g + 1]; k += blockDim.x)
+                        warmRow(A, A.order[k]);
+                    __syncthreads();
+                }
+            for (int it = 0; it < A.sweeps; ++it)
+                for (uint32_t g = g0; g < g1; ++g) {
+                    for (uint32_t k = A.segStart[g] + threadIdx.x; k < A.segStart[g + 1]; k += blockDim.x)
+                        solveRowAt(A, A.order[k]);
+                    __syncthreads();
+                }
+            if (A.integrate) {
+                for (uint32_t k = b0 + threadIdx.x; k < b1; k += blockDim.x)
+                    integrateTransform(A.B, A.bodyOrder[k], A.h);
+                __syncthreads();
+            }
+        }
+    }
+}
+
+// Bodies without contacts: the substep loop's integration only.
+__global__ void freeBodiesKernel(BodyArrays B, const uint32_t* bodyOrder, uint32_t from, uint32_t to, V3 g, float h,
+                                 int substeps) {
+    for (uint32_t k = from + blockIdx.x * blockDim.x + threadIdx.x; k < to; k += gridDim.x * blockDim.x) {
+        const uint32_t i = bodyOrder[k];
+        for (int s = 0; s < substeps; ++s) {
+            if (s > 0) integrateVelocity(B, i, g, h);
+            integrateTransform(B, i, h);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// conservative-advancement rewind (src/world.cpp:4233-4357, gapAt :2916-2958)
+// ---------------------------------------------------------------------------
+
+struct GapProbe { float gap; V3 normal; };
+
+VXD BodyView withPose(BodyView b, const V3& p, const Q4& q) {
+    b.p = p;
+    b.q = q;
+    return b;
+}
+
+__device__ __noinline__ GapProbe gapAt(const BodyView& a, const BodyView& b, const Soup& soup) {
+    if (shapeOf(b.flags) == kPlane) {
+        const Convex c = makeConvex(a, soup);
+        const V3 deep = support(c, -b.planeN);
+        return GapProbe{dot(b.planeN, deep) - b.planeOff - c.radius, b.planeN};
+    }
+    const GjkResult r = gjkDistance(makeConvex(a, soup), makeConvex(b, soup));
+    return GapProbe{r.distance, r.normal};
+}
+
+VXD Mass massOfView(const BodyArrays& B, uint32_t i) { return loadMass(B, i); }
+
+// Conditions of the rewind loop for an oriented pair (a dynamic).
+VXD bool caEligible(const BodyView& a, const BodyView& b, const BodyArrays& B, uint32_t ia) {
+    if (isSensor(a.flags) || isSensor(b.flags)) return false;
+    if (!isDynamic(a.flags)) return false;
+    const float minVel = B.ccd[ia].y;
+    if (!(a.flags & kContinuousBit) || qualityOf(a.flags) == kQualityLow || isLocked(a.flags) ||
+        maxPointSpeed(a) < minVel)
+        return false;
+    return true;
+}
+
+VXD void orientPair(const BodyArrays& B, uint64_t key, uint32_t& i, uint32_t& j) {
+    i = (uint32_t)(key >> 32);
+    j = (uint32_t)key;
+    if (!isDynamic(B.filt[i].x) && isDynamic(B.filt[j].x)) { const uint32_t t = i; i = j; j = t; }
+}
+
+__global__ void caProbeKernel(BodyArrays B, Soup soup, const uint64_t* pairKeys, uint32_t npairs,
+                              uint32_t* flags, uint32_t* bodyMark) {
+    for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < npairs; r += gridDim.x * blockDim.x) {
+        uint32_t i, j;
+        orientPair(B, pairKeys[r], i, j);
+        const BodyView a = loadView(B, i), b = loadView(B, j);
+        uint32_t flag = 0;
+        if (caEligible(a, b, B, i)) {
+            const GapProbe end = gapAt(a, b, soup);
+            if (end.gap < -8e-3f) {
+                flag = 1;
+                bodyMark[i] = 1;
+                bodyMark[j] = 1;
+            }
+        }
+        flags[r] = flag;
+    }
+}
+
+__global__ void caCandidateKernel(const BodyArrays B, const uint64_t* pairKeys, uint32_t npairs, uint32_t* flags,
+                                  const uint32_t* bodyMark, uint32_t* candidates, Counters* C) {
+    for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < npairs; r += gridDim.x * blockDim.x) {
+        const uint32_t i = (uint32_t)(pairKeys[r] >> 32), j = (uint32_t)pairKeys[r];
+        if (flags[r] || bodyMark[i] || bodyMark[j]) candidates[r] = 1;
+        else candidates[r] = 0;
+    }
+}
+
+VXD Q4 orientationAt(const Mass& m, const Q4& start, const V3& L, float elapsed) {
+    Q4 q = start;
+    V3 w = invInertiaMulAt(m, L, start);
+    advanceOrientation(m, q, w, elapsed);
+    return q;
+}
+
+// Full rewind logic for one oriented pair on the current state. Returns true
+// when the pair was rewound.
+__device__ __noinline__ bool caRewind(BodyArrays& B, const Soup& soup, uint32_t i, uint32_t j, float dt,
+                                      const float4* prevPos, const float4* prevRot) {
+    BodyView a = loadView(B, i), b = loadView(B, j);
+    if (!caEligible(a, b, B, i)) return false;
+    const GapProbe end = gapAt(a, b, soup);
+    if (end.gap >= -8e-3f) return false;
+    const bool bStatic = isStaticBody(b.flags), bDyn = isDynamic(b.flags);
+    const V3 pa0 = f3(prevPos[i]), da = a.p - pa0;
+    const Q4 qa0 = q4(prevRot[i]);
+    const V3 pb0 = bStatic ? b.p : f3(prevPos[j]);
+    const V3 db = b.p - pb0;
+    const Q4 qb0 = bStatic ? b.q : q4(prevRot[j]);
+    const float bound = maxPointSpeed(a) * dt + (bStatic ? 0.0f : maxPointSpeed(b) * dt);
+    if (bound < 1e-9f) return false;
+    const Mass ma = loadMass(B, i), mb = loadMass(B, j);
+    const V3 La = inertiaMulAt(ma, a.w, a.q);
+    const V3 Lb = bDyn ? inertiaMulAt(mb, b.w, b.q) : V3{0.0f, 0.0f, 0.0f};
+    float t = 0.0f;
+    V3 n = end.normal;
+    for (int iter = 0; iter < 24 && t < 1.0f; ++iter) {
+        const Q4 qa = orientationAt(ma, qa0, La, dt * t);
+        const Q4 qb = bStatic ? qb0 : orientationAt(mb, qb0, Lb, dt * t);
+        const GapProbe g = gapAt(withPose(a, pa0 + da * t, qa), withPose(b, pb0 + db * t, qb), soup);
+        n = g.normal;
+        if (g.gap < 1e-3f) break;
+        t = vmin(1.0f, t + g.gap / bound);
+    }
+    if (t >= 1.0f) return false;
+    a.p = pa0 + da * t;
+    a.q = qa0;
+    a.w = invInertiaMulAt(ma, La, qa0);
+    advanceOrientation(ma, a.q, a.w, dt * t);
+    if (bDyn) {
+        b.p = pb0 + db * t;
+        b.q = qb0;
+        b.w = invInertiaMulAt(mb, Lb, qb0);
+        advanceOrientation(mb, b.q, b.w, dt * t);
+    }
+    const float ima = solverInvMass(ma), imb = solverInvMass(mb);
+    const float vn = dot(a.v - b.v, n);
+    const float invMassSum = ima + imb;
+    if (vn < 0.0f && invMassSum > 0.0f) {
+        const float restitution = vn < -1.0f
+            ? combineMaterial(a.restitution, b.restitution, (a.flags >> kRestitutionCombineShift) & 7u,
+                              (b.flags >> kRestitutionCombineShift) & 7u)
+            : 0.0f;
+        const float impulse = -(1.0f + restitution) * vn / invMassSum;
+        a.v += n * (impulse * ima);
+        if (bDyn) b.v -= n * (impulse * imb);
+    }
+    const float remaining = dt * (1.0f - t);
+    advanceTransform(ma, a.p, a.q, a.v, a.w, remaining);
+    if (bDyn) advanceTransform(mb, b.p, b.q, b.v, b.w, remaining);
+    B.pos[i] = pack(a.p, 0.0f); B.rot[i] = pack(a.q); B.vel[i] = pack(a.v, 0.0f); B.ang[i] = pack(a.w, 0.0f);
+    if (bDyn) {
+        B.pos[j] = pack(b.p, 0.0f); B.rot[j] = pack(b.q); B.vel[j] = pack(b.v, 0.0f); B.ang[j] = pack(b.w, 0.0f);
+    }
+    return true;
+}
+
+// Serial pass in pair order over the candidates (flagged pairs and pairs
+// sharing a body with one). A pair is re-evaluated when it was flagged or
+// one of its bodies moved earlier in this pass; if a rewind moves a body
+// outside the candidate neighbourhood, every later pair is visited.
+__global__ void caSerialKernel(BodyArrays B, Soup soup, const uint64_t* pairKeys, uint32_t npairs,
+                               const uint32_t* flags, const uint32_t* candidateFlags, const uint32_t* candIndex,
+                               uint32_t ncand, const uint32_t* bodyMark, uint32_t* rewound, float dt,
+                               const float4* prevPos, const float4* prevRot, Counters* C) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    bool overflow = false;
+    uint32_t rewinds = 0;
+    uint32_t r = 0;
+    uint32_t ci = 0;
+    while (true) {
+        if (!overflow) {
+            if (ci >= ncand) break;
+            r = candIndex[ci++];
+        } else {
+            if (r >= npairs) break;
+        }
+        const uint64_t key = pairKeys[r];
+        const uint32_t ri = (uint32_t)(key >> 32), rj = (uint32_t)key;
+        const bool visit = flags[r] || rewound[ri] || rewound[rj];
+        if (visit) {
+            uint32_t i, j;
+            orientPair(B, key, i, j);
+            if (caRewind(B, soup, i, j, dt, prevPos, prevRot)) {
+                ++rewinds;
+                rewound[i] = 1;
+                if (isDynamic(B.filt[j].x)) rewound[j] = 1;
+                if (!overflow && (!bodyMark[i] || (isDynamic(B.filt[j].x) && !bodyMark[j]))) {
+                    overflow = true;
+                    C->caOverflow = 1;
+                }
+            }
+        }
+        if (overflow) ++r;
+        (void)candidateFlags;
+    }
+    C->rewinds += rewinds;
+}
+
+// prefix ranks of candidate flags -> candidate index list
+__global__ void compactKernel(const uint32_t* flags, const uint32_t* ranks, uint32_t n, uint32_t* out) {
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
+        if (flags[k]) out[ranks[k]] = k;
+}
+
+__global__ void clearForcesKernel(BodyArrays B, uint32_t n) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        B.force[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        B.torque[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    }
+}
+
+__global__ void gatherContactsKernel(const vx_contact* in, const uint32_t* order, uint32_t m, vx_contact* out) {
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < m; k += gridDim.x * blockDim.x)
+        out[k] = in[order[k]];
+}
+
+__global__ void contactKeysKernel(const vx_contact* cs, uint32_t m, uint64_t* keys) {
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < m; k += gridDim.x * blockDim.x)
+        keys[k] = ((uint64_t)cs[k].a << 32) | cs[k].b;
+}
+
+// ===========================================================================
+// host orchestration
+// ===========================================================================
+
+static int sortPairs(Context& c, uint64_t* keys, uint32_t* vals, uint32_t n, int bits) {
+    if (n <= 1 || bits <= 0) return VXB_OK;
+    const uint32_t tiles = (n + kSortTile - 1) / kSortTile;
+    VXB_TRY(ensure(c, c.sortKeysAlt, (size_t)n * 8));
+    VXB_TRY(ensure(c, c.sortValsAlt, (size_t)n * 4));
+    VXB_TRY(ensure(c, c.sortHist, (size_t)tiles * 256 * 4));
+    c.sortScratch.keysAlt = P<uint64_t>(c.sortKeysAlt);
+    c.sortScratch.valsAlt = P<uint32_t>(c.sortValsAlt);
+    c.sortScratch.hist = P<uint32_t>(c.sortHist);
+    cudaError_t e = cudaSuccess;
+    c.launches += radixSortPairs(keys, vals, n, 0, bits, c.sortScratch, c.stream, &e);
+    if (e != cudaSuccess) return cudaStatus(c, e, "radix sort");
+    return VXB_OK;
+}
+
+static int readCounters(Context& c) {
+    VXB_CUDA(c, cudaMemcpyAsync(&c.hostCounters, c.dCounters, sizeof(Counters), cudaMemcpyDeviceToHost, c.stream));
+    VXB_CUDA(c, cudaStreamSynchronize(c.stream));
+    return VXB_OK;
+}
+
+static int resetCounters(Context& c) {
+    Counters z;
+    std::memset(&z, 0, sizeof(z));
+    for (int a = 0; a < 3; ++a) { z.cellMinBits[a] = 0xffffffffu; z.cellMaxBits[a] = 0u; }
+    VXB_CUDA(c, cudaMemcpyAsync(c.dCounters, &z, sizeof(Counters), cudaMemcpyHostToDevice, c.stream));
+    return VXB_OK;
+}
+
+int loadSoup(Context& c, const vx_soup* soup) {
+    c.hullPointCount = soup ? soup->hullPointCount : 0;
+    c.faceIndexCount = soup ? soup->hullFaceIndexCount : 0;
+    VXB_TRY(ensure(c, c.hullPtsBuf, c.hullPointCount * 12 + 16));
+    VXB_TRY(ensure(c, c.facesBuf, c.faceIndexCount * 4 + 16));
+    if (c.hullPointCount)
+        VXB_CUDA(c, cudaMemcpyAsync(c.hullPtsBuf.ptr, soup->hullPoints, c.hullPointCount * 12, cudaMemcpyHostToDevice,
+                                    c.stream));
+    if (c.faceIndexCount)
+        VXB_CUDA(c, cudaMemcpyAsync(c.facesBuf.ptr, soup->hullFaceIndices, c.faceIndexCount * 4,
+                                    cudaMemcpyHostToDevice, c.stream));
+    return VXB_OK;
+}
+
+static Soup soupOf(Context& c) { return Soup{P<float>(c.hullPtsBuf), P<uint32_t>(c.facesBuf)}; }
+
+int loadBodies(Context& c, const vx_body* bodies, uint32_t n, const uint32_t* worldOf) {
+    if (n == 0) return fail(c, VXB_ERR_INVALID, "no bodies");
+    for (uint32_t i = 0; i < n; ++i) {
+        const uint8_t s = bodies[i].shape;
+        if (s == VX_SHAPE_MESH || s == VX_SHAPE_COMPOUND)
+            return fail(c, VXB_ERR_UNSUPPORTED, "mesh and compound bodies are not supported by the device pipeline");
+        if (bodies[i].motionType == VX_MOTION_KINEMATIC)
+            return fail(c, VXB_ERR_UNSUPPORTED, "kinematic bodies are not supported by the device pipeline");
+    }
+    c.n = n;
+    // SoA arrays in one allocation (16 arrays of 16-byte elements).
+    const size_t stride = ((size_t)n * 16 + 255) & ~(size_t)255;
+    VXB_TRY(ensure(c, c.bodyBuf, stride * 16));
+    char* base = P<char>(c.bodyBuf);
+    float4** f4[] = {&c.B.pos, &c.B.rot, &c.B.vel, &c.B.ang, &c.B.inertia, &c.B.iq, &c.B.dims, &c.B.extra,
+                     &c.B.mat, &c.B.fscale, &c.B.ccd, &c.B.plane, &c.B.force, &c.B.torque};
+    int slot = 0;
+    for (float4** p : f4) *p = reinterpret_cast<float4*>(base + stride * slot++);
+    c.B.hull = reinterpret_cast<uint4*>(base + stride * slot++);
+    c.B.filt = reinterpret_cast<uint4*>(base + stride * slot++);
+    VXB_TRY(ensure(c, c.aosBuf, (size_t)n * sizeof(vx_body)));
+    VXB_CUDA(c, cudaMemcpyAsync(c.aosBuf.ptr, bodies, (size_t)n * sizeof(vx_body), cudaMemcpyHostToDevice, c.stream));
+    LAUNCH(c, packBodiesKernel, blocksFor(n, 256), 256, P<vx_body>(c.aosBuf), n, c.B);
+    // worlds and per-world plane lists
+    c.hostWorldOf.assign(n, 0u);
+    uint32_t worlds = 1;
+    if (worldOf) {
+        for (uint32_t i = 0; i < n; ++i) {
+            c.hostWorldOf[i] = worldOf[i];
+            if (i > 0 && worldOf[i] < worldOf[i - 1])
+                return fail(c, VXB_ERR_INVALID, "bodies of one world must be contiguous and worlds ascending");
+            worlds = std::max(worlds, worldOf[i] + 1);
+        }
+    }
+    c.worlds = worlds;
+    std::vector<uint32_t> planeStart(worlds + 1, 0), planeList;
+    for (uint32_t i = 0; i < n; ++i)
+        if (bodies[i].shape == VX_SHAPE_PLANE) ++planeStart[c.hostWorldOf[i] + 1];
+    for (uint32_t w = 0; w < worlds; ++w) planeStart[w + 1] += planeStart[w];
+    planeList.resize(planeStart[worlds]);
+    {
+        std::vector<uint32_t> fill(planeStart.begin(), planeStart.end() - 1);
+        for (uint32_t i = 0; i < n; ++i)
+            if (bodies[i].shape == VX_SHAPE_PLANE) planeList[fill[c.hostWorldOf[i]]++] = i;
+    }
+    VXB_TRY(ensure(c, c.worldOfBuf, (size_t)n * 4));
+    VXB_TRY(ensure(c, c.planeStartBuf, planeStart.size() * 4));
+    VXB_TRY(ensure(c, c.planeListBuf, planeList.size() * 4 + 4));
+    VXB_CUDA(c, cudaMemcpyAsync(c.worldOfBuf.ptr, c.hostWorldOf.data(), (size_t)n * 4, cudaMemcpyHostToDevice, c.stream));
+    VXB_CUDA(c, cudaMemcpyAsync(c.planeStartBuf.ptr, planeStart.data(), planeStart.size() * 4, cudaMemcpyHostToDevice,
+                                c.stream));
+    if (!planeList.empty())
+        VXB_CUDA(c, cudaMemcpyAsync(c.planeListBuf.ptr, planeList.data(), planeList.size() * 4, cudaMemcpyHostToDevice,
+                                    c.stream));
+    VXB_CUDA(c, cudaStreamSynchronize(c.stream));  // host vectors above are freed on return
+    c.prevCount = 0;
+    c.backendContacts = 0;
+    return VXB_OK;
+}
+
+int readBodies(Context& c, vx_body* out, uint32_t n) {
+    if (n != c.n) return fail(c, VXB_ERR_INVALID, "body count mismatch");
+    LAUNCH(c, unpackBodiesKernel, blocksFor(n, 256), 256, P<vx_body>(c.aosBuf), n, c.B);
+    VXB_CUDA(c, cudaMemcpyAsync(out, c.aosBuf.ptr, (size_t)n * sizeof(vx_body), cudaMemcpyDeviceToHost, c.stream));
+    VXB_CUDA(c, cudaStreamSynchronize(c.stream));
+    return VXB_OK;
+}
+
+int readPoses(Context& c, float* out, uint32_t n) {
+    if (n != c.n) return fail(c, VXB_ERR_INVALID, "body count mismatch");
+    VXB_TRY(ensure(c, c.scanBuf, (size_t)n * 28 + 16));
+    LAUNCH(c, posesKernel, blocksFor(n, 256), 256, P<float>(c.scanBuf), n, c.B);
+    VXB_CUDA(c, cudaMemcpyAsync(out, c.scanBuf.ptr, (size_t)n * 28, cudaMemcpyDeviceToHost, c.stream));
+    VXB_CUDA(c, cudaStreamSynchronize(c.stream));
+    return VXB_OK;
+}
+
+int writeForces(Context& c, const float* in, uint32_t n) {
+    if (n != c.n) return fail(c, VXB_ERR_INVALID, "body count mismatch");
+    VXB_TRY(ensure(c, c.scanBuf, (size_t)n * 28 + 16));
+    VXB_CUDA(c, cudaMemcpyAsync(c.scanBuf.ptr, in, (size_t)n * 24, cudaMemcpyHostToDevice, c.stream));
+    LAUNCH(c, forcesKernel, blocksFor(n, 256), 256, P<float>(c.scanBuf), n, c.B);
+    return VXB_OK;
+}
+
+// ---- broad phase ----------------------------------------------------------
+
+static int broadPhase(Context& c, float dt, uint32_t* pairCount) {
+    const uint32_t n = c.n;
+    VXB_TRY(ensure(c, c.aabbBuf, (size_t)n * 32));
+    float4* lo = P<float4>(c.aabbBuf);
+    float4* hi = lo + n;
+    LAUNCH(c, aabbKernel, std::min<uint32_t>(blocksFor(n, 256), (uint32_t)c.smCount * 8), 256, c.B, n, dt, lo, hi,
+           c.dCounters);
+    const int worldBits = bitsFor(c.worlds > 1 ? c.worlds - 1 : 0);
+    const int keyBitsTotal = 3 * kCellBits + worldBits + 1;
+    const uint64_t planeKey = 1ull << (3 * kCellBits + worldBits);
+    VXB_TRY(ensure(c, c.cellKeyBuf, (size_t)n * 8));
+    VXB_TRY(ensure(c, c.cellValBuf, (size_t)n * 4));
+    uint64_t* keys = P<uint64_t>(c.cellKeyBuf);
+    uint32_t* vals = P<uint32_t>(c.cellValBuf);
+    LAUNCH(c, keyKernel, blocksFor(n, 256), 256, c.B, n, c.worlds > 1 ? P<uint32_t>(c.worldOfBuf) : nullptr, lo, hi,
+           c.dCounters, keys, vals, planeKey);
+    VXB_TRY(sortPairs(c, keys, vals, n, keyBitsTotal));
+    uint32_t hashCap = 1024;
+    while (hashCap < 2 * n) hashCap <<= 1;
+    c.hashCap = hashCap;
+    VXB_TRY(ensure(c, c.hashKeyBuf, (size_t)hashCap * 8));
+    VXB_TRY(ensure(c, c.hashValBuf, (size_t)hashCap * 4));
+    VXB_CUDA(c, cudaMemsetAsync(c.hashKeyBuf.ptr, 0xff, (size_t)hashCap * 8, c.stream));
+    LAUNCH(c, cellTableKernel, blocksFor(n, 256), 256, keys, n, planeKey, P<uint64_t>(c.hashKeyBuf),
+           P<uint32_t>(c.hashValBuf), hashCap - 1);
+    if (c.pairCap == 0) c.pairCap = std::max<uint32_t>(n * 8u, 4096u);
+    for (int attempt = 0; attempt < 3; ++attempt) {
+        VXB_TRY(ensure(c, c.pairBuf, (size_t)c.pairCap * 8));
+        VXB_CUDA(c, cudaMemsetAsync(&c.dCounters->pairs, 0, 4, c.stream));
+        VXB_CUDA(c, cudaMemsetAsync(&c.dCounters->overflow, 0, 4, c.stream));
+        LAUNCH(c, pairKernel, blocksFor(n, 128), 128, c.B, n, keys, vals, lo, hi, P<uint64_t>(c.hashKeyBuf),
+               P<uint32_t>(c.hashValBuf), hashCap - 1, planeKey,
+               c.worlds > 1 ? P<uint32_t>(c.worldOfBuf) : nullptr, P<uint32_t>(c.planeStartBuf),
+               P<uint32_t>(c.planeListBuf), P<uint64_t>(c.pairBuf), c.pairCap, c.dCounters);
+        VXB_TRY(readCounters(c));
+        if (c.hostCounters.pairs <= c.pairCap) break;
+        c.pairCap = c.hostCounters.pairs + c.hostCounters.pairs / 4 + 1024;
+    }
+    *pairCount = c.hostCounters.pairs;
+    return VXB_OK;
+}
+
+// ---- narrow phase ---------------------------------------------------------
+
+// Runs the narrow phase on `npairs` device pairs and leaves the contacts
+// sorted in contactBuf[c.cur] (mode 0) or grouped in pair order (mode 1).
+static int narrowPhase(Context& c, const uint64_t* pairs, uint32_t npairs, float dt, int mode, uint32_t* contactCount,
+                       uint32_t* recordCount) {
+    const int bodyBits = std::max(1, bitsFor(c.n - 1));
+    if (c.contactCap == 0) c.contactCap = std::max<uint32_t>(npairs * 2u, 4096u);
+    if (c.recCap < npairs) c.recCap = npairs + 1024;
+    for (int attempt = 0; attempt < 3; ++attempt) {
+        VXB_TRY(ensure(c, c.contactTmpBuf, (size_t)c.contactCap * sizeof(vx_contact)));
+        VXB_TRY(ensure(c, c.recKeyBuf, (size_t)c.recCap * 8));
+        VXB_TRY(ensure(c, c.recValBuf, (size_t)c.recCap * 4));
+        VXB_TRY(ensure(c, c.recInfoBuf, (size_t)c.recCap * 8));
+        VXB_CUDA(c, cudaMemsetAsync(&c.dCounters->contactsTmp, 0, 8, c.stream));  // contactsTmp + records
+        VXB_CUDA(c, cudaMemsetAsync(&c.dCounters->overflow, 0, 4, c.stream));
+        if (npairs)
+            LAUNCH(c, collideKernel, std::min<uint32_t>(blocksFor(npairs, 128), (uint32_t)c.smCount * 16), 128, c.B,
+                   soupOf(c), pairs, npairs, dt, mode, bodyBits, P<vx_contact>(c.contactTmpBuf), c.contactCap,
+                   P<uint64_t>(c.recKeyBuf), P<uint32_t>(c.recValBuf), P<uint2>(c.recInfoBuf), c.recCap, c.dCounters);
+        VXB_TRY(readCounters(c));
+        if (!(c.hostCounters.overflow & 2u)) break;
+        c.contactCap = c.hostCounters.contactsTmp + c.hostCounters.contactsTmp / 4 + 1024;
+        c.recCap = std::max(c.recCap, c.hostCounters.records + 1024);
+    }
+    const uint32_t m = c.hostCounters.contactsTmp, nrec = c.hostCounters.records;
+    *contactCount = m;
+    *recordCount = nrec;
+    const int recBits = mode == 0 ? 2 * bodyBits : bitsFor(npairs);
+    VXB_TRY(sortPairs(c, P<uint64_t>(c.recKeyBuf), P<uint32_t>(c.recValBuf), nrec, recBits));
+    VXB_TRY(ensure(c, c.recCountBuf, (size_t)nrec * 4 + 16));
+    VXB_TRY(ensure(c, c.recOffsetBuf, (size_t)nrec * 4 + 16));
+    VXB_TRY(ensure(c, c.pairKeyBuf, (size_t)nrec * 8 + 16));
+    VXB_TRY(ensure(c, c.contactBuf[c.cur], (size_t)m * sizeof(vx_contact) + 128));
+    VXB_TRY(ensure(c, c.scanBuf, (size_t)nrec * 4 + 16));
+    if (nrec) {
+        LAUNCH(c, gatherCountsKernel, blocksFor(nrec, 256), 256, P<uint32_t>(c.recValBuf), P<uint2>(c.recInfoBuf), nrec,
+               P<uint32_t>(c.recCountBuf));
+        VXB_TRY(exclusiveScan(c, P<uint32_t>(c.recCountBuf), P<uint32_t>(c.scanBuf), nrec, nullptr));
+        LAUNCH(c, placeKernel, blocksFor(nrec, 128), 128, P<uint32_t>(c.recValBuf), P<uint2>(c.recInfoBuf),
+               P<uint32_t>(c.scanBuf), nrec, P<vx_contact>(c.contactTmpBuf), P<vx_contact>(c.contactBuf[c.cur]),
+               (uint64_t*)nullptr, P<uint64_t>(c.pairKeyBuf), P<uint32_t>(c.recOffsetBuf));
+    }
+    return VXB_OK;
+}
+
+// ---- islands + colouring --------------------------------------------------
+
+// Groups the m contacts of `cs` into islands, colours them and builds the
+// solve order (island, colour, contact order) plus per-island body lists.
+static int buildIslands(Context& c, const vx_contact* cs, uint32_t m, IslandPlan& plan, uint32_t* colorOut) {
+    const uint32_t n = c.n;
+    VXB_TRY(ensure(c, c.parentBuf, (size_t)n * 4));
+    VXB_TRY(ensure(c, c.islandOfBodyBuf, (size_t)n * 4));
+    VXB_TRY(ensure(c, c.maskBuf, (size_t)n * 8));
+    VXB_TRY(ensure(c, c.nextColorBuf, (size_t)n * 4));
+    VXB_TRY(ensure(c, c.bodyKeyBuf, (size_t)n * 8));
+    VXB_TRY(ensure(c, c.bodyValBuf, (size_t)n * 4));
+    VXB_TRY(ensure(c, c.islandKeyBuf, (size_t)m * 8 + 16));
+    VXB_TRY(ensure(c, c.islandValBuf, (size_t)m * 4 + 16));
+    VXB_TRY(ensure(c, c.colorBuf, (size_t)m * 4 + 16));
+    VXB_TRY(ensure(c, c.flagBuf, (size_t)m * 4 + 16));
+    VXB_TRY(ensure(c, c.scanBuf, (size_t)m * 4 + 16));
+    VXB_TRY(ensure(c, c.islandStartBuf, (size_t)m * 4 + 16));
+    VXB_TRY(ensure(c, c.segStartBuf, (size_t)m * 4 + 16));
+    VXB_TRY(ensure(c, c.islandSegBuf, (size_t)m * 4 + 16));
+    uint32_t* parent = P<uint32_t>(c.parentBuf);
+    LAUNCH(c, iotaKernel, blocksFor(n, 256), 256, parent, n);
+    if (m == 0) {
+        plan = IslandPlan{};
+        VXB_CUDA(c, cudaMemsetAsync(c.islandOfBodyBuf.ptr, 0xff, (size_t)n * 4, c.stream));
+    } else {
+        LAUNCH(c, unionKernel, blocksFor(m, 256), 256, cs, m, c.B, parent);
+        LAUNCH(c, compressKernel, blocksFor(n, 256), 256, parent, n);
+        uint64_t* ikeys = P<uint64_t>(c.islandKeyBuf);
+        uint32_t* ivals = P<uint32_t>(c.islandValBuf);
+        LAUNCH(c, islandKeyKernel, blocksFor(m, 256), 256, cs, m, c.B, parent, n, ikeys, ivals);
+        VXB_TRY(sortPairs(c, ikeys, ivals, m, bitsFor(n)));
+        uint32_t* flags = P<uint32_t>(c.flagBuf);
+        uint32_t* index = P<uint32_t>(c.scanBuf);
+        uint32_t* islandStart = P<uint32_t>(c.islandStartBuf);
+        LAUNCH(c, runFlagKernel, blocksFor(m, 256), 256, ikeys, m, flags);
+        VXB_TRY(exclusiveScan(c, flags, index, m, &c.dCounters->islands));
+        LAUNCH(c, runStartKernel, blocksFor(m, 256), 256, flags, index, m, islandStart);
+        VXB_TRY(readCounters(c));
+        plan.islands = c.hostCounters.islands;
+        // is the last island the null island (key n)?
+        uint64_t lastKey = 0;
+        VXB_CUDA(c, cudaMemcpyAsync(&lastKey, ikeys + (m - 1), 8, cudaMemcpyDeviceToHost, c.stream));
+        VXB_CUDA(c, cudaStreamSynchronize(c.stream));
+        plan.realIslands = lastKey == n ? plan.islands - 1 : plan.islands;
+        // colour each island; colour keys (island << 16 | colour) in island order
+        VXB_TRY(ensure(c, c.colorKeyBuf, (size_t)m * 8 + 16));
+        uint64_t* ckeys = P<uint64_t>(c.colorKeyBuf);
+        LAUNCH(c, colorKernel, blocksFor(plan.islands, 64), 64, cs, ivals, islandStart, plan.islands, c.B,
+               P<unsigned long long>(c.maskBuf), P<uint32_t>(c.nextColorBuf), P<uint32_t>(c.colorBuf), ckeys,
+               c.dCounters);
+        if (colorOut)
+            VXB_CUDA(c, cudaMemcpyAsync(colorOut, c.colorBuf.ptr, (size_t)m * 4, cudaMemcpyDeviceToHost, c.stream));
+        // solve order: stable sort by (island, colour)
+        VXB_TRY(sortPairs(c, ckeys, ivals, m, 16 + bitsFor(plan.islands)));
+        LAUNCH(c, runFlagKernel, blocksFor(m, 256), 256, ckeys, m, flags);
+        VXB_TRY(exclusiveScan(c, flags, index, m, &c.dCounters->segments));
+        LAUNCH(c, runStartKernel, blocksFor(m, 256), 256, flags, index, m, P<uint32_t>(c.segStartBuf));
+        // first segment of each island: index[islandStart[isl]]
+        VXB_TRY(readCounters(c));
+        plan.segments = c.hostCounters.segments;
+        // island bodies
+        VXB_CUDA(c, cudaMemsetAsync(c.islandOfBodyBuf.ptr, 0xff, (size_t)n * 4, c.stream));
+        LAUNCH(c, islandBodyKernel, std::min<uint32_t>(std::max<uint32_t>(plan.realIslands, 1), 65535u), 64, cs, ivals,
+               islandStart, plan.realIslands, c.B, P<uint32_t>(c.islandOfBodyBuf));
+    }
+    const uint32_t freeKey = plan.realIslands;
+    LAUNCH(c, bodyKeyKernel, blocksFor(n, 256), 256, P<uint32_t>(c.islandOfBodyBuf), n, freeKey,
+           P<uint64_t>(c.bodyKeyBuf), P<uint32_t>(c.bodyValBuf));
+    VXB_TRY(sortPairs(c, P<uint64_t>(c.bodyKeyBuf), P<uint32_t>(c.bodyValBuf), n, bitsFor(freeKey)));
+    VXB_TRY(ensure(c, c.islandBodyStartBuf, ((size_t)plan.realIslands + 2) * 4 + 16));
+    LAUNCH(c, bodyStartKernel, blocksFor(n, 256), 256, P<uint64_t>(c.bodyKeyBuf), n, P<uint32_t>(c.islandBodyStartBuf),
+           plan.realIslands + 2);
+    std::vector<uint32_t> bs(plan.realIslands + 2);
+    VXB_CUDA(c, cudaMemcpyAsync(bs.data(), c.islandBodyStartBuf.ptr, bs.size() * 4, cudaMemcpyDeviceToHost, c.stream));
+    VXB_CUDA(c, cudaStreamSynchronize(c.stream));
+    plan.freeFrom = bs[plan.realIslands];
+    plan.freeTo = bs[plan.realIslands + 1];
+    return VXB_OK;
+}
+
+__global__ void islandSegKernel(const uint32_t* islandStart, const uint32_t* segIndex, uint32_t islands,
+                                uint32_t segments, uint32_t* islandSeg) {
+    for (uint32_t isl = blockIdx.x * blockDim.x + threadIdx.x; isl <= islands; isl += gridDim.x * blockDim.x)
+        islandSeg[isl] = isl == islands ? segments : segIndex[islandStart[isl]];
+}
+
+static SolveArgs solveArgs(Context& c, vx_contact* cs, const IslandPlan& plan) {
+    SolveArgs A;
+    std::memset(&A, 0, sizeof(A));
+    A.B = c.B;
+    A.contacts = cs;
+    A.order = P<uint32_t>(c.islandValBuf);
+    A.islandStart = P<uint32_t>(c.islandStartBuf);
+    A.segStart = P<uint32_t>(c.segStartBuf);
+    A.islandSeg = P<uint32_t>(c.islandSegBuf);
+    A.bodyOrder = P<uint32_t>(c.bodyValBuf);
+    A.bodyStart = P<uint32_t>(c.islandBodyStartBuf);
+    A.islands = plan.islands;
+    A.realIslands = plan.realIslands;
+    A.tinyLimit = 16;
+    return A;
+}
+
+static int prepareSegments(Context& c, const IslandPlan& plan) {
+    if (plan.islands == 0) return VXB_OK;
+    LAUNCH(c, islandSegKernel, blocksFor(plan.islands + 1, 256), 256, P<uint32_t>(c.islandStartBuf),
+           P<uint32_t>(c.scanBuf), plan.islands, plan.segments, P<uint32_t>(c.islandSegBuf));
+    return VXB_OK;
+}
+
+static void launchSolve(Context& c, const SolveArgs& A) {
+    if (A.islands == 0) return;
+    LAUNCH(c, solveTinyKernel, blocksFor(A.islands, 128), 128, A);
+    LAUNCH(c, solveBlockKernel, std::min<uint32_t>(A.islands, (uint32_t)c.smCount * 8), 256, A);
+}
+
+// Substep loop over islands + contact-free bodies (advanceSubsteps).
+static int runSubsteps(Context& c, vx_contact* cs, const IslandPlan& plan, const V3& g, float h, int substeps,
+                       const vx_solver_options& o, bool warmStart, bool integrate) {
+    SolveArgs A = solveArgs(c, cs, plan);
+    A.gravity = g;
+    A.h = h;
+    A.substeps = substeps;
+    A.sweeps = 2 * o.velocityIterations;
+    A.warmStart = warmStart ? 1 : 0;
+    A.integrate = integrate ? 1 : 0;
+    A.coneBlock = o.frictionModel == VX_FRICTION_CONE_BLOCK;
+    launchSolve(c, A);
+    if (integrate && plan.freeTo > plan.freeFrom)
+        LAUNCH(c, freeBodiesKernel, blocksFor(plan.freeTo - plan.freeFrom, 128), 128, c.B, P<uint32_t>(c.bodyValBuf),
+               plan.freeFrom, plan.freeTo, g, h, substeps);
+    return VXB_OK;
+}
+
+static int positionCorrection(Context& c, vx_contact* cs, const IslandPlan& plan, const vx_solver_options& o, float h) {
+    if (o.positionIterations <= 0 || plan.islands == 0) return VXB_OK;
+    SolveArgs A = solveArgs(c, cs, plan);
+    A.positionIterations = o.positionIterations;
+    A.stackStabilization = o.enableStackStabilization;
+    A.stackStiffness = o.stackStiffness;
+    A.stackDamping = o.stackDamping;
+    A.h = h;
+    launchSolve(c, A);
+    return VXB_OK;
+}
+
+static int conservativeAdvancement(Context& c, uint32_t npairs, float dt) {
+    if (npairs == 0) return VXB_OK;
+    const uint32_t n = c.n;
+    VXB_TRY(ensure(c, c.caFlagBuf, (size_t)npairs * 8 + 16));
+    VXB_TRY(ensure(c, c.caBodyMarkBuf, (size_t)n * 8 + 16));
+    VXB_TRY(ensure(c, c.caCandBuf, (size_t)npairs * 8 + 16));
+    uint32_t* flags = P<uint32_t>(c.caFlagBuf);
+    uint32_t* candFlags = flags + npairs;
+    uint32_t* bodyMark = P<uint32_t>(c.caBodyMarkBuf);
+    uint32_t* rewound = bodyMark + n;
+    uint32_t* ranks = P<uint32_t>(c.caCandBuf);
+    uint32_t* candIndex = ranks + npairs;
+    VXB_CUDA(c, cudaMemsetAsync(bodyMark, 0, (size_t)n * 8, c.stream));
+    const uint64_t* pk = P<uint64_t>(c.pairKeyBuf);
+    const float4* prevPos = P<float4>(c.prevPoseBuf);
+    const float4* prevRot = prevPos + n;
+    LAUNCH(c, caProbeKernel, std::min<uint32_t>(blocksFor(npairs, 128), (uint32_t)c.smCount * 16), 128, c.B, soupOf(c),
+           pk, npairs, flags, bodyMark);
+    LAUNCH(c, caCandidateKernel, blocksFor(npairs, 256), 256, c.B, pk, npairs, flags, bodyMark, candFlags, c.dCounters);
+    VXB_TRY(exclusiveScan(c, candFlags, ranks, npairs, &c.dCounters->caCandidates));
+    VXB_TRY(readCounters(c));
+    const uint32_t ncand = c.hostCounters.caCandidates;
+    if (ncand == 0) return VXB_OK;
+    LAUNCH(c, compactKernel, blocksFor(npairs, 256), 256, candFlags, ranks, npairs, candIndex);
+    LAUNCH(c, caSerialKernel, 1, 32, c.B, soupOf(c), pk, npairs, flags, candFlags, candIndex, ncand, bodyMark, rewound,
+           dt, prevPos, prevRot, c.dCounters);
+    return VXB_OK;
+}
+
+// One World::step on the device world.
+static int stepOnce(Context& c) {
+    const vxb_step_config& cfg = c.config;
+    const uint32_t n = c.n;
+    const int substeps = cfg.substeps > 0 ? cfg.substeps : 1;
+    const float dt = cfg.dt;
+    const float h = dt / substeps;
+    const V3 g{cfg.gravity.x, cfg.gravity.y, cfg.gravity.z};
+    VXB_TRY(resetCounters(c));
+    VXB_TRY(ensure(c, c.prevPoseBuf, (size_t)n * 32));
+    float4* prevPos = P<float4>(c.prevPoseBuf);
+    LAUNCH(c, prepareKernel, blocksFor(n, 256), 256, c.B, n, g, h, prevPos, prevPos + n, 1);
+    uint32_t npairs = 0, m = 0, nrec = 0;
+    VXB_TRY(broadPhase(c, dt, &npairs));
+    c.stats.candidatePairs = npairs;
+    VXB_TRY(narrowPhase(c, P<uint64_t>(c.pairBuf), npairs, dt, 0, &m, &nrec));
+    vx_contact* cs = P<vx_contact>(c.contactBuf[c.cur]);
+    if (c.prevCount && m)
+        LAUNCH(c, matchKernel, blocksFor(m, 128), 128, cs, m, P<vx_contact>(c.contactBuf[c.cur ^ 1]),
+               P<uint64_t>(c.prevKeyBuf), c.prevCount, c.dCounters);
+    IslandPlan plan;
+    VXB_TRY(buildIslands(c, cs, m, plan, nullptr));
+    VXB_TRY(prepareSegments(c, plan));
+    VXB_TRY(runSubsteps(c, cs, plan, g, h, substeps, cfg.solver, true, true));
+    if (m) VXB_TRY(conservativeAdvancement(c, nrec, dt));
+    VXB_TRY(positionCorrection(c, cs, plan, cfg.solver, h));
+    LAUNCH(c, clearForcesKernel, blocksFor(n, 256), 256, c.B, n);
+    // previous-contact cache: this step's contacts in (a, b, point) order
+    VXB_TRY(ensure(c, c.prevKeyBuf, (size_t)m * 8 + 16));
+    if (m) LAUNCH(c, contactKeysKernel, blocksFor(m, 256), 256, cs, m, P<uint64_t>(c.prevKeyBuf));
+    c.prevCount = m;
+    c.cur ^= 1;
+    VXB_TRY(readCounters(c));
+    c.stats.contacts = m;
+    c.stats.islands = plan.realIslands;
+    c.stats.colors = c.hostCounters.maxColors;
+    c.stats.largestIsland = c.hostCounters.largestIsland;
+    c.stats.rewinds = c.hostCounters.rewinds;
+    c.stats.warmStarted = c.hostCounters.warmStarted;
+    c.stats.velocityIterations = (uint32_t)(2 * cfg.solver.velocityIterations * substeps);
+    if (c.hostCounters.timeout) return fail(c, VXB_ERR_TIMEOUT, "a bounded device wait gave up");
+    return VXB_OK;
+}
+
+int worldStep(Context& c, int steps) {
+    if (!c.configured) return fail(c, VXB_ERR_INVALID, "vxb_world_configure was not called");
+    if (c.n == 0) return fail(c, VXB_ERR_INVALID, "no bodies loaded");
+    VXB_TRY(ensure(c, c.countersBuf, sizeof(Counters)));
+    c.dCounters = P<Counters>(c.countersBuf);
+    for (int s = 0; s < steps; ++s) VXB_TRY(stepOnce(c));
+    VXB_CUDA(c, cudaStreamSynchronize(c.stream));
+    VXB_CUDA(c, cudaGetLastError());
+    return VXB_OK;
+}
+
+int readContacts(Context& c, vx_contact* out, uint32_t cap, uint32_t* count) {
+    const uint32_t m = c.prevCount;
+    if (count) *count = m;
+    if (out && m) {
+        VXB_CUDA(c, cudaMemcpyAsync(out, c.contactBuf[c.cur ^ 1].ptr, (size_t)std::min(m, cap) * sizeof(vx_contact),
+                                    cudaMemcpyDeviceToHost, c.stream));
+        VXB_CUDA(c, cudaStreamSynchronize(c.stream));
+    }
+    return VXB_OK;
+}
+
+// ---- stage entry points -----------------------------------------------------
+
+int stagePairs(Context& c, float dt, uint64_t* out, uint32_t cap, uint32_t* count) {
+    VXB_TRY(ensure(c, c.countersBuf, sizeof(Counters)));
+    c.dCounters = P<Counters>(c.countersBuf);
+    VXB_TRY(resetCounters(c));
+    uint32_t npairs = 0;
+    VXB_TRY(broadPhase(c, dt, &npairs));
+    *count = npairs;
+    if (out) {
+        std::vector<uint64_t> host(npairs);
+        if (npairs)
+            VXB_CUDA(c, cudaMemcpyAsync(host.data(), c.pairBuf.ptr, (size_t)npairs * 8, cudaMemcpyDeviceToHost, c.stream));
+        VXB_CUDA(c, cudaStreamSynchronize(c.stream));
+        std::sort(host.begin(), host.end());
+        std::memcpy(out, host.data(), (size_t)std::min(npairs, cap) * 8);
+    }
+    return npairs > cap && out ? fail(c, VXB_ERR_CAPACITY, "pair buffer too small") : VXB_OK;
+}
+
+int stageCollide(Context& c, const uint64_t* pairs, uint32_t npairs, float dt, vx_contact* out, uint32_t cap,
+                 uint32_t* counts, uint32_t* total) {
+    VXB_TRY(ensure(c, c.countersBuf, sizeof(Counters)));
+    c.dCounters = P<Counters>(c.countersBuf);
+    VXB_TRY(resetCounters(c));
+    VXB_TRY(ensure(c, c.pairBuf, (size_t)npairs * 8 + 16));
+    if (npairs)
+        VXB_CUDA(c, cudaMemcpyAsync(c.pairBuf.ptr, pairs, (size_t)npairs * 8, cudaMemcpyHostToDevice, c.stream));
+    uint32_t m = 0, nrec = 0;
+    VXB_TRY(narrowPhase(c, P<uint64_t>(c.pairBuf), npairs, dt, 1, &m, &nrec));
+    *total = m;
+    if (m > cap) return fail(c, VXB_ERR_CAPACITY, "contact buffer too small");
+    if (m) VXB_CUDA(c, cudaMemcpyAsync(out, c.contactBuf[c.cur].ptr, (size_t)m * sizeof(vx_contact),
+                                       cudaMemcpyDeviceToHost, c.stream));
+    if (counts) {
+        std::vector<uint64_t> keys(nrec);
+        std::vector<uint32_t> cnt(nrec);
+        if (nrec) {
+            VXB_CUDA(c, cudaMemcpyAsync(keys.data(), c.recKeyBuf.ptr, (size_t)nrec * 8, cudaMemcpyDeviceToHost, c.stream));
+            VXB_CUDA(c, cudaMemcpyAsync(cnt.data(), c.recCountBuf.ptr, (size_t)nrec * 4, cudaMemcpyDeviceToHost, c.stream));
+        }
+        VXB_CUDA(c, cudaStreamSynchronize(c.stream));
+        std::fill(counts, counts + npairs, 0u);
+        for (uint32_t r = 0; r < nrec; ++r) counts[keys[r]] = cnt[r];
+    }
+    VXB_CUDA(c, cudaStreamSynchronize(c.stream));
+    return VXB_OK;
+}
+
+int stageColor(Context& c, const vx_contact* contacts, uint32_t m, int32_t* colorOf, uint32_t* numColors) {
+    VXB_TRY(ensure(c, c.countersBuf, sizeof(Counters)));
+    c.dCounters = P<Counters>(c.countersBuf);
+    VXB_TRY(resetCounters(c));
+    VXB_TRY(ensure(c, c.contactBuf[c.cur], (size_t)m * sizeof(vx_contact) + 128));
+    if (m) VXB_CUDA(c, cudaMemcpyAsync(c.contactBuf[c.cur].ptr, contacts, (size_t)m * sizeof(vx_contact),
+                                       cudaMemcpyHostToDevice, c.stream));
+    IslandPlan plan;
+    VXB_TRY(buildIslands(c, P<vx_contact>(c.contactBuf[c.cur]), m, plan, reinterpret_cast<uint32_t*>(colorOf)));
+    VXB_TRY(readCounters(c));
+    *numColors = c.hostCounters.maxColors;
+    return VXB_OK;
+}
+
+// ---- Backend-interface mode ---------------------------------------------------
+
+int backendIntegrate(Context& c, vx_vec3 gravity, float dt) {
+    LAUNCH(c, integrateKernel, blocksFor(c.n, 256), 256, c.B, c.n, V3{gravity.x, gravity.y, gravity.z}, dt);
+    return VXB_OK;
+}
+
+int backendFindContacts(Context& c, float dt, uint32_t* count) {
+    VXB_TRY(ensure(c, c.countersBuf, sizeof(Counters)));
+    c.dCounters = P<Counters>(c.countersBuf);
+    VXB_TRY(resetCounters(c));
+    uint32_t npairs = 0, m = 0, nrec = 0;
+    VXB_TRY(broadPhase(c, dt, &npairs));
+    VXB_TRY(narrowPhase(c, P<uint64_t>(c.pairBuf), npairs, dt, 0, &m, &nrec));
+    c.backendContacts = m;
+    c.backendColored = false;
+    *count = m;
+    return VXB_OK;
+}
+
+int backendCopyContacts(Context& c, vx_contact* out, uint32_t cap) {
+    const uint32_t m = c.backendContacts;
+    if (m > cap) return fail(c, VXB_ERR_CAPACITY, "contact buffer too small");
+    if (m) VXB_CUDA(c, cudaMemcpyAsync(out, c.contactBuf[c.cur].ptr, (size_t)m * sizeof(vx_contact),
+                                       cudaMemcpyDeviceToHost, c.stream));
+    VXB_CUDA(c, cudaStreamSynchronize(c.stream));
+    return VXB_OK;
+}
+
+static bool hostContactLess(const vx_contact& x, const vx_contact& y) {
+    const uint64_t kx = ((uint64_t)x.a << 32) | x.b, ky = ((uint64_t)y.a << 32) | y.b;
+    if (kx != ky) return kx < ky;
+    if (x.point.x != y.point.x) return x.point.x < y.point.x;
+    if (x.point.y != y.point.y) return x.point.y < y.point.y;
+    return x.point.z < y.point.z;
+}
+
+// solveVelocities / advanceSubsteps. On warm start the contacts are sorted,
+// coloured, written back in colour order and kept resident; the solve then
+// runs `substeps` substeps (fullSubsteps) or one velocity solve.
+int backendSolve(Context& c, vx_contact* contacts, uint32_t m, float h, bool warmStart, const vx_solver_options& o,
+                 vx_vec3 gravity, int substeps, bool fullSubsteps) {
+    VXB_TRY(ensure(c, c.countersBuf, sizeof(Counters)));
+    c.dCounters = P<Counters>(c.countersBuf);
+    IslandPlan& plan = c.backendPlan;  // retained between the warm-start call and later calls
+    if (warmStart) {
+        VXB_TRY(resetCounters(c));
+        c.hostSorted.assign(contacts, contacts + m);
+        std::stable_sort(c.hostSorted.begin(), c.hostSorted.end(), hostContactLess);
+        VXB_TRY(ensure(c, c.contactBuf[c.cur], (size_t)m * sizeof(vx_contact) + 128));
+        if (m) VXB_CUDA(c, cudaMemcpyAsync(c.contactBuf[c.cur].ptr, c.hostSorted.data(), (size_t)m * sizeof(vx_contact),
+                                           cudaMemcpyHostToDevice, c.stream));
+        VXB_TRY(buildIslands(c, P<vx_contact>(c.contactBuf[c.cur]), m, plan, nullptr));
+        VXB_TRY(prepareSegments(c, plan));
+        // colour order back to the host (pre-solve values, like the reference's sorted_ copy)
+        std::vector<uint32_t> order(m);
+        if (m) VXB_CUDA(c, cudaMemcpyAsync(order.data(), c.islandValBuf.ptr, (size_t)m * 4, cudaMemcpyDeviceToHost,
+                                           c.stream));
+        VXB_CUDA(c, cudaStreamSynchronize(c.stream));
+        for (uint32_t k = 0; k < m; ++k) contacts[k] = c.hostSorted[order[k]];
+        c.backendContacts = m;
+        c.backendColored = true;
+    }
+    if (m == 0 && !fullSubsteps) return VXB_OK;
+    const V3 g{gravity.x, gravity.y, gravity.z};
+    if (fullSubsteps) {
+        VXB_TRY(runSubsteps(c, P<vx_contact>(c.contactBuf[c.cur]), plan, g, h, substeps, o, warmStart, true));
+    } else {
+        VXB_TRY(runSubsteps(c, P<vx_contact>(c.contactBuf[c.cur]), plan, g, h, 1, o, warmStart, false));
+    }
+    VXB_CUDA(c, cudaGetLastError());
+    return VXB_OK;
+}
+
+int backendFetchImpulses(Context& c, vx_contact* contacts, uint32_t m) {
+    if (!c.backendColored || m != c.backendContacts || m == 0) return VXB_OK;
+    VXB_TRY(ensure(c, c.contactTmpBuf, (size_t)m * sizeof(vx_contact)));
+    LAUNCH(c, gatherContactsKernel, blocksFor(m, 128), 128, P<vx_contact>(c.contactBuf[c.cur]),
+           P<uint32_t>(c.islandValBuf), m, P<vx_contact>(c.contactTmpBuf));
+    VXB_CUDA(c, cudaMemcpyAsync(contacts, c.contactTmpBuf.ptr, (size_t)m * sizeof(vx_contact), cudaMemcpyDeviceToHost,
+                                c.stream));
+    VXB_CUDA(c, cudaStreamSynchronize(c.stream));
+    return VXB_OK;
+}
+
+}  // namespace vxb
