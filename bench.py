@@ -1,0 +1,299 @@
+"""Benchmark: body-steps/s of the device contact pipeline on the 100,000-body
+mixed-shape scene (spheres, boxes, capsules, cylinders, 16-vertex hulls in a
+200 x 200 x 60 m box above a plane; dt = 1/60 s, 4 substeps), seeded synthetic
+data.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+b200 arm: one process per GPU (torchrun for N > 1); every rank steps its own
+replica of the world ("replicas only": a single world does not shard), the
+timed region is K steps on the device (CUDA events on the pipeline's stream,
+L2 flushed with a 256 MiB write before every step, outside the events), and
+the value is all ranks' bodies x steps / max-over-ranks time.
+
+reference arm: the reference engine's CPU backend (built from its sources
+into oracle/_ref), all host cores, on the same scene; rank 0 only.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "body-steps/s @100k bodies"
+DT = 1.0 / 60.0
+CONFIG = 2            # the 100k-body mixed-shape scene
+SUBSTEPS = 4
+L2_FLUSH_BYTES = 256 << 20
+
+# Roofline of the narrow phase's neighbour, the island solve: algorithmic bytes
+# per contact row and sweep (contact constants 64 + impulses r/w 48 + two
+# bodies' pose/velocity/mass reads 168 + velocity writes 48).
+SOLVER_BYTES_PER_ROW = 328
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, f[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def build_scene(size):
+    import velox_b200 as vb
+    specs, pool = vb.generate_scene(CONFIG, seed=CONFIG, size=size)
+    bodies, hull, faces = vb.bodies_from_specs(specs, pool)
+    return specs, pool, bodies, vb.make_soup(hull, faces)
+
+
+def cpu_baseline(specs, pool, n_bodies, budget_s=20.0, max_steps=40, warm_steps=1):
+    """The reference CPU backend (default Release build, all host threads) on
+    the same scene, timed for a bounded number of steps."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref
+    if not ref.available(strict=False):
+        return None
+    w = ref.RefWorld(specs, pool, backend=ref.BACKEND_CPU, strict=False)
+    w.configure(substeps=SUBSTEPS, workers=0)
+    workers = int(w.L.ref_world_worker_count(w.h))
+    w.step(DT, warm_steps)
+    steps, total = 0, 0.0
+    while steps < max_steps and total < budget_s:
+        total += w.step(DT, 1) / 1000.0
+        steps += 1
+    w.close()
+    value = n_bodies * steps / total
+    return {"value": value, "unit": "body-steps/s", "cores": workers, "kind": "reference",
+            "sample": f"{steps} steps of the {n_bodies}-body scene after {warm_steps} warm-up step(s), "
+                      f"reference CPU backend (Release build) with {workers} worker threads on "
+                      f"{os.cpu_count()} host cores, {total:.1f} s"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    specs, pool, bodies, soup = build_scene(args.size)
+    n = len(bodies)
+    budget = float(os.environ.get("VXB_REFERENCE_BUDGET_S", "150"))
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref
+    if not ref.available(strict=False):
+        print(json.dumps({"impl": "reference", "unavailable": "reference CPU build (oracle/_ref) missing"}))
+        return 0
+    w = ref.RefWorld(specs, pool, backend=ref.BACKEND_CPU, strict=False)
+    w.configure(substeps=SUBSTEPS, workers=0)
+    workers = int(w.L.ref_world_worker_count(w.h))
+    w.step(DT, args.warmup)
+    steps, total = 0, 0.0
+    while steps < args.steps and total < budget:
+        total += w.step(DT, 1) / 1000.0
+        steps += 1
+    w.close()
+    value = n * steps / total
+    sample = (f"{steps} of {args.steps} requested steps (time budget {budget:.0f} s) of the {n}-body scene after "
+              f"{args.warmup} warm-up steps; reference CPU backend (Release build), {workers} worker threads")
+    line = {"metric": METRIC, "value": value, "unit": "body-steps/s", "impl": "reference", "n_gpus": 0,
+            "steps": steps, "warmup": args.warmup, "ms_per_step": total / steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+            "config": {"workload": f"mixed-shape scene, {n} bodies (1 plane), dt 1/60 s, {SUBSTEPS} substeps",
+                       "bodies": n},
+            "cpu_baseline": {"value": value, "unit": "body-steps/s", "cores": workers, "kind": "reference",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": "body-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--size", type=int, default=100000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    import velox_b200 as vb
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    specs, pool, bodies, soup = build_scene(args.size)
+    n = len(bodies)
+    stream = torch.cuda.Stream()
+    ctx = vb.Context(local)
+    ctx.set_stream(stream.cuda_stream)
+    ctx.load(bodies, soup)
+    ctx.configure(dt=DT, substeps=SUBSTEPS)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    ctx.step(max(args.warmup, 3) if args.warmup >= 3 else args.warmup)
+    sampler = ClockSampler(local)
+    sampler.start()
+    barrier()
+    launches0 = ctx.launches
+    ctx.enable_timing(True)
+    events = []
+    contacts_total = 0
+    with torch.cuda.stream(stream):
+        for _ in range(args.steps):
+            flush.fill_(1)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            ctx.step(1)
+            e1.record(stream)
+            events.append((e0, e1))
+            contacts_total += ctx.stats()["contacts"]
+    barrier()
+    clocks = sampler.stop()
+    launches = ctx.launches - launches0
+    stage = ctx.stage_times()
+    ctx.enable_timing(False)
+    ms = sum(a.elapsed_time(b) for a, b in events)
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * n * args.steps / (ms / 1e3)
+
+    # Roofline of the island solve (memory-bound sweeps over contact rows).
+    peak, peak_kind = measured_peaks()
+    solve_ms, solve_calls = stage["solve"]
+    rows = contacts_total * 2 * 8 * SUBSTEPS  # sweeps * substeps per step
+    solve_bytes = rows * SOLVER_BYTES_PER_ROW
+    achieved = solve_bytes / (solve_ms / 1e3) / 1e9 if solve_ms > 0 else 0.0
+    roofline = {"bound": "hbm", "kernel": "solveBlockKernel+solveTinyKernel (island substep solve)",
+                "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "peak_source": peak_kind, "traffic": None,
+                "algorithmic_bytes_per_launch": solve_bytes / max(solve_calls, 1),
+                "avg_launch_ms": solve_ms / max(solve_calls, 1)}
+
+    # End to end through the C ABI: forces in from pinned host memory, one
+    # step, poses back to pinned host memory, every step.
+    forces = torch.zeros((n, 6), dtype=torch.float32).pin_memory()
+    poses = torch.zeros((n, 7), dtype=torch.float32).pin_memory()
+    fptr, pptr = forces.numpy(), poses.numpy()
+    e2e_steps = max(1, min(args.steps, 50))
+    barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    t0 = time.perf_counter()
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        ctx.write_forces(fptr)
+        ctx.step(1)
+        ctx.read_poses(pptr)
+    e1.record(stream)
+    barrier()
+    wall = time.perf_counter() - t0
+    e2e_ms = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e = {"value": world * n * e2e_steps / (e2e_ms / 1e3), "unit": "body-steps/s",
+           "h2d_bytes_per_step": int(forces.numel() * 4), "d2h_bytes_per_step": int(poses.numel() * 4),
+           "steps": e2e_steps, "wall_s": wall}
+
+    baseline = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            baseline = cpu_baseline(specs, pool, n)
+        except Exception as exc:  # reported, not fatal
+            baseline = {"error": str(exc)}
+
+    stats = ctx.stats()
+    ctx.close()
+    if dist:
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    line = {"metric": METRIC, "value": value, "unit": "body-steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+            "config": {"workload": f"mixed-shape scene, {n} bodies (1 plane), dt 1/60 s, {SUBSTEPS} substeps",
+                       "bodies": n, "parallelism": f"replicas x{world}",
+                       "l2": "flushed (256 MiB write) before every timed step, outside the step's events"},
+            "contacts_per_s": contacts_total / (ms / 1e3), "last_step": stats,
+            "stage_ms_per_step": {k: v[0] / args.steps for k, v in stage.items()},
+            "roofline": roofline, "cpu_baseline": baseline, "e2e": e2e, "clocks": clocks,
+            "gpu_launches": int(launches)}
+    print(json.dumps(line))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -86,6 +86,15 @@ int vxb_context_set_stream(vxb_context* ctx, void* stream);
 /* Number of kernel launches this context issued since it was created. */
 uint64_t vxb_context_launch_count(const vxb_context* ctx);
 
+/* Per-stage device timing with CUDA events recorded on the context's stream
+ * (stages: 0 prepare, 1 broad phase, 2 cell-key sort, 3 narrow phase,
+ * 4 contact placement, 5 warm start, 6 islands + colouring, 7 substep solve,
+ * 8 rewind, 9 position correction). Enabling resets the totals. */
+int vxb_context_enable_timing(vxb_context* ctx, int enable);
+/* Totals since timing was enabled: ms[stage] and calls[stage] for
+ * `count` stages (<= 10). Synchronises the stream. */
+int vxb_context_stage_times(vxb_context* ctx, double* ms, uint64_t* calls, uint32_t count);
+
 /* ---- Backend interface over host arrays ------------------------------- */
 
 /* Backend::integrate (backend.h:116; CudaBackend::integrate,

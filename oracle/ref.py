@@ -13,20 +13,30 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.join(HERE, "_ref")
 STRICT = os.path.join(REF_DIR, "libvelox_ref_strict.so")
 FAST = os.path.join(REF_DIR, "libvelox_ref_fast.so")
+# The reference engine whose CUDA backend is velox_b200/dropin/b200_backend.cpp.
+DROPIN = os.path.join(REF_DIR, "libvelox_ref_dropin.so")
 
 BACKEND_CPU = 1
 BACKEND_CUDA_EMULATED = 2
 
 
+def _path(strict):
+    if strict == "dropin":
+        return DROPIN
+    return STRICT if strict else FAST
+
+
 def available(strict=True):
-    return os.path.exists(STRICT if strict else FAST)
+    return os.path.exists(_path(strict))
 
 
 _libs = {}
 
 
 def lib(strict=True):
-    path = STRICT if strict else FAST
+    """strict=True: strict-FP build; False: default Release build; "dropin":
+    strict build whose CUDA backend is the B200 library."""
+    path = _path(strict)
     if path in _libs:
         return _libs[path]
     if not os.path.exists(path):

@@ -252,11 +252,15 @@ thread_local ColoredCpuBackend* g_lastEmulated = nullptr;
 
 }  // namespace
 
+// The drop-in build links velox_b200/dropin/b200_backend.cpp instead, whose
+// createCudaBackend() serves World(BackendType::Cuda) from libvelox_b200.so.
+#ifndef REF_SHIM_DROPIN
 Backend* createCudaBackend() {
     auto* backend = new ColoredCpuBackend();
     g_lastEmulated = backend;
     return backend;
 }
+#endif
 
 }  // namespace velox
 

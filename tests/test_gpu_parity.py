@@ -36,8 +36,10 @@ def _compare_contacts(mine, theirs):
         assert np.abs(mine[f] - theirs[f]).max() <= POS_TOL, f
     for f in ("gap", "bias0"):
         assert np.abs(mine[f] - theirs[f]).max() <= POS_TOL, f
-    cosang = np.clip(np.sum(mine["normal"] * theirs["normal"], 1), -1, 1)
-    assert np.arccos(cosang).max() <= ANGLE_TOL
+    a = mine["normal"].astype(np.float64)
+    b = theirs["normal"].astype(np.float64)
+    angle = np.arctan2(np.linalg.norm(np.cross(a, b), axis=1), np.sum(a * b, 1))
+    assert angle.max() <= ANGLE_TOL
     for f in ("vn0", "restitution", "friction1", "friction2"):
         assert np.allclose(mine[f], theirs[f], rtol=1e-5, atol=1e-5), f
 

@@ -141,6 +141,8 @@ def lib(path=LIB_PATH):
         "vxb_context_last_error": ([vp], ctypes.c_char_p),
         "vxb_context_set_stream": ([vp, vp], i32),
         "vxb_context_launch_count": ([vp], ctypes.c_uint64),
+        "vxb_context_enable_timing": ([vp, i32], i32),
+        "vxb_context_stage_times": ([vp, vp, vp, u32], i32),
         "vxb_backend_integrate": ([vp, vp, u32, Vec3, f32], i32),
         "vxb_backend_find_contacts": ([vp, vp, u32, ctypes.POINTER(Soup), f32, p_u32], i32),
         "vxb_backend_copy_contacts": ([vp, vp, u32], i32),
@@ -246,6 +248,18 @@ class Context:
     @property
     def launches(self):
         return int(self.L.vxb_context_launch_count(self.h))
+
+    STAGES = ["prepare", "broadphase", "cell_sort", "narrowphase", "placement", "warm_start",
+              "islands", "solve", "rewind", "positions"]
+
+    def enable_timing(self, on=True):
+        self._check(self.L.vxb_context_enable_timing(self.h, int(on)))
+
+    def stage_times(self):
+        ms = np.zeros(10, np.float64)
+        calls = np.zeros(10, np.uint64)
+        self._check(self.L.vxb_context_stage_times(self.h, ptr(ms), ptr(calls), 10))
+        return {n: (float(ms[i]), int(calls[i])) for i, n in enumerate(self.STAGES)}
 
     def set_stream(self, stream_handle):
         self._check(self.L.vxb_context_set_stream(self.h, ctypes.c_void_p(stream_handle)))

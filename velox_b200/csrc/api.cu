@@ -101,7 +101,7 @@ void vxb_context_destroy(vxb_context* ctx) {
                            &c.colorKeyBuf, &c.maskBuf, &c.nextColorBuf, &c.islandStartBuf, &c.islandInfoBuf,
                            &c.flagBuf, &c.scanBuf, &c.scanTmp, &c.segStartBuf, &c.islandSegBuf, &c.bodyKeyBuf,
                            &c.bodyValBuf, &c.islandBodyStartBuf, &c.caFlagBuf, &c.caBodyMarkBuf, &c.caCandBuf,
-                           &c.countersBuf};
+                           &c.localIdxBuf, &c.countersBuf};
     for (vxb::DevBuf* b : bufs)
         if (b->ptr) cudaFree(b->ptr);
     if (c.ownStream) cudaStreamDestroy(c.ownStream);
@@ -119,6 +119,30 @@ int vxb_context_set_stream(vxb_context* ctx, void* stream) {
 }
 
 uint64_t vxb_context_launch_count(const vxb_context* ctx) { return ctx ? ctx->impl.launches : 0; }
+
+int vxb_context_enable_timing(vxb_context* ctx, int enable) {
+    GUARD(ctx);
+    Context& c = ctx->impl;
+    TRY(vxb::stageResolve(c));
+    for (int s = 0; s < vxb::kStageCount; ++s) {
+        c.timer.ms[s] = 0.0;
+        c.timer.calls[s] = 0;
+    }
+    c.timing = enable != 0;
+    return VXB_OK;
+}
+
+int vxb_context_stage_times(vxb_context* ctx, double* ms, uint64_t* calls, uint32_t count) {
+    GUARD(ctx);
+    if (!ms || !calls || count > (uint32_t)vxb::kStageCount) return VXB_ERR_INVALID;
+    Context& c = ctx->impl;
+    TRY(vxb::stageResolve(c));
+    for (uint32_t s = 0; s < count; ++s) {
+        ms[s] = c.timer.ms[s];
+        calls[s] = c.timer.calls[s];
+    }
+    return VXB_OK;
+}
 
 // ---- Backend interface ---------------------------------------------------
 

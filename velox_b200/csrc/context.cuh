@@ -51,6 +51,20 @@ struct Counters {
     uint32_t pad[8];
 };
 
+// Pipeline stages timed with CUDA events when timing is enabled.
+enum Stage : int {
+    kStagePrepare = 0, kStageBroadphase, kStageCellSort, kStageNarrowphase, kStagePlacement,
+    kStageWarmStart, kStageIslands, kStageSolve, kStageRewind, kStagePositions, kStageCount
+};
+
+struct StageTimer {
+    std::vector<cudaEvent_t> pool;         // free events
+    std::vector<cudaEvent_t> open[kStageCount];
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> done[kStageCount];
+    double ms[kStageCount] = {};
+    uint64_t calls[kStageCount] = {};
+};
+
 struct Context {
     int device = 0;
     int smCount = 148;
@@ -109,6 +123,7 @@ struct Context {
     DevBuf segStartBuf, islandSegBuf;
     DevBuf bodyKeyBuf, bodyValBuf, islandBodyStartBuf;
     DevBuf caFlagBuf, caBodyMarkBuf, caCandBuf;
+    DevBuf localIdxBuf;                 // island-local body index (block solve)
 
     DevBuf countersBuf;
     Counters* dCounters = nullptr;
@@ -127,8 +142,15 @@ struct Context {
     std::vector<vx_contact> hostSorted;
     IslandPlan backendPlan;
 
+    bool timing = false;
+    StageTimer timer;
+
     cudaError_t err = cudaSuccess;
 };
+
+void stageBegin(Context& c, int stage);
+void stageEnd(Context& c, int stage);
+int stageResolve(Context& c);
 
 // Records a failure on the context; returns the mapped status.
 int fail(Context& c, int status, const std::string& message);

@@ -61,6 +61,50 @@ int ensure(Context& c, DevBuf& b, size_t bytes) {
 
 template <class T> T* P(DevBuf& b) { return reinterpret_cast<T*>(b.ptr); }
 
+static cudaEvent_t takeEvent(Context& c) {
+    if (c.timer.pool.empty()) {
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        return e;
+    }
+    cudaEvent_t e = c.timer.pool.back();
+    c.timer.pool.pop_back();
+    return e;
+}
+
+void stageBegin(Context& c, int stage) {
+    if (!c.timing) return;
+    cudaEvent_t e = takeEvent(c);
+    cudaEventRecord(e, c.stream);
+    c.timer.open[stage].push_back(e);
+}
+
+void stageEnd(Context& c, int stage) {
+    if (!c.timing || c.timer.open[stage].empty()) return;
+    cudaEvent_t e = takeEvent(c);
+    cudaEventRecord(e, c.stream);
+    c.timer.done[stage].push_back({c.timer.open[stage].back(), e});
+    c.timer.open[stage].pop_back();
+}
+
+// Folds completed event pairs into the per-stage totals.
+int stageResolve(Context& c) {
+    cudaError_t e = cudaStreamSynchronize(c.stream);
+    if (e != cudaSuccess) return cudaStatus(c, e, "stage timing");
+    for (int s = 0; s < kStageCount; ++s) {
+        for (auto& pr : c.timer.done[s]) {
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, pr.first, pr.second);
+            c.timer.ms[s] += ms;
+            c.timer.calls[s] += 1;
+            c.timer.pool.push_back(pr.first);
+            c.timer.pool.push_back(pr.second);
+        }
+        c.timer.done[s].clear();
+    }
+    return VXB_OK;
+}
+
 #define VXB_TRY(expr)                  \
     do {                               \
         int s_ = (expr);               \
@@ -678,11 +722,14 @@ __global__ void iotaKernel(uint32_t* a, uint32_t n) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) a[i] = i;
 }
 
+// Union-find root with path halving. Parent links are read with ld.global.cg
+// (L2, not the SM's L1): other SMs relink roots concurrently and a stale L1
+// line would otherwise keep a thread spinning on an outdated root.
 VXD uint32_t ufFind(uint32_t* parent, uint32_t x) {
-    uint32_t p = parent[x];
+    uint32_t p = __ldcg(parent + x);
     while (p != x) {
-        const uint32_t gp = parent[p];
-        if (gp != p) parent[x] = gp;  // path halving (benign race: any ancestor is valid)
+        const uint32_t gp = __ldcg(parent + p);
+        if (gp != p) __stcg(parent + x, gp);  // path halving (benign race: any ancestor is valid)
         x = p;
         p = gp;
     }
@@ -691,12 +738,19 @@ VXD uint32_t ufFind(uint32_t* parent, uint32_t x) {
 
 VXD bool solvedContact(uint32_t fa, uint32_t fb) { return !isSensor(fa) && !isSensor(fb); }
 
-__global__ void unionKernel(const vx_contact* cs, uint32_t m, const BodyArrays B, uint32_t* parent) {
+// Lock-free linking: a failed CAS means another thread linked that root, so
+// the retry loop always makes global progress; the bound only turns a
+// malfunction into a reported error instead of a hang.
+constexpr uint32_t kUnionRetryLimit = 1u << 24;
+
+__global__ void unionKernel(const vx_contact* cs, uint32_t m, const BodyArrays B, uint32_t* parent, Counters* C) {
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < m; k += gridDim.x * blockDim.x) {
         const uint32_t a = cs[k].a, b = cs[k].b;
         const uint32_t fa = B.filt[a].x, fb = B.filt[b].x;
         if (!solvedContact(fa, fb) || !isDynamic(fa) || !isDynamic(fb)) continue;
-        for (int guard = 0; guard < 1 << 20; ++guard) {
+        uint32_t tries = 0;
+        for (;; ++tries) {
+            if (tries == kUnionRetryLimit) { atomicOr(&C->timeout, 1u); break; }
             uint32_t ra = ufFind(parent, a), rb = ufFind(parent, b);
             if (ra == rb) break;
             if (ra < rb) { const uint32_t t = ra; ra = rb; rb = t; }
@@ -931,52 +985,316 @@ VXD void solveIslandSerial(const SolveArgs& A, uint32_t isl) {
     }
 }
 
-__global__ void __launch_bounds__(128) solveTinyKernel(SolveArgs A) {
-    for (uint32_t isl = blockIdx.x * blockDim.x + threadIdx.x; isl < A.islands; isl += gridDim.x * blockDim.x)
-        if (islandSize(A, isl) <= A.tinyLimit) solveIslandSerial(A, isl);
+// Tiny islands (at most kTinyContacts contacts): one thread gathers the
+// island's bodies and contacts into local arrays once, runs the whole substep
+// loop on them (same row order as the coloured sweeps: colour-major) and
+// writes the results back. Static endpoints are local read-only copies.
+constexpr int kTinyContacts = 16;
+constexpr int kTinyBodies = 2 * kTinyContacts;
+
+struct LocalBody {
+    SolverBody s;
+    float gs, ld, ad;  // gravityScale, linear / angular damping
+    V3 force, torque;
+    uint32_t id;
+};
+
+VXD void localIntegrateVelocity(LocalBody& b, const V3& g, float dt) {
+    const Mass& m = b.s.m;
+    if (!isDynamic(m.flags) || isLocked(m.flags) || isAsleep(m.flags)) return;
+    b.s.v += (g * b.gs + b.force * solverInvMass(m)) * dt;
+    b.s.w += invInertiaMulAt(m, b.torque, b.s.q) * dt;
+    b.s.v *= 1.0f / (1.0f + b.ld * dt);
+    b.s.w *= 1.0f / (1.0f + b.ad * dt);
+}
+
+VXD void localIntegrateTransform(LocalBody& b, float dt) {
+    const Mass& m = b.s.m;
+    if (isStaticBody(m.flags) || isLocked(m.flags) || isAsleep(m.flags)) return;
+    advanceTransform(m, b.s.p, b.s.q, b.s.v, b.s.w, dt);
+}
+
+__global__ void __launch_bounds__(64) solveTinyKernel(SolveArgs A) {
+    for (uint32_t isl = blockIdx.x * blockDim.x + threadIdx.x; isl < A.islands; isl += gridDim.x * blockDim.x) {
+        const uint32_t s0 = A.islandStart[isl], s1 = A.islandStart[isl + 1];
+        const uint32_t count = s1 - s0;
+        if (count > A.tinyLimit) continue;
+        if (count > (uint32_t)kTinyContacts) { solveIslandSerial(A, isl); continue; }
+        LocalBody bodies[kTinyBodies];
+        RowContact rows[kTinyContacts];
+        uint8_t ra[kTinyContacts], rb[kTinyContacts];
+        bool live[kTinyContacts];
+        int nb = 0;
+        auto slot = [&](uint32_t id) -> int {
+            for (int i = 0; i < nb; ++i)
+                if (bodies[i].id == id) return i;
+            LocalBody& b = bodies[nb];
+            b.s = loadSolverBody(A.B, id);
+            const float4 ex = A.B.extra[id];
+            b.gs = ex.y; b.ld = ex.z; b.ad = ex.w;
+            b.force = f3(A.B.force[id]);
+            b.torque = f3(A.B.torque[id]);
+            b.id = id;
+            return nb++;
+        };
+        for (uint32_t k = 0; k < count; ++k) {
+            const vx_contact& cc = A.contacts[A.order[s0 + k]];
+            loadRow(cc, rows[k]);
+            ra[k] = (uint8_t)slot(cc.a);
+            rb[k] = (uint8_t)slot(cc.b);
+            live[k] = solvedContact(bodies[ra[k]].s.m.flags, bodies[rb[k]].s.m.flags);
+        }
+        if (A.positionIterations > 0) {
+            for (int it = 0; it < A.positionIterations; ++it)
+                for (uint32_t k = 0; k < count; ++k) {
+                    if (!live[k]) continue;
+                    SolverBody& a = bodies[ra[k]].s;
+                    SolverBody& b = bodies[rb[k]].s;
+                    const float ima = solverInvMass(a.m), imb = solverInvMass(b.m);
+                    const float invMassSum = ima + imb;
+                    if (invMassSum <= 0.0f) continue;
+                    const RowContact& r = rows[k];
+                    const V3 wa = anchorWorld(a.sphere, a.p, a.q, r.la);
+                    const V3 wb = anchorWorld(b.sphere, b.p, b.q, r.lb);
+                    const float gap = r.bias0 + dot(r.normal, wa - wb);
+                    if (gap >= -1e-3f) continue;
+                    float resolve = 0.6f;
+                    if (A.stackStabilization && lengthSq(a.v - b.v) < 1e-4f)
+                        resolve += 0.2f * (A.stackStiffness / 1000.0f) / (1.0f + A.stackDamping * A.h);
+                    const float push = -resolve * (gap + 1e-3f) / invMassSum;
+                    if (isDynamic(a.m.flags) && !isAsleep(a.m.flags)) a.p += r.normal * (push * ima);
+                    if (isDynamic(b.m.flags) && !isAsleep(b.m.flags)) b.p -= r.normal * (push * imb);
+                }
+            for (int i = 0; i < nb; ++i)
+                if (isDynamic(bodies[i].s.m.flags)) A.B.pos[bodies[i].id] = pack(bodies[i].s.p, 0.0f);
+            continue;
+        }
+        for (int s = 0; s < A.substeps; ++s) {
+            if (A.integrate && s > 0)
+                for (int i = 0; i < nb; ++i) localIntegrateVelocity(bodies[i], A.gravity, A.h);
+            if (A.warmStart && s == 0)
+                for (uint32_t k = 0; k < count; ++k)
+                    if (live[k]) warmStartRow(bodies[ra[k]].s, bodies[rb[k]].s, rows[k]);
+            for (int it = 0; it < A.sweeps; ++it)
+                for (uint32_t k = 0; k < count; ++k)
+                    if (live[k]) solveRow(bodies[ra[k]].s, bodies[rb[k]].s, rows[k], A.h, A.coneBlock != 0);
+            if (A.integrate)
+                for (int i = 0; i < nb; ++i) localIntegrateTransform(bodies[i], A.h);
+        }
+        for (int i = 0; i < nb; ++i) {
+            const LocalBody& b = bodies[i];
+            if (!isDynamic(b.s.m.flags)) continue;
+            A.B.pos[b.id] = pack(b.s.p, 0.0f);
+            A.B.rot[b.id] = pack(b.s.q);
+            A.B.vel[b.id] = pack(b.s.v, 0.0f);
+            A.B.ang[b.id] = pack(b.s.w, 0.0f);
+        }
+        for (uint32_t k = 0; k < count; ++k) storeRow(A.contacts[A.order[s0 + k]], rows[k]);
+    }
 }
 
 // Block-cooperative island processing: contacts of one colour in parallel,
-// a block barrier between colours.
-__global__ void __launch_bounds__(256) solveBlockKernel(SolveArgs A) {
+// a block barrier between colours. The island's dynamic bodies live in shared
+// memory for the whole substep loop (islands of up to kBlockBodies bodies and
+// kBlockRows contacts); larger islands run the same schedule on global memory.
+constexpr int kBlockThreads = 256;
+constexpr int kBlockBodies = 512;
+constexpr int kBlockRows = 3072;
+constexpr size_t kBlockSmem = (size_t)kBlockBodies * (6 * sizeof(float4) + sizeof(uint32_t)) +
+                              (size_t)kBlockRows * sizeof(int2);
+
+struct SharedBodies {
+    float4 *p, *q, *v, *w, *inertia, *iq;
+    uint32_t* flags;
+    int2* rowIdx;  // per island row: local index of a / b, -1 = read-only global body
+};
+
+VXD SharedBodies carve(float4* base) {
+    SharedBodies S;
+    S.p = base;
+    S.q = S.p + kBlockBodies;
+    S.v = S.q + kBlockBodies;
+    S.w = S.v + kBlockBodies;
+    S.inertia = S.w + kBlockBodies;
+    S.iq = S.inertia + kBlockBodies;
+    S.flags = reinterpret_cast<uint32_t*>(S.iq + kBlockBodies);
+    S.rowIdx = reinterpret_cast<int2*>(S.flags + kBlockBodies);
+    return S;
+}
+
+VXD SolverBody sharedBody(const SharedBodies& S, int li) {
+    SolverBody b;
+    b.p = f3(S.p[li]);
+    b.q = q4(S.q[li]);
+    b.v = f3(S.v[li]);
+    b.w = f3(S.w[li]);
+    const float4 in = S.inertia[li];
+    b.m.invI = V3{in.x, in.y, in.z};
+    b.m.invMass = in.w;
+    b.m.iq = q4(S.iq[li]);
+    b.m.flags = S.flags[li];
+    b.sphere = shapeOf(b.m.flags) == kSphere;
+    return b;
+}
+
+// op: 0 warm start, 1 velocity row, 2 position row
+VXD void sharedRow(const SolveArgs& A, const SharedBodies& S, uint32_t k, uint32_t s0, int op) {
+    vx_contact& cc = A.contacts[A.order[s0 + k]];
+    const int2 li = S.rowIdx[k];
+    SolverBody a = li.x >= 0 ? sharedBody(S, li.x) : loadSolverBody(A.B, cc.a);
+    SolverBody b = li.y >= 0 ? sharedBody(S, li.y) : loadSolverBody(A.B, cc.b);
+    if (!solvedContact(a.m.flags, b.m.flags)) return;
+    if (op == 2) {
+        const float ima = solverInvMass(a.m), imb = solverInvMass(b.m);
+        const float invMassSum = ima + imb;
+        if (invMassSum <= 0.0f) return;
+        const V3 n{cc.normal.x, cc.normal.y, cc.normal.z};
+        const V3 wa = anchorWorld(a.sphere, a.p, a.q, V3{cc.localAnchorA.x, cc.localAnchorA.y, cc.localAnchorA.z});
+        const V3 wb = anchorWorld(b.sphere, b.p, b.q, V3{cc.localAnchorB.x, cc.localAnchorB.y, cc.localAnchorB.z});
+        const float gap = cc.bias0 + dot(n, wa - wb);
+        if (gap >= -1e-3f) return;
+        float resolve = 0.6f;
+        if (A.stackStabilization && lengthSq(a.v - b.v) < 1e-4f)
+            resolve += 0.2f * (A.stackStiffness / 1000.0f) / (1.0f + A.stackDamping * A.h);
+        const float push = -resolve * (gap + 1e-3f) / invMassSum;
+        if (isDynamic(a.m.flags) && !isAsleep(a.m.flags) && li.x >= 0) S.p[li.x] = pack(a.p + n * (push * ima), 0.0f);
+        if (isDynamic(b.m.flags) && !isAsleep(b.m.flags) && li.y >= 0) S.p[li.y] = pack(b.p - n * (push * imb), 0.0f);
+        return;
+    }
+    RowContact r;
+    loadRow(cc, r);
+    if (op == 0) warmStartRow(a, b, r);
+    else solveRow(a, b, r, A.h, A.coneBlock != 0);
+    if (li.x >= 0 && isDynamic(a.m.flags)) { S.v[li.x] = pack(a.v, 0.0f); S.w[li.x] = pack(a.w, 0.0f); }
+    if (li.y >= 0 && isDynamic(b.m.flags)) { S.v[li.y] = pack(b.v, 0.0f); S.w[li.y] = pack(b.w, 0.0f); }
+    storeRow(cc, r);
+}
+
+VXD void sharedIntegrateVelocity(const SolveArgs& A, const SharedBodies& S, int li, uint32_t id) {
+    SolverBody b = sharedBody(S, li);
+    const Mass& m = b.m;
+    if (!isDynamic(m.flags) || isLocked(m.flags) || isAsleep(m.flags)) return;
+    const float4 ex = A.B.extra[id];
+    b.v += (A.gravity * ex.y + f3(A.B.force[id]) * solverInvMass(m)) * A.h;
+    b.w += invInertiaMulAt(m, f3(A.B.torque[id]), b.q) * A.h;
+    b.v *= 1.0f / (1.0f + ex.z * A.h);
+    b.w *= 1.0f / (1.0f + ex.w * A.h);
+    S.v[li] = pack(b.v, 0.0f);
+    S.w[li] = pack(b.w, 0.0f);
+}
+
+VXD void sharedIntegrateTransform(const SolveArgs& A, const SharedBodies& S, int li) {
+    SolverBody b = sharedBody(S, li);
+    if (isStaticBody(b.m.flags) || isLocked(b.m.flags) || isAsleep(b.m.flags)) return;
+    advanceTransform(b.m, b.p, b.q, b.v, b.w, A.h);
+    S.p[li] = pack(b.p, 0.0f);
+    S.q[li] = pack(b.q);
+    S.w[li] = pack(b.w, 0.0f);
+}
+
+__device__ void solveIslandGlobal(const SolveArgs& A, uint32_t isl) {
+    const uint32_t g0 = A.islandSeg[isl], g1 = A.islandSeg[isl + 1];
+    if (A.positionIterations > 0) {
+        for (int it = 0; it < A.positionIterations; ++it)
+            for (uint32_t g = g0; g < g1; ++g) {
+                for (uint32_t k = A.segStart[g] + threadIdx.x; k < A.segStart[g + 1]; k += blockDim.x)
+                    positionRow(A, A.order[k]);
+                __syncthreads();
+            }
+        return;
+    }
+    const uint32_t b0 = isl < A.realIslands ? A.bodyStart[isl] : 0u;
+    const uint32_t b1 = isl < A.realIslands ? A.bodyStart[isl + 1] : 0u;
+    for (int s = 0; s < A.substeps; ++s) {
+        if (A.integrate && s > 0) {
+            for (uint32_t k = b0 + threadIdx.x; k < b1; k += blockDim.x)
+                integrateVelocity(A.B, A.bodyOrder[k], A.gravity, A.h);
+            __syncthreads();
+        }
+        if (A.warmStart && s == 0)
+            for (uint32_t g = g0; g < g1; ++g) {
+                for (uint32_t k = A.segStart[g] + threadIdx.x; k < A.segStart[g + 1]; k += blockDim.x)
+                    warmRow(A, A.order[k]);
+                __syncthreads();
+            }
+        for (int it = 0; it < A.sweeps; ++it)
+            for (uint32_t g = g0; g < g1; ++g) {
+                for (uint32_t k = A.segStart[g] + threadIdx.x; k < A.segStart[g + 1]; k += blockDim.x)
+                    solveRowAt(A, A.order[k]);
+                __syncthreads();
+            }
+        if (A.integrate) {
+            for (uint32_t k = b0 + threadIdx.x; k < b1; k += blockDim.x)
+                integrateTransform(A.B, A.bodyOrder[k], A.h);
+            __syncthreads();
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kBlockThreads) solveBlockKernel(SolveArgs A, uint32_t* localIdx) {
+    extern __shared__ float4 smemRaw[];
+    const SharedBodies S = carve(smemRaw);
     for (uint32_t isl = blockIdx.x; isl < A.islands; isl += gridDim.x) {
-        if (islandSize(A, isl) <= A.tinyLimit) continue;
+        const uint32_t s0 = A.islandStart[isl], s1 = A.islandStart[isl + 1];
+        if (s1 - s0 <= A.tinyLimit) continue;
+        const uint32_t b0 = isl < A.realIslands ? A.bodyStart[isl] : 0u;
+        const uint32_t b1 = isl < A.realIslands ? A.bodyStart[isl + 1] : 0u;
+        const uint32_t nb = b1 - b0, rows = s1 - s0;
+        if (nb > (uint32_t)kBlockBodies || rows > (uint32_t)kBlockRows) {
+            solveIslandGlobal(A, isl);
+            continue;
+        }
+        for (uint32_t k = threadIdx.x; k < nb; k += blockDim.x) {
+            const uint32_t id = A.bodyOrder[b0 + k];
+            S.p[k] = A.B.pos[id]; S.q[k] = A.B.rot[id]; S.v[k] = A.B.vel[id]; S.w[k] = A.B.ang[id];
+            S.inertia[k] = A.B.inertia[id]; S.iq[k] = A.B.iq[id]; S.flags[k] = A.B.filt[id].x;
+            localIdx[id] = k;
+        }
+        __syncthreads();
+        for (uint32_t k = threadIdx.x; k < rows; k += blockDim.x) {
+            const vx_contact& cc = A.contacts[A.order[s0 + k]];
+            const bool da = isDynamic(A.B.filt[cc.a].x), db = isDynamic(A.B.filt[cc.b].x);
+            S.rowIdx[k] = make_int2(da ? (int)localIdx[cc.a] : -1, db ? (int)localIdx[cc.b] : -1);
+        }
+        __syncthreads();
         const uint32_t g0 = A.islandSeg[isl], g1 = A.islandSeg[isl + 1];
         if (A.positionIterations > 0) {
             for (int it = 0; it < A.positionIterations; ++it)
                 for (uint32_t g = g0; g < g1; ++g) {
-                    for (uint32_t k = A.segStart[g] + threadIdx.x; k < A.segStart[g + 1]; k += blockDim.x)
-                        positionRow(A, A.order[k]);
+                    for (uint32_t k = A.segStart[g] - s0 + threadIdx.x; k < A.segStart[g + 1] - s0; k += blockDim.x)
+                        sharedRow(A, S, k, s0, 2);
                     __syncthreads();
                 }
-            continue;
-        }
-        const uint32_t b0 = isl < A.realIslands ? A.bodyStart[isl] : 0u;
-        const uint32_t b1 = isl < A.realIslands ? A.bodyStart[isl + 1] : 0u;
-        for (int s = 0; s < A.substeps; ++s) {
-            if (A.integrate && s > 0) {
-                for (uint32_t k = b0 + threadIdx.x; k < b1; k += blockDim.x)
-                    integrateVelocity(A.B, A.bodyOrder[k], A.gravity, A.h);
-                __syncthreads();
-            }
-            if (A.warmStart && s == 0)
-                for (uint32_t g = g0; g < g1; ++g) {
-                    for (uint32_t k = A.segStart[g] + threadIdx.x; k < A.segStart[g + 1]; k += blockDim.x)
-                        warmRow(A, A.order[k]);
+        } else {
+            for (int s = 0; s < A.substeps; ++s) {
+                if (A.integrate && s > 0) {
+                    for (uint32_t k = threadIdx.x; k < nb; k += blockDim.x)
+                        sharedIntegrateVelocity(A, S, (int)k, A.bodyOrder[b0 + k]);
                     __syncthreads();
                 }
-            for (int it = 0; it < A.sweeps; ++it)
-                for (uint32_t g = g0; g < g1; ++g) {
-                    for (uint32_t k = A.segStart[g] + threadIdx.x; k < A.segStart[g + 1]; k += blockDim.x)
-                        solveRowAt(A, A.order[k]);
+                if (A.warmStart && s == 0)
+                    for (uint32_t g = g0; g < g1; ++g) {
+                        for (uint32_t k = A.segStart[g] - s0 + threadIdx.x; k < A.segStart[g + 1] - s0; k += blockDim.x)
+                            sharedRow(A, S, k, s0, 0);
+                        __syncthreads();
+                    }
+                for (int it = 0; it < A.sweeps; ++it)
+                    for (uint32_t g = g0; g < g1; ++g) {
+                        for (uint32_t k = A.segStart[g] - s0 + threadIdx.x; k < A.segStart[g + 1] - s0; k += blockDim.x)
+                            sharedRow(A, S, k, s0, 1);
+                        __syncthreads();
+                    }
+                if (A.integrate) {
+                    for (uint32_t k = threadIdx.x; k < nb; k += blockDim.x) sharedIntegrateTransform(A, S, (int)k);
                     __syncthreads();
                 }
-            if (A.integrate) {
-                for (uint32_t k = b0 + threadIdx.x; k < b1; k += blockDim.x)
-                    integrateTransform(A.B, A.bodyOrder[k], A.h);
-                __syncthreads();
             }
         }
+        for (uint32_t k = threadIdx.x; k < nb; k += blockDim.x) {
+            const uint32_t id = A.bodyOrder[b0 + k];
+            A.B.pos[id] = S.p[k]; A.B.rot[id] = S.q[k]; A.B.vel[id] = S.v[k]; A.B.ang[id] = S.w[k];
+        }
+        __syncthreads();
     }
 }
 
@@ -1044,8 +1362,8 @@ __global__ void caProbeKernel(BodyArrays B, Soup soup, const uint64_t* pairKeys,
             const GapProbe end = gapAt(a, b, soup);
             if (end.gap < -8e-3f) {
                 flag = 1;
-                bodyMark[i] = 1;
-                bodyMark[j] = 1;
+                bodyMark[i] = 1;  // only dynamic bodies move in a rewind
+                if (isDynamic(b.flags)) bodyMark[j] = 1;
             }
         }
         flags[r] = flag;
@@ -1130,46 +1448,93 @@ __device__ __noinline__ bool caRewind(BodyArrays& B, const Soup& soup, uint32_t 
     return true;
 }
 
-// Serial pass in pair order over the candidates (flagged pairs and pairs
-// sharing a body with one). A pair is re-evaluated when it was flagged or
-// one of its bodies moved earlier in this pass; if a rewind moves a body
-// outside the candidate neighbourhood, every later pair is visited.
-__global__ void caSerialKernel(BodyArrays B, Soup soup, const uint64_t* pairKeys, uint32_t npairs,
-                               const uint32_t* flags, const uint32_t* candidateFlags, const uint32_t* candIndex,
-                               uint32_t ncand, const uint32_t* bodyMark, uint32_t* rewound, float dt,
-                               const float4* prevPos, const float4* prevRot, Counters* C) {
-    if (blockIdx.x != 0 || threadIdx.x != 0) return;
-    bool overflow = false;
-    uint32_t rewinds = 0;
-    uint32_t r = 0;
-    uint32_t ci = 0;
-    while (true) {
-        if (!overflow) {
-            if (ci >= ncand) break;
-            r = candIndex[ci++];
-        } else {
-            if (r >= npairs) break;
-        }
-        const uint64_t key = pairKeys[r];
-        const uint32_t ri = (uint32_t)(key >> 32), rj = (uint32_t)key;
-        const bool visit = flags[r] || rewound[ri] || rewound[rj];
-        if (visit) {
+// Rewind pass over one component of candidate pairs (candidates connected
+// through shared dynamic bodies), in pair order. Components share no dynamic
+// body, so running them concurrently equals the reference's single ordered
+// loop as long as no rewind moves a body outside the candidate set; that case
+// is flagged and the caller replays the whole pass serially from a snapshot.
+__global__ void caComponentKernel(BodyArrays B, Soup soup, const uint64_t* pairKeys, const uint32_t* flags,
+                                  const uint32_t* runStart, uint32_t runs, const uint32_t* members,
+                                  const uint32_t* bodyMark, uint32_t* rewound, float dt, const float4* prevPos,
+                                  const float4* prevRot, Counters* C) {
+    for (uint32_t run = blockIdx.x * blockDim.x + threadIdx.x; run < runs; run += gridDim.x * blockDim.x) {
+        uint32_t rewinds = 0;
+        for (uint32_t k = runStart[run]; k < runStart[run + 1]; ++k) {
+            const uint32_t r = members[k];
+            const uint64_t key = pairKeys[r];
+            const uint32_t ri = (uint32_t)(key >> 32), rj = (uint32_t)key;
+            if (!(flags[r] || rewound[ri] || rewound[rj])) continue;
             uint32_t i, j;
             orientPair(B, key, i, j);
             if (caRewind(B, soup, i, j, dt, prevPos, prevRot)) {
                 ++rewinds;
+                const bool jDyn = isDynamic(B.filt[j].x);
                 rewound[i] = 1;
-                if (isDynamic(B.filt[j].x)) rewound[j] = 1;
-                if (!overflow && (!bodyMark[i] || (isDynamic(B.filt[j].x) && !bodyMark[j]))) {
-                    overflow = true;
-                    C->caOverflow = 1;
-                }
+                if (jDyn) rewound[j] = 1;
+                if (!bodyMark[i] || (jDyn && !bodyMark[j])) atomicOr(&C->caOverflow, 1u);
             }
         }
-        if (overflow) ++r;
-        (void)candidateFlags;
+        if (rewinds) atomicAdd(&C->rewinds, rewinds);
     }
-    C->rewinds += rewinds;
+}
+
+// The reference's loop verbatim in pair order (one thread): the fallback when
+// a rewind cascades beyond the candidate neighbourhood.
+__global__ void caFullSerialKernel(BodyArrays B, Soup soup, const uint64_t* pairKeys, uint32_t npairs,
+                                   const uint32_t* flags, uint32_t* rewound, float dt, const float4* prevPos,
+                                   const float4* prevRot, Counters* C) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    uint32_t rewinds = 0;
+    for (uint32_t r = 0; r < npairs; ++r) {
+        const uint64_t key = pairKeys[r];
+        const uint32_t ri = (uint32_t)(key >> 32), rj = (uint32_t)key;
+        if (!(flags[r] || rewound[ri] || rewound[rj])) continue;
+        uint32_t i, j;
+        orientPair(B, key, i, j);
+        if (caRewind(B, soup, i, j, dt, prevPos, prevRot)) {
+            ++rewinds;
+            rewound[i] = 1;
+            if (isDynamic(B.filt[j].x)) rewound[j] = 1;
+        }
+    }
+    C->rewinds = rewinds;
+}
+
+__global__ void caUnionKernel(const BodyArrays B, const uint64_t* pairKeys, const uint32_t* cand, uint32_t ncand,
+                              uint32_t* parent, Counters* C) {
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < ncand; k += gridDim.x * blockDim.x) {
+        const uint64_t key = pairKeys[cand[k]];
+        const uint32_t a = (uint32_t)(key >> 32), b = (uint32_t)key;
+        if (!isDynamic(B.filt[a].x) || !isDynamic(B.filt[b].x)) continue;
+        for (uint32_t tries = 0;; ++tries) {
+            if (tries == kUnionRetryLimit) { atomicOr(&C->timeout, 1u); break; }
+            uint32_t x = ufFind(parent, a), y = ufFind(parent, b);
+            if (x == y) break;
+            if (x < y) { const uint32_t t = x; x = y; y = t; }
+            if (atomicCAS(&parent[x], x, y) == x) break;
+        }
+    }
+}
+
+__global__ void caKeyKernel(const BodyArrays B, const uint64_t* pairKeys, const uint32_t* cand, uint32_t ncand,
+                            const uint32_t* root, uint64_t* keys, uint32_t* vals) {
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < ncand; k += gridDim.x * blockDim.x) {
+        uint32_t i, j;
+        orientPair(B, pairKeys[cand[k]], i, j);
+        keys[k] = root[i];
+        vals[k] = cand[k];
+    }
+}
+
+__global__ void copyStateKernel(const BodyArrays B, uint32_t n, float4* snap, int restore) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        float4* s = snap + 4 * (size_t)i;
+        if (restore) {
+            B.pos[i] = s[0]; B.rot[i] = s[1]; B.vel[i] = s[2]; B.ang[i] = s[3];
+        } else {
+            s[0] = B.pos[i]; s[1] = B.rot[i]; s[2] = B.vel[i]; s[3] = B.ang[i];
+        }
+    }
 }
 
 // prefix ranks of candidate flags -> candidate index list
@@ -1299,6 +1664,23 @@ int loadBodies(Context& c, const vx_body* bodies, uint32_t n, const uint32_t* wo
         VXB_CUDA(c, cudaMemcpyAsync(c.planeListBuf.ptr, planeList.data(), planeList.size() * 4, cudaMemcpyHostToDevice,
                                     c.stream));
     VXB_CUDA(c, cudaStreamSynchronize(c.stream));  // host vectors above are freed on return
+    // Reserve step buffers up front so steady stepping never reallocates
+    // (cudaFree synchronises the device).
+    if (c.pairCap < 16u * n) c.pairCap = 16u * n + 4096u;
+    if (c.contactCap < 8u * n) c.contactCap = 8u * n + 4096u;
+    if (c.recCap < 8u * n) c.recCap = 8u * n + 4096u;
+    const size_t mcap = c.contactCap;
+    VXB_TRY(ensure(c, c.pairBuf, (size_t)c.pairCap * 8));
+    VXB_TRY(ensure(c, c.contactTmpBuf, mcap * sizeof(vx_contact)));
+    VXB_TRY(ensure(c, c.contactBuf[0], mcap * sizeof(vx_contact) + 128));
+    VXB_TRY(ensure(c, c.contactBuf[1], mcap * sizeof(vx_contact) + 128));
+    for (DevBuf* b : {&c.recValBuf, &c.recCountBuf, &c.recOffsetBuf, &c.islandValBuf, &c.colorBuf, &c.flagBuf,
+                      &c.scanBuf, &c.islandStartBuf, &c.segStartBuf, &c.islandSegBuf})
+        VXB_TRY(ensure(c, *b, mcap * 4 + 64));
+    for (DevBuf* b : {&c.recKeyBuf, &c.recInfoBuf, &c.pairKeyBuf, &c.prevKeyBuf, &c.islandKeyBuf, &c.colorKeyBuf,
+                      &c.sortKeysAlt})
+        VXB_TRY(ensure(c, *b, mcap * 8 + 64));
+    VXB_TRY(ensure(c, c.sortValsAlt, std::max<size_t>(mcap, (size_t)c.pairCap) * 4 + 64));
     c.prevCount = 0;
     c.backendContacts = 0;
     return VXB_OK;
@@ -1336,6 +1718,7 @@ static int broadPhase(Context& c, float dt, uint32_t* pairCount) {
     VXB_TRY(ensure(c, c.aabbBuf, (size_t)n * 32));
     float4* lo = P<float4>(c.aabbBuf);
     float4* hi = lo + n;
+    stageBegin(c, kStageBroadphase);
     LAUNCH(c, aabbKernel, std::min<uint32_t>(blocksFor(n, 256), (uint32_t)c.smCount * 8), 256, c.B, n, dt, lo, hi,
            c.dCounters);
     const int worldBits = bitsFor(c.worlds > 1 ? c.worlds - 1 : 0);
@@ -1347,7 +1730,11 @@ static int broadPhase(Context& c, float dt, uint32_t* pairCount) {
     uint32_t* vals = P<uint32_t>(c.cellValBuf);
     LAUNCH(c, keyKernel, blocksFor(n, 256), 256, c.B, n, c.worlds > 1 ? P<uint32_t>(c.worldOfBuf) : nullptr, lo, hi,
            c.dCounters, keys, vals, planeKey);
+    stageEnd(c, kStageBroadphase);
+    stageBegin(c, kStageCellSort);
     VXB_TRY(sortPairs(c, keys, vals, n, keyBitsTotal));
+    stageEnd(c, kStageCellSort);
+    stageBegin(c, kStageBroadphase);
     uint32_t hashCap = 1024;
     while (hashCap < 2 * n) hashCap <<= 1;
     c.hashCap = hashCap;
@@ -1365,6 +1752,7 @@ static int broadPhase(Context& c, float dt, uint32_t* pairCount) {
                P<uint32_t>(c.hashValBuf), hashCap - 1, planeKey,
                c.worlds > 1 ? P<uint32_t>(c.worldOfBuf) : nullptr, P<uint32_t>(c.planeStartBuf),
                P<uint32_t>(c.planeListBuf), P<uint64_t>(c.pairBuf), c.pairCap, c.dCounters);
+        stageEnd(c, kStageBroadphase);
         VXB_TRY(readCounters(c));
         if (c.hostCounters.pairs <= c.pairCap) break;
         c.pairCap = c.hostCounters.pairs + c.hostCounters.pairs / 4 + 1024;
@@ -1389,10 +1777,12 @@ static int narrowPhase(Context& c, const uint64_t* pairs, uint32_t npairs, float
         VXB_TRY(ensure(c, c.recInfoBuf, (size_t)c.recCap * 8));
         VXB_CUDA(c, cudaMemsetAsync(&c.dCounters->contactsTmp, 0, 8, c.stream));  // contactsTmp + records
         VXB_CUDA(c, cudaMemsetAsync(&c.dCounters->overflow, 0, 4, c.stream));
+        stageBegin(c, kStageNarrowphase);
         if (npairs)
             LAUNCH(c, collideKernel, std::min<uint32_t>(blocksFor(npairs, 128), (uint32_t)c.smCount * 16), 128, c.B,
                    soupOf(c), pairs, npairs, dt, mode, bodyBits, P<vx_contact>(c.contactTmpBuf), c.contactCap,
                    P<uint64_t>(c.recKeyBuf), P<uint32_t>(c.recValBuf), P<uint2>(c.recInfoBuf), c.recCap, c.dCounters);
+        stageEnd(c, kStageNarrowphase);
         VXB_TRY(readCounters(c));
         if (!(c.hostCounters.overflow & 2u)) break;
         c.contactCap = c.hostCounters.contactsTmp + c.hostCounters.contactsTmp / 4 + 1024;
@@ -1402,6 +1792,7 @@ static int narrowPhase(Context& c, const uint64_t* pairs, uint32_t npairs, float
     *contactCount = m;
     *recordCount = nrec;
     const int recBits = mode == 0 ? 2 * bodyBits : bitsFor(npairs);
+    stageBegin(c, kStagePlacement);
     VXB_TRY(sortPairs(c, P<uint64_t>(c.recKeyBuf), P<uint32_t>(c.recValBuf), nrec, recBits));
     VXB_TRY(ensure(c, c.recCountBuf, (size_t)nrec * 4 + 16));
     VXB_TRY(ensure(c, c.recOffsetBuf, (size_t)nrec * 4 + 16));
@@ -1416,6 +1807,7 @@ static int narrowPhase(Context& c, const uint64_t* pairs, uint32_t npairs, float
                P<uint32_t>(c.scanBuf), nrec, P<vx_contact>(c.contactTmpBuf), P<vx_contact>(c.contactBuf[c.cur]),
                (uint64_t*)nullptr, P<uint64_t>(c.pairKeyBuf), P<uint32_t>(c.recOffsetBuf));
     }
+    stageEnd(c, kStagePlacement);
     return VXB_OK;
 }
 
@@ -1445,7 +1837,7 @@ static int buildIslands(Context& c, const vx_contact* cs, uint32_t m, IslandPlan
         plan = IslandPlan{};
         VXB_CUDA(c, cudaMemsetAsync(c.islandOfBodyBuf.ptr, 0xff, (size_t)n * 4, c.stream));
     } else {
-        LAUNCH(c, unionKernel, blocksFor(m, 256), 256, cs, m, c.B, parent);
+        LAUNCH(c, unionKernel, blocksFor(m, 256), 256, cs, m, c.B, parent, c.dCounters);
         LAUNCH(c, compressKernel, blocksFor(n, 256), 256, parent, n);
         uint64_t* ikeys = P<uint64_t>(c.islandKeyBuf);
         uint32_t* ivals = P<uint32_t>(c.islandValBuf);
@@ -1532,8 +1924,16 @@ static int prepareSegments(Context& c, const IslandPlan& plan) {
 
 static void launchSolve(Context& c, const SolveArgs& A) {
     if (A.islands == 0) return;
-    LAUNCH(c, solveTinyKernel, blocksFor(A.islands, 128), 128, A);
-    LAUNCH(c, solveBlockKernel, std::min<uint32_t>(A.islands, (uint32_t)c.smCount * 8), 256, A);
+    LAUNCH(c, solveTinyKernel, blocksFor(A.islands, 64), 64, A);
+    static bool configured = false;
+    if (!configured) {
+        cudaFuncSetAttribute(solveBlockKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBlockSmem);
+        configured = true;
+    }
+    ensure(c, c.localIdxBuf, (size_t)c.n * 4 + 16);
+    solveBlockKernel<<<std::min<uint32_t>(A.islands, (uint32_t)c.smCount * 2), kBlockThreads, kBlockSmem, c.stream>>>(
+        A, P<uint32_t>(c.localIdxBuf));
+    ++c.launches;
 }
 
 // Substep loop over islands + contact-free bodies (advanceSubsteps).
@@ -1570,14 +1970,20 @@ static int conservativeAdvancement(Context& c, uint32_t npairs, float dt) {
     if (npairs == 0) return VXB_OK;
     const uint32_t n = c.n;
     VXB_TRY(ensure(c, c.caFlagBuf, (size_t)npairs * 8 + 16));
-    VXB_TRY(ensure(c, c.caBodyMarkBuf, (size_t)n * 8 + 16));
-    VXB_TRY(ensure(c, c.caCandBuf, (size_t)npairs * 8 + 16));
+    VXB_TRY(ensure(c, c.caBodyMarkBuf, (size_t)n * 12 + 16));
+    VXB_TRY(ensure(c, c.caCandBuf, (size_t)npairs * 24 + 16));
     uint32_t* flags = P<uint32_t>(c.caFlagBuf);
     uint32_t* candFlags = flags + npairs;
     uint32_t* bodyMark = P<uint32_t>(c.caBodyMarkBuf);
     uint32_t* rewound = bodyMark + n;
+    uint32_t* parent = rewound + n;
     uint32_t* ranks = P<uint32_t>(c.caCandBuf);
     uint32_t* candIndex = ranks + npairs;
+    uint32_t* runFlags = candIndex + npairs;
+    uint32_t* runIndex = runFlags + npairs;
+    uint32_t* runStart = runIndex + npairs;
+    uint32_t* members = runStart + npairs;  // sorted candidate values (aliases below)
+    (void)members;
     VXB_CUDA(c, cudaMemsetAsync(bodyMark, 0, (size_t)n * 8, c.stream));
     const uint64_t* pk = P<uint64_t>(c.pairKeyBuf);
     const float4* prevPos = P<float4>(c.prevPoseBuf);
@@ -1590,8 +1996,32 @@ static int conservativeAdvancement(Context& c, uint32_t npairs, float dt) {
     const uint32_t ncand = c.hostCounters.caCandidates;
     if (ncand == 0) return VXB_OK;
     LAUNCH(c, compactKernel, blocksFor(npairs, 256), 256, candFlags, ranks, npairs, candIndex);
-    LAUNCH(c, caSerialKernel, 1, 32, c.B, soupOf(c), pk, npairs, flags, candFlags, candIndex, ncand, bodyMark, rewound,
-           dt, prevPos, prevRot, c.dCounters);
+    // components of candidates through shared dynamic bodies
+    LAUNCH(c, iotaKernel, blocksFor(n, 256), 256, parent, n);
+    LAUNCH(c, caUnionKernel, blocksFor(ncand, 256), 256, c.B, pk, candIndex, ncand, parent, c.dCounters);
+    LAUNCH(c, compressKernel, blocksFor(n, 256), 256, parent, n);
+    const size_t valsOffset = ((size_t)ncand * 8 + 255) & ~(size_t)255;  // keep both arrays 256-byte aligned
+    VXB_TRY(ensure(c, c.islandInfoBuf, valsOffset + (size_t)ncand * 4 + 16));
+    uint64_t* ckeys = P<uint64_t>(c.islandInfoBuf);
+    uint32_t* cvals = reinterpret_cast<uint32_t*>(P<char>(c.islandInfoBuf) + valsOffset);
+    LAUNCH(c, caKeyKernel, blocksFor(ncand, 256), 256, c.B, pk, candIndex, ncand, parent, ckeys, cvals);
+    VXB_TRY(sortPairs(c, ckeys, cvals, ncand, bitsFor(n)));
+    LAUNCH(c, runFlagKernel, blocksFor(ncand, 256), 256, ckeys, ncand, runFlags);
+    VXB_TRY(exclusiveScan(c, runFlags, runIndex, ncand, &c.dCounters->segments));
+    LAUNCH(c, runStartKernel, blocksFor(ncand, 256), 256, runFlags, runIndex, ncand, runStart);
+    VXB_TRY(readCounters(c));
+    const uint32_t runs = c.hostCounters.segments;
+    VXB_TRY(ensure(c, c.snapBuf, (size_t)n * 64));
+    LAUNCH(c, copyStateKernel, blocksFor(n, 256), 256, c.B, n, P<float4>(c.snapBuf), 0);
+    LAUNCH(c, caComponentKernel, blocksFor(runs, 32), 32, c.B, soupOf(c), pk, flags, runStart, runs, cvals, bodyMark,
+           rewound, dt, prevPos, prevRot, c.dCounters);
+    VXB_TRY(readCounters(c));
+    if (c.hostCounters.caOverflow) {
+        LAUNCH(c, copyStateKernel, blocksFor(n, 256), 256, c.B, n, P<float4>(c.snapBuf), 1);
+        VXB_CUDA(c, cudaMemsetAsync(rewound, 0, (size_t)n * 4, c.stream));
+        LAUNCH(c, caFullSerialKernel, 1, 32, c.B, soupOf(c), pk, npairs, flags, rewound, dt, prevPos, prevRot,
+               c.dCounters);
+    }
     return VXB_OK;
 }
 
@@ -1606,21 +2036,33 @@ static int stepOnce(Context& c) {
     VXB_TRY(resetCounters(c));
     VXB_TRY(ensure(c, c.prevPoseBuf, (size_t)n * 32));
     float4* prevPos = P<float4>(c.prevPoseBuf);
+    stageBegin(c, kStagePrepare);
     LAUNCH(c, prepareKernel, blocksFor(n, 256), 256, c.B, n, g, h, prevPos, prevPos + n, 1);
+    stageEnd(c, kStagePrepare);
     uint32_t npairs = 0, m = 0, nrec = 0;
     VXB_TRY(broadPhase(c, dt, &npairs));
     c.stats.candidatePairs = npairs;
     VXB_TRY(narrowPhase(c, P<uint64_t>(c.pairBuf), npairs, dt, 0, &m, &nrec));
     vx_contact* cs = P<vx_contact>(c.contactBuf[c.cur]);
+    stageBegin(c, kStageWarmStart);
     if (c.prevCount && m)
         LAUNCH(c, matchKernel, blocksFor(m, 128), 128, cs, m, P<vx_contact>(c.contactBuf[c.cur ^ 1]),
                P<uint64_t>(c.prevKeyBuf), c.prevCount, c.dCounters);
+    stageEnd(c, kStageWarmStart);
     IslandPlan plan;
+    stageBegin(c, kStageIslands);
     VXB_TRY(buildIslands(c, cs, m, plan, nullptr));
     VXB_TRY(prepareSegments(c, plan));
+    stageEnd(c, kStageIslands);
+    stageBegin(c, kStageSolve);
     VXB_TRY(runSubsteps(c, cs, plan, g, h, substeps, cfg.solver, true, true));
+    stageEnd(c, kStageSolve);
+    stageBegin(c, kStageRewind);
     if (m) VXB_TRY(conservativeAdvancement(c, nrec, dt));
+    stageEnd(c, kStageRewind);
+    stageBegin(c, kStagePositions);
     VXB_TRY(positionCorrection(c, cs, plan, cfg.solver, h));
+    stageEnd(c, kStagePositions);
     LAUNCH(c, clearForcesKernel, blocksFor(n, 256), 256, c.B, n);
     // previous-contact cache: this step's contacts in (a, b, point) order
     VXB_TRY(ensure(c, c.prevKeyBuf, (size_t)m * 8 + 16));

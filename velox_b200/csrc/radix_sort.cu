@@ -1,17 +1,21 @@
 #include "radix_sort.cuh"
 
+#include <cstdint>
+
 namespace vxb {
 
 namespace {
 
 constexpr int kWarps = kSortThreads / 32;
 
+__device__ __forceinline__ bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
 // Stage [base, base + count) of keys into shared memory with 16-byte loads
-// where the alignment allows it.
+// when the address is 16-byte aligned (callers may pass sub-buffers).
 __device__ void stageKeys(const uint64_t* __restrict__ keys, uint32_t base, uint32_t count,
                           uint64_t* sk) {
     const uint32_t pairs = count / 2;
-    if ((base & 1u) == 0) {
+    if (aligned16(keys + base)) {
         const ulonglong2* src = reinterpret_cast<const ulonglong2*>(keys + base);
         for (uint32_t i = threadIdx.x; i < pairs; i += blockDim.x) {
             ulonglong2 v = src[i];
@@ -86,7 +90,7 @@ __global__ void scatterKernel(const uint64_t* __restrict__ keysIn, const uint32_
     const uint32_t base = tile * kSortTile;
     const uint32_t count = min((uint32_t)kSortTile, n - base);
     stageKeys(keysIn, base, count, sk);
-    if ((base & 3u) == 0) {
+    if (aligned16(valsIn + base)) {
         const uint4* src = reinterpret_cast<const uint4*>(valsIn + base);
         for (uint32_t i = threadIdx.x; i < count / 4; i += blockDim.x) {
             uint4 v = src[i];
