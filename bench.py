@@ -167,6 +167,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--size", type=int, default=100000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile", action="store_true",
+                    help="bracket the timed steps with cudaProfilerStart/Stop (ncu --profile-from-start off)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -207,6 +209,8 @@ def main():
     ctx.enable_timing(True)
     events = []
     contacts_total = 0
+    if args.profile:
+        torch.cuda.cudart().cudaProfilerStart()
     with torch.cuda.stream(stream):
         for _ in range(args.steps):
             flush.fill_(1)
@@ -217,6 +221,8 @@ def main():
             e1.record(stream)
             events.append((e0, e1))
             contacts_total += ctx.stats()["contacts"]
+    if args.profile:
+        torch.cuda.cudart().cudaProfilerStop()
     barrier()
     clocks = sampler.stop()
     launches = ctx.launches - launches0

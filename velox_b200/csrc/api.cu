@@ -101,7 +101,7 @@ void vxb_context_destroy(vxb_context* ctx) {
                            &c.colorKeyBuf, &c.maskBuf, &c.nextColorBuf, &c.islandStartBuf, &c.islandInfoBuf,
                            &c.flagBuf, &c.scanBuf, &c.scanTmp, &c.segStartBuf, &c.islandSegBuf, &c.bodyKeyBuf,
                            &c.bodyValBuf, &c.islandBodyStartBuf, &c.caFlagBuf, &c.caBodyMarkBuf, &c.caCandBuf,
-                           &c.localIdxBuf, &c.countersBuf};
+                           &c.localIdxBuf, &c.prepBuf, &c.frameBuf, &c.countersBuf};
     for (vxb::DevBuf* b : bufs)
         if (b->ptr) cudaFree(b->ptr);
     if (c.ownStream) cudaStreamDestroy(c.ownStream);

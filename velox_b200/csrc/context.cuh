@@ -19,6 +19,7 @@ struct IslandPlan {
     uint32_t islands = 0;      // including the null island when present
     uint32_t realIslands = 0;  // islands with a dynamic body
     uint32_t segments = 0;     // (island, colour) runs
+    uint32_t contacts = 0;     // contacts in the plan
     uint32_t freeFrom = 0, freeTo = 0;  // contact-free bodies (range in the island-sorted body order)
 };
 
@@ -30,7 +31,8 @@ struct DevBuf {
 
 // Device-side counters and flags (one small allocation, read back once per call).
 struct Counters {
-    uint32_t pairs;          // candidate pairs emitted (may exceed capacity)
+    uint32_t pairs;          // convex candidate pairs emitted (may exceed capacity)
+    uint32_t planePairs;     // body-plane candidate pairs emitted
     uint32_t contactsTmp;    // contacts appended by the narrow phase
     uint32_t records;        // pairs with at least one contact
     uint32_t contacts;       // contacts after placement (== contactsTmp when no overflow)
@@ -48,7 +50,7 @@ struct Counters {
     uint32_t cellMaxBits[3]; // ordered-int encodings of the maximum AABB centre
     uint32_t extentBits;     // float bits of the largest non-plane AABB extent
     uint32_t worldBits;      // bits of the world id in cell keys
-    uint32_t pad[8];
+    uint32_t pad[7];
 };
 
 // Pipeline stages timed with CUDA events when timing is enabled.
@@ -97,8 +99,11 @@ struct Context {
     DevBuf sortKeysAlt, sortValsAlt, sortHist;
     DevBuf hashKeyBuf, hashValBuf;
     uint32_t hashCap = 0;
-    DevBuf pairBuf;
+    DevBuf pairBuf;            // convex pairs, then plane pairs
     uint32_t pairCap = 0;
+    uint32_t convexPairs = 0;  // last broad phase: convex pairs at [0, convexPairs) of pairBuf
+    uint32_t planePairs = 0;   // and plane pairs at [pairCap, pairCap + planePairs)
+    std::vector<uint32_t> hostPlaneStart;
 
     // ---- narrow phase ----
     DevBuf contactTmpBuf;
@@ -124,6 +129,7 @@ struct Context {
     DevBuf bodyKeyBuf, bodyValBuf, islandBodyStartBuf;
     DevBuf caFlagBuf, caBodyMarkBuf, caCandBuf;
     DevBuf localIdxBuf;                 // island-local body index (block solve)
+    DevBuf prepBuf, frameBuf;           // per-row pose terms / per-body inertia frames (solve)
 
     DevBuf countersBuf;
     Counters* dCounters = nullptr;

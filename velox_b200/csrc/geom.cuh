@@ -98,6 +98,21 @@ VXD float maxPointSpeed(const BodyView& b) {
     return maxPointSpeedOf(shapeOf(b.flags), b.half, b.radius, b.hh, b.v, b.w);
 }
 
+// Bound on the distance from a body's position to any point of its shape
+// (the `ext` term of bodyAabb, narrowphase.h:371-390).
+VXD float coreExtent(uint32_t shape, const V3& half, float radius, float hh) {
+    switch (shape) {
+    case kBox: return length(half);
+    case kRoundedBox: return length(half) + radius;
+    case kEllipsoid: return vmax(half.x, vmax(half.y, half.z));
+    case kCapsule: return hh + radius;
+    case kSphere: case kHull: case kCompound: return radius;
+    case kCylinder: return sqrtf(radius * radius + hh * hh);
+    case kCone: return vmax(1.5f * hh, sqrtf(radius * radius + 0.25f * hh * hh));
+    default: return 0.0f;
+    }
+}
+
 // Swept AABB half width of bodyAabb (narrowphase.h:369-398) minus position.
 VXD float aabbReach(uint32_t flags, const V3& half, float radius, float hh, float margin,
                     const V3& v, const V3& w, float dt) {
@@ -1203,9 +1218,19 @@ struct SolverBody {
     V3 p; Q4 q; V3 v; V3 w;
     Mass m;
     bool sphere;
+    Q4 frame;  // inertiaFrameAt(q): constant while q is (one substep's sweeps)
 };
 
 VXD V3 invI(const SolverBody& b, const V3& v) { return invInertiaMulAt(b.m, v, b.q); }
+
+VXD void cacheFrame(SolverBody& b) { b.frame = inertiaFrameAt(b.m, b.q); }
+
+// invInertiaMulAt(b.m, v, b.q) with the frame cached by cacheFrame (same arithmetic).
+VXD V3 invIF(const SolverBody& b, const V3& v) {
+    if (!isDynamic(b.m.flags) || isRotationLocked(b.m.flags)) return V3{0.0f, 0.0f, 0.0f};
+    const V3 l = rotateInv(b.frame, v);
+    return rotate(b.frame, V3{l.x * b.m.invI.x, l.y * b.m.invI.y, l.z * b.m.invI.z});
+}
 
 // The contact fields the solver reads and writes.
 struct RowContact {
@@ -1240,7 +1265,7 @@ VXD void warmStartRow(SolverBody& a, SolverBody& b, RowContact& c) {
 // One sequential-impulse pass over one contact: normal row against the live
 // gap with restitution, then two-axis elliptic Coulomb friction (or the
 // coupled cone block), then rolling and spinning resistance.
-static __device__ __noinline__ void solveRow(SolverBody& a, SolverBody& b, RowContact& c, float dt, bool coneBlock) {
+static __device__ __forceinline__ void solveRow(SolverBody& a, SolverBody& b, RowContact& c, float dt, bool coneBlock) {
     const V3 pa = anchorWorld(a.sphere, a.p, a.q, c.la);
     const V3 pb = anchorWorld(b.sphere, b.p, b.q, c.lb);
     c.point = (pa + pb) * 0.5f;
@@ -1367,6 +1392,180 @@ static __device__ __noinline__ void solveRow(SolverBody& a, SolverBody& b, RowCo
         const V3 tq = c.normal * (next - old);
         if (dynA) a.w += invI(a, tq);
         if (dynB) b.w -= invI(b, tq);
+    }
+}
+
+// ---- solver rows split by what changes -------------------------------------
+//
+// Within one substep's warm start and sweeps only velocities and impulses
+// change; poses are fixed. Every pose-dependent quantity of solveRow (anchors,
+// arms, tangents, effective masses, the live gap) is therefore the same value
+// in every sweep. prepRow evaluates them once per substep with exactly the
+// expressions of solveRow, and sweepRow / warmPrepRow consume them, so the
+// results equal solveRow / warmStartRow bit for bit.
+
+struct RowPrep {
+    V3 ra, rb, point;
+    V3 raxn, rbxn, t1, t2, raxt1, rbxt1, raxt2, rbxt2;
+    float kNormal, liveGap, targetBase, k1, k2, kN1, kN2, k12, kr1, kr2, ks;
+};
+
+// Bodies must have their frames cached (cacheFrame) for the current poses.
+VXD void prepRow(const SolverBody& a, const SolverBody& b, const RowContact& c, float dt, bool coneBlock,
+                 RowPrep& P) {
+    const V3 pa = anchorWorld(a.sphere, a.p, a.q, c.la);
+    const V3 pb = anchorWorld(b.sphere, b.p, b.q, c.lb);
+    P.point = (pa + pb) * 0.5f;
+    P.ra = pa - a.p;
+    P.rb = pb - b.p;
+    const float ima = solverInvMass(a.m), imb = solverInvMass(b.m);
+    P.raxn = cross(P.ra, c.normal);
+    P.rbxn = cross(P.rb, c.normal);
+    P.kNormal = ima + imb + dot(P.raxn, invIF(a, P.raxn)) + dot(P.rbxn, invIF(b, P.rbxn));
+    P.liveGap = c.bias0 + dot(c.normal, pa - pb);
+    P.targetBase = P.liveGap > 0.0f ? -P.liveGap / dt : 0.0f;
+    contactTangents(c.normal, P.t1, P.t2);
+    P.raxt1 = cross(P.ra, P.t1); P.rbxt1 = cross(P.rb, P.t1);
+    P.raxt2 = cross(P.ra, P.t2); P.rbxt2 = cross(P.rb, P.t2);
+    P.k1 = ima + imb + dot(P.raxt1, invIF(a, P.raxt1)) + dot(P.rbxt1, invIF(b, P.rbxt1));
+    P.k2 = ima + imb + dot(P.raxt2, invIF(a, P.raxt2)) + dot(P.rbxt2, invIF(b, P.rbxt2));
+    P.kN1 = dot(P.raxn, invIF(a, P.raxt1)) + dot(P.rbxn, invIF(b, P.rbxt1));
+    P.kN2 = dot(P.raxn, invIF(a, P.raxt2)) + dot(P.rbxn, invIF(b, P.rbxt2));
+    P.k12 = coneBlock ? dot(P.raxt1, invIF(a, P.raxt2)) + dot(P.rbxt1, invIF(b, P.rbxt2)) : 0.0f;
+    P.kr1 = c.rolling > 0.0f ? dot(P.t1, invIF(a, P.t1)) + dot(P.t1, invIF(b, P.t1)) : 0.0f;
+    P.kr2 = c.rolling > 0.0f ? dot(P.t2, invIF(a, P.t2)) + dot(P.t2, invIF(b, P.t2)) : 0.0f;
+    P.ks = c.spinning > 0.0f ? dot(c.normal, invIF(a, c.normal)) + dot(c.normal, invIF(b, c.normal)) : 0.0f;
+}
+
+// warmStartContact with prepared arms (narrowphase.h:80-124).
+VXD void warmPrepRow(SolverBody& a, SolverBody& b, RowContact& c, const RowPrep& P) {
+    if (c.nImp <= 0.0f && c.t1Imp == 0.0f && c.t2Imp == 0.0f && c.r1Imp == 0.0f && c.r2Imp == 0.0f &&
+        c.sImp == 0.0f)
+        return;
+    c.point = P.point;
+    const V3 impulse = c.normal * c.nImp + P.t1 * c.t1Imp + P.t2 * c.t2Imp;
+    const V3 angular = P.t1 * c.r1Imp + P.t2 * c.r2Imp + c.normal * c.sImp;
+    if (isDynamic(a.m.flags)) {
+        a.v += impulse * solverInvMass(a.m);
+        a.w += invIF(a, cross(P.ra, impulse));
+        a.w += invIF(a, angular);
+    }
+    if (isDynamic(b.m.flags)) {
+        b.v -= impulse * solverInvMass(b.m);
+        b.w -= invIF(b, cross(P.rb, impulse));
+        b.w -= invIF(b, angular);
+    }
+}
+
+// One sweep of solveContact (narrowphase.h:130-366) with prepared pose terms.
+VXD void sweepRow(SolverBody& a, SolverBody& b, RowContact& c, const RowPrep& P, bool coneBlock) {
+    c.point = P.point;
+    if (P.kNormal <= 0.0f) return;
+    const float ima = solverInvMass(a.m), imb = solverInvMass(b.m);
+    const bool dynA = isDynamic(a.m.flags), dynB = isDynamic(b.m.flags);
+    const float vn = dot((a.v + cross(a.w, P.ra)) - (b.v + cross(b.w, P.rb)), c.normal);
+    float target = P.targetBase;
+    if (c.vn0 < -1.0f && (P.liveGap <= 0.0f || vn > 0.0f)) target = vmax(target, -c.restitution * c.vn0);
+    if (!coneBlock) {
+        float jn = (target - vn) / P.kNormal;
+        const float nextNormal = vmax(c.nImp + jn, 0.0f);
+        jn = nextNormal - c.nImp;
+        c.nImp = nextNormal;
+        const V3 ni = c.normal * jn;
+        if (dynA) { a.v += ni * ima; a.w += invIF(a, cross(P.ra, ni)); }
+        if (dynB) { b.v -= ni * imb; b.w -= invIF(b, cross(P.rb, ni)); }
+        if (P.k1 > 0.0f && P.k2 > 0.0f) {
+            const V3 rv = (a.v + cross(a.w, P.ra)) - (b.v + cross(b.w, P.rb));
+            const float old1 = c.t1Imp, old2 = c.t2Imp;
+            float next1 = old1 - dot(rv, P.t1) / P.k1;
+            float next2 = old2 - dot(rv, P.t2) / P.k2;
+            const float max1 = c.friction1 * c.nImp;
+            const float max2 = c.friction2 * c.nImp;
+            if (max1 <= 0.0f) next1 = 0.0f;
+            if (max2 <= 0.0f) next2 = 0.0f;
+            const float ellipse = (max1 > 0.0f ? next1 * next1 / (max1 * max1) : 0.0f) +
+                                  (max2 > 0.0f ? next2 * next2 / (max2 * max2) : 0.0f);
+            if (ellipse > 1.0f) {
+                const float sc = 1.0f / sqrtf(ellipse);
+                next1 *= sc;
+                next2 *= sc;
+            }
+            c.t1Imp = next1;
+            c.t2Imp = next2;
+            const V3 fi = P.t1 * (next1 - old1) + P.t2 * (next2 - old2);
+            if (dynA) { a.v += fi * ima; a.w += invIF(a, cross(P.ra, fi)); }
+            if (dynB) { b.v -= fi * imb; b.w -= invIF(b, cross(P.rb, fi)); }
+        }
+    } else {
+        const float oldNormal = c.nImp;
+        const float old1 = c.t1Imp, old2 = c.t2Imp;
+        float nextNormal = oldNormal, next1 = old1, next2 = old2;
+        if (P.k1 > 0.0f && P.k2 > 0.0f) {
+            const float kNormal = P.kNormal, k1 = P.k1, k2 = P.k2, kN1 = P.kN1, kN2 = P.kN2, k12 = P.k12;
+            const float det = kNormal * (k1 * k2 - k12 * k12) - kN1 * (kN1 * k2 - kN2 * k12) +
+                              kN2 * (kN1 * k12 - kN2 * k1);
+            if (fabsf(det) > 1e-12f) {
+                const V3 rv = (a.v + cross(a.w, P.ra)) - (b.v + cross(b.w, P.rb));
+                const float bN = target - dot(rv, c.normal);
+                const float b1 = -dot(rv, P.t1);
+                const float b2 = -dot(rv, P.t2);
+                const float dN = (bN * (k1 * k2 - k12 * k12) + b1 * (kN2 * k12 - kN1 * k2) +
+                                  b2 * (kN1 * k12 - kN2 * k1)) / det;
+                const float d1 = (bN * (kN2 * k12 - kN1 * k2) + b1 * (kNormal * k2 - kN2 * kN2) +
+                                  b2 * (kN1 * kN2 - kNormal * k12)) / det;
+                const float d2 = (bN * (kN1 * k12 - kN2 * k1) + b1 * (kN1 * kN2 - kNormal * k12) +
+                                  b2 * (kNormal * k1 - kN1 * kN1)) / det;
+                nextNormal = vmax(oldNormal + dN, 0.0f);
+                next1 = old1 + d1;
+                next2 = old2 + d2;
+            }
+        }
+        const float max1 = c.friction1 * nextNormal;
+        const float max2 = c.friction2 * nextNormal;
+        if (max1 <= 0.0f) next1 = 0.0f;
+        if (max2 <= 0.0f) next2 = 0.0f;
+        const float ellipse = (max1 > 0.0f ? next1 * next1 / (max1 * max1) : 0.0f) +
+                              (max2 > 0.0f ? next2 * next2 / (max2 * max2) : 0.0f);
+        if (ellipse > 1.0f) {
+            const float sc = 1.0f / sqrtf(ellipse);
+            next1 *= sc;
+            next2 *= sc;
+        }
+        c.nImp = nextNormal;
+        c.t1Imp = next1;
+        c.t2Imp = next2;
+        const V3 imp = c.normal * (nextNormal - oldNormal) + P.t1 * (next1 - old1) + P.t2 * (next2 - old2);
+        if (dynA) { a.v += imp * ima; a.w += invIF(a, cross(P.ra, imp)); }
+        if (dynB) { b.v -= imp * imb; b.w -= invIF(b, cross(P.rb, imp)); }
+    }
+    if (c.rolling > 0.0f && P.kr1 > 0.0f && P.kr2 > 0.0f) {
+        const V3 wr = a.w - b.w;
+        const float o1 = c.r1Imp, o2 = c.r2Imp;
+        float n1 = o1 - dot(wr, P.t1) / P.kr1;
+        float n2 = o2 - dot(wr, P.t2) / P.kr2;
+        const float limit = c.rolling * c.nImp;
+        const float mag = sqrtf(n1 * n1 + n2 * n2);
+        if (mag > limit && mag > 1e-9f) {
+            const float sc = limit / mag;
+            n1 *= sc;
+            n2 *= sc;
+        }
+        c.r1Imp = n1;
+        c.r2Imp = n2;
+        const V3 tq = P.t1 * (n1 - o1) + P.t2 * (n2 - o2);
+        if (dynA) a.w += invIF(a, tq);
+        if (dynB) b.w -= invIF(b, tq);
+    }
+    if (c.spinning > 0.0f && P.ks > 0.0f) {
+        const V3 wr = a.w - b.w;
+        const float old = c.sImp;
+        float next = old - dot(wr, c.normal) / P.ks;
+        const float limit = c.spinning * c.nImp;
+        next = vclamp(next, -limit, limit);
+        c.sImp = next;
+        const V3 tq = c.normal * (next - old);
+        if (dynA) a.w += invIF(a, tq);
+        if (dynB) b.w -= invIF(b, tq);
     }
 }
 

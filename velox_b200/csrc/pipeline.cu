@@ -422,8 +422,8 @@ VXD uint32_t cellLookup(const uint64_t* hk, const uint32_t* hv, uint32_t mask, u
     return 0xffffffffu;
 }
 
-VXD void emitPair(uint64_t pair, uint64_t* pairs, uint32_t cap, Counters* C) {
-    const uint32_t slot = aggregatedSlot(&C->pairs);
+VXD void emitPair(uint64_t pair, uint64_t* pairs, uint32_t cap, uint32_t* counter, Counters* C) {
+    const uint32_t slot = aggregatedSlot(counter);
     if (slot < cap) pairs[slot] = pair;
     else atomicOr(&C->overflow, 1u);
 }
@@ -434,7 +434,7 @@ VXD void emitPair(uint64_t pair, uint64_t* pairs, uint32_t cap, Counters* C) {
 __global__ void pairKernel(BodyArrays B, uint32_t n, const uint64_t* keys, const uint32_t* vals, const float4* lo,
                            const float4* hi, const uint64_t* hk, const uint32_t* hv, uint32_t mask, uint64_t planeKey,
                            const uint32_t* worldOf, const uint32_t* planeStart, const uint32_t* planeList,
-                           uint64_t* pairs, uint32_t cap, Counters* C) {
+                           uint64_t* pairs, uint32_t cap, uint64_t* planePairs, uint32_t planeCap, Counters* C) {
     for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
         const uint64_t key = keys[s];
         if (key == planeKey) continue;
@@ -460,7 +460,7 @@ __global__ void pairKernel(BodyArrays B, uint32_t n, const uint64_t* keys, const
                         const uint4 fj = B.filt[j];
                         if (inert(fi.x) && inert(fj.x)) continue;
                         if (!canCollide(fi.y, fi.z, (int32_t)fi.w, fj.y, fj.z, (int32_t)fj.w)) continue;
-                        emitPair(((uint64_t)i << 32) | j, pairs, cap, C);
+                        emitPair(((uint64_t)i << 32) | j, pairs, cap, &C->pairs, C);
                     }
                 }
         const uint32_t w = worldOf ? worldOf[i] : 0u;
@@ -471,7 +471,7 @@ __global__ void pairKernel(BodyArrays B, uint32_t n, const uint64_t* keys, const
             const uint32_t a = i < p ? i : p, b = i < p ? p : i;
             const uint4 fa = a == i ? fi : fp, fb = a == i ? fp : fi;
             if (!canCollide(fa.y, fa.z, (int32_t)fa.w, fb.y, fb.z, (int32_t)fb.w)) continue;
-            emitPair(((uint64_t)a << 32) | b, pairs, cap, C);
+            emitPair(((uint64_t)a << 32) | b, planePairs, planeCap, &C->planePairs, C);
         }
     }
 }
@@ -490,6 +490,11 @@ VXD bool pointLess(const vx_contact& x, const vx_contact& y) {
 // pair's contacts by point (the host sort of src/backend_cuda.cu:587-595
 // within one (a, b) key), append them and a record keyed for the global sort.
 // mode 0: key = (a << bodyBits) | b; mode 1: key = pair index, emission order kept.
+// Which pair classes one instantiation handles: plane pairs compile to a
+// light kernel (high occupancy), convex pairs to the GJK/EPA kernel.
+enum PairClass : int { kAnyPairs = 0, kPlanePairs = 1, kConvexPairs = 2 };
+
+template <int Class>
 __global__ void __launch_bounds__(128) collideKernel(BodyArrays B, Soup soup, const uint64_t* pairs,
                                                      uint32_t npairs, float dt, int mode, int bodyBits,
                                                      vx_contact* tmp, uint32_t contactCap, uint64_t* recKeys,
@@ -506,7 +511,14 @@ __global__ void __launch_bounds__(128) collideKernel(BodyArrays B, Soup soup, co
             const uint32_t i = (uint32_t)(pr >> 32), j = (uint32_t)pr;
             const BodyView a = loadView(B, i);
             const BodyView b = loadView(B, j);
-            count = collidePair(a, b, i, j, soup, dt, buf, kMaxContactsPerPair);
+            if (Class == kAnyPairs) {
+                count = collidePair(a, b, i, j, soup, dt, buf, kMaxContactsPerPair);
+            } else if (Class == kPlanePairs) {
+                if (shapeOf(b.flags) == kPlane) planeConvex(a, b, i, j, soup, dt, buf, kMaxContactsPerPair, count);
+                else planeConvex(b, a, j, i, soup, dt, buf, kMaxContactsPerPair, count);
+            } else {
+                convexConvex(a, b, i, j, soup, dt, buf, kMaxContactsPerPair, count);
+            }
             if (mode == 0)
                 for (int x = 1; x < count; ++x) {
                     vx_contact key = buf[x];
@@ -900,6 +912,8 @@ struct SolveArgs {
     int coneBlock;
     uint32_t tinyLimit;
     int positionIterations;  // position-correction mode when > 0
+    RowPrep* prep;           // per solve-order row, rebuilt every substep (block / global paths)
+    float4* frames;          // per body inertia frame, rebuilt every substep (global path)
     int stackStabilization;
     float stackStiffness, stackDamping;
 };
@@ -1069,15 +1083,19 @@ __global__ void __launch_bounds__(64) solveTinyKernel(SolveArgs A) {
                 if (isDynamic(bodies[i].s.m.flags)) A.B.pos[bodies[i].id] = pack(bodies[i].s.p, 0.0f);
             continue;
         }
+        RowPrep prep[kTinyContacts];
         for (int s = 0; s < A.substeps; ++s) {
             if (A.integrate && s > 0)
                 for (int i = 0; i < nb; ++i) localIntegrateVelocity(bodies[i], A.gravity, A.h);
+            for (int i = 0; i < nb; ++i) cacheFrame(bodies[i].s);
+            for (uint32_t k = 0; k < count; ++k)
+                if (live[k]) prepRow(bodies[ra[k]].s, bodies[rb[k]].s, rows[k], A.h, A.coneBlock != 0, prep[k]);
             if (A.warmStart && s == 0)
                 for (uint32_t k = 0; k < count; ++k)
-                    if (live[k]) warmStartRow(bodies[ra[k]].s, bodies[rb[k]].s, rows[k]);
+                    if (live[k]) warmPrepRow(bodies[ra[k]].s, bodies[rb[k]].s, rows[k], prep[k]);
             for (int it = 0; it < A.sweeps; ++it)
                 for (uint32_t k = 0; k < count; ++k)
-                    if (live[k]) solveRow(bodies[ra[k]].s, bodies[rb[k]].s, rows[k], A.h, A.coneBlock != 0);
+                    if (live[k]) sweepRow(bodies[ra[k]].s, bodies[rb[k]].s, rows[k], prep[k], A.coneBlock != 0);
             if (A.integrate)
                 for (int i = 0; i < nb; ++i) localIntegrateTransform(bodies[i], A.h);
         }
@@ -1100,11 +1118,11 @@ __global__ void __launch_bounds__(64) solveTinyKernel(SolveArgs A) {
 constexpr int kBlockThreads = 256;
 constexpr int kBlockBodies = 512;
 constexpr int kBlockRows = 3072;
-constexpr size_t kBlockSmem = (size_t)kBlockBodies * (6 * sizeof(float4) + sizeof(uint32_t)) +
+constexpr size_t kBlockSmem = (size_t)kBlockBodies * (7 * sizeof(float4) + sizeof(uint32_t)) +
                               (size_t)kBlockRows * sizeof(int2);
 
 struct SharedBodies {
-    float4 *p, *q, *v, *w, *inertia, *iq;
+    float4 *p, *q, *v, *w, *inertia, *iq, *frame;
     uint32_t* flags;
     int2* rowIdx;  // per island row: local index of a / b, -1 = read-only global body
 };
@@ -1117,7 +1135,8 @@ VXD SharedBodies carve(float4* base) {
     S.w = S.v + kBlockBodies;
     S.inertia = S.w + kBlockBodies;
     S.iq = S.inertia + kBlockBodies;
-    S.flags = reinterpret_cast<uint32_t*>(S.iq + kBlockBodies);
+    S.frame = S.iq + kBlockBodies;
+    S.flags = reinterpret_cast<uint32_t*>(S.frame + kBlockBodies);
     S.rowIdx = reinterpret_cast<int2*>(S.flags + kBlockBodies);
     return S;
 }
@@ -1134,15 +1153,23 @@ VXD SolverBody sharedBody(const SharedBodies& S, int li) {
     b.m.iq = q4(S.iq[li]);
     b.m.flags = S.flags[li];
     b.sphere = shapeOf(b.m.flags) == kSphere;
+    b.frame = q4(S.frame[li]);
     return b;
 }
 
-// op: 0 warm start, 1 velocity row, 2 position row
+// A body outside the island's shared copy (static endpoints): frame computed here.
+VXD SolverBody globalBody(const BodyArrays& B, uint32_t id) {
+    SolverBody b = loadSolverBody(B, id);
+    cacheFrame(b);
+    return b;
+}
+
+// op: 0 warm start, 1 velocity sweep, 2 position row, 3 prepare (pose terms)
 VXD void sharedRow(const SolveArgs& A, const SharedBodies& S, uint32_t k, uint32_t s0, int op) {
     vx_contact& cc = A.contacts[A.order[s0 + k]];
     const int2 li = S.rowIdx[k];
-    SolverBody a = li.x >= 0 ? sharedBody(S, li.x) : loadSolverBody(A.B, cc.a);
-    SolverBody b = li.y >= 0 ? sharedBody(S, li.y) : loadSolverBody(A.B, cc.b);
+    SolverBody a = li.x >= 0 ? sharedBody(S, li.x) : globalBody(A.B, cc.a);
+    SolverBody b = li.y >= 0 ? sharedBody(S, li.y) : globalBody(A.B, cc.b);
     if (!solvedContact(a.m.flags, b.m.flags)) return;
     if (op == 2) {
         const float ima = solverInvMass(a.m), imb = solverInvMass(b.m);
@@ -1163,8 +1190,13 @@ VXD void sharedRow(const SolveArgs& A, const SharedBodies& S, uint32_t k, uint32
     }
     RowContact r;
     loadRow(cc, r);
-    if (op == 0) warmStartRow(a, b, r);
-    else solveRow(a, b, r, A.h, A.coneBlock != 0);
+    RowPrep& P = A.prep[s0 + k];
+    if (op == 3) {  // prepare
+        prepRow(a, b, r, A.h, A.coneBlock != 0, P);
+        return;
+    }
+    if (op == 0) warmPrepRow(a, b, r, P);
+    else sweepRow(a, b, r, P, A.coneBlock != 0);
     if (li.x >= 0 && isDynamic(a.m.flags)) { S.v[li.x] = pack(a.v, 0.0f); S.w[li.x] = pack(a.w, 0.0f); }
     if (li.y >= 0 && isDynamic(b.m.flags)) { S.v[li.y] = pack(b.v, 0.0f); S.w[li.y] = pack(b.w, 0.0f); }
     storeRow(cc, r);
@@ -1192,6 +1224,30 @@ VXD void sharedIntegrateTransform(const SolveArgs& A, const SharedBodies& S, int
     S.w[li] = pack(b.w, 0.0f);
 }
 
+// Island bodies read from global memory with frames from A.frames.
+VXD SolverBody framedBody(const SolveArgs& A, uint32_t id) {
+    SolverBody b = loadSolverBody(A.B, id);
+    if (isDynamic(b.m.flags)) b.frame = q4(A.frames[id]);
+    else cacheFrame(b);
+    return b;
+}
+
+// op: 0 warm start, 1 velocity sweep, 3 prepare
+VXD void globalRow(const SolveArgs& A, uint32_t pos, int op) {
+    vx_contact& cc = A.contacts[A.order[pos]];
+    SolverBody a = framedBody(A, cc.a), b = framedBody(A, cc.b);
+    if (!solvedContact(a.m.flags, b.m.flags)) return;
+    RowContact r;
+    loadRow(cc, r);
+    RowPrep& P = A.prep[pos];
+    if (op == 3) { prepRow(a, b, r, A.h, A.coneBlock != 0, P); return; }
+    if (op == 0) warmPrepRow(a, b, r, P);
+    else sweepRow(a, b, r, P, A.coneBlock != 0);
+    if (isDynamic(a.m.flags)) { A.B.vel[cc.a] = pack(a.v, 0.0f); A.B.ang[cc.a] = pack(a.w, 0.0f); }
+    if (isDynamic(b.m.flags)) { A.B.vel[cc.b] = pack(b.v, 0.0f); A.B.ang[cc.b] = pack(b.w, 0.0f); }
+    storeRow(cc, r);
+}
+
 __device__ void solveIslandGlobal(const SolveArgs& A, uint32_t isl) {
     const uint32_t g0 = A.islandSeg[isl], g1 = A.islandSeg[isl + 1];
     if (A.positionIterations > 0) {
@@ -1203,24 +1259,28 @@ __device__ void solveIslandGlobal(const SolveArgs& A, uint32_t isl) {
             }
         return;
     }
+    const uint32_t s0 = A.islandStart[isl], s1 = A.islandStart[isl + 1];
     const uint32_t b0 = isl < A.realIslands ? A.bodyStart[isl] : 0u;
     const uint32_t b1 = isl < A.realIslands ? A.bodyStart[isl + 1] : 0u;
     for (int s = 0; s < A.substeps; ++s) {
-        if (A.integrate && s > 0) {
-            for (uint32_t k = b0 + threadIdx.x; k < b1; k += blockDim.x)
-                integrateVelocity(A.B, A.bodyOrder[k], A.gravity, A.h);
-            __syncthreads();
+        for (uint32_t k = b0 + threadIdx.x; k < b1; k += blockDim.x) {
+            const uint32_t id = A.bodyOrder[k];
+            if (A.integrate && s > 0) integrateVelocity(A.B, id, A.gravity, A.h);
+            A.frames[id] = pack(inertiaFrameAt(loadMass(A.B, id), q4(A.B.rot[id])));
         }
+        __syncthreads();
+        for (uint32_t k = s0 + threadIdx.x; k < s1; k += blockDim.x) globalRow(A, k, 3);
+        __syncthreads();
         if (A.warmStart && s == 0)
             for (uint32_t g = g0; g < g1; ++g) {
                 for (uint32_t k = A.segStart[g] + threadIdx.x; k < A.segStart[g + 1]; k += blockDim.x)
-                    warmRow(A, A.order[k]);
+                    globalRow(A, k, 0);
                 __syncthreads();
             }
         for (int it = 0; it < A.sweeps; ++it)
             for (uint32_t g = g0; g < g1; ++g) {
                 for (uint32_t k = A.segStart[g] + threadIdx.x; k < A.segStart[g + 1]; k += blockDim.x)
-                    solveRowAt(A, A.order[k]);
+                    globalRow(A, k, 1);
                 __syncthreads();
             }
         if (A.integrate) {
@@ -1267,11 +1327,21 @@ __global__ void __launch_bounds__(kBlockThreads) solveBlockKernel(SolveArgs A, u
                 }
         } else {
             for (int s = 0; s < A.substeps; ++s) {
-                if (A.integrate && s > 0) {
+                if (A.integrate && s > 0)
                     for (uint32_t k = threadIdx.x; k < nb; k += blockDim.x)
                         sharedIntegrateVelocity(A, S, (int)k, A.bodyOrder[b0 + k]);
-                    __syncthreads();
+                for (uint32_t k = threadIdx.x; k < nb; k += blockDim.x) {
+                    Mass m;
+                    const float4 in = S.inertia[k];
+                    m.invI = V3{in.x, in.y, in.z};
+                    m.invMass = in.w;
+                    m.iq = q4(S.iq[k]);
+                    m.flags = S.flags[k];
+                    S.frame[k] = pack(inertiaFrameAt(m, q4(S.q[k])));
                 }
+                __syncthreads();
+                for (uint32_t k = threadIdx.x; k < rows; k += blockDim.x) sharedRow(A, S, k, s0, 3);
+                __syncthreads();
                 if (A.warmStart && s == 0)
                     for (uint32_t g = g0; g < g1; ++g) {
                         for (uint32_t k = A.segStart[g] - s0 + threadIdx.x; k < A.segStart[g + 1] - s0; k += blockDim.x)
@@ -1358,7 +1428,15 @@ __global__ void caProbeKernel(BodyArrays B, Soup soup, const uint64_t* pairKeys,
         orientPair(B, pairKeys[r], i, j);
         const BodyView a = loadView(B, i), b = loadView(B, j);
         uint32_t flag = 0;
-        if (caEligible(a, b, B, i)) {
+        bool separated = false;
+        if (shapeOf(b.flags) != kPlane) {
+            // Bounding spheres apart by more than 1 mm: the end gap is positive,
+            // so the reference's `gap >= -8 mm` test skips the pair.
+            const float reach = coreExtent(shapeOf(a.flags), a.half, a.radius, a.hh) +
+                                coreExtent(shapeOf(b.flags), b.half, b.radius, b.hh) + 1e-3f;
+            separated = lengthSq(a.p - b.p) > reach * reach;
+        }
+        if (!separated && caEligible(a, b, B, i)) {
             const GapProbe end = gapAt(a, b, soup);
             if (end.gap < -8e-3f) {
                 flag = 1;
@@ -1657,6 +1735,7 @@ int loadBodies(Context& c, const vx_body* bodies, uint32_t n, const uint32_t* wo
     VXB_TRY(ensure(c, c.worldOfBuf, (size_t)n * 4));
     VXB_TRY(ensure(c, c.planeStartBuf, planeStart.size() * 4));
     VXB_TRY(ensure(c, c.planeListBuf, planeList.size() * 4 + 4));
+    c.hostPlaneStart = planeStart;
     VXB_CUDA(c, cudaMemcpyAsync(c.worldOfBuf.ptr, c.hostWorldOf.data(), (size_t)n * 4, cudaMemcpyHostToDevice, c.stream));
     VXB_CUDA(c, cudaMemcpyAsync(c.planeStartBuf.ptr, planeStart.data(), planeStart.size() * 4, cudaMemcpyHostToDevice,
                                 c.stream));
@@ -1744,20 +1823,32 @@ static int broadPhase(Context& c, float dt, uint32_t* pairCount) {
     LAUNCH(c, cellTableKernel, blocksFor(n, 256), 256, keys, n, planeKey, P<uint64_t>(c.hashKeyBuf),
            P<uint32_t>(c.hashValBuf), hashCap - 1);
     if (c.pairCap == 0) c.pairCap = std::max<uint32_t>(n * 8u, 4096u);
+    // plane pairs: at most bodies x planes of a world
+    uint32_t planeCap = 16;
+    {
+        uint32_t maxPlanes = 0;
+        for (uint32_t w = 0; w < c.worlds; ++w) maxPlanes = std::max(maxPlanes, c.hostPlaneStart[w + 1] - c.hostPlaneStart[w]);
+        planeCap = std::max<uint32_t>(16u, n * std::max<uint32_t>(maxPlanes, 1u));
+    }
     for (int attempt = 0; attempt < 3; ++attempt) {
-        VXB_TRY(ensure(c, c.pairBuf, (size_t)c.pairCap * 8));
+        VXB_TRY(ensure(c, c.pairBuf, ((size_t)c.pairCap + planeCap) * 8));
         VXB_CUDA(c, cudaMemsetAsync(&c.dCounters->pairs, 0, 4, c.stream));
+        VXB_CUDA(c, cudaMemsetAsync(&c.dCounters->planePairs, 0, 4, c.stream));
         VXB_CUDA(c, cudaMemsetAsync(&c.dCounters->overflow, 0, 4, c.stream));
         LAUNCH(c, pairKernel, blocksFor(n, 128), 128, c.B, n, keys, vals, lo, hi, P<uint64_t>(c.hashKeyBuf),
                P<uint32_t>(c.hashValBuf), hashCap - 1, planeKey,
                c.worlds > 1 ? P<uint32_t>(c.worldOfBuf) : nullptr, P<uint32_t>(c.planeStartBuf),
-               P<uint32_t>(c.planeListBuf), P<uint64_t>(c.pairBuf), c.pairCap, c.dCounters);
+               P<uint32_t>(c.planeListBuf), P<uint64_t>(c.pairBuf), c.pairCap, P<uint64_t>(c.pairBuf) + c.pairCap,
+               planeCap, c.dCounters);
         stageEnd(c, kStageBroadphase);
         VXB_TRY(readCounters(c));
-        if (c.hostCounters.pairs <= c.pairCap) break;
+        if (c.hostCounters.pairs <= c.pairCap && c.hostCounters.planePairs <= planeCap) break;
         c.pairCap = c.hostCounters.pairs + c.hostCounters.pairs / 4 + 1024;
     }
-    *pairCount = c.hostCounters.pairs;
+    // Convex pairs live at [0, pairs), plane pairs at [pairCap, pairCap + planePairs).
+    c.convexPairs = c.hostCounters.pairs;
+    c.planePairs = c.hostCounters.planePairs;
+    *pairCount = c.convexPairs + c.planePairs;
     return VXB_OK;
 }
 
@@ -1765,8 +1856,11 @@ static int broadPhase(Context& c, float dt, uint32_t* pairCount) {
 
 // Runs the narrow phase on `npairs` device pairs and leaves the contacts
 // sorted in contactBuf[c.cur] (mode 0) or grouped in pair order (mode 1).
+// World path: `pairs` holds convexSplit convex-convex pairs and `planePairs`
+// holds npairs - convexSplit plane pairs. Stage path (convexSplit = ~0u):
+// `pairs` holds npairs unclassified pairs.
 static int narrowPhase(Context& c, const uint64_t* pairs, uint32_t npairs, float dt, int mode, uint32_t* contactCount,
-                       uint32_t* recordCount) {
+                       uint32_t* recordCount, uint32_t convexSplit = ~0u, const uint64_t* planePairs = nullptr) {
     const int bodyBits = std::max(1, bitsFor(c.n - 1));
     if (c.contactCap == 0) c.contactCap = std::max<uint32_t>(npairs * 2u, 4096u);
     if (c.recCap < npairs) c.recCap = npairs + 1024;
@@ -1778,10 +1872,23 @@ static int narrowPhase(Context& c, const uint64_t* pairs, uint32_t npairs, float
         VXB_CUDA(c, cudaMemsetAsync(&c.dCounters->contactsTmp, 0, 8, c.stream));  // contactsTmp + records
         VXB_CUDA(c, cudaMemsetAsync(&c.dCounters->overflow, 0, 4, c.stream));
         stageBegin(c, kStageNarrowphase);
-        if (npairs)
-            LAUNCH(c, collideKernel, std::min<uint32_t>(blocksFor(npairs, 128), (uint32_t)c.smCount * 16), 128, c.B,
-                   soupOf(c), pairs, npairs, dt, mode, bodyBits, P<vx_contact>(c.contactTmpBuf), c.contactCap,
+        if (npairs && convexSplit <= npairs) {
+            const uint32_t np = npairs - convexSplit;
+            if (convexSplit)
+                LAUNCH(c, collideKernel<kConvexPairs>, std::min<uint32_t>(blocksFor(convexSplit, 128), (uint32_t)c.smCount * 16),
+                       128, c.B, soupOf(c), pairs, convexSplit, dt, mode, bodyBits, P<vx_contact>(c.contactTmpBuf),
+                       c.contactCap, P<uint64_t>(c.recKeyBuf), P<uint32_t>(c.recValBuf), P<uint2>(c.recInfoBuf),
+                       c.recCap, c.dCounters);
+            if (np)
+                LAUNCH(c, collideKernel<kPlanePairs>, std::min<uint32_t>(blocksFor(np, 128), (uint32_t)c.smCount * 16),
+                       128, c.B, soupOf(c), planePairs, np, dt, mode, bodyBits,
+                       P<vx_contact>(c.contactTmpBuf), c.contactCap, P<uint64_t>(c.recKeyBuf),
+                       P<uint32_t>(c.recValBuf), P<uint2>(c.recInfoBuf), c.recCap, c.dCounters);
+        } else if (npairs) {
+            LAUNCH(c, collideKernel<kAnyPairs>, std::min<uint32_t>(blocksFor(npairs, 128), (uint32_t)c.smCount * 16), 128,
+                   c.B, soupOf(c), pairs, npairs, dt, mode, bodyBits, P<vx_contact>(c.contactTmpBuf), c.contactCap,
                    P<uint64_t>(c.recKeyBuf), P<uint32_t>(c.recValBuf), P<uint2>(c.recInfoBuf), c.recCap, c.dCounters);
+        }
         stageEnd(c, kStageNarrowphase);
         VXB_TRY(readCounters(c));
         if (!(c.hostCounters.overflow & 2u)) break;
@@ -1817,6 +1924,7 @@ static int narrowPhase(Context& c, const uint64_t* pairs, uint32_t npairs, float
 // solve order (island, colour, contact order) plus per-island body lists.
 static int buildIslands(Context& c, const vx_contact* cs, uint32_t m, IslandPlan& plan, uint32_t* colorOut) {
     const uint32_t n = c.n;
+    plan.contacts = m;
     VXB_TRY(ensure(c, c.parentBuf, (size_t)n * 4));
     VXB_TRY(ensure(c, c.islandOfBodyBuf, (size_t)n * 4));
     VXB_TRY(ensure(c, c.maskBuf, (size_t)n * 8));
@@ -1835,6 +1943,7 @@ static int buildIslands(Context& c, const vx_contact* cs, uint32_t m, IslandPlan
     LAUNCH(c, iotaKernel, blocksFor(n, 256), 256, parent, n);
     if (m == 0) {
         plan = IslandPlan{};
+        plan.contacts = 0;
         VXB_CUDA(c, cudaMemsetAsync(c.islandOfBodyBuf.ptr, 0xff, (size_t)n * 4, c.stream));
     } else {
         LAUNCH(c, unionKernel, blocksFor(m, 256), 256, cs, m, c.B, parent, c.dCounters);
@@ -1912,6 +2021,8 @@ static SolveArgs solveArgs(Context& c, vx_contact* cs, const IslandPlan& plan) {
     A.islands = plan.islands;
     A.realIslands = plan.realIslands;
     A.tinyLimit = 16;
+    A.prep = P<RowPrep>(c.prepBuf);
+    A.frames = P<float4>(c.frameBuf);
     return A;
 }
 
@@ -1937,8 +2048,15 @@ static void launchSolve(Context& c, const SolveArgs& A) {
 }
 
 // Substep loop over islands + contact-free bodies (advanceSubsteps).
+static int solveBuffers(Context& c, uint32_t m) {
+    VXB_TRY(ensure(c, c.prepBuf, (size_t)m * sizeof(RowPrep) + 256));
+    VXB_TRY(ensure(c, c.frameBuf, (size_t)c.n * 16 + 256));
+    return VXB_OK;
+}
+
 static int runSubsteps(Context& c, vx_contact* cs, const IslandPlan& plan, const V3& g, float h, int substeps,
                        const vx_solver_options& o, bool warmStart, bool integrate) {
+    VXB_TRY(solveBuffers(c, plan.contacts + 1));
     SolveArgs A = solveArgs(c, cs, plan);
     A.gravity = g;
     A.h = h;
@@ -2042,7 +2160,8 @@ static int stepOnce(Context& c) {
     uint32_t npairs = 0, m = 0, nrec = 0;
     VXB_TRY(broadPhase(c, dt, &npairs));
     c.stats.candidatePairs = npairs;
-    VXB_TRY(narrowPhase(c, P<uint64_t>(c.pairBuf), npairs, dt, 0, &m, &nrec));
+    VXB_TRY(narrowPhase(c, P<uint64_t>(c.pairBuf), npairs, dt, 0, &m, &nrec, c.convexPairs,
+                        P<uint64_t>(c.pairBuf) + c.pairCap));
     vx_contact* cs = P<vx_contact>(c.contactBuf[c.cur]);
     stageBegin(c, kStageWarmStart);
     if (c.prevCount && m)
@@ -2114,8 +2233,12 @@ int stagePairs(Context& c, float dt, uint64_t* out, uint32_t cap, uint32_t* coun
     *count = npairs;
     if (out) {
         std::vector<uint64_t> host(npairs);
-        if (npairs)
-            VXB_CUDA(c, cudaMemcpyAsync(host.data(), c.pairBuf.ptr, (size_t)npairs * 8, cudaMemcpyDeviceToHost, c.stream));
+        if (c.convexPairs)
+            VXB_CUDA(c, cudaMemcpyAsync(host.data(), c.pairBuf.ptr, (size_t)c.convexPairs * 8, cudaMemcpyDeviceToHost,
+                                        c.stream));
+        if (c.planePairs)
+            VXB_CUDA(c, cudaMemcpyAsync(host.data() + c.convexPairs, P<uint64_t>(c.pairBuf) + c.pairCap,
+                                        (size_t)c.planePairs * 8, cudaMemcpyDeviceToHost, c.stream));
         VXB_CUDA(c, cudaStreamSynchronize(c.stream));
         std::sort(host.begin(), host.end());
         std::memcpy(out, host.data(), (size_t)std::min(npairs, cap) * 8);
@@ -2179,7 +2302,8 @@ int backendFindContacts(Context& c, float dt, uint32_t* count) {
     VXB_TRY(resetCounters(c));
     uint32_t npairs = 0, m = 0, nrec = 0;
     VXB_TRY(broadPhase(c, dt, &npairs));
-    VXB_TRY(narrowPhase(c, P<uint64_t>(c.pairBuf), npairs, dt, 0, &m, &nrec));
+    VXB_TRY(narrowPhase(c, P<uint64_t>(c.pairBuf), npairs, dt, 0, &m, &nrec, c.convexPairs,
+                        P<uint64_t>(c.pairBuf) + c.pairCap));
     c.backendContacts = m;
     c.backendColored = false;
     *count = m;
