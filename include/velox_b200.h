@@ -166,6 +166,23 @@ int vxb_stage_color(vxb_context* ctx, const vx_body* bodies, uint32_t n,
                     const vx_contact* contacts, uint32_t m, int32_t* colorOf,
                     uint32_t* numColors);
 
+/* Broad-phase candidate pairs, as vxb_stage_pairs, for callers that must not
+ * allocate device memory during the call (frame-locked loops with a fixed
+ * memory budget, plugin hosts that own all device memory, code running on a
+ * nearly full device). No counterpart in the reference: it exists for such
+ * callers only. Needs no context. All device memory it uses is one
+ * library-owned array of about 4.3 MB, held on every device that loads the
+ * library until exit; the call allocates nothing (device or host heap).
+ * Limits: n <= 4096 bodies, <= 32768 body-body and <= 8192 body-plane pairs;
+ * beyond them it returns VXB_ERR_CAPACITY (*count still reports the pairs
+ * found when the body limit was met). The first call on a device resolves
+ * the array's device address; make that first call before any stream
+ * capture. Every call shares the array, so calls that overlap on the GPU
+ * (other threads or streams) race. Works on the current device and `stream`
+ * (null = the default stream); returns after the pairs are in `out`. */
+int vxb_stage_pairs_noalloc(const vx_body* bodies, uint32_t n, float dt, uint64_t* out, uint32_t cap,
+                            uint32_t* count, void* stream);
+
 /* ---- scene construction (host only) ------------------------------------- */
 
 /* Shape-level specs of a benchmark workload (1..5); `size` overrides its

@@ -164,6 +164,7 @@ def lib(path=LIB_PATH):
         "vxb_stage_pairs": ([vp, vp, u32, f32, vp, u32, p_u32], i32),
         "vxb_stage_collide": ([vp, vp, u32, ctypes.POINTER(Soup), vp, u32, f32, vp, u32, vp, p_u32], i32),
         "vxb_stage_color": ([vp, vp, u32, vp, u32, vp, p_u32], i32),
+        "vxb_stage_pairs_noalloc": ([vp, u32, f32, vp, u32, p_u32, vp], i32),
         "vxb_scene_generate": ([i32, ctypes.c_uint64, u32, vp, u32, p_u32, vp, u32, p_u32], i32),
         "vxb_bodies_from_specs": ([vp, u32, vp, vp, vp, u32, p_u32, vp, u32, p_u32], i32),
     }
