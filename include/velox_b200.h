@@ -16,6 +16,7 @@
  *   VXB_ERR_DEVICE_LOST  -> BackendFailure(DeviceLost)
  *   VXB_ERR_TIMEOUT      -> BackendFailure(DeviceLost) (a bounded device wait gave up)
  *   VXB_ERR_CAPACITY     -> VeloxCapacityExceeded(ContactCountOverflow)
+ *   VXB_ERR_INTERNAL     -> VeloxRuntimeError(BackendUnavailable)
  *   VXB_ERR_NO_DEVICE    -> createCudaBackend() returning nullptr
  *   others               -> VeloxRuntimeError(BackendUnavailable)
  * Threading matches the reference backend: one owner thread per context.
@@ -41,6 +42,7 @@ extern "C" {
 #define VXB_ERR_CAPACITY 5
 #define VXB_ERR_UNSUPPORTED 6
 #define VXB_ERR_TIMEOUT 7
+#define VXB_ERR_INTERNAL 8 /* a device-side consistency check failed; the step's results are void */
 
 typedef struct vxb_context vxb_context;
 
@@ -64,6 +66,11 @@ typedef struct vxb_step_stats {
     uint32_t rewinds;            /* conservative-advancement rewinds */
     uint32_t velocityIterations; /* sweeps per step (2*velocityIterations*substeps) */
     uint32_t warmStarted;        /* contacts that inherited impulses */
+    uint32_t colorRounds;        /* fixed-point rounds of the parallel colouring (0 = none) */
+    uint32_t giantIslands;       /* islands solved by the whole grid (cooperative launch) */
+    uint32_t rewindRounds;       /* wavefront rounds of the rewind passes */
+    uint32_t rewindReplays;      /* rewind passes replayed with a widened body set */
+    uint32_t rewindGapQueries;   /* distance queries of the rewind passes */
 } vxb_step_stats;
 
 /* ---- library / context ------------------------------------------------ */

@@ -113,7 +113,8 @@ class StepConfig(ctypes.Structure):
 class StepStats(ctypes.Structure):
     _fields_ = [(n, ctypes.c_uint32) for n in ("candidatePairs", "contacts", "colors", "islands",
                                                "largestIsland", "rewinds", "velocityIterations",
-                                               "warmStarted")]
+                                               "warmStarted", "colorRounds", "giantIslands",
+                                               "rewindRounds", "rewindReplays", "rewindGapQueries")]
 
 
 def ptr(a):

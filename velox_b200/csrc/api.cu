@@ -54,6 +54,7 @@ const char* vxb_status_string(int status) {
     case VXB_ERR_CAPACITY: return "caller buffer too small";
     case VXB_ERR_UNSUPPORTED: return "unsupported input";
     case VXB_ERR_TIMEOUT: return "bounded device wait timed out";
+    case VXB_ERR_INTERNAL: return "device-side consistency check failed";
     default: return "unknown status";
     }
 }
@@ -73,6 +74,7 @@ int vxb_context_create(int device, vxb_context** out) {
     Context& c = ctx->impl;
     c.device = device;
     cudaDeviceGetAttribute(&c.smCount, cudaDevAttrMultiProcessorCount, device);
+    cudaDeviceGetAttribute(&c.cooperative, cudaDevAttrCooperativeLaunch, device);
     if (cudaStreamCreateWithFlags(&c.ownStream, cudaStreamNonBlocking) != cudaSuccess) {
         delete ctx;
         return VXB_ERR_DEVICE_LOST;
@@ -101,7 +103,9 @@ void vxb_context_destroy(vxb_context* ctx) {
                            &c.colorKeyBuf, &c.maskBuf, &c.nextColorBuf, &c.islandStartBuf, &c.islandInfoBuf,
                            &c.flagBuf, &c.scanBuf, &c.scanTmp, &c.segStartBuf, &c.islandSegBuf, &c.bodyKeyBuf,
                            &c.bodyValBuf, &c.islandBodyStartBuf, &c.caFlagBuf, &c.caBodyMarkBuf, &c.caCandBuf,
-                           &c.localIdxBuf, &c.prepBuf, &c.frameBuf, &c.countersBuf};
+                           &c.localIdxBuf, &c.prepBuf, &c.frameBuf, &c.fpKeyBuf, &c.fpValBuf,
+                           &c.fpSlotBuf, &c.fpColorBuf, &c.fpRunStartBuf, &c.fpIslandBuf, &c.coopBuf,
+                           &c.giantBuf, &c.countersBuf};
     for (vxb::DevBuf* b : bufs)
         if (b->ptr) cudaFree(b->ptr);
     if (c.ownStream) cudaStreamDestroy(c.ownStream);

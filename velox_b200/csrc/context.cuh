@@ -8,6 +8,7 @@
 #include <string>
 #include <vector>
 
+#include "coop.cuh"
 #include "geom.cuh"
 #include "radix_sort.cuh"
 #include "velox_b200.h"
@@ -21,6 +22,16 @@ struct IslandPlan {
     uint32_t segments = 0;     // (island, colour) runs
     uint32_t contacts = 0;     // contacts in the plan
     uint32_t freeFrom = 0, freeTo = 0;  // contact-free bodies (range in the island-sorted body order)
+};
+
+// State of one cooperative launch (zeroed before it).
+struct CoopState {
+    GridBarrier bar;
+    uint32_t changed[3];  // per-round counters, rotated
+    uint32_t spill;       // bit 0: fall back to the serial path; bit 1: no progress
+    uint32_t rounds;      // rounds the kernel ran (or a count the launch returns)
+    uint32_t timeout;     // a barrier wait gave up
+    uint32_t pad[8];
 };
 
 // Grow-only device allocation.
@@ -50,7 +61,12 @@ struct Counters {
     uint32_t cellMaxBits[3]; // ordered-int encodings of the maximum AABB centre
     uint32_t extentBits;     // float bits of the largest non-plane AABB extent
     uint32_t worldBits;      // bits of the world id in cell keys
-    uint32_t pad[7];
+    uint32_t lastIslandKey;  // island key of the last contact (n = the null island)
+    uint32_t maxIslandSize;  // contacts of the largest island (before colouring)
+    uint32_t freeFrom, freeTo;  // contact-free bodies: range in the island-sorted body order
+    uint32_t planFault;      // a solve kernel found an inconsistent island plan
+    uint32_t caGapQueries;   // distance queries of the rewind passes
+    uint32_t pad[1];
 };
 
 // Pipeline stages timed with CUDA events when timing is enabled.
@@ -70,6 +86,9 @@ struct StageTimer {
 struct Context {
     int device = 0;
     int smCount = 148;
+    int cooperative = 0;  // cudaDevAttrCooperativeLaunch
+    uint32_t caRounds = 0;     // rewind wavefront rounds of the last step
+    uint32_t caWidenings = 0;  // rewind replays with a widened body set (last step)
     cudaStream_t ownStream = nullptr;
     cudaStream_t stream = nullptr;
     std::string lastError;
@@ -130,6 +149,9 @@ struct Context {
     DevBuf caFlagBuf, caBodyMarkBuf, caCandBuf;
     DevBuf localIdxBuf;                 // island-local body index (block solve)
     DevBuf prepBuf, frameBuf;           // per-row pose terms / per-body inertia frames (solve)
+    DevBuf fpKeyBuf, fpValBuf, fpSlotBuf, fpColorBuf, fpRunStartBuf, fpIslandBuf;  // parallel colouring
+    DevBuf coopBuf;                     // CoopState of cooperative launches
+    DevBuf giantBuf;                    // giant island list (solve)
 
     DevBuf countersBuf;
     Counters* dCounters = nullptr;

@@ -812,9 +812,10 @@ __global__ void runStartKernel(const uint32_t* flags, const uint32_t* index, uin
 // each body continues from its own spill counter.
 __global__ void colorKernel(const vx_contact* cs, const uint32_t* order, const uint32_t* islandStart,
                             uint32_t islands, const BodyArrays B, unsigned long long* mask, uint32_t* nextColor,
-                            uint32_t* colorOf, uint64_t* colorKeys, Counters* C) {
+                            uint32_t* colorOf, uint64_t* colorKeys, Counters* C, uint32_t sizeLimit) {
     for (uint32_t isl = blockIdx.x * blockDim.x + threadIdx.x; isl < islands; isl += gridDim.x * blockDim.x) {
         const uint32_t s0 = islandStart[isl], s1 = islandStart[isl + 1];
+        if (s1 - s0 > sizeLimit) continue;  // coloured by the parallel fixed point
         for (uint32_t k = s0; k < s1; ++k) {
             const vx_contact& c = cs[order[k]];
             mask[c.a] = 0ull; mask[c.b] = 0ull;
@@ -852,6 +853,125 @@ __global__ void colorKernel(const vx_contact* cs, const uint32_t* order, const u
     }
 }
 
+// Islands above this many contacts are coloured by the parallel fixed point.
+constexpr uint32_t kSerialColorLimit = 4096;
+
+// Run number of each position: inclusive scan of the head flags minus one.
+__global__ void runOfKernel(const uint32_t* flags, const uint32_t* index, uint32_t m, uint32_t* runOf) {
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < m; k += gridDim.x * blockDim.x)
+        runOf[k] = index[k] + flags[k] - 1u;
+}
+
+__global__ void lastKeyKernel(const uint64_t* keys, uint32_t m, Counters* C) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) C->lastIslandKey = (uint32_t)keys[m - 1];
+}
+
+__global__ void islandMaxKernel(const uint32_t* islandStart, Counters* C) {
+    const uint32_t islands = C->islands;
+    uint32_t mx = 0;
+    for (uint32_t isl = blockIdx.x * blockDim.x + threadIdx.x; isl < islands; isl += gridDim.x * blockDim.x)
+        mx = max(mx, islandStart[isl + 1] - islandStart[isl]);
+    for (int off = 16; off > 0; off >>= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+    if ((threadIdx.x & 31) == 0 && mx) atomicMax(&C->maxIslandSize, mx);
+}
+
+// Parallel greedy colouring of large islands. The greedy colour of a contact
+// is the first colour unused by the earlier contacts (island order) that
+// share one of its dynamic bodies; that is the unique fixed point of
+//   colour[k] = first colour not in { colour[j] : j < k, j shares a body with k }
+// reached by iterating the rule from all-zero colours (a contact is final
+// once every earlier neighbour is). Every round runs over all contacts of the
+// large islands in parallel; a round without changes is the fixed point.
+// Entries (body, 2k + side) sorted by body list each contact's earlier
+// neighbours as the entries before its own in the body's run.
+__global__ void colorEntryKernel(const vx_contact* cs, const uint32_t* order, uint32_t m, const uint32_t* islandIdx,
+                                 const uint32_t* islandStart, const BodyArrays B, uint32_t n, uint64_t* keys,
+                                 uint32_t* vals, uint32_t* slot) {
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < m; k += gridDim.x * blockDim.x) {
+        const uint32_t isl = islandIdx[k];
+        const bool big = islandStart[isl + 1] - islandStart[isl] > kSerialColorLimit;
+        const vx_contact& c = cs[order[k]];
+        const uint32_t fa = B.filt[c.a].x, fb = B.filt[c.b].x;
+        const bool sensor = isSensor(fa) || isSensor(fb);
+        keys[2 * k] = big && !sensor && isDynamic(fa) ? c.a : n;
+        keys[2 * k + 1] = big && !sensor && isDynamic(fb) ? c.b : n;
+        vals[2 * k] = 2 * k;
+        vals[2 * k + 1] = 2 * k + 1;
+        slot[2 * k] = slot[2 * k + 1] = 0xffffffffu;
+    }
+}
+
+__global__ void colorSlotKernel(const uint64_t* keys, const uint32_t* vals, uint32_t entries, uint32_t n,
+                                uint32_t* slot, uint32_t* runStart) {
+    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < entries; e += gridDim.x * blockDim.x) {
+        const uint64_t key = keys[e];
+        if (key >= n) continue;
+        slot[vals[e]] = e;
+        if (e == 0 || keys[e - 1] != key) runStart[key] = e;
+    }
+}
+
+// Cooperative launch. changed[3] rotate per round: the counter of round r + 1
+// is cleared during round r, after every block has read round r - 2's value.
+// color[] is indexed by island-order position and zero on entry.
+__global__ void colorFixedPointKernel(const uint64_t* keys, const uint32_t* vals, const uint32_t* slot,
+                                      const uint32_t* runStart, const uint32_t* islandIdx,
+                                      const uint32_t* islandStart, uint32_t m, uint32_t* color, CoopState* st,
+                                      uint32_t maxRounds) {
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+    for (uint32_t r = 0; r < maxRounds; ++r) {
+        if (tid == 0) st->changed[(r + 1) % 3] = 0u;
+        uint32_t local = 0;
+        for (uint32_t k = tid; k < m; k += stride) {
+            const uint32_t isl = islandIdx[k];
+            if (islandStart[isl + 1] - islandStart[isl] <= kSerialColorLimit) continue;
+            unsigned long long used = 0ull;
+            bool over = false;
+            for (int side = 0; side < 2; ++side) {
+                const uint32_t e = slot[2 * k + side];
+                if (e == 0xffffffffu) continue;
+                const uint32_t body = (uint32_t)keys[e];
+                for (uint32_t f = runStart[body]; f < e; ++f) {
+                    const uint32_t cq = __ldcg(color + (vals[f] >> 1));
+                    if (cq < 64u) used |= 1ull << cq;
+                    else over = true;
+                }
+            }
+            if (over || ~used == 0ull) { atomicOr(&st->spill, 1u); continue; }
+            const uint32_t next = (uint32_t)(__ffsll((long long)~used) - 1);
+            if (next != __ldcg(color + k)) {
+                __stcg(color + k, next);
+                ++local;
+            }
+        }
+        if (local) atomicAdd(&st->changed[r % 3], local);
+        if (!gridSync(&st->bar, &st->timeout)) return;
+        if (__ldcg(&st->changed[r % 3]) == 0u || __ldcg(&st->spill) != 0u) {
+            if (tid == 0) st->rounds = r + 1;
+            return;
+        }
+    }
+    if (tid == 0) { st->rounds = maxRounds; atomicOr(&st->spill, 2u); }  // no fixed point within the bound
+}
+
+__global__ void colorFinishKernel(const uint32_t* order, uint32_t m, const uint32_t* islandIdx,
+                                  const uint32_t* islandStart, const uint32_t* color, uint32_t* colorOf,
+                                  uint64_t* colorKeys, Counters* C) {
+    uint32_t mx = 0;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < m; k += gridDim.x * blockDim.x) {
+        const uint32_t isl = islandIdx[k];
+        const uint32_t size = islandStart[isl + 1] - islandStart[isl];
+        if (size <= kSerialColorLimit) continue;
+        const uint32_t c = color[k];
+        colorOf[order[k]] = c;
+        colorKeys[k] = ((uint64_t)isl << 16) | c;
+        mx = max(mx, c + 1);
+        if (k == islandStart[isl]) atomicMax(&C->largestIsland, size);
+    }
+    for (int off = 16; off > 0; off >>= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+    if ((threadIdx.x & 31) == 0 && mx) atomicMax(&C->maxColors, mx);
+}
+
 __global__ void islandBodyKernel(const vx_contact* cs, const uint32_t* order, const uint32_t* islandStart,
                                  uint32_t realIslands, const BodyArrays B, uint32_t* islandOfBody) {
     for (uint32_t isl = blockIdx.x; isl < realIslands; isl += gridDim.x) {
@@ -885,6 +1005,14 @@ __global__ void bodyStartKernel(const uint64_t* keys, uint32_t n, uint32_t* body
         }
         if (k == n - 1)
             for (uint64_t x = key + 1; x < entries; ++x) bodyStart[x] = n;
+    }
+}
+
+// Contact-free bodies: the last two bodyStart entries, for the host's single read.
+__global__ void freeRangeKernel(const uint32_t* bodyStart, uint32_t entries, Counters* C) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        C->freeFrom = bodyStart[entries - 2];
+        C->freeTo = bodyStart[entries - 1];
     }
 }
 
@@ -1922,6 +2050,63 @@ static int narrowPhase(Context& c, const uint64_t* pairs, uint32_t npairs, float
 
 // Groups the m contacts of `cs` into islands, colours them and builds the
 // solve order (island, colour, contact order) plus per-island body lists.
+// Cooperative launch of `kernel` with as many blocks as fit on the device at
+// once. VXB_ERR_UNSUPPORTED (nothing recorded) when the device cannot run it:
+// callers then take their serial path.
+template <class Kernel, class... Args>
+static int launchCooperative(Context& c, Kernel kernel, int threads, Args... args) {
+    int perSm = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kernel, threads, 0);
+    if (e != cudaSuccess) return cudaStatus(c, e, "cooperative occupancy");
+    if (perSm <= 0 || !c.cooperative) return VXB_ERR_UNSUPPORTED;
+    void* params[] = {&args...};
+    e = cudaLaunchCooperativeKernel((const void*)kernel, dim3(perSm * c.smCount), dim3(threads), params, 0, c.stream);
+    ++c.launches;
+    return cudaStatus(c, e, "cudaLaunchCooperativeKernel");
+}
+
+// Colours of the islands above kSerialColorLimit contacts (colorOf, colour
+// keys, maxColors). VXB_ERR_UNSUPPORTED / VXB_ERR_TIMEOUT: the caller colours
+// every island serially instead.
+static int parallelColor(Context& c, const vx_contact* cs, const uint32_t* order, const uint32_t* runFlags,
+                         const uint32_t* runIndex, const uint32_t* islandStart, uint32_t m, uint64_t* colorKeys) {
+    const uint32_t n = c.n;
+    VXB_TRY(ensure(c, c.fpKeyBuf, (size_t)m * 16 + 64));
+    VXB_TRY(ensure(c, c.fpValBuf, (size_t)m * 8 + 64));
+    VXB_TRY(ensure(c, c.fpSlotBuf, (size_t)m * 8 + 64));
+    VXB_TRY(ensure(c, c.fpColorBuf, (size_t)m * 4 + 64));
+    VXB_TRY(ensure(c, c.fpRunStartBuf, (size_t)n * 4 + 64));
+    VXB_TRY(ensure(c, c.fpIslandBuf, (size_t)m * 4 + 64));
+    VXB_TRY(ensure(c, c.coopBuf, sizeof(CoopState)));
+    uint64_t* keys = P<uint64_t>(c.fpKeyBuf);
+    uint32_t* vals = P<uint32_t>(c.fpValBuf);
+    uint32_t* slot = P<uint32_t>(c.fpSlotBuf);
+    uint32_t* color = P<uint32_t>(c.fpColorBuf);
+    uint32_t* runStart = P<uint32_t>(c.fpRunStartBuf);
+    uint32_t* islandIdx = P<uint32_t>(c.fpIslandBuf);
+    CoopState* st = P<CoopState>(c.coopBuf);
+    LAUNCH(c, runOfKernel, blocksFor(m, 256), 256, runFlags, runIndex, m, islandIdx);
+    LAUNCH(c, colorEntryKernel, blocksFor(m, 256), 256, cs, order, m, (const uint32_t*)islandIdx, islandStart, c.B, n,
+           keys, vals, slot);
+    VXB_TRY(sortPairs(c, keys, vals, 2 * m, bitsFor(n)));
+    LAUNCH(c, colorSlotKernel, blocksFor(2 * m, 256), 256, keys, vals, 2 * m, n, slot, runStart);
+    VXB_CUDA(c, cudaMemsetAsync(color, 0, (size_t)m * 4, c.stream));
+    VXB_CUDA(c, cudaMemsetAsync(st, 0, sizeof(CoopState), c.stream));
+    const int rc = launchCooperative(c, colorFixedPointKernel, 256, (const uint64_t*)keys, (const uint32_t*)vals,
+                                     (const uint32_t*)slot, (const uint32_t*)runStart, (const uint32_t*)islandIdx,
+                                     islandStart, m, color, st, 4096u);
+    if (rc != VXB_OK) return rc;
+    CoopState host;
+    VXB_CUDA(c, cudaMemcpyAsync(&host, st, sizeof(host), cudaMemcpyDeviceToHost, c.stream));
+    VXB_CUDA(c, cudaStreamSynchronize(c.stream));
+    c.stats.colorRounds = host.rounds;
+    if (host.timeout || (host.spill & 2u)) return VXB_ERR_TIMEOUT;
+    if (host.spill) return VXB_ERR_UNSUPPORTED;
+    LAUNCH(c, colorFinishKernel, blocksFor(m, 256), 256, order, m, (const uint32_t*)islandIdx, islandStart,
+           (const uint32_t*)color, P<uint32_t>(c.colorBuf), colorKeys, c.dCounters);
+    return VXB_OK;
+}
+
 static int buildIslands(Context& c, const vx_contact* cs, uint32_t m, IslandPlan& plan, uint32_t* colorOut) {
     const uint32_t n = c.n;
     plan.contacts = m;
@@ -1958,19 +2143,25 @@ static int buildIslands(Context& c, const vx_contact* cs, uint32_t m, IslandPlan
         LAUNCH(c, runFlagKernel, blocksFor(m, 256), 256, ikeys, m, flags);
         VXB_TRY(exclusiveScan(c, flags, index, m, &c.dCounters->islands));
         LAUNCH(c, runStartKernel, blocksFor(m, 256), 256, flags, index, m, islandStart);
+        LAUNCH(c, lastKeyKernel, 1, 32, ikeys, m, c.dCounters);
+        LAUNCH(c, islandMaxKernel, std::min<uint32_t>(blocksFor(m, 256), (uint32_t)c.smCount * 4), 256, islandStart,
+               c.dCounters);
         VXB_TRY(readCounters(c));
         plan.islands = c.hostCounters.islands;
         // is the last island the null island (key n)?
-        uint64_t lastKey = 0;
-        VXB_CUDA(c, cudaMemcpyAsync(&lastKey, ikeys + (m - 1), 8, cudaMemcpyDeviceToHost, c.stream));
-        VXB_CUDA(c, cudaStreamSynchronize(c.stream));
-        plan.realIslands = lastKey == n ? plan.islands - 1 : plan.islands;
+        plan.realIslands = c.hostCounters.lastIslandKey == n ? plan.islands - 1 : plan.islands;
         // colour each island; colour keys (island << 16 | colour) in island order
         VXB_TRY(ensure(c, c.colorKeyBuf, (size_t)m * 8 + 16));
         uint64_t* ckeys = P<uint64_t>(c.colorKeyBuf);
+        bool serialAll = false;
+        if (c.hostCounters.maxIslandSize > kSerialColorLimit) {
+            const int status = parallelColor(c, cs, ivals, flags, index, islandStart, m, ckeys);
+            if (status == VXB_ERR_TIMEOUT || status == VXB_ERR_UNSUPPORTED) serialAll = true;  // exact serial path
+            else if (status != VXB_OK) return status;
+        }
         LAUNCH(c, colorKernel, blocksFor(plan.islands, 64), 64, cs, ivals, islandStart, plan.islands, c.B,
                P<unsigned long long>(c.maskBuf), P<uint32_t>(c.nextColorBuf), P<uint32_t>(c.colorBuf), ckeys,
-               c.dCounters);
+               c.dCounters, serialAll ? 0xffffffffu : kSerialColorLimit);
         if (colorOut)
             VXB_CUDA(c, cudaMemcpyAsync(colorOut, c.colorBuf.ptr, (size_t)m * 4, cudaMemcpyDeviceToHost, c.stream));
         // solve order: stable sort by (island, colour)
@@ -1978,9 +2169,6 @@ static int buildIslands(Context& c, const vx_contact* cs, uint32_t m, IslandPlan
         LAUNCH(c, runFlagKernel, blocksFor(m, 256), 256, ckeys, m, flags);
         VXB_TRY(exclusiveScan(c, flags, index, m, &c.dCounters->segments));
         LAUNCH(c, runStartKernel, blocksFor(m, 256), 256, flags, index, m, P<uint32_t>(c.segStartBuf));
-        // first segment of each island: index[islandStart[isl]]
-        VXB_TRY(readCounters(c));
-        plan.segments = c.hostCounters.segments;
         // island bodies
         VXB_CUDA(c, cudaMemsetAsync(c.islandOfBodyBuf.ptr, 0xff, (size_t)n * 4, c.stream));
         LAUNCH(c, islandBodyKernel, std::min<uint32_t>(std::max<uint32_t>(plan.realIslands, 1), 65535u), 64, cs, ivals,
@@ -1993,11 +2181,11 @@ static int buildIslands(Context& c, const vx_contact* cs, uint32_t m, IslandPlan
     VXB_TRY(ensure(c, c.islandBodyStartBuf, ((size_t)plan.realIslands + 2) * 4 + 16));
     LAUNCH(c, bodyStartKernel, blocksFor(n, 256), 256, P<uint64_t>(c.bodyKeyBuf), n, P<uint32_t>(c.islandBodyStartBuf),
            plan.realIslands + 2);
-    std::vector<uint32_t> bs(plan.realIslands + 2);
-    VXB_CUDA(c, cudaMemcpyAsync(bs.data(), c.islandBodyStartBuf.ptr, bs.size() * 4, cudaMemcpyDeviceToHost, c.stream));
-    VXB_CUDA(c, cudaStreamSynchronize(c.stream));
-    plan.freeFrom = bs[plan.realIslands];
-    plan.freeTo = bs[plan.realIslands + 1];
+    LAUNCH(c, freeRangeKernel, 1, 32, P<uint32_t>(c.islandBodyStartBuf), plan.realIslands + 2, c.dCounters);
+    VXB_TRY(readCounters(c));  // one read for the segment count and the free-body range
+    plan.segments = m ? c.hostCounters.segments : 0;
+    plan.freeFrom = c.hostCounters.freeFrom;
+    plan.freeTo = c.hostCounters.freeTo;
     return VXB_OK;
 }
 
