@@ -1044,6 +1044,7 @@ struct SolveArgs {
     float4* frames;          // per body inertia frame, rebuilt every substep (global path)
     int stackStabilization;
     float stackStiffness, stackDamping;
+    uint32_t* fault;         // set when the island plan is inconsistent (Counters::planFault)
 };
 
 VXD void warmRow(const SolveArgs& A, uint32_t ci) {
@@ -1428,10 +1429,7 @@ __global__ void __launch_bounds__(kBlockThreads) solveBlockKernel(SolveArgs A, u
         const uint32_t b0 = isl < A.realIslands ? A.bodyStart[isl] : 0u;
         const uint32_t b1 = isl < A.realIslands ? A.bodyStart[isl + 1] : 0u;
         const uint32_t nb = b1 - b0, rows = s1 - s0;
-        if (nb > (uint32_t)kBlockBodies || rows > (uint32_t)kBlockRows) {
-            solveIslandGlobal(A, isl);
-            continue;
-        }
+        if (nb > (uint32_t)kBlockBodies || rows > (uint32_t)kBlockRows) continue;  // solveGiantKernel
         for (uint32_t k = threadIdx.x; k < nb; k += blockDim.x) {
             const uint32_t id = A.bodyOrder[b0 + k];
             S.p[k] = A.B.pos[id]; S.q[k] = A.B.rot[id]; S.v[k] = A.B.vel[id]; S.w[k] = A.B.ang[id];
@@ -1442,7 +1440,11 @@ __global__ void __launch_bounds__(kBlockThreads) solveBlockKernel(SolveArgs A, u
         for (uint32_t k = threadIdx.x; k < rows; k += blockDim.x) {
             const vx_contact& cc = A.contacts[A.order[s0 + k]];
             const bool da = isDynamic(A.B.filt[cc.a].x), db = isDynamic(A.B.filt[cc.b].x);
-            S.rowIdx[k] = make_int2(da ? (int)localIdx[cc.a] : -1, db ? (int)localIdx[cc.b] : -1);
+            int la = da ? (int)localIdx[cc.a] : -1, lb = db ? (int)localIdx[cc.b] : -1;
+            // a dynamic body outside this island's list means an inconsistent plan: report it, never index smem
+            if (la >= 0 && ((uint32_t)la >= nb || A.bodyOrder[b0 + la] != cc.a)) { atomicOr(A.fault, 1u); la = -1; }
+            if (lb >= 0 && ((uint32_t)lb >= nb || A.bodyOrder[b0 + lb] != cc.b)) { atomicOr(A.fault, 1u); lb = -1; }
+            S.rowIdx[k] = make_int2(la, lb);
         }
         __syncthreads();
         const uint32_t g0 = A.islandSeg[isl], g1 = A.islandSeg[isl + 1];
@@ -1494,6 +1496,193 @@ __global__ void __launch_bounds__(kBlockThreads) solveBlockKernel(SolveArgs A, u
         }
         __syncthreads();
     }
+}
+
+// ---- giant islands: the whole grid on one island ----------------------------
+//
+// Islands too large for one block's shared memory run on every block of a
+// cooperative launch, with a grid barrier between colours. Mutable data that
+// other blocks wrote since the last barrier (velocities, poses, impulses, row
+// terms, frames) is read with ld.global.cg and written with st.global.cg, so
+// no SM works from a stale L1 line.
+
+VXD float4 ldcg4(const float4* p) { return __ldcg(p); }
+
+VXD SolverBody coherentBody(const SolveArgs& A, uint32_t id) {
+    SolverBody b;
+    b.p = f3(ldcg4(A.B.pos + id));
+    b.q = q4(ldcg4(A.B.rot + id));
+    b.v = f3(ldcg4(A.B.vel + id));
+    b.w = f3(ldcg4(A.B.ang + id));
+    b.m = loadMass(A.B, id);
+    b.sphere = shapeOf(b.m.flags) == kSphere;
+    if (isDynamic(b.m.flags)) b.frame = q4(ldcg4(A.frames + id));
+    else cacheFrame(b);
+    return b;
+}
+
+// Whole 128-byte contact records through L2 (one thread owns a row per colour).
+VXD void loadContactCoherent(const vx_contact* p, vx_contact& c) {
+    const float4* src = reinterpret_cast<const float4*>(p);
+    float4* dst = reinterpret_cast<float4*>(&c);
+#pragma unroll
+    for (int i = 0; i < (int)(sizeof(vx_contact) / 16); ++i) dst[i] = __ldcg(src + i);
+}
+
+VXD void storeContactCoherent(vx_contact* p, const vx_contact& c) {
+    const float4* src = reinterpret_cast<const float4*>(&c);
+    float4* dst = reinterpret_cast<float4*>(p);
+#pragma unroll
+    for (int i = 0; i < (int)(sizeof(vx_contact) / 16); ++i) __stcg(dst + i, src[i]);
+}
+
+VXD void coherentPrep(const RowPrep* p, RowPrep& P) {
+    const float* s = reinterpret_cast<const float*>(p);
+    float* d = reinterpret_cast<float*>(&P);
+#pragma unroll
+    for (int i = 0; i < (int)(sizeof(RowPrep) / 4); ++i) d[i] = __ldcg(s + i);
+}
+
+// op: 0 warm start, 1 velocity sweep, 2 position row, 3 prepare
+VXD void giantRow(const SolveArgs& A, uint32_t pos, int op) {
+    vx_contact* cp = A.contacts + A.order[pos];
+    alignas(16) vx_contact cc;
+    loadContactCoherent(cp, cc);
+    SolverBody a = coherentBody(A, cc.a), b = coherentBody(A, cc.b);
+    if (!solvedContact(a.m.flags, b.m.flags)) return;
+    RowContact r;
+    loadRow(cc, r);
+    if (op == 2) {
+        const float ima = solverInvMass(a.m), imb = solverInvMass(b.m);
+        const float invMassSum = ima + imb;
+        if (invMassSum <= 0.0f) return;
+        const V3 wa = anchorWorld(a.sphere, a.p, a.q, r.la);
+        const V3 wb = anchorWorld(b.sphere, b.p, b.q, r.lb);
+        const float gap = r.bias0 + dot(r.normal, wa - wb);
+        if (gap >= -1e-3f) return;
+        float resolve = 0.6f;
+        if (A.stackStabilization && lengthSq(a.v - b.v) < 1e-4f)
+            resolve += 0.2f * (A.stackStiffness / 1000.0f) / (1.0f + A.stackDamping * A.h);
+        const float push = -resolve * (gap + 1e-3f) / invMassSum;
+        if (isDynamic(a.m.flags) && !isAsleep(a.m.flags))
+            __stcg(A.B.pos + cc.a, pack(a.p + r.normal * (push * ima), 0.0f));
+        if (isDynamic(b.m.flags) && !isAsleep(b.m.flags))
+            __stcg(A.B.pos + cc.b, pack(b.p - r.normal * (push * imb), 0.0f));
+        return;
+    }
+    RowPrep* Pg = A.prep + pos;
+    RowPrep P;
+    if (op == 3) {
+        prepRow(a, b, r, A.h, A.coneBlock != 0, P);
+        const float* src = reinterpret_cast<const float*>(&P);
+        float* dst = reinterpret_cast<float*>(Pg);
+#pragma unroll
+        for (int i = 0; i < (int)(sizeof(RowPrep) / 4); ++i) __stcg(dst + i, src[i]);
+        return;
+    }
+    coherentPrep(Pg, P);
+    if (op == 0) warmPrepRow(a, b, r, P);
+    else sweepRow(a, b, r, P, A.coneBlock != 0);
+    if (isDynamic(a.m.flags)) { __stcg(A.B.vel + cc.a, pack(a.v, 0.0f)); __stcg(A.B.ang + cc.a, pack(a.w, 0.0f)); }
+    if (isDynamic(b.m.flags)) { __stcg(A.B.vel + cc.b, pack(b.v, 0.0f)); __stcg(A.B.ang + cc.b, pack(b.w, 0.0f)); }
+    storeRow(cc, r);
+    storeContactCoherent(cp, cc);
+}
+
+// integrateKernel semantics (src/backend_cuda.cu:80-89) on coherent loads.
+VXD void giantIntegrateVelocity(const SolveArgs& A, uint32_t i) {
+    const Mass m = loadMass(A.B, i);
+    if (!isDynamic(m.flags) || isLocked(m.flags) || isAsleep(m.flags)) return;
+    const Q4 q = q4(ldcg4(A.B.rot + i));
+    V3 v = f3(ldcg4(A.B.vel + i));
+    V3 w = f3(ldcg4(A.B.ang + i));
+    const V3 F = f3(A.B.force[i]);
+    const V3 T = f3(A.B.torque[i]);
+    const float4 ex = A.B.extra[i];
+    v += (A.gravity * ex.y + F * solverInvMass(m)) * A.h;
+    w += invInertiaMulAt(m, T, q) * A.h;
+    v *= 1.0f / (1.0f + ex.z * A.h);
+    w *= 1.0f / (1.0f + ex.w * A.h);
+    __stcg(A.B.vel + i, pack(v, 0.0f));
+    __stcg(A.B.ang + i, pack(w, 0.0f));
+}
+
+// integrateTransformsKernel semantics (src/backend_cuda.cu:91-97) on coherent loads.
+VXD void giantIntegrateTransform(const SolveArgs& A, uint32_t i) {
+    const Mass m = loadMass(A.B, i);
+    if (isStaticBody(m.flags) || isLocked(m.flags) || isAsleep(m.flags)) return;
+    V3 p = f3(ldcg4(A.B.pos + i));
+    Q4 q = q4(ldcg4(A.B.rot + i));
+    const V3 v = f3(ldcg4(A.B.vel + i));
+    V3 w = f3(ldcg4(A.B.ang + i));
+    advanceTransform(m, p, q, v, w, A.h);
+    __stcg(A.B.pos + i, pack(p, 0.0f));
+    __stcg(A.B.rot + i, pack(q));
+    __stcg(A.B.ang + i, pack(w, 0.0f));
+}
+
+// Cooperative launch over the giant islands listed in `giants`, one after the
+// other, with the block path's schedule (solveIslandGlobal) and a grid barrier
+// wherever that path has a block barrier.
+__global__ void __launch_bounds__(256) solveGiantKernel(SolveArgs A, const uint32_t* giants, uint32_t count,
+                                                        CoopState* st) {
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+    for (uint32_t gi = 0; gi < count; ++gi) {
+        const uint32_t isl = giants[gi];
+        const uint32_t s0 = A.islandStart[isl], s1 = A.islandStart[isl + 1];
+        const uint32_t g0 = A.islandSeg[isl], g1 = A.islandSeg[isl + 1];
+        const uint32_t b0 = isl < A.realIslands ? A.bodyStart[isl] : 0u;
+        const uint32_t b1 = isl < A.realIslands ? A.bodyStart[isl + 1] : 0u;
+        if (A.positionIterations > 0) {
+            for (int it = 0; it < A.positionIterations; ++it)
+                for (uint32_t g = g0; g < g1; ++g) {
+                    for (uint32_t k = A.segStart[g] + tid; k < A.segStart[g + 1]; k += stride) giantRow(A, k, 2);
+                    if (!gridSync(&st->bar, &st->timeout)) return;
+                }
+            continue;
+        }
+        for (int s = 0; s < A.substeps; ++s) {
+            for (uint32_t k = b0 + tid; k < b1; k += stride) {
+                const uint32_t id = A.bodyOrder[k];
+                if (A.integrate && s > 0) giantIntegrateVelocity(A, id);
+                __stcg(A.frames + id, pack(inertiaFrameAt(loadMass(A.B, id), q4(ldcg4(A.B.rot + id)))));
+            }
+            if (!gridSync(&st->bar, &st->timeout)) return;
+            for (uint32_t k = s0 + tid; k < s1; k += stride) giantRow(A, k, 3);
+            if (!gridSync(&st->bar, &st->timeout)) return;
+            if (A.warmStart && s == 0)
+                for (uint32_t g = g0; g < g1; ++g) {
+                    for (uint32_t k = A.segStart[g] + tid; k < A.segStart[g + 1]; k += stride) giantRow(A, k, 0);
+                    if (!gridSync(&st->bar, &st->timeout)) return;
+                }
+            for (int it = 0; it < A.sweeps; ++it)
+                for (uint32_t g = g0; g < g1; ++g) {
+                    for (uint32_t k = A.segStart[g] + tid; k < A.segStart[g + 1]; k += stride) giantRow(A, k, 1);
+                    if (!gridSync(&st->bar, &st->timeout)) return;
+                }
+            if (A.integrate) {
+                for (uint32_t k = b0 + tid; k < b1; k += stride) giantIntegrateTransform(A, A.bodyOrder[k]);
+                if (!gridSync(&st->bar, &st->timeout)) return;
+            }
+        }
+    }
+}
+
+// The block kernel's complement among the islands above tinyLimit.
+VXD bool isGiant(const SolveArgs& A, uint32_t isl) {
+    const uint32_t rows = A.islandStart[isl + 1] - A.islandStart[isl];
+    const uint32_t nb = isl < A.realIslands ? A.bodyStart[isl + 1] - A.bodyStart[isl] : 0u;
+    return rows > A.tinyLimit && (nb > (uint32_t)kBlockBodies || rows > (uint32_t)kBlockRows);
+}
+
+__global__ void giantListKernel(SolveArgs A, uint32_t* list, uint32_t* count) {
+    for (uint32_t isl = blockIdx.x * blockDim.x + threadIdx.x; isl < A.islands; isl += gridDim.x * blockDim.x)
+        if (isGiant(A, isl)) list[atomicAdd(count, 1u)] = isl;
+}
+
+// Fallback when the device cannot run a cooperative grid: one block per giant island.
+__global__ void __launch_bounds__(kBlockThreads) solveGiantBlockKernel(SolveArgs A, const uint32_t* giants) {
+    solveIslandGlobal(A, giants[blockIdx.x]);
 }
 
 // Bodies without contacts: the substep loop's integration only.
@@ -2209,6 +2398,7 @@ static SolveArgs solveArgs(Context& c, vx_contact* cs, const IslandPlan& plan) {
     A.islands = plan.islands;
     A.realIslands = plan.realIslands;
     A.tinyLimit = 16;
+    A.fault = &c.dCounters->planFault;
     A.prep = P<RowPrep>(c.prepBuf);
     A.frames = P<float4>(c.frameBuf);
     return A;
@@ -2221,8 +2411,8 @@ static int prepareSegments(Context& c, const IslandPlan& plan) {
     return VXB_OK;
 }
 
-static void launchSolve(Context& c, const SolveArgs& A) {
-    if (A.islands == 0) return;
+static int launchSolve(Context& c, const SolveArgs& A) {
+    if (A.islands == 0) return VXB_OK;
     LAUNCH(c, solveTinyKernel, blocksFor(A.islands, 64), 64, A);
     static bool configured = false;
     if (!configured) {
@@ -2233,6 +2423,31 @@ static void launchSolve(Context& c, const SolveArgs& A) {
     solveBlockKernel<<<std::min<uint32_t>(A.islands, (uint32_t)c.smCount * 2), kBlockThreads, kBlockSmem, c.stream>>>(
         A, P<uint32_t>(c.localIdxBuf));
     ++c.launches;
+    // giant islands: list them, then one cooperative launch over all of them
+    VXB_TRY(ensure(c, c.giantBuf, ((size_t)A.islands + 1) * 4 + 64));
+    VXB_TRY(ensure(c, c.coopBuf, sizeof(CoopState)));
+    CoopState* st = P<CoopState>(c.coopBuf);
+    uint32_t* list = P<uint32_t>(c.giantBuf);
+    VXB_CUDA(c, cudaMemsetAsync(st, 0, sizeof(CoopState), c.stream));
+    LAUNCH(c, giantListKernel, std::min<uint32_t>(blocksFor(A.islands, 256), (uint32_t)c.smCount * 4), 256, A, list,
+           &st->rounds);
+    uint32_t giants = 0;
+    VXB_CUDA(c, cudaMemcpyAsync(&giants, &st->rounds, 4, cudaMemcpyDeviceToHost, c.stream));
+    VXB_CUDA(c, cudaStreamSynchronize(c.stream));
+    if (!giants) return VXB_OK;
+    c.stats.giantIslands = std::max(c.stats.giantIslands, giants);
+    VXB_CUDA(c, cudaMemsetAsync(st, 0, sizeof(CoopState), c.stream));
+    const int rc = launchCooperative(c, solveGiantKernel, 256, A, (const uint32_t*)list, giants, st);
+    if (rc == VXB_ERR_UNSUPPORTED) {
+        LAUNCH(c, solveGiantBlockKernel, giants, kBlockThreads, A, (const uint32_t*)list);
+        return VXB_OK;
+    }
+    VXB_TRY(rc);
+    uint32_t timeout = 0;
+    VXB_CUDA(c, cudaMemcpyAsync(&timeout, &st->timeout, 4, cudaMemcpyDeviceToHost, c.stream));
+    VXB_CUDA(c, cudaStreamSynchronize(c.stream));
+    if (timeout) return fail(c, VXB_ERR_TIMEOUT, "grid barrier timed out in the giant-island solve");
+    return VXB_OK;
 }
 
 // Substep loop over islands + contact-free bodies (advanceSubsteps).
@@ -2253,7 +2468,7 @@ static int runSubsteps(Context& c, vx_contact* cs, const IslandPlan& plan, const
     A.warmStart = warmStart ? 1 : 0;
     A.integrate = integrate ? 1 : 0;
     A.coneBlock = o.frictionModel == VX_FRICTION_CONE_BLOCK;
-    launchSolve(c, A);
+    VXB_TRY(launchSolve(c, A));
     if (integrate && plan.freeTo > plan.freeFrom)
         LAUNCH(c, freeBodiesKernel, blocksFor(plan.freeTo - plan.freeFrom, 128), 128, c.B, P<uint32_t>(c.bodyValBuf),
                plan.freeFrom, plan.freeTo, g, h, substeps);
@@ -2268,7 +2483,7 @@ static int positionCorrection(Context& c, vx_contact* cs, const IslandPlan& plan
     A.stackStiffness = o.stackStiffness;
     A.stackDamping = o.stackDamping;
     A.h = h;
-    launchSolve(c, A);
+    VXB_TRY(launchSolve(c, A));
     return VXB_OK;
 }
 
@@ -2340,6 +2555,10 @@ static int stepOnce(Context& c) {
     const float h = dt / substeps;
     const V3 g{cfg.gravity.x, cfg.gravity.y, cfg.gravity.z};
     VXB_TRY(resetCounters(c));
+    c.stats.colorRounds = 0;
+    c.stats.giantIslands = 0;
+    c.caRounds = 0;
+    c.caWidenings = 0;
     VXB_TRY(ensure(c, c.prevPoseBuf, (size_t)n * 32));
     float4* prevPos = P<float4>(c.prevPoseBuf);
     stageBegin(c, kStagePrepare);
@@ -2382,9 +2601,13 @@ static int stepOnce(Context& c) {
     c.stats.colors = c.hostCounters.maxColors;
     c.stats.largestIsland = c.hostCounters.largestIsland;
     c.stats.rewinds = c.hostCounters.rewinds;
+    c.stats.rewindRounds = c.caRounds;
+    c.stats.rewindReplays = c.caWidenings;
+    c.stats.rewindGapQueries = c.hostCounters.caGapQueries;
     c.stats.warmStarted = c.hostCounters.warmStarted;
     c.stats.velocityIterations = (uint32_t)(2 * cfg.solver.velocityIterations * substeps);
     if (c.hostCounters.timeout) return fail(c, VXB_ERR_TIMEOUT, "a bounded device wait gave up");
+    if (c.hostCounters.planFault) return fail(c, VXB_ERR_INTERNAL, "inconsistent island plan in the solve");
     return VXB_OK;
 }
 
@@ -2549,6 +2772,9 @@ int backendSolve(Context& c, vx_contact* contacts, uint32_t m, float h, bool war
         VXB_TRY(runSubsteps(c, P<vx_contact>(c.contactBuf[c.cur]), plan, g, h, 1, o, warmStart, false));
     }
     VXB_CUDA(c, cudaGetLastError());
+    VXB_TRY(readCounters(c));
+    if (c.hostCounters.timeout) return fail(c, VXB_ERR_TIMEOUT, "a bounded device wait gave up");
+    if (c.hostCounters.planFault) return fail(c, VXB_ERR_INTERNAL, "inconsistent island plan in the solve");
     return VXB_OK;
 }
 
