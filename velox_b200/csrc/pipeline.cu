@@ -1784,7 +1784,7 @@ VXD Q4 orientationAt(const Mass& m, const Q4& start, const V3& L, float elapsed)
 // Full rewind logic for one oriented pair on the current state. Returns true
 // when the pair was rewound.
 __device__ __noinline__ bool caRewind(BodyArrays& B, const Soup& soup, uint32_t i, uint32_t j, float dt,
-                                      const float4* prevPos, const float4* prevRot) {
+                                      const float4* prevPos, const float4* prevRot, uint32_t* gapQueries) {
     BodyView a = loadView(B, i), b = loadView(B, j);
     if (!caEligible(a, b, B, i)) return false;
     const GapProbe end = gapAt(a, b, soup);
@@ -1802,7 +1802,9 @@ __device__ __noinline__ bool caRewind(BodyArrays& B, const Soup& soup, uint32_t 
     const V3 Lb = bDyn ? inertiaMulAt(mb, b.w, b.q) : V3{0.0f, 0.0f, 0.0f};
     float t = 0.0f;
     V3 n = end.normal;
+    uint32_t queries = 1;
     for (int iter = 0; iter < 24 && t < 1.0f; ++iter) {
+        ++queries;
         const Q4 qa = orientationAt(ma, qa0, La, dt * t);
         const Q4 qb = bStatic ? qb0 : orientationAt(mb, qb0, Lb, dt * t);
         const GapProbe g = gapAt(withPose(a, pa0 + da * t, qa), withPose(b, pb0 + db * t, qb), soup);
@@ -1810,6 +1812,7 @@ __device__ __noinline__ bool caRewind(BodyArrays& B, const Soup& soup, uint32_t 
         if (g.gap < 1e-3f) break;
         t = vmin(1.0f, t + g.gap / bound);
     }
+    atomicAdd(gapQueries, queries);
     if (t >= 1.0f) return false;
     a.p = pa0 + da * t;
     a.q = qa0;
@@ -1843,34 +1846,99 @@ __device__ __noinline__ bool caRewind(BodyArrays& B, const Soup& soup, uint32_t 
     return true;
 }
 
-// Rewind pass over one component of candidate pairs (candidates connected
-// through shared dynamic bodies), in pair order. Components share no dynamic
-// body, so running them concurrently equals the reference's single ordered
-// loop as long as no rewind moves a body outside the candidate set; that case
-// is flagged and the caller replays the whole pass serially from a snapshot.
-__global__ void caComponentKernel(BodyArrays B, Soup soup, const uint64_t* pairKeys, const uint32_t* flags,
-                                  const uint32_t* runStart, uint32_t runs, const uint32_t* members,
-                                  const uint32_t* bodyMark, uint32_t* rewound, float dt, const float4* prevPos,
-                                  const float4* prevRot, Counters* C) {
-    for (uint32_t run = blockIdx.x * blockDim.x + threadIdx.x; run < runs; run += gridDim.x * blockDim.x) {
-        uint32_t rewinds = 0;
-        for (uint32_t k = runStart[run]; k < runStart[run + 1]; ++k) {
-            const uint32_t r = members[k];
+// Rewind pass over the candidate pairs in wavefronts. A candidate's
+// predecessors are the latest earlier candidates sharing one of its dynamic
+// bodies; it runs in the first round after both have run. Candidates of one
+// round share no dynamic body, and each sees exactly the body states and
+// rewound marks that the reference's single ordered loop would show it, as
+// long as no rewind moves a body outside the marked set; that case is flagged
+// and the caller widens the set and replays the pass from a snapshot.
+// Cooperative launch; every wait is bounded (gridSync).
+constexpr uint32_t kNoPred = 0xffffffffu;
+constexpr int kCaWidenLimit = 8;  // replays with a widened marked set before the serial loop
+
+__global__ void __launch_bounds__(256) caWaveKernel(BodyArrays B, Soup soup, const uint64_t* pairKeys,
+                                                    const uint32_t* flags, const uint32_t* cand, uint32_t ncand,
+                                                    const uint32_t* pred, uint32_t* doneRound,
+                                                    const uint32_t* bodyMark, uint32_t* rewound, float dt,
+                                                    const float4* prevPos, const float4* prevRot, Counters* C,
+                                                    CoopState* st) {
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+    uint32_t finished = 0;
+    for (uint32_t round = 1; round <= ncand; ++round) {
+        if (tid == 0) st->changed[(round + 1) % 3] = 0u;  // counter of the next round
+        uint32_t ran = 0, rewinds = 0;
+        for (uint32_t k = tid; k < ncand; k += stride) {
+            if (doneRound[k]) continue;  // written by this thread only
+            const uint32_t p0 = pred[2 * k], p1 = pred[2 * k + 1];
+            if (p0 != kNoPred) {
+                const uint32_t d = __ldcg(doneRound + p0);
+                if (d == 0u || d == round) continue;
+            }
+            if (p1 != kNoPred) {
+                const uint32_t d = __ldcg(doneRound + p1);
+                if (d == 0u || d == round) continue;
+            }
+            const uint32_t r = cand[k];
             const uint64_t key = pairKeys[r];
             const uint32_t ri = (uint32_t)(key >> 32), rj = (uint32_t)key;
-            if (!(flags[r] || rewound[ri] || rewound[rj])) continue;
-            uint32_t i, j;
-            orientPair(B, key, i, j);
-            if (caRewind(B, soup, i, j, dt, prevPos, prevRot)) {
-                ++rewinds;
-                const bool jDyn = isDynamic(B.filt[j].x);
-                rewound[i] = 1;
-                if (jDyn) rewound[j] = 1;
-                if (!bodyMark[i] || (jDyn && !bodyMark[j])) atomicOr(&C->caOverflow, 1u);
+            if (flags[r] || __ldcg(rewound + ri) || __ldcg(rewound + rj)) {
+                uint32_t i, j;
+                orientPair(B, key, i, j);
+                if (caRewind(B, soup, i, j, dt, prevPos, prevRot, &C->caGapQueries)) {
+                    ++rewinds;
+                    const bool jDyn = isDynamic(B.filt[j].x);
+                    __stcg(rewound + i, 1u);
+                    if (jDyn) __stcg(rewound + j, 1u);
+                    if (!bodyMark[i] || (jDyn && !bodyMark[j])) atomicOr(&C->caOverflow, 1u);
+                }
             }
+            __stcg(doneRound + k, round);
+            ++ran;
         }
+        if (ran) atomicAdd(&st->changed[round % 3], ran);
         if (rewinds) atomicAdd(&C->rewinds, rewinds);
+        if (!gridSync(&st->bar, &st->timeout)) return;
+        const uint32_t now = __ldcg(&st->changed[round % 3]);
+        if (now == 0u) {  // nothing ready: impossible while predecessors precede
+            if (tid == 0) atomicOr(&st->spill, 2u);
+            return;
+        }
+        finished += now;
+        if (finished >= ncand) {
+            if (tid == 0) st->rounds = round;
+            return;
+        }
     }
+    if (tid == 0) atomicOr(&st->spill, 2u);
+}
+
+// Entries (dynamic body, 2k + side) of the candidates; other endpoints sort last.
+__global__ void caEntryKernel(const BodyArrays B, const uint64_t* pairKeys, const uint32_t* cand, uint32_t ncand,
+                              uint32_t n, uint64_t* keys, uint32_t* vals) {
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < ncand; k += gridDim.x * blockDim.x) {
+        const uint64_t key = pairKeys[cand[k]];
+        const uint32_t a = (uint32_t)(key >> 32), b = (uint32_t)key;
+        keys[2 * k] = isDynamic(B.filt[a].x) ? a : n;
+        keys[2 * k + 1] = isDynamic(B.filt[b].x) ? b : n;
+        vals[2 * k] = 2 * k;
+        vals[2 * k + 1] = 2 * k + 1;
+    }
+}
+
+// Entries sorted stably by body: the previous entry of the same body is the predecessor.
+__global__ void caPredKernel(const uint64_t* keys, const uint32_t* vals, uint32_t entries, uint32_t n,
+                             uint32_t* pred) {
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < entries; p += gridDim.x * blockDim.x) {
+        const bool chained = p > 0 && keys[p] != (uint64_t)n && keys[p - 1] == keys[p];
+        pred[vals[p]] = chained ? (vals[p - 1] >> 1) : kNoPred;
+    }
+}
+
+// Widen the marked set by the bodies a failed pass rewound.
+__global__ void caWidenKernel(uint32_t* bodyMark, const uint32_t* rewound, uint32_t n) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        if (rewound[i]) bodyMark[i] = 1u;
 }
 
 // The reference's loop verbatim in pair order (one thread): the fallback when
@@ -1886,39 +1954,13 @@ __global__ void caFullSerialKernel(BodyArrays B, Soup soup, const uint64_t* pair
         if (!(flags[r] || rewound[ri] || rewound[rj])) continue;
         uint32_t i, j;
         orientPair(B, key, i, j);
-        if (caRewind(B, soup, i, j, dt, prevPos, prevRot)) {
+        if (caRewind(B, soup, i, j, dt, prevPos, prevRot, &C->caGapQueries)) {
             ++rewinds;
             rewound[i] = 1;
             if (isDynamic(B.filt[j].x)) rewound[j] = 1;
         }
     }
     C->rewinds = rewinds;
-}
-
-__global__ void caUnionKernel(const BodyArrays B, const uint64_t* pairKeys, const uint32_t* cand, uint32_t ncand,
-                              uint32_t* parent, Counters* C) {
-    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < ncand; k += gridDim.x * blockDim.x) {
-        const uint64_t key = pairKeys[cand[k]];
-        const uint32_t a = (uint32_t)(key >> 32), b = (uint32_t)key;
-        if (!isDynamic(B.filt[a].x) || !isDynamic(B.filt[b].x)) continue;
-        for (uint32_t tries = 0;; ++tries) {
-            if (tries == kUnionRetryLimit) { atomicOr(&C->timeout, 1u); break; }
-            uint32_t x = ufFind(parent, a), y = ufFind(parent, b);
-            if (x == y) break;
-            if (x < y) { const uint32_t t = x; x = y; y = t; }
-            if (atomicCAS(&parent[x], x, y) == x) break;
-        }
-    }
-}
-
-__global__ void caKeyKernel(const BodyArrays B, const uint64_t* pairKeys, const uint32_t* cand, uint32_t ncand,
-                            const uint32_t* root, uint64_t* keys, uint32_t* vals) {
-    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < ncand; k += gridDim.x * blockDim.x) {
-        uint32_t i, j;
-        orientPair(B, pairKeys[cand[k]], i, j);
-        keys[k] = root[i];
-        vals[k] = cand[k];
-    }
 }
 
 __global__ void copyStateKernel(const BodyArrays B, uint32_t n, float4* snap, int restore) {
@@ -2491,54 +2533,71 @@ static int conservativeAdvancement(Context& c, uint32_t npairs, float dt) {
     if (npairs == 0) return VXB_OK;
     const uint32_t n = c.n;
     VXB_TRY(ensure(c, c.caFlagBuf, (size_t)npairs * 8 + 16));
-    VXB_TRY(ensure(c, c.caBodyMarkBuf, (size_t)n * 12 + 16));
-    VXB_TRY(ensure(c, c.caCandBuf, (size_t)npairs * 24 + 16));
+    VXB_TRY(ensure(c, c.caBodyMarkBuf, (size_t)n * 8 + 16));
+    VXB_TRY(ensure(c, c.caCandBuf, (size_t)npairs * 20 + 16));
     uint32_t* flags = P<uint32_t>(c.caFlagBuf);
     uint32_t* candFlags = flags + npairs;
     uint32_t* bodyMark = P<uint32_t>(c.caBodyMarkBuf);
     uint32_t* rewound = bodyMark + n;
-    uint32_t* parent = rewound + n;
     uint32_t* ranks = P<uint32_t>(c.caCandBuf);
     uint32_t* candIndex = ranks + npairs;
-    uint32_t* runFlags = candIndex + npairs;
-    uint32_t* runIndex = runFlags + npairs;
-    uint32_t* runStart = runIndex + npairs;
-    uint32_t* members = runStart + npairs;  // sorted candidate values (aliases below)
-    (void)members;
+    uint32_t* pred = candIndex + npairs;  // two per candidate
+    uint32_t* doneRound = pred + 2 * (size_t)npairs;
     VXB_CUDA(c, cudaMemsetAsync(bodyMark, 0, (size_t)n * 8, c.stream));
     const uint64_t* pk = P<uint64_t>(c.pairKeyBuf);
     const float4* prevPos = P<float4>(c.prevPoseBuf);
     const float4* prevRot = prevPos + n;
     LAUNCH(c, caProbeKernel, std::min<uint32_t>(blocksFor(npairs, 128), (uint32_t)c.smCount * 16), 128, c.B, soupOf(c),
            pk, npairs, flags, bodyMark);
-    LAUNCH(c, caCandidateKernel, blocksFor(npairs, 256), 256, c.B, pk, npairs, flags, bodyMark, candFlags, c.dCounters);
-    VXB_TRY(exclusiveScan(c, candFlags, ranks, npairs, &c.dCounters->caCandidates));
-    VXB_TRY(readCounters(c));
-    const uint32_t ncand = c.hostCounters.caCandidates;
-    if (ncand == 0) return VXB_OK;
-    LAUNCH(c, compactKernel, blocksFor(npairs, 256), 256, candFlags, ranks, npairs, candIndex);
-    // components of candidates through shared dynamic bodies
-    LAUNCH(c, iotaKernel, blocksFor(n, 256), 256, parent, n);
-    LAUNCH(c, caUnionKernel, blocksFor(ncand, 256), 256, c.B, pk, candIndex, ncand, parent, c.dCounters);
-    LAUNCH(c, compressKernel, blocksFor(n, 256), 256, parent, n);
-    const size_t valsOffset = ((size_t)ncand * 8 + 255) & ~(size_t)255;  // keep both arrays 256-byte aligned
-    VXB_TRY(ensure(c, c.islandInfoBuf, valsOffset + (size_t)ncand * 4 + 16));
-    uint64_t* ckeys = P<uint64_t>(c.islandInfoBuf);
-    uint32_t* cvals = reinterpret_cast<uint32_t*>(P<char>(c.islandInfoBuf) + valsOffset);
-    LAUNCH(c, caKeyKernel, blocksFor(ncand, 256), 256, c.B, pk, candIndex, ncand, parent, ckeys, cvals);
-    VXB_TRY(sortPairs(c, ckeys, cvals, ncand, bitsFor(n)));
-    LAUNCH(c, runFlagKernel, blocksFor(ncand, 256), 256, ckeys, ncand, runFlags);
-    VXB_TRY(exclusiveScan(c, runFlags, runIndex, ncand, &c.dCounters->segments));
-    LAUNCH(c, runStartKernel, blocksFor(ncand, 256), 256, runFlags, runIndex, ncand, runStart);
-    VXB_TRY(readCounters(c));
-    const uint32_t runs = c.hostCounters.segments;
     VXB_TRY(ensure(c, c.snapBuf, (size_t)n * 64));
-    LAUNCH(c, copyStateKernel, blocksFor(n, 256), 256, c.B, n, P<float4>(c.snapBuf), 0);
-    LAUNCH(c, caComponentKernel, blocksFor(runs, 32), 32, c.B, soupOf(c), pk, flags, runStart, runs, cvals, bodyMark,
-           rewound, dt, prevPos, prevRot, c.dCounters);
-    VXB_TRY(readCounters(c));
-    if (c.hostCounters.caOverflow) {
+    VXB_TRY(ensure(c, c.coopBuf, sizeof(CoopState)));
+    CoopState* st = P<CoopState>(c.coopBuf);
+    bool snapped = false, serial = false;
+    for (int pass = 0;; ++pass) {
+        if (pass == kCaWidenLimit) { serial = true; break; }
+        LAUNCH(c, caCandidateKernel, blocksFor(npairs, 256), 256, c.B, pk, npairs, flags, bodyMark, candFlags,
+               c.dCounters);
+        VXB_TRY(exclusiveScan(c, candFlags, ranks, npairs, &c.dCounters->caCandidates));
+        VXB_TRY(readCounters(c));
+        const uint32_t ncand = c.hostCounters.caCandidates;
+        if (ncand == 0) return VXB_OK;
+        LAUNCH(c, compactKernel, blocksFor(npairs, 256), 256, candFlags, ranks, npairs, candIndex);
+        // predecessors through shared dynamic bodies
+        const size_t valsOffset = ((size_t)ncand * 16 + 255) & ~(size_t)255;  // both arrays 256-byte aligned
+        VXB_TRY(ensure(c, c.islandInfoBuf, valsOffset + (size_t)ncand * 8 + 16));
+        uint64_t* ekeys = P<uint64_t>(c.islandInfoBuf);
+        uint32_t* evals = reinterpret_cast<uint32_t*>(P<char>(c.islandInfoBuf) + valsOffset);
+        LAUNCH(c, caEntryKernel, blocksFor(ncand, 256), 256, c.B, pk, candIndex, ncand, n, ekeys, evals);
+        VXB_TRY(sortPairs(c, ekeys, evals, 2 * ncand, bitsFor(n)));
+        LAUNCH(c, caPredKernel, blocksFor(2 * ncand, 256), 256, ekeys, evals, 2 * ncand, n, pred);
+        if (!snapped) {
+            LAUNCH(c, copyStateKernel, blocksFor(n, 256), 256, c.B, n, P<float4>(c.snapBuf), 0);
+            snapped = true;
+        }
+        VXB_CUDA(c, cudaMemsetAsync(doneRound, 0, (size_t)ncand * 4, c.stream));
+        VXB_CUDA(c, cudaMemsetAsync(st, 0, sizeof(CoopState), c.stream));
+        const int rc = launchCooperative(c, caWaveKernel, 256, c.B, soupOf(c), pk, (const uint32_t*)flags,
+                                         (const uint32_t*)candIndex, ncand, (const uint32_t*)pred, doneRound,
+                                         (const uint32_t*)bodyMark, rewound, dt, prevPos, prevRot, c.dCounters, st);
+        if (rc == VXB_ERR_UNSUPPORTED) { serial = true; break; }
+        VXB_TRY(rc);
+        CoopState host;
+        VXB_CUDA(c, cudaMemcpyAsync(&host, st, sizeof(host), cudaMemcpyDeviceToHost, c.stream));
+        VXB_TRY(readCounters(c));
+        if (host.timeout) return fail(c, VXB_ERR_TIMEOUT, "grid barrier timed out in the rewind pass");
+        c.caRounds += host.rounds;
+        if (host.spill) { serial = true; break; }
+        if (!c.hostCounters.caOverflow) return VXB_OK;
+        // a rewind reached an unmarked body: widen the marked set and replay from the snapshot
         LAUNCH(c, copyStateKernel, blocksFor(n, 256), 256, c.B, n, P<float4>(c.snapBuf), 1);
+        LAUNCH(c, caWidenKernel, blocksFor(n, 256), 256, bodyMark, rewound, n);
+        VXB_CUDA(c, cudaMemsetAsync(rewound, 0, (size_t)n * 4, c.stream));
+        VXB_CUDA(c, cudaMemsetAsync(&c.dCounters->rewinds, 0, 4, c.stream));
+        VXB_CUDA(c, cudaMemsetAsync(&c.dCounters->caOverflow, 0, 4, c.stream));
+        ++c.caWidenings;
+    }
+    if (serial) {
+        if (snapped) LAUNCH(c, copyStateKernel, blocksFor(n, 256), 256, c.B, n, P<float4>(c.snapBuf), 1);
         VXB_CUDA(c, cudaMemsetAsync(rewound, 0, (size_t)n * 4, c.stream));
         LAUNCH(c, caFullSerialKernel, 1, 32, c.B, soupOf(c), pk, npairs, flags, rewound, dt, prevPos, prevRot,
                c.dCounters);
