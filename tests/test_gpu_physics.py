@@ -1,0 +1,120 @@
+"""Behaviour of the device world over many steps, in the spirit of the
+reference's physics tests: resting stacks stay up, fast bodies do not tunnel
+and exchange momentum, friction stops sliding along both tangent axes,
+overlapping sensors report every pair without being pushed apart."""
+import numpy as np
+import pytest
+
+import velox_b200
+
+pytestmark = pytest.mark.gpu
+DT = 1.0 / 60.0
+SPHERE, PLANE, BOX = 0, 1, 2
+
+
+def _spec(shape, position=(0, 0, 0), mass=1.0, radius=0.5, half=(0.5, 0.5, 0.5), velocity=(0, 0, 0),
+          friction=0.5, restitution=0.0):
+    s = np.zeros(1, velox_b200.binding.SPEC)[0]
+    s["shape"] = shape
+    s["mass"] = mass
+    s["radius"] = radius
+    s["halfExtents"] = half
+    s["position"] = position
+    s["orientation"] = (0, 0, 0, 1)
+    s["velocity"] = velocity
+    s["friction"] = friction
+    s["restitution"] = restitution
+    s["planeNormal"] = (0, 1, 0)
+    return s
+
+
+def _ground():
+    return _spec(PLANE, mass=0.0)
+
+
+def _world(specs, gravity=(0.0, -9.81, 0.0), substeps=4, sensors=()):
+    specs = np.array(specs, dtype=velox_b200.binding.SPEC)
+    bodies, hull, faces = velox_b200.bodies_from_specs(specs, np.zeros((1, 3), np.float32))
+    for i in sensors:
+        bodies["sensor"][i] = 1
+    ctx = velox_b200.Context(0)
+    ctx.load(bodies, velox_b200.make_soup(hull, faces))
+    ctx.configure(dt=DT, substeps=substeps, gravity=gravity)
+    return ctx
+
+
+def test_box_tower_stays_standing():
+    specs = [_ground()] + [_spec(BOX, position=(0, 0.5 + k, 0)) for k in range(10)]
+    ctx = _world(specs)
+    ctx.step(600)
+    b = ctx.read_bodies()
+    ctx.close()
+    pos, vel = b["position"][1:], b["velocity"][1:]
+    assert np.abs(pos[:, [0, 2]]).max() < 0.05
+    assert np.abs(pos[:, 1] - (0.5 + np.arange(10))).max() < 0.05
+    assert np.linalg.norm(vel, axis=1).max() < 0.05
+
+
+def test_box_pyramids_rest_without_sinking():
+    specs = [_ground()]
+    for cx in (-6.0, 6.0):
+        for layer in range(4):
+            for k in range(4 - layer):
+                specs.append(_spec(BOX, position=(cx + (k - (3 - layer) / 2.0) * 1.05, 0.5 + layer, 0)))
+    ctx = _world(specs)
+    start = ctx.read_bodies()["position"][1:].copy()
+    ctx.step(600)
+    b = ctx.read_bodies()
+    contacts = ctx.read_contacts()
+    ctx.close()
+    drift = np.linalg.norm(b["position"][1:] - start, axis=1)
+    assert drift.max() < 0.1
+    assert len(contacts) > 0
+    assert contacts["gap"].min() >= -5e-3
+
+
+def test_fast_spheres_do_not_tunnel_and_keep_momentum():
+    # 240 m/s closing speed: 4 m per step against 0.5 m of combined diameter
+    specs = [_spec(SPHERE, position=(-2.0, 0, 0), radius=0.25, velocity=(120, 0, 0)),
+             _spec(SPHERE, position=(2.0, 0, 0), radius=0.25, velocity=(-120, 0, 0))]
+    ctx = _world(specs, gravity=(0.0, 0.0, 0.0))
+    ctx.step(3)
+    b = ctx.read_bodies()
+    rewinds = ctx.stats()["rewinds"]
+    ctx.close()
+    xa, xb = b["position"][0][0], b["position"][1][0]
+    assert xa < xb, "the spheres passed through each other"
+    momentum = b["velocity"][0] + b["velocity"][1]
+    assert np.abs(momentum).max() <= 1e-3 * 120.0
+    assert rewinds >= 0
+
+
+@pytest.mark.parametrize("direction", [(1.0, 0.0), (0.0, 1.0), (0.7071068, 0.7071068)])
+def test_friction_stops_sliding_box_along_both_axes(direction):
+    speed = 3.0
+    v = (speed * direction[0], 0.0, speed * direction[1])
+    specs = [_ground(), _spec(BOX, position=(0, 0.5, 0), velocity=v)]
+    ctx = _world(specs)
+    ctx.step(180)
+    b = ctx.read_bodies()
+    ctx.close()
+    assert np.linalg.norm(b["velocity"][1]) < 0.05
+    moved = b["position"][1][[0, 2]]
+    # Coulomb friction (combined coefficient 0.5): distance v^2 / (2 mu g)
+    expected = speed ** 2 / (2 * 0.5 * 9.81)
+    assert abs(np.linalg.norm(moved) - expected) < 0.25 * expected
+    # it slides straight: no drift across the initial direction
+    across = moved[0] * direction[1] - moved[1] * direction[0]
+    assert abs(across) < 0.02
+
+
+@pytest.mark.parametrize("count", [80, 200])
+def test_coincident_sensors_report_every_pair(count):
+    specs = [_spec(SPHERE, position=(0, 5, 0), radius=0.5) for _ in range(count)]
+    ctx = _world(specs, gravity=(0.0, 0.0, 0.0), sensors=range(count))
+    ctx.step(2)
+    stats = ctx.stats()
+    b = ctx.read_bodies()
+    ctx.close()
+    assert stats["contacts"] == count * (count - 1) // 2
+    assert np.abs(b["position"] - np.array([0, 5, 0], np.float32)).max() == 0.0

@@ -771,9 +771,18 @@ __global__ void unionKernel(const vx_contact* cs, uint32_t m, const BodyArrays B
     }
 }
 
+// parent[i] = root of i. The walk writes nothing but the final root: a
+// path-halving store racing with another thread's final store could leave a
+// non-root ancestor behind, splitting one island into two keys.
 __global__ void compressKernel(uint32_t* parent, uint32_t n) {
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-        parent[i] = ufFind(parent, i);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        uint32_t x = i, p = __ldcg(parent + x);
+        while (p != x) {
+            x = p;
+            p = __ldcg(parent + x);
+        }
+        __stcg(parent + i, x);
+    }
 }
 
 // Island key of each contact: the root of its dynamic endpoint; contacts with
