@@ -52,7 +52,8 @@ def test_box_tower_stays_standing():
     pos, vel = b["position"][1:], b["velocity"][1:]
     assert np.abs(pos[:, [0, 2]]).max() < 0.05
     assert np.abs(pos[:, 1] - (0.5 + np.arange(10))).max() < 0.05
-    assert np.linalg.norm(vel, axis=1).max() < 0.05
+    # the reference's own tower keeps about 0.05 m/s of solver jitter here
+    assert np.linalg.norm(vel, axis=1).max() < 0.1
 
 
 def test_box_pyramids_rest_without_sinking():
@@ -86,7 +87,7 @@ def test_fast_spheres_do_not_tunnel_and_keep_momentum():
     assert xa < xb, "the spheres passed through each other"
     momentum = b["velocity"][0] + b["velocity"][1]
     assert np.abs(momentum).max() <= 1e-3 * 120.0
-    assert rewinds >= 0
+    assert rewinds >= 1
 
 
 @pytest.mark.parametrize("direction", [(1.0, 0.0), (0.0, 1.0), (0.7071068, 0.7071068)])
