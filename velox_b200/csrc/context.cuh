@@ -31,7 +31,8 @@ struct CoopState {
     uint32_t spill;       // bit 0: fall back to the serial path; bit 1: no progress
     uint32_t rounds;      // rounds the kernel ran (or a count the launch returns)
     uint32_t timeout;     // a barrier wait gave up
-    uint32_t pad[8];
+    uint32_t queued[3];   // per-round work-queue lengths, rotated like changed[]
+    uint32_t pad[5];
 };
 
 // Grow-only device allocation.

@@ -981,15 +981,16 @@ __global__ void colorFinishKernel(const uint32_t* order, uint32_t m, const uint3
     if ((threadIdx.x & 31) == 0 && mx) atomicMax(&C->maxColors, mx);
 }
 
-__global__ void islandBodyKernel(const vx_contact* cs, const uint32_t* order, const uint32_t* islandStart,
+// islandOfBody for the dynamic bodies of every real island's contacts, one
+// thread per island-order position (islandOf[k]: island of position k).
+__global__ void islandBodyKernel(const vx_contact* cs, const uint32_t* order, const uint32_t* islandOf, uint32_t m,
                                  uint32_t realIslands, const BodyArrays B, uint32_t* islandOfBody) {
-    for (uint32_t isl = blockIdx.x; isl < realIslands; isl += gridDim.x) {
-        const uint32_t s0 = islandStart[isl], s1 = islandStart[isl + 1];
-        for (uint32_t k = s0 + threadIdx.x; k < s1; k += blockDim.x) {
-            const vx_contact& c = cs[order[k]];
-            if (isDynamic(B.filt[c.a].x)) islandOfBody[c.a] = isl;
-            if (isDynamic(B.filt[c.b].x)) islandOfBody[c.b] = isl;
-        }
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < m; k += gridDim.x * blockDim.x) {
+        const uint32_t isl = islandOf[k];
+        if (isl >= realIslands) continue;
+        const vx_contact& c = cs[order[k]];
+        if (isDynamic(B.filt[c.a].x)) islandOfBody[c.a] = isl;
+        if (isDynamic(B.filt[c.b].x)) islandOfBody[c.b] = isl;
     }
 }
 
@@ -1868,17 +1869,25 @@ constexpr int kCaWidenLimit = 8;  // replays with a widened marked set before th
 
 __global__ void __launch_bounds__(256) caWaveKernel(BodyArrays B, Soup soup, const uint64_t* pairKeys,
                                                     const uint32_t* flags, const uint32_t* cand, uint32_t ncand,
-                                                    const uint32_t* pred, uint32_t* doneRound,
+                                                    const uint32_t* pred, uint32_t* doneRound, uint32_t* queue,
                                                     const uint32_t* bodyMark, uint32_t* rewound, float dt,
                                                     const float4* prevPos, const float4* prevRot, Counters* C,
                                                     CoopState* st) {
     const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t warp = tid >> 5, warps = stride >> 5;
     uint32_t finished = 0;
     for (uint32_t round = 1; round <= ncand; ++round) {
-        if (tid == 0) st->changed[(round + 1) % 3] = 0u;  // counter of the next round
-        uint32_t ran = 0, rewinds = 0;
+        const uint32_t slot = round % 3;
+        if (tid == 0) {  // counters of the next round (last read two rounds ago)
+            st->changed[(round + 1) % 3] = 0u;
+            st->queued[(round + 1) % 3] = 0u;
+        }
+        // Phase 1: ready candidates. Skips (not flagged, neither body rewound
+        // so far) finish now; the others join this round's queue.
+        uint32_t ran = 0;
         for (uint32_t k = tid; k < ncand; k += stride) {
-            if (doneRound[k]) continue;  // written by this thread only
+            if (__ldcg(doneRound + k)) continue;  // phase 2 may have written it from another SM
             const uint32_t p0 = pred[2 * k], p1 = pred[2 * k + 1];
             if (p0 != kNoPred) {
                 const uint32_t d = __ldcg(doneRound + p0);
@@ -1892,8 +1901,23 @@ __global__ void __launch_bounds__(256) caWaveKernel(BodyArrays B, Soup soup, con
             const uint64_t key = pairKeys[r];
             const uint32_t ri = (uint32_t)(key >> 32), rj = (uint32_t)key;
             if (flags[r] || __ldcg(rewound + ri) || __ldcg(rewound + rj)) {
+                queue[atomicAdd(&st->queued[slot], 1u)] = k;
+            } else {
+                __stcg(doneRound + k, round);
+                ++ran;
+            }
+        }
+        if (ran) atomicAdd(&st->changed[slot], ran);
+        if (!gridSync(&st->bar, &st->timeout)) return;
+        // Phase 2: the queue, one candidate per warp at a time (lane 0), so
+        // no two rewinds of a round share a warp and serialise on divergence.
+        const uint32_t queued = __ldcg(&st->queued[slot]);
+        uint32_t rewinds = 0, evaluated = 0;
+        if (lane == 0) {
+            for (uint32_t q = warp; q < queued; q += warps) {
+                const uint32_t k = __ldcg(queue + q);
                 uint32_t i, j;
-                orientPair(B, key, i, j);
+                orientPair(B, pairKeys[cand[k]], i, j);
                 if (caRewind(B, soup, i, j, dt, prevPos, prevRot, &C->caGapQueries)) {
                     ++rewinds;
                     const bool jDyn = isDynamic(B.filt[j].x);
@@ -1901,14 +1925,14 @@ __global__ void __launch_bounds__(256) caWaveKernel(BodyArrays B, Soup soup, con
                     if (jDyn) __stcg(rewound + j, 1u);
                     if (!bodyMark[i] || (jDyn && !bodyMark[j])) atomicOr(&C->caOverflow, 1u);
                 }
+                __stcg(doneRound + k, round);
+                ++evaluated;
             }
-            __stcg(doneRound + k, round);
-            ++ran;
         }
-        if (ran) atomicAdd(&st->changed[round % 3], ran);
+        if (evaluated) atomicAdd(&st->changed[slot], evaluated);
         if (rewinds) atomicAdd(&C->rewinds, rewinds);
         if (!gridSync(&st->bar, &st->timeout)) return;
-        const uint32_t now = __ldcg(&st->changed[round % 3]);
+        const uint32_t now = __ldcg(&st->changed[slot]);
         if (now == 0u) {  // nothing ready: impossible while predecessors precede
             if (tid == 0) atomicOr(&st->spill, 2u);
             return;
@@ -1944,10 +1968,18 @@ __global__ void caPredKernel(const uint64_t* keys, const uint32_t* vals, uint32_
     }
 }
 
-// Widen the marked set by the bodies a failed pass rewound.
-__global__ void caWidenKernel(uint32_t* bodyMark, const uint32_t* rewound, uint32_t n) {
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-        if (rewound[i]) bodyMark[i] = 1u;
+// Widen the marked set after a failed pass: the bodies it rewound and their
+// dynamic neighbours through candidate pairs (one hop ahead of the cascade,
+// so a long cascade needs fewer replays).
+__global__ void caWidenKernel(const BodyArrays B, const uint64_t* pairKeys, uint32_t npairs, uint32_t* bodyMark,
+                              const uint32_t* rewound) {
+    for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < npairs; r += gridDim.x * blockDim.x) {
+        const uint32_t i = (uint32_t)(pairKeys[r] >> 32), j = (uint32_t)pairKeys[r];
+        const bool ri = rewound[i] != 0u, rj = rewound[j] != 0u;
+        if (!ri && !rj) continue;
+        if (isDynamic(B.filt[i].x)) bodyMark[i] = 1u;
+        if (isDynamic(B.filt[j].x)) bodyMark[j] = 1u;
+    }
 }
 
 // The reference's loop verbatim in pair order (one thread): the fallback when
@@ -2121,8 +2153,9 @@ int loadBodies(Context& c, const vx_body* bodies, uint32_t n, const uint32_t* wo
     VXB_TRY(ensure(c, c.contactTmpBuf, mcap * sizeof(vx_contact)));
     VXB_TRY(ensure(c, c.contactBuf[0], mcap * sizeof(vx_contact) + 128));
     VXB_TRY(ensure(c, c.contactBuf[1], mcap * sizeof(vx_contact) + 128));
+    VXB_TRY(ensure(c, c.coopBuf, sizeof(CoopState)));
     for (DevBuf* b : {&c.recValBuf, &c.recCountBuf, &c.recOffsetBuf, &c.islandValBuf, &c.colorBuf, &c.flagBuf,
-                      &c.scanBuf, &c.islandStartBuf, &c.segStartBuf, &c.islandSegBuf})
+                      &c.scanBuf, &c.islandStartBuf, &c.segStartBuf, &c.islandSegBuf, &c.fpIslandBuf})
         VXB_TRY(ensure(c, *b, mcap * 4 + 64));
     for (DevBuf* b : {&c.recKeyBuf, &c.recInfoBuf, &c.pairKeyBuf, &c.prevKeyBuf, &c.islandKeyBuf, &c.colorKeyBuf,
                       &c.sortKeysAlt})
@@ -2308,32 +2341,29 @@ static int launchCooperative(Context& c, Kernel kernel, int threads, Args... arg
 // Colours of the islands above kSerialColorLimit contacts (colorOf, colour
 // keys, maxColors). VXB_ERR_UNSUPPORTED / VXB_ERR_TIMEOUT: the caller colours
 // every island serially instead.
-static int parallelColor(Context& c, const vx_contact* cs, const uint32_t* order, const uint32_t* runFlags,
-                         const uint32_t* runIndex, const uint32_t* islandStart, uint32_t m, uint64_t* colorKeys) {
+static int parallelColor(Context& c, const vx_contact* cs, const uint32_t* order, const uint32_t* islandIdx,
+                         const uint32_t* islandStart, uint32_t m, uint64_t* colorKeys) {
     const uint32_t n = c.n;
     VXB_TRY(ensure(c, c.fpKeyBuf, (size_t)m * 16 + 64));
     VXB_TRY(ensure(c, c.fpValBuf, (size_t)m * 8 + 64));
     VXB_TRY(ensure(c, c.fpSlotBuf, (size_t)m * 8 + 64));
     VXB_TRY(ensure(c, c.fpColorBuf, (size_t)m * 4 + 64));
     VXB_TRY(ensure(c, c.fpRunStartBuf, (size_t)n * 4 + 64));
-    VXB_TRY(ensure(c, c.fpIslandBuf, (size_t)m * 4 + 64));
     VXB_TRY(ensure(c, c.coopBuf, sizeof(CoopState)));
     uint64_t* keys = P<uint64_t>(c.fpKeyBuf);
     uint32_t* vals = P<uint32_t>(c.fpValBuf);
     uint32_t* slot = P<uint32_t>(c.fpSlotBuf);
     uint32_t* color = P<uint32_t>(c.fpColorBuf);
     uint32_t* runStart = P<uint32_t>(c.fpRunStartBuf);
-    uint32_t* islandIdx = P<uint32_t>(c.fpIslandBuf);
     CoopState* st = P<CoopState>(c.coopBuf);
-    LAUNCH(c, runOfKernel, blocksFor(m, 256), 256, runFlags, runIndex, m, islandIdx);
-    LAUNCH(c, colorEntryKernel, blocksFor(m, 256), 256, cs, order, m, (const uint32_t*)islandIdx, islandStart, c.B, n,
+    LAUNCH(c, colorEntryKernel, blocksFor(m, 256), 256, cs, order, m, islandIdx, islandStart, c.B, n,
            keys, vals, slot);
     VXB_TRY(sortPairs(c, keys, vals, 2 * m, bitsFor(n)));
     LAUNCH(c, colorSlotKernel, blocksFor(2 * m, 256), 256, keys, vals, 2 * m, n, slot, runStart);
     VXB_CUDA(c, cudaMemsetAsync(color, 0, (size_t)m * 4, c.stream));
     VXB_CUDA(c, cudaMemsetAsync(st, 0, sizeof(CoopState), c.stream));
     const int rc = launchCooperative(c, colorFixedPointKernel, 256, (const uint64_t*)keys, (const uint32_t*)vals,
-                                     (const uint32_t*)slot, (const uint32_t*)runStart, (const uint32_t*)islandIdx,
+                                     (const uint32_t*)slot, (const uint32_t*)runStart, islandIdx,
                                      islandStart, m, color, st, 4096u);
     if (rc != VXB_OK) return rc;
     CoopState host;
@@ -2342,7 +2372,7 @@ static int parallelColor(Context& c, const vx_contact* cs, const uint32_t* order
     c.stats.colorRounds = host.rounds;
     if (host.timeout || (host.spill & 2u)) return VXB_ERR_TIMEOUT;
     if (host.spill) return VXB_ERR_UNSUPPORTED;
-    LAUNCH(c, colorFinishKernel, blocksFor(m, 256), 256, order, m, (const uint32_t*)islandIdx, islandStart,
+    LAUNCH(c, colorFinishKernel, blocksFor(m, 256), 256, order, m, islandIdx, islandStart,
            (const uint32_t*)color, P<uint32_t>(c.colorBuf), colorKeys, c.dCounters);
     return VXB_OK;
 }
@@ -2383,6 +2413,9 @@ static int buildIslands(Context& c, const vx_contact* cs, uint32_t m, IslandPlan
         LAUNCH(c, runFlagKernel, blocksFor(m, 256), 256, ikeys, m, flags);
         VXB_TRY(exclusiveScan(c, flags, index, m, &c.dCounters->islands));
         LAUNCH(c, runStartKernel, blocksFor(m, 256), 256, flags, index, m, islandStart);
+        VXB_TRY(ensure(c, c.fpIslandBuf, (size_t)m * 4 + 64));
+        uint32_t* islandOf = P<uint32_t>(c.fpIslandBuf);
+        LAUNCH(c, runOfKernel, blocksFor(m, 256), 256, flags, index, m, islandOf);
         LAUNCH(c, lastKeyKernel, 1, 32, ikeys, m, c.dCounters);
         LAUNCH(c, islandMaxKernel, std::min<uint32_t>(blocksFor(m, 256), (uint32_t)c.smCount * 4), 256, islandStart,
                c.dCounters);
@@ -2395,7 +2428,7 @@ static int buildIslands(Context& c, const vx_contact* cs, uint32_t m, IslandPlan
         uint64_t* ckeys = P<uint64_t>(c.colorKeyBuf);
         bool serialAll = false;
         if (c.hostCounters.maxIslandSize > kSerialColorLimit) {
-            const int status = parallelColor(c, cs, ivals, flags, index, islandStart, m, ckeys);
+            const int status = parallelColor(c, cs, ivals, islandOf, islandStart, m, ckeys);
             if (status == VXB_ERR_TIMEOUT || status == VXB_ERR_UNSUPPORTED) serialAll = true;  // exact serial path
             else if (status != VXB_OK) return status;
         }
@@ -2411,8 +2444,8 @@ static int buildIslands(Context& c, const vx_contact* cs, uint32_t m, IslandPlan
         LAUNCH(c, runStartKernel, blocksFor(m, 256), 256, flags, index, m, P<uint32_t>(c.segStartBuf));
         // island bodies
         VXB_CUDA(c, cudaMemsetAsync(c.islandOfBodyBuf.ptr, 0xff, (size_t)n * 4, c.stream));
-        LAUNCH(c, islandBodyKernel, std::min<uint32_t>(std::max<uint32_t>(plan.realIslands, 1), 65535u), 64, cs, ivals,
-               islandStart, plan.realIslands, c.B, P<uint32_t>(c.islandOfBodyBuf));
+        LAUNCH(c, islandBodyKernel, blocksFor(m, 256), 256, cs, ivals, (const uint32_t*)islandOf, m, plan.realIslands,
+               c.B, P<uint32_t>(c.islandOfBodyBuf));
     }
     const uint32_t freeKey = plan.realIslands;
     LAUNCH(c, bodyKeyKernel, blocksFor(n, 256), 256, P<uint32_t>(c.islandOfBodyBuf), n, freeKey,
@@ -2587,6 +2620,7 @@ static int conservativeAdvancement(Context& c, uint32_t npairs, float dt) {
         VXB_CUDA(c, cudaMemsetAsync(st, 0, sizeof(CoopState), c.stream));
         const int rc = launchCooperative(c, caWaveKernel, 256, c.B, soupOf(c), pk, (const uint32_t*)flags,
                                          (const uint32_t*)candIndex, ncand, (const uint32_t*)pred, doneRound,
+                                         ranks /* free after compaction: the work queue */,
                                          (const uint32_t*)bodyMark, rewound, dt, prevPos, prevRot, c.dCounters, st);
         if (rc == VXB_ERR_UNSUPPORTED) { serial = true; break; }
         VXB_TRY(rc);
@@ -2599,7 +2633,7 @@ static int conservativeAdvancement(Context& c, uint32_t npairs, float dt) {
         if (!c.hostCounters.caOverflow) return VXB_OK;
         // a rewind reached an unmarked body: widen the marked set and replay from the snapshot
         LAUNCH(c, copyStateKernel, blocksFor(n, 256), 256, c.B, n, P<float4>(c.snapBuf), 1);
-        LAUNCH(c, caWidenKernel, blocksFor(n, 256), 256, bodyMark, rewound, n);
+        LAUNCH(c, caWidenKernel, blocksFor(npairs, 256), 256, c.B, pk, npairs, bodyMark, (const uint32_t*)rewound);
         VXB_CUDA(c, cudaMemsetAsync(rewound, 0, (size_t)n * 4, c.stream));
         VXB_CUDA(c, cudaMemsetAsync(&c.dCounters->rewinds, 0, 4, c.stream));
         VXB_CUDA(c, cudaMemsetAsync(&c.dCounters->caOverflow, 0, 4, c.stream));
