@@ -1909,12 +1909,15 @@ __global__ void __launch_bounds__(256) caWaveKernel(BodyArrays B, Soup soup, con
         }
         if (ran) atomicAdd(&st->changed[slot], ran);
         if (!gridSync(&st->bar, &st->timeout)) return;
-        // Phase 2: the queue, one candidate per warp at a time (lane 0), so
-        // no two rewinds of a round share a warp and serialise on divergence.
+        // Phase 2: the queue. A short queue runs one candidate per warp
+        // (lane 0), so no two evaluations share a warp and serialise on
+        // divergence; a long one runs one per thread for throughput.
         const uint32_t queued = __ldcg(&st->queued[slot]);
+        const bool perWarp = queued <= warps;
         uint32_t rewinds = 0, evaluated = 0;
-        if (lane == 0) {
-            for (uint32_t q = warp; q < queued; q += warps) {
+        if (!perWarp || lane == 0) {
+            const uint32_t first = perWarp ? warp : tid, step = perWarp ? warps : stride;
+            for (uint32_t q = first; q < queued; q += step) {
                 const uint32_t k = __ldcg(queue + q);
                 uint32_t i, j;
                 orientPair(B, pairKeys[cand[k]], i, j);
