@@ -36,6 +36,8 @@ L2_FLUSH_BYTES = 256 << 20
 # per contact row and sweep (contact constants 64 + impulses r/w 48 + two
 # bodies' pose/velocity/mass reads 168 + velocity writes 48).
 SOLVER_BYTES_PER_ROW = 328
+# Rewind: one distance query reads both bodies' 256-byte records.
+REWIND_BYTES_PER_QUERY = 512
 
 
 def measured_peaks():
@@ -100,9 +102,13 @@ def build_scene(size):
     return specs, pool, bodies, vb.make_soup(hull, faces)
 
 
-def cpu_baseline(specs, pool, n_bodies, budget_s=20.0, max_steps=40, warm_steps=1):
+def cpu_baseline(specs, pool, n_bodies, checkpoints, total_steps):
     """The reference CPU backend (default Release build, all host threads) on
-    the same scene, timed for a bounded number of steps."""
+    the same scene, sampled along the trajectory: from each checkpoint state
+    (captured during the timed device steps, evenly spaced), one step to settle
+    the contact caches and one timed step. Each timed step stands for its
+    share of the trajectory, so early cheap steps and late pile steps weigh
+    what they weigh in the device run."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import ref
     if not ref.available(strict=False):
@@ -110,17 +116,20 @@ def cpu_baseline(specs, pool, n_bodies, budget_s=20.0, max_steps=40, warm_steps=
     w = ref.RefWorld(specs, pool, backend=ref.BACKEND_CPU, strict=False)
     w.configure(substeps=SUBSTEPS, workers=0)
     workers = int(w.L.ref_world_worker_count(w.h))
-    w.step(DT, warm_steps)
-    steps, total = 0, 0.0
-    while steps < max_steps and total < budget_s:
-        total += w.step(DT, 1) / 1000.0
-        steps += 1
+    est, spent = 0.0, 0.0
+    t0 = time.perf_counter()
+    for state in checkpoints:
+        w.set_bodies(state)
+        w.step(DT, 1)
+        est += (w.step(DT, 1) / 1000.0) * (total_steps / len(checkpoints))
+    spent = time.perf_counter() - t0
     w.close()
-    value = n_bodies * steps / total
+    value = n_bodies * total_steps / est
     return {"value": value, "unit": "body-steps/s", "cores": workers, "kind": "reference",
-            "sample": f"{steps} steps of the {n_bodies}-body scene after {warm_steps} warm-up step(s), "
-                      f"reference CPU backend (Release build) with {workers} worker threads on "
-                      f"{os.cpu_count()} host cores, {total:.1f} s"}
+            "sample": f"{len(checkpoints)} timed steps of the {n_bodies}-body scene, one from each of "
+                      f"{len(checkpoints)} evenly spaced states of the {total_steps}-step device trajectory "
+                      f"(each after one settling step), weighted equally; reference CPU backend (Release "
+                      f"build), {workers} worker threads on {os.cpu_count()} host cores; {spent:.1f} s"}
 
 
 def run_reference(args):
@@ -129,7 +138,7 @@ def run_reference(args):
         return 0
     specs, pool, bodies, soup = build_scene(args.size)
     n = len(bodies)
-    budget = float(os.environ.get("VXB_REFERENCE_BUDGET_S", "150"))
+    budget = float(os.environ.get("VXB_REFERENCE_BUDGET_S", "240"))
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import ref
     if not ref.available(strict=False):
@@ -209,10 +218,15 @@ def main():
     ctx.enable_timing(True)
     events = []
     contacts_total = 0
+    gap_queries_total = 0
     if args.profile:
         torch.cuda.cudart().cudaProfilerStart()
+    checkpoints = []
+    marks = {int(args.steps * i / 5) for i in range(5)}
     with torch.cuda.stream(stream):
-        for _ in range(args.steps):
+        for step in range(args.steps):
+            if step in marks and rank == 0 and world == 1 and not args.no_cpu_baseline:
+                checkpoints.append(ctx.read_bodies())  # between steps, outside the events
             flush.fill_(1)
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
@@ -220,7 +234,9 @@ def main():
             ctx.step(1)
             e1.record(stream)
             events.append((e0, e1))
-            contacts_total += ctx.stats()["contacts"]
+            st = ctx.stats()
+            contacts_total += st["contacts"]
+            gap_queries_total += st["rewindGapQueries"]
     if args.profile:
         torch.cuda.cudart().cudaProfilerStop()
     barrier()
@@ -235,49 +251,69 @@ def main():
         ms = float(t.item())
     value = world * n * args.steps / (ms / 1e3)
 
-    # Roofline of the island solve (memory-bound sweeps over contact rows).
+    # Roofline. Island solve: memory-bound sweeps over contact rows.
+    # Rewind: distance queries on two bodies' records along a dependency
+    # chain (latency-bound; reported against the same HBM peak).
     peak, peak_kind = measured_peaks()
     solve_ms, solve_calls = stage["solve"]
     rows = contacts_total * 2 * 8 * SUBSTEPS  # sweeps * substeps per step
     solve_bytes = rows * SOLVER_BYTES_PER_ROW
-    achieved = solve_bytes / (solve_ms / 1e3) / 1e9 if solve_ms > 0 else 0.0
-    roofline = {"bound": "hbm", "kernel": "solveBlockKernel+solveTinyKernel (island substep solve)",
-                "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "peak_source": peak_kind, "traffic": None,
-                "algorithmic_bytes_per_launch": solve_bytes / max(solve_calls, 1),
-                "avg_launch_ms": solve_ms / max(solve_calls, 1)}
+    solve_gbs = solve_bytes / (solve_ms / 1e3) / 1e9 if solve_ms > 0 else 0.0
+    solve_roofline = {"bound": "hbm", "kernel": "solveTinyKernel+solveBlockKernel+solveGiantKernel (substep solve)",
+                      "achieved": solve_gbs, "peak": peak, "unit": "GB/s", "frac": solve_gbs / peak,
+                      "peak_source": peak_kind, "traffic": None,
+                      "algorithmic_bytes_per_launch": solve_bytes / max(solve_calls, 1),
+                      "avg_launch_ms": solve_ms / max(solve_calls, 1)}
+    rewind_ms, rewind_calls = stage["rewind"]
+    rewind_bytes = gap_queries_total * REWIND_BYTES_PER_QUERY
+    rewind_gbs = rewind_bytes / (rewind_ms / 1e3) / 1e9 if rewind_ms > 0 else 0.0
+    rewind_roofline = {"bound": "hbm", "kernel": "caProbeKernel+caWaveKernel (rewind pass)",
+                       "achieved": rewind_gbs, "peak": peak, "unit": "GB/s", "frac": rewind_gbs / peak,
+                       "peak_source": peak_kind, "traffic": None,
+                       "algorithmic_bytes_per_launch": rewind_bytes / max(rewind_calls, 1),
+                       "avg_launch_ms": rewind_ms / max(rewind_calls, 1),
+                       "note": "a chain of dependent distance queries: latency-bound, not bandwidth-bound"}
+    dominant = max(stage.items(), key=lambda kv: kv[1][0])[0]
+    roofline = rewind_roofline if dominant == "rewind" else solve_roofline
+    roofline = dict(roofline, stage=dominant)
 
-    # End to end through the C ABI: forces in from pinned host memory, one
-    # step, poses back to pinned host memory, every step.
+    # End to end through the C ABI, on a fresh world over the same steps:
+    # forces in from pinned host memory, one step, poses back to pinned host
+    # memory, every step (host copies inside the timed region).
+    ctx2 = vb.Context(local)
+    ctx2.set_stream(stream.cuda_stream)
+    ctx2.load(bodies, soup)
+    ctx2.configure(dt=DT, substeps=SUBSTEPS)
+    ctx2.step(max(args.warmup, 3) if args.warmup >= 3 else args.warmup)
     forces = torch.zeros((n, 6), dtype=torch.float32).pin_memory()
     poses = torch.zeros((n, 7), dtype=torch.float32).pin_memory()
     fptr, pptr = forces.numpy(), poses.numpy()
-    e2e_steps = max(1, min(args.steps, 50))
     barrier()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     t0 = time.perf_counter()
     e0.record(stream)
-    for _ in range(e2e_steps):
-        ctx.write_forces(fptr)
-        ctx.step(1)
-        ctx.read_poses(pptr)
+    for _ in range(args.steps):
+        ctx2.write_forces(fptr)
+        ctx2.step(1)
+        ctx2.read_poses(pptr)
     e1.record(stream)
     barrier()
     wall = time.perf_counter() - t0
+    ctx2.close()
     e2e_ms = e0.elapsed_time(e1)
     if dist:
         t = torch.tensor([e2e_ms], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_ms = float(t.item())
-    e2e = {"value": world * n * e2e_steps / (e2e_ms / 1e3), "unit": "body-steps/s",
+    e2e = {"value": world * n * args.steps / (e2e_ms / 1e3), "unit": "body-steps/s",
            "h2d_bytes_per_step": int(forces.numel() * 4), "d2h_bytes_per_step": int(poses.numel() * 4),
-           "steps": e2e_steps, "wall_s": wall}
+           "steps": args.steps, "wall_s": wall}
 
     baseline = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            baseline = cpu_baseline(specs, pool, n)
+            baseline = cpu_baseline(specs, pool, n, checkpoints, args.steps)
         except Exception as exc:  # reported, not fatal
             baseline = {"error": str(exc)}
 
@@ -295,7 +331,8 @@ def main():
                        "l2": "flushed (256 MiB write) before every timed step, outside the step's events"},
             "contacts_per_s": contacts_total / (ms / 1e3), "last_step": stats,
             "stage_ms_per_step": {k: v[0] / args.steps for k, v in stage.items()},
-            "roofline": roofline, "cpu_baseline": baseline, "e2e": e2e, "clocks": clocks,
+            "roofline": roofline, "solve_roofline": solve_roofline, "rewind_roofline": rewind_roofline,
+            "cpu_baseline": baseline, "e2e": e2e, "clocks": clocks,
             "gpu_launches": int(launches)}
     print(json.dumps(line))
     return 0

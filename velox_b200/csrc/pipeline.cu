@@ -1797,6 +1797,12 @@ __device__ __noinline__ bool caRewind(BodyArrays& B, const Soup& soup, uint32_t 
                                       const float4* prevPos, const float4* prevRot, uint32_t* gapQueries) {
     BodyView a = loadView(B, i), b = loadView(B, j);
     if (!caEligible(a, b, B, i)) return false;
+    if (shapeOf(b.flags) != kPlane) {
+        // bounding spheres more than 1 mm apart: positive end gap, no rewind (the probe's test)
+        const float reach = coreExtent(shapeOf(a.flags), a.half, a.radius, a.hh) +
+                            coreExtent(shapeOf(b.flags), b.half, b.radius, b.hh) + 1e-3f;
+        if (lengthSq(a.p - b.p) > reach * reach) return false;
+    }
     const GapProbe end = gapAt(a, b, soup);
     if (end.gap >= -8e-3f) return false;
     const bool bStatic = isStaticBody(b.flags), bDyn = isDynamic(b.flags);
