@@ -167,6 +167,12 @@ int vxb_stage_pairs(vxb_context* ctx, const vx_body* bodies, uint32_t n, float d
 int vxb_stage_collide(vxb_context* ctx, const vx_body* bodies, uint32_t n, const vx_soup* soup,
                       const uint64_t* pairs, uint32_t npairs, float dt, vx_contact* out,
                       uint32_t cap, uint32_t* counts, uint32_t* total);
+/* gjkDistance(makeConvex(a), makeConvex(b)) (include/velox/gjk.h:751-777)
+ * for each listed pair: out[11*p ..] = distance, normal xyz, pointA xyz,
+ * pointB xyz, overlapping (1/0). path 0 = the rewind's query (register GJK,
+ * general GJK/EPA on overlap), 1 = the general GJK/EPA only. */
+int vxb_stage_distance(vxb_context* ctx, const vx_body* bodies, uint32_t n, const vx_soup* soup,
+                       const uint64_t* pairs, uint32_t npairs, int path, float* out);
 /* Greedy first-free-bit colouring (src/backend_cuda.cu:603-630) of contacts
  * already in (a, b, point) order. */
 int vxb_stage_color(vxb_context* ctx, const vx_body* bodies, uint32_t n,

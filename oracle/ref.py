@@ -168,6 +168,20 @@ def collide_pairs(bodies, soup, pairs, dt, strict=True):
     return out[:total], counts[:len(pairs)]
 
 
+def gjk_distances(bodies, soup, pairs, strict=True):
+    """gjkDistance(makeConvex(a), makeConvex(b)) per pair, rows of 11 floats
+    (distance, normal, pointA, pointB, overlapping) like vxb_stage_distance."""
+    L = lib(strict)
+    pairs = np.ascontiguousarray(pairs, np.uint64)
+    out = np.zeros((max(len(pairs), 1), 11), np.float32)
+    row = np.zeros(11, np.float32)
+    for k, key in enumerate(pairs.tolist()):
+        a, b = key >> 32, key & 0xffffffff
+        L.ref_gjk(_p(bodies[a:a + 1]), _p(bodies[b:b + 1]), ctypes.byref(soup), _p(row))
+        out[k] = row
+    return out[:len(pairs)]
+
+
 def sort_contacts(contacts, strict=True):
     c = np.ascontiguousarray(contacts).copy()
     lib(strict).ref_sort_contacts(_p(c), len(c))

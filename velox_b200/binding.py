@@ -164,6 +164,7 @@ def lib(path=LIB_PATH):
         "vxb_world_stats": ([vp, ctypes.POINTER(StepStats)], i32),
         "vxb_stage_pairs": ([vp, vp, u32, f32, vp, u32, p_u32], i32),
         "vxb_stage_collide": ([vp, vp, u32, ctypes.POINTER(Soup), vp, u32, f32, vp, u32, vp, p_u32], i32),
+        "vxb_stage_distance": ([vp, vp, u32, ctypes.POINTER(Soup), vp, u32, i32, vp], i32),
         "vxb_stage_color": ([vp, vp, u32, vp, u32, vp, p_u32], i32),
         "vxb_stage_pairs_noalloc": ([vp, u32, f32, vp, u32, p_u32, vp], i32),
         "vxb_scene_generate": ([i32, ctypes.c_uint64, u32, vp, u32, p_u32, vp, u32, p_u32], i32),
@@ -323,6 +324,15 @@ class Context:
         self._check(self.L.vxb_stage_collide(self.h, ptr(bodies), len(bodies), ctypes.byref(soup), ptr(pairs),
                                              len(pairs), dt, ptr(out), cap, ptr(counts), ctypes.byref(total)))
         return out[:total.value], counts[:len(pairs)]
+
+    def distance(self, bodies, soup, pairs, path=0):
+        """gjkDistance per pair: (npairs, 11) float32 rows (distance, normal,
+        pointA, pointB, overlapping)."""
+        pairs = np.ascontiguousarray(pairs, np.uint64)
+        out = np.zeros((max(len(pairs), 1), 11), np.float32)
+        self._check(self.L.vxb_stage_distance(self.h, ptr(bodies), len(bodies), ctypes.byref(soup), ptr(pairs),
+                                              len(pairs), path, ptr(out)))
+        return out[:len(pairs)]
 
     def color(self, bodies, contacts):
         colors = np.zeros(max(len(contacts), 1), np.int32)

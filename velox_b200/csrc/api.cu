@@ -304,6 +304,19 @@ int vxb_stage_pairs(vxb_context* ctx, const vx_body* bodies, uint32_t n, float d
     return vxb::stagePairs(c, dt, out, cap, count);
 }
 
+int vxb_stage_distance(vxb_context* ctx, const vx_body* bodies, uint32_t n, const vx_soup* soup,
+                       const uint64_t* pairs, uint32_t npairs, int path, float* out) {
+    GUARD(ctx);
+    if (!bodies || n == 0 || (npairs && (!pairs || !out)) || (path != 0 && path != 1)) return VXB_ERR_INVALID;
+    Context& c = ctx->impl;
+    for (uint32_t p = 0; p < npairs; ++p)
+        if ((uint32_t)(pairs[p] >> 32) >= n || (uint32_t)pairs[p] >= n) return VXB_ERR_INVALID;
+    TRY(ensureCounters(c));
+    TRY(vxb::loadBodies(c, bodies, n, nullptr));
+    TRY(vxb::loadSoup(c, soup));
+    return vxb::stageDistance(c, pairs, npairs, path, out);
+}
+
 int vxb_stage_collide(vxb_context* ctx, const vx_body* bodies, uint32_t n, const vx_soup* soup,
                       const uint64_t* pairs, uint32_t npairs, float dt, vx_contact* out, uint32_t cap,
                       uint32_t* counts, uint32_t* total) {

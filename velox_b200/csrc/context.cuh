@@ -197,6 +197,7 @@ int stagePairs(Context& c, float dt, uint64_t* out, uint32_t cap, uint32_t* coun
 int stageCollide(Context& c, const uint64_t* pairs, uint32_t npairs, float dt, vx_contact* out,
                  uint32_t cap, uint32_t* counts, uint32_t* total);
 int stageColor(Context& c, const vx_contact* contacts, uint32_t m, int32_t* colorOf, uint32_t* numColors);
+int stageDistance(Context& c, const uint64_t* pairs, uint32_t npairs, int path, float* out);
 int backendIntegrate(Context& c, vx_vec3 gravity, float dt);
 int backendFindContacts(Context& c, float dt, uint32_t* count);
 int backendCopyContacts(Context& c, vx_contact* out, uint32_t cap);

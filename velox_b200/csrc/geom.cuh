@@ -175,7 +175,7 @@ VXD V3 hullPoint(const float* pts, uint32_t i) {
     return V3{pts[3 * i], pts[3 * i + 1], pts[3 * i + 2]};
 }
 
-static __device__ __noinline__ V3 supportOffset(const Convex& c, const V3& dir) {
+VXD V3 supportOffsetBody(const Convex& c, const V3& dir) {
     switch (c.kind) {
     case cPoint: return V3{0.0f, 0.0f, 0.0f};
     case cSegment: {
@@ -235,6 +235,8 @@ static __device__ __noinline__ V3 supportOffset(const Convex& c, const V3& dir) 
     default: return V3{0.0f, 0.0f, 0.0f};
     }
 }
+// Out-of-line copy for the general GJK/EPA paths (keeps their code size down).
+static __device__ __noinline__ V3 supportOffset(const Convex& c, const V3& dir) { return supportOffsetBody(c, dir); }
 VXD V3 support(const Convex& c, const V3& dir) { return c.position + supportOffset(c, dir); }
 
 // makeConvex (gjk.h:155-226).
@@ -345,56 +347,67 @@ VXD SupportVert supportVertex(const Convex& A, const Convex& B, const V3& dir) {
     return s;
 }
 
-VXD void solveSegment(Simplex& s) {
-    const V3 a = s.v[0].p, b = s.v[1].p;
+// Closest point of a segment / triangle simplex to the origin (gjk.h:301-380)
+// on named vertices, so the register-resident GJK below and the general one
+// run the same arithmetic.
+VXD void solveSegmentV(SupportVert& v0, const SupportVert& v1, float& b0, float& b1, int& count) {
+    const V3 a = v0.p, b = v1.p;
     const V3 ab = b - a;
     float t = -dot(a, ab);
-    if (t <= 0.0f) { s.count = 1; s.bary[0] = 1.0f; return; }
+    if (t <= 0.0f) { count = 1; b0 = 1.0f; return; }
     const float denom = dot(ab, ab);
-    if (t >= denom) { s.v[0] = s.v[1]; s.count = 1; s.bary[0] = 1.0f; return; }
+    if (t >= denom) { v0 = v1; count = 1; b0 = 1.0f; return; }
     t /= denom;
-    s.count = 2; s.bary[0] = 1.0f - t; s.bary[1] = t;
+    count = 2; b0 = 1.0f - t; b1 = t;
 }
 
-static __device__ __noinline__ void solveTriangle(Simplex& s) {
-    const V3 a = s.v[0].p, b = s.v[1].p, c = s.v[2].p;
+VXD void solveTriangleV(SupportVert& v0, SupportVert& v1, const SupportVert& v2, float& b0, float& b1, float& b2,
+                        int& count) {
+    const V3 a = v0.p, b = v1.p, c = v2.p;
     const V3 ab = b - a, ac = c - a, ap = -a;
     const float d1 = dot(ab, ap), d2 = dot(ac, ap);
-    if (d1 <= 0.0f && d2 <= 0.0f) { s.count = 1; s.bary[0] = 1.0f; return; }
+    if (d1 <= 0.0f && d2 <= 0.0f) { count = 1; b0 = 1.0f; return; }
     const V3 bp = -b;
     const float d3 = dot(ab, bp), d4 = dot(ac, bp);
-    if (d3 >= 0.0f && d4 <= d3) { s.v[0] = s.v[1]; s.count = 1; s.bary[0] = 1.0f; return; }
+    if (d3 >= 0.0f && d4 <= d3) { v0 = v1; count = 1; b0 = 1.0f; return; }
     const float vc = d1 * d4 - d3 * d2;
     if (vc <= 0.0f && d1 >= 0.0f && d3 <= 0.0f) {
         const float t = d1 / (d1 - d3);
-        s.count = 2; s.bary[0] = 1.0f - t; s.bary[1] = t; return;
+        count = 2; b0 = 1.0f - t; b1 = t; return;
     }
     const V3 cp = -c;
     const float d5 = dot(ab, cp), d6 = dot(ac, cp);
-    if (d6 >= 0.0f && d5 <= d6) { s.v[0] = s.v[2]; s.count = 1; s.bary[0] = 1.0f; return; }
+    if (d6 >= 0.0f && d5 <= d6) { v0 = v2; count = 1; b0 = 1.0f; return; }
     const float vb = d5 * d2 - d1 * d6;
     if (vb <= 0.0f && d2 >= 0.0f && d6 <= 0.0f) {
         const float t = d2 / (d2 - d6);
-        s.v[1] = s.v[2];
-        s.count = 2; s.bary[0] = 1.0f - t; s.bary[1] = t; return;
+        v1 = v2;
+        count = 2; b0 = 1.0f - t; b1 = t; return;
     }
     const float va = d3 * d6 - d5 * d4;
     if (va <= 0.0f && (d4 - d3) >= 0.0f && (d5 - d6) >= 0.0f) {
         const float t = (d4 - d3) / ((d4 - d3) + (d5 - d6));
-        s.v[0] = s.v[1]; s.v[1] = s.v[2];
-        s.count = 2; s.bary[0] = 1.0f - t; s.bary[1] = t; return;
+        v0 = v1; v1 = v2;
+        count = 2; b0 = 1.0f - t; b1 = t; return;
     }
     const float sum = va + vb + vc;
     if (sum < 1e-20f) {  // degenerate triangle: keep the vertex nearest the origin
         int best = 0;
-        for (int i = 1; i < 3; ++i)
-            if (lengthSq(s.v[i].p) < lengthSq(s.v[best].p)) best = i;
-        s.v[0] = s.v[best];
-        s.count = 1; s.bary[0] = 1.0f;
+        if (lengthSq(v1.p) < lengthSq(v0.p)) best = 1;
+        if (lengthSq(v2.p) < lengthSq((best == 0 ? v0 : v1).p)) best = 2;
+        if (best == 1) v0 = v1;
+        else if (best == 2) v0 = v2;
+        count = 1; b0 = 1.0f;
         return;
     }
     const float inv = 1.0f / sum;
-    s.count = 3; s.bary[0] = va * inv; s.bary[1] = vb * inv; s.bary[2] = vc * inv;
+    count = 3; b0 = va * inv; b1 = vb * inv; b2 = vc * inv;
+}
+
+VXD void solveSegment(Simplex& s) { solveSegmentV(s.v[0], s.v[1], s.bary[0], s.bary[1], s.count); }
+
+static __device__ __noinline__ void solveTriangle(Simplex& s) {
+    solveTriangleV(s.v[0], s.v[1], s.v[2], s.bary[0], s.bary[1], s.bary[2], s.count);
 }
 
 static __constant__ int kTetFaces[4][3] = {{0, 1, 2}, {0, 1, 3}, {0, 2, 3}, {1, 2, 3}};
@@ -716,6 +729,139 @@ VXD GjkResult gjkDistance(const Convex& A, const Convex& B) {
         }
     }
     return best;
+}
+
+// ---- register-resident GJK distance --------------------------------------
+//
+// gjkSeeded for Normal-quality pairs (quality 0: 32 iterations, no re-seeding)
+// with the same arithmetic in the same order, the simplex in named registers
+// instead of an indexed array, and the support mappings inlined: a single
+// thread runs it at register latency rather than local-memory latency, which
+// is what the rewind pass's chains of dependent queries wait on. When the
+// general routine would report an overlap (and go on to EPA) this one returns
+// false and the caller runs gjkDistance, which then produces that result.
+
+VXD SupportVert supportVertexInline(const Convex& A, const Convex& B, const V3& dir) {
+    SupportVert s;
+    const V3 oa = supportOffsetBody(A, dir);
+    const V3 ob = supportOffsetBody(B, -dir);
+    s.a = A.position + oa;
+    s.b = B.position + ob;
+    s.p = (A.position - B.position) + (oa - ob);
+    return s;
+}
+
+// One face of solveTetrahedron: solve the triangle (x, y, z) and keep it when
+// its closest point is nearer than the best so far (strictly).
+VXD void tetFaceCandidate(const SupportVert& x, const SupportVert& y, const SupportVert& z, SupportVert& t0,
+                          SupportVert& t1, SupportVert& t2, float& c0, float& c1, float& c2, int& bc,
+                          float& bestDist) {
+    SupportVert u0 = x, u1 = y, u2 = z;
+    float e0 = 0.0f, e1 = 0.0f, e2 = 0.0f;
+    int n = 3;
+    solveTriangleV(u0, u1, u2, e0, e1, e2, n);
+    V3 c{0.0f, 0.0f, 0.0f};
+    c += u0.p * e0;
+    if (n > 1) c += u1.p * e1;
+    if (n > 2) c += u2.p * e2;
+    const float d = lengthSq(c);
+    if (d < bestDist) {
+        bestDist = d;
+        t0 = u0; t1 = u1; t2 = u2;
+        c0 = e0; c1 = e1; c2 = e2;
+        bc = n;
+    }
+}
+
+// solveTetrahedron (gjk.h:382-445) on named vertices; true = origin inside.
+VXD bool solveTetrahedronV(SupportVert& v0, SupportVert& v1, SupportVert& v2, const SupportVert& v3, float& b0,
+                           float& b1, float& b2, int& count, float scale) {
+    const float volume = dot(v1.p - v0.p, cross(v2.p - v0.p, v3.p - v0.p));
+    const float floorVol = 1e-10f * scale * scale * scale;
+    SupportVert t0 = v0, t1 = v0, t2 = v0;
+    float c0 = 0.0f, c1 = 0.0f, c2 = 0.0f;
+    int bc = 0;
+    float bestDist = 1e30f;
+    if (fabsf(volume) < floorVol) {
+        tetFaceCandidate(v0, v1, v2, t0, t1, t2, c0, c1, c2, bc, bestDist);
+        tetFaceCandidate(v0, v1, v3, t0, t1, t2, c0, c1, c2, bc, bestDist);
+        tetFaceCandidate(v0, v2, v3, t0, t1, t2, c0, c1, c2, bc, bestDist);
+        tetFaceCandidate(v1, v2, v3, t0, t1, t2, c0, c1, c2, bc, bestDist);
+        v0 = t0; v1 = t1; v2 = t2; b0 = c0; b1 = c1; b2 = c2; count = bc;
+        return false;
+    }
+    bool inside = true;
+    const float boundary = 3e-6f * scale;
+#pragma unroll
+    for (int f = 0; f < 4; ++f) {
+        const SupportVert& x = f == 3 ? v1 : v0;
+        const SupportVert& y = f == 0 || f == 1 ? v1 : v2;
+        const SupportVert& z = f == 0 ? v2 : v3;
+        const SupportVert& o = f == 0 ? v3 : f == 1 ? v2 : f == 2 ? v1 : v0;
+        const V3 a = x.p, b = y.p, c = z.p;
+        const V3 n = cross(b - a, c - a);
+        const float nLen = length(n);
+        if (nLen < 1e-20f) continue;
+        const float originDist = dot(n, -a) / nLen;
+        const float oppositeDist = dot(n, o.p - a) / nLen;
+        if (originDist * oppositeDist < 0.0f || fabsf(originDist) <= boundary) {
+            inside = false;
+            tetFaceCandidate(x, y, z, t0, t1, t2, c0, c1, c2, bc, bestDist);
+        }
+    }
+    if (!inside) { v0 = t0; v1 = t1; v2 = t2; b0 = c0; b1 = c1; b2 = c2; count = bc; }
+    return inside;
+}
+
+VXD bool gjkDistanceFast(const Convex& A, const Convex& B, GjkResult& r) {
+    if (pairQuality(A, B) != 0) return false;
+    const float scale = pairScale(A, B);
+    V3 dir = A.position - B.position;
+    if (lengthSq(dir) < 1e-12f) dir = V3{1.0f, 0.0f, 0.0f};
+    SupportVert v0 = supportVertexInline(A, B, dir), v1 = v0, v2 = v0, v3 = v0;
+    float b0 = 1.0f, b1 = 0.0f, b2 = 0.0f;
+    int count = 1;
+    for (int it = 0; it < 32; ++it) {
+        V3 closest{0.0f, 0.0f, 0.0f};
+        if (count > 0) closest += v0.p * b0;
+        if (count > 1) closest += v1.p * b1;
+        if (count > 2) closest += v2.p * b2;
+        const float distSq = lengthSq(closest);
+        if (distSq < 1e-10f) return false;  // overlap: the general path runs EPA
+        const V3 d = -closest;
+        const SupportVert w = supportVertexInline(A, B, d);
+        const float progress = dot(w.p, d) - dot(closest, d);
+        const float progressFloor = 1e-6f * sqrtf(distSq) + 1e-9f;
+        if (progress < progressFloor) break;
+        bool duplicate = count > 0 && lengthSq(w.p - v0.p) < 1e-12f;
+        if (!duplicate && count > 1) duplicate = lengthSq(w.p - v1.p) < 1e-12f;
+        if (!duplicate && count > 2) duplicate = lengthSq(w.p - v2.p) < 1e-12f;
+        if (duplicate) break;
+        if (count == 0) {
+            v0 = w; count = 1;  // appended to an emptied simplex: no solve step (gjkSeeded does none)
+        } else if (count == 1) {
+            v1 = w; count = 2;
+            solveSegmentV(v0, v1, b0, b1, count);
+        } else if (count == 2) {
+            v2 = w; count = 3;
+            solveTriangleV(v0, v1, v2, b0, b1, b2, count);
+        } else {
+            v3 = w; count = 4;
+            if (solveTetrahedronV(v0, v1, v2, v3, b0, b1, b2, count, scale)) return false;
+        }
+    }
+    V3 pa{0.0f, 0.0f, 0.0f}, pb{0.0f, 0.0f, 0.0f};
+    if (count > 0) { pa += v0.a * b0; pb += v0.b * b0; }
+    if (count > 1) { pa += v1.a * b1; pb += v1.b * b1; }
+    if (count > 2) { pa += v2.a * b2; pb += v2.b * b2; }
+    const V3 delta = pa - pb;
+    const float coreDist = length(delta);
+    r.normal = coreDist > 1e-8f ? delta * (1.0f / coreDist) : V3{0.0f, 1.0f, 0.0f};
+    r.distance = coreDist - A.radius - B.radius;
+    r.pointA = pa - r.normal * A.radius;
+    r.pointB = pb + r.normal * B.radius;
+    r.overlapping = false;
+    return true;
 }
 
 // ---- face clipping manifolds (manifold.h:38-367) ---------------------------

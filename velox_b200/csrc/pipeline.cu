@@ -1719,13 +1719,21 @@ VXD BodyView withPose(BodyView b, const V3& p, const Q4& q) {
     return b;
 }
 
+// Distance query of the rewind (register-resident GJK first; overlaps and
+// higher geometry qualities take the general GJK/EPA, same results).
+__device__ __noinline__ GjkResult distanceQuery(const Convex& ca, const Convex& cb) {
+    GjkResult r;
+    if (!gjkDistanceFast(ca, cb, r)) r = gjkDistance(ca, cb);
+    return r;
+}
+
 __device__ __noinline__ GapProbe gapAt(const BodyView& a, const BodyView& b, const Soup& soup) {
     if (shapeOf(b.flags) == kPlane) {
         const Convex c = makeConvex(a, soup);
-        const V3 deep = support(c, -b.planeN);
+        const V3 deep = c.position + supportOffsetBody(c, -b.planeN);
         return GapProbe{dot(b.planeN, deep) - b.planeOff - c.radius, b.planeN};
     }
-    const GjkResult r = gjkDistance(makeConvex(a, soup), makeConvex(b, soup));
+    const GjkResult r = distanceQuery(makeConvex(a, soup), makeConvex(b, soup));
     return GapProbe{r.distance, r.normal};
 }
 
@@ -2808,6 +2816,33 @@ int stageColor(Context& c, const vx_contact* contacts, uint32_t m, int32_t* colo
     VXB_TRY(buildIslands(c, P<vx_contact>(c.contactBuf[c.cur]), m, plan, reinterpret_cast<uint32_t*>(colorOf)));
     VXB_TRY(readCounters(c));
     *numColors = c.hostCounters.maxColors;
+    return VXB_OK;
+}
+
+__global__ void distanceKernel(BodyArrays B, Soup soup, const uint64_t* pairs, uint32_t npairs, int path,
+                               float* out) {
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < npairs; p += gridDim.x * blockDim.x) {
+        const Convex ca = makeConvex(loadView(B, (uint32_t)(pairs[p] >> 32)), soup);
+        const Convex cb = makeConvex(loadView(B, (uint32_t)pairs[p]), soup);
+        const GjkResult r = path == 0 ? distanceQuery(ca, cb) : gjkDistance(ca, cb);
+        float* o = out + 11 * (size_t)p;
+        o[0] = r.distance;
+        o[1] = r.normal.x; o[2] = r.normal.y; o[3] = r.normal.z;
+        o[4] = r.pointA.x; o[5] = r.pointA.y; o[6] = r.pointA.z;
+        o[7] = r.pointB.x; o[8] = r.pointB.y; o[9] = r.pointB.z;
+        o[10] = r.overlapping ? 1.0f : 0.0f;
+    }
+}
+
+int stageDistance(Context& c, const uint64_t* pairs, uint32_t npairs, int path, float* out) {
+    if (npairs == 0) return VXB_OK;
+    VXB_TRY(ensure(c, c.pairBuf, (size_t)npairs * 8 + 16));
+    VXB_TRY(ensure(c, c.contactTmpBuf, (size_t)npairs * 44 + 16));
+    VXB_CUDA(c, cudaMemcpyAsync(c.pairBuf.ptr, pairs, (size_t)npairs * 8, cudaMemcpyHostToDevice, c.stream));
+    LAUNCH(c, distanceKernel, blocksFor(npairs, 64), 64, c.B, soupOf(c), P<uint64_t>(c.pairBuf), npairs, path,
+           P<float>(c.contactTmpBuf));
+    VXB_CUDA(c, cudaMemcpyAsync(out, c.contactTmpBuf.ptr, (size_t)npairs * 44, cudaMemcpyDeviceToHost, c.stream));
+    VXB_CUDA(c, cudaStreamSynchronize(c.stream));
     return VXB_OK;
 }
 
