@@ -71,6 +71,8 @@ typedef struct vxb_step_stats {
     uint32_t rewindRounds;       /* wavefront rounds of the rewind passes */
     uint32_t rewindReplays;      /* rewind passes replayed with a widened body set */
     uint32_t rewindGapQueries;   /* distance queries of the rewind passes */
+    uint32_t rewindScanMicros;   /* rewind rounds: microseconds in the ready scans */
+    uint32_t rewindEvalMicros;   /* rewind rounds: microseconds in the evaluations */
 } vxb_step_stats;
 
 /* ---- library / context ------------------------------------------------ */

@@ -114,7 +114,8 @@ class StepStats(ctypes.Structure):
     _fields_ = [(n, ctypes.c_uint32) for n in ("candidatePairs", "contacts", "colors", "islands",
                                                "largestIsland", "rewinds", "velocityIterations",
                                                "warmStarted", "colorRounds", "giantIslands",
-                                               "rewindRounds", "rewindReplays", "rewindGapQueries")]
+                                               "rewindRounds", "rewindReplays", "rewindGapQueries",
+                                               "rewindScanMicros", "rewindEvalMicros")]
 
 
 def ptr(a):

@@ -67,7 +67,9 @@ struct Counters {
     uint32_t freeFrom, freeTo;  // contact-free bodies: range in the island-sorted body order
     uint32_t planFault;      // a solve kernel found an inconsistent island plan
     uint32_t caGapQueries;   // distance queries of the rewind passes
-    uint32_t pad[1];
+    uint32_t caScanMicros;   // rewind rounds: time in the ready scans (block 0's clock)
+    uint32_t caEvalMicros;   // rewind rounds: time in the evaluations
+    uint32_t pad[3];
 };
 
 // Pipeline stages timed with CUDA events when timing is enabled.

@@ -79,6 +79,17 @@ VXD BodyView loadView(const BodyArrays& B, uint32_t i) {
     return b;
 }
 
+// loadView with the mutable state (pose, velocities) read through L2: for
+// kernels where other SMs move bodies between this thread's reads.
+VXD BodyView loadViewCoherent(const BodyArrays& B, uint32_t i) {
+    BodyView b = loadView(B, i);
+    b.p = f3(__ldcg(B.pos + i));
+    b.q = q4(__ldcg(B.rot + i));
+    b.v = f3(__ldcg(B.vel + i));
+    b.w = f3(__ldcg(B.ang + i));
+    return b;
+}
+
 // Body::maxPointSpeed (body.h:329-344).
 VXD float maxPointSpeedOf(uint32_t shape, const V3& half, float radius, float hh, const V3& v,
                           const V3& w) {

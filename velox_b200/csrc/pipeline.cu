@@ -1803,7 +1803,7 @@ VXD Q4 orientationAt(const Mass& m, const Q4& start, const V3& L, float elapsed)
 // when the pair was rewound.
 __device__ __noinline__ bool caRewind(BodyArrays& B, const Soup& soup, uint32_t i, uint32_t j, float dt,
                                       const float4* prevPos, const float4* prevRot, uint32_t* gapQueries) {
-    BodyView a = loadView(B, i), b = loadView(B, j);
+    BodyView a = loadViewCoherent(B, i), b = loadViewCoherent(B, j);
     if (!caEligible(a, b, B, i)) return false;
     if (shapeOf(b.flags) != kPlane) {
         // bounding spheres more than 1 mm apart: positive end gap, no rewind (the probe's test)
@@ -1870,6 +1870,12 @@ __device__ __noinline__ bool caRewind(BodyArrays& B, const Soup& soup, uint32_t 
     return true;
 }
 
+VXD uint64_t globalTimerNs() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
 // Rewind pass over the candidate pairs in wavefronts. A candidate's
 // predecessors are the latest earlier candidates sharing one of its dynamic
 // bodies; it runs in the first round after both have run. Candidates of one
@@ -1891,6 +1897,7 @@ __global__ void __launch_bounds__(256) caWaveKernel(BodyArrays B, Soup soup, con
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t warp = tid >> 5, warps = stride >> 5;
     uint32_t finished = 0;
+    uint64_t scanNs = 0, evalNs = 0, t0 = tid == 0 ? globalTimerNs() : 0;
     for (uint32_t round = 1; round <= ncand; ++round) {
         const uint32_t slot = round % 3;
         if (tid == 0) {  // counters of the next round (last read two rounds ago)
@@ -1923,6 +1930,7 @@ __global__ void __launch_bounds__(256) caWaveKernel(BodyArrays B, Soup soup, con
         }
         if (ran) atomicAdd(&st->changed[slot], ran);
         if (!gridSync(&st->bar, &st->timeout)) return;
+        if (tid == 0) { const uint64_t t = globalTimerNs(); scanNs += t - t0; t0 = t; }
         // Phase 2: the queue. A short queue runs one candidate per warp
         // (lane 0), so no two evaluations share a warp and serialise on
         // divergence; a long one runs one per thread for throughput.
@@ -1949,6 +1957,17 @@ __global__ void __launch_bounds__(256) caWaveKernel(BodyArrays B, Soup soup, con
         if (evaluated) atomicAdd(&st->changed[slot], evaluated);
         if (rewinds) atomicAdd(&C->rewinds, rewinds);
         if (!gridSync(&st->bar, &st->timeout)) return;
+        if (tid == 0) {
+            const uint64_t t = globalTimerNs();
+            evalNs += t - t0;
+            t0 = t;
+            if (round % 8 == 0 || __ldcg(&st->changed[slot]) + finished >= ncand) {  // publish as we go
+                atomicAdd(&C->caScanMicros, (uint32_t)(scanNs / 1000));
+                atomicAdd(&C->caEvalMicros, (uint32_t)(evalNs / 1000));
+                scanNs -= scanNs / 1000 * 1000;
+                evalNs -= evalNs / 1000 * 1000;
+            }
+        }
         const uint32_t now = __ldcg(&st->changed[slot]);
         if (now == 0u) {  // nothing ready: impossible while predecessors precede
             if (tid == 0) atomicOr(&st->spill, 2u);
@@ -2723,6 +2742,8 @@ static int stepOnce(Context& c) {
     c.stats.rewindRounds = c.caRounds;
     c.stats.rewindReplays = c.caWidenings;
     c.stats.rewindGapQueries = c.hostCounters.caGapQueries;
+    c.stats.rewindScanMicros = c.hostCounters.caScanMicros;
+    c.stats.rewindEvalMicros = c.hostCounters.caEvalMicros;
     c.stats.warmStarted = c.hostCounters.warmStarted;
     c.stats.velocityIterations = (uint32_t)(2 * cfg.solver.velocityIterations * substeps);
     if (c.hostCounters.timeout) return fail(c, VXB_ERR_TIMEOUT, "a bounded device wait gave up");
