@@ -68,11 +68,10 @@ typedef struct vxb_step_stats {
     uint32_t warmStarted;        /* contacts that inherited impulses */
     uint32_t colorRounds;        /* fixed-point rounds of the parallel colouring (0 = none) */
     uint32_t giantIslands;       /* islands solved by the whole grid (cooperative launch) */
-    uint32_t rewindRounds;       /* wavefront rounds of the rewind passes */
+    uint32_t rewindRounds;       /* dependency depth of the rewind passes (summed over passes) */
     uint32_t rewindReplays;      /* rewind passes replayed with a widened body set */
     uint32_t rewindGapQueries;   /* distance queries of the rewind passes */
-    uint32_t rewindScanMicros;   /* rewind rounds: microseconds in the ready scans */
-    uint32_t rewindEvalMicros;   /* rewind rounds: microseconds in the evaluations */
+    uint32_t rewindCriticalMicros; /* evaluation time along the longest rewind dependency chain */
 } vxb_step_stats;
 
 /* ---- library / context ------------------------------------------------ */

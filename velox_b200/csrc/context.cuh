@@ -67,9 +67,8 @@ struct Counters {
     uint32_t freeFrom, freeTo;  // contact-free bodies: range in the island-sorted body order
     uint32_t planFault;      // a solve kernel found an inconsistent island plan
     uint32_t caGapQueries;   // distance queries of the rewind passes
-    uint32_t caScanMicros;   // rewind rounds: time in the ready scans (block 0's clock)
-    uint32_t caEvalMicros;   // rewind rounds: time in the evaluations
-    uint32_t pad[3];
+    uint32_t caCritMicros;   // rewind: evaluation time along the longest dependency chain
+    uint32_t pad[4];
 };
 
 // Pipeline stages timed with CUDA events when timing is enabled.
@@ -90,7 +89,7 @@ struct Context {
     int device = 0;
     int smCount = 148;
     int cooperative = 0;  // cudaDevAttrCooperativeLaunch
-    uint32_t caRounds = 0;     // rewind wavefront rounds of the last step
+    uint32_t caRounds = 0;     // rewind dependency depth of the last step (all passes)
     uint32_t caWidenings = 0;  // rewind replays with a widened body set (last step)
     cudaStream_t ownStream = nullptr;
     cudaStream_t stream = nullptr;

@@ -651,6 +651,29 @@ static __device__ __noinline__ bool epaPenetration(const Convex& A, const Convex
     return false;
 }
 
+// The overlap branch of gjkSeeded: expand the simplex when the loop stopped
+// on a vanishing distance (not inside a tetrahedron), then EPA, else the
+// centre-line estimate.
+static __device__ __noinline__ GjkResult gjkOverlapTail(const Convex& A, const Convex& B, Simplex& s, bool expand) {
+    const float scale = pairScale(A, B);
+    const float scaleSq = scale * scale;
+    const bool robust = pairQuality(A, B) != 0;
+    if (expand && s.count < 4) expandOverlapSimplex(A, B, s);
+    GjkResult r;
+    r.distance = 0.0f;
+    r.normal = r.pointA = r.pointB = V3{0.0f, 0.0f, 0.0f};
+    r.overlapping = true;
+    if (s.count == 4 && epaPenetration(A, B, s, r)) return r;
+    V3 n = A.position - B.position;
+    n = lengthSq(n) > (robust ? scaleSq * 1e-14f : 1e-12f) ? normalize(n) : V3{0.0f, 1.0f, 0.0f};
+    const float depth = dot(n, support(B, n) - support(A, -n));
+    r.normal = n;
+    r.distance = -depth - A.radius - B.radius;
+    r.pointA = support(A, -n);
+    r.pointB = support(B, n);
+    return r;
+}
+
 static __device__ __noinline__ GjkResult gjkSeeded(const Convex& A, const Convex& B, V3 dir) {
     Simplex s;
     const float scale = pairScale(A, B);
@@ -672,11 +695,7 @@ static __device__ __noinline__ GjkResult gjkSeeded(const Convex& A, const Convex
     for (int it = 0; it < maxIterations; ++it) {
         const V3 closest = simplexClosest(s);
         const float distSq = lengthSq(closest);
-        if (distSq < (robust ? scaleSq * 1e-10f : 1e-10f)) {
-            if (s.count < 4) expandOverlapSimplex(A, B, s);
-            r.overlapping = true;
-            break;
-        }
+        if (distSq < (robust ? scaleSq * 1e-10f : 1e-10f)) return gjkOverlapTail(A, B, s, true);
         const V3 d = -closest;
         const SupportVert w = supportVertex(A, B, d);
         const float progress = dot(w.p, d) - dot(closest, d);
@@ -690,23 +709,12 @@ static __device__ __noinline__ GjkResult gjkSeeded(const Convex& A, const Convex
         s.v[s.count++] = w;
         if (s.count == 2) solveSegment(s);
         else if (s.count == 3) solveTriangle(s);
-        else if (solveTetrahedron(s, scale)) { r.overlapping = true; break; }
+        else if (solveTetrahedron(s, scale)) return gjkOverlapTail(A, B, s, false);
     }
     V3 pa{0.0f, 0.0f, 0.0f}, pb{0.0f, 0.0f, 0.0f};
     for (int i = 0; i < s.count; ++i) {
         pa += s.v[i].a * s.bary[i];
         pb += s.v[i].b * s.bary[i];
-    }
-    if (r.overlapping) {
-        if (s.count == 4 && epaPenetration(A, B, s, r)) return r;
-        V3 n = A.position - B.position;
-        n = lengthSq(n) > (robust ? scaleSq * 1e-14f : 1e-12f) ? normalize(n) : V3{0.0f, 1.0f, 0.0f};
-        const float depth = dot(n, support(B, n) - support(A, -n));
-        r.normal = n;
-        r.distance = -depth - A.radius - B.radius;
-        r.pointA = support(A, -n);
-        r.pointB = support(B, n);
-        return r;
     }
     const V3 delta = pa - pb;
     const float coreDist = length(delta);
@@ -749,8 +757,8 @@ VXD GjkResult gjkDistance(const Convex& A, const Convex& B) {
 // instead of an indexed array, and the support mappings inlined: a single
 // thread runs it at register latency rather than local-memory latency, which
 // is what the rewind pass's chains of dependent queries wait on. When the
-// general routine would report an overlap (and go on to EPA) this one returns
-// false and the caller runs gjkDistance, which then produces that result.
+// general routine would report an overlap (and go on to EPA) this one hands
+// the simplex to gjkOverlapTail, the branch gjkSeeded itself would take.
 
 VXD SupportVert supportVertexInline(const Convex& A, const Convex& B, const V3& dir) {
     SupportVert s;
@@ -824,8 +832,20 @@ VXD bool solveTetrahedronV(SupportVert& v0, SupportVert& v1, SupportVert& v2, co
     return inside;
 }
 
-VXD bool gjkDistanceFast(const Convex& A, const Convex& B, GjkResult& r) {
-    if (pairQuality(A, B) != 0) return false;
+enum : int { kGjkSeparated = 0, kGjkOverlapExpand = 1, kGjkOverlapInside = 2, kGjkGeneral = 3 };
+
+VXD void toSimplex(const SupportVert& v0, const SupportVert& v1, const SupportVert& v2, const SupportVert& v3,
+                   float b0, float b1, float b2, int count, Simplex& s) {
+    s.v[0] = v0; s.v[1] = v1; s.v[2] = v2; s.v[3] = v3;
+    s.bary[0] = b0; s.bary[1] = b1; s.bary[2] = b2; s.bary[3] = 0.0f;
+    s.count = count;
+}
+
+// kGjkSeparated: r holds the result. kGjkOverlap*: gjkSeeded would take its
+// overlap branch with simplex s (kGjkOverlapExpand: after expanding it).
+// kGjkGeneral: not a Normal-quality pair.
+VXD int gjkDistanceFast(const Convex& A, const Convex& B, GjkResult& r, Simplex& s) {
+    if (pairQuality(A, B) != 0) return kGjkGeneral;
     const float scale = pairScale(A, B);
     V3 dir = A.position - B.position;
     if (lengthSq(dir) < 1e-12f) dir = V3{1.0f, 0.0f, 0.0f};
@@ -838,7 +858,10 @@ VXD bool gjkDistanceFast(const Convex& A, const Convex& B, GjkResult& r) {
         if (count > 1) closest += v1.p * b1;
         if (count > 2) closest += v2.p * b2;
         const float distSq = lengthSq(closest);
-        if (distSq < 1e-10f) return false;  // overlap: the general path runs EPA
+        if (distSq < 1e-10f) {  // overlap
+            toSimplex(v0, v1, v2, v3, b0, b1, b2, count, s);
+            return kGjkOverlapExpand;
+        }
         const V3 d = -closest;
         const SupportVert w = supportVertexInline(A, B, d);
         const float progress = dot(w.p, d) - dot(closest, d);
@@ -858,7 +881,10 @@ VXD bool gjkDistanceFast(const Convex& A, const Convex& B, GjkResult& r) {
             solveTriangleV(v0, v1, v2, b0, b1, b2, count);
         } else {
             v3 = w; count = 4;
-            if (solveTetrahedronV(v0, v1, v2, v3, b0, b1, b2, count, scale)) return false;
+            if (solveTetrahedronV(v0, v1, v2, v3, b0, b1, b2, count, scale)) {
+                toSimplex(v0, v1, v2, v3, b0, b1, b2, 4, s);
+                return kGjkOverlapInside;
+            }
         }
     }
     V3 pa{0.0f, 0.0f, 0.0f}, pb{0.0f, 0.0f, 0.0f};
@@ -872,7 +898,18 @@ VXD bool gjkDistanceFast(const Convex& A, const Convex& B, GjkResult& r) {
     r.pointA = pa - r.normal * A.radius;
     r.pointB = pb + r.normal * B.radius;
     r.overlapping = false;
-    return true;
+    return kGjkSeparated;
+}
+
+// gjkDistance with the register-resident loop for Normal-quality pairs; an
+// overlap continues into gjkSeeded's overlap branch from the same simplex.
+static __device__ __noinline__ GjkResult gjkDistanceQuick(const Convex& A, const Convex& B) {
+    GjkResult r;
+    Simplex s;
+    const int status = gjkDistanceFast(A, B, r, s);
+    if (status == kGjkSeparated) return r;
+    if (status == kGjkGeneral) return gjkDistance(A, B);
+    return gjkOverlapTail(A, B, s, status == kGjkOverlapExpand);
 }
 
 // ---- face clipping manifolds (manifold.h:38-367) ---------------------------

@@ -1719,13 +1719,8 @@ VXD BodyView withPose(BodyView b, const V3& p, const Q4& q) {
     return b;
 }
 
-// Distance query of the rewind (register-resident GJK first; overlaps and
-// higher geometry qualities take the general GJK/EPA, same results).
-__device__ __noinline__ GjkResult distanceQuery(const Convex& ca, const Convex& cb) {
-    GjkResult r;
-    if (!gjkDistanceFast(ca, cb, r)) r = gjkDistance(ca, cb);
-    return r;
-}
+// Distance query of the rewind: gjkDistance's results, the common case in registers.
+VXD GjkResult distanceQuery(const Convex& ca, const Convex& cb) { return gjkDistanceQuick(ca, cb); }
 
 __device__ __noinline__ GapProbe gapAt(const BodyView& a, const BodyView& b, const Soup& soup) {
     if (shapeOf(b.flags) == kPlane) {
@@ -1757,7 +1752,7 @@ VXD void orientPair(const BodyArrays& B, uint64_t key, uint32_t& i, uint32_t& j)
 }
 
 __global__ void caProbeKernel(BodyArrays B, Soup soup, const uint64_t* pairKeys, uint32_t npairs,
-                              uint32_t* flags, uint32_t* bodyMark) {
+                              uint32_t* flags, uint32_t* bodyMark, float4* endGap) {
     for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < npairs; r += gridDim.x * blockDim.x) {
         uint32_t i, j;
         orientPair(B, pairKeys[r], i, j);
@@ -1775,6 +1770,7 @@ __global__ void caProbeKernel(BodyArrays B, Soup soup, const uint64_t* pairKeys,
             const GapProbe end = gapAt(a, b, soup);
             if (end.gap < -8e-3f) {
                 flag = 1;
+                endGap[r] = make_float4(end.gap, end.normal.x, end.normal.y, end.normal.z);
                 bodyMark[i] = 1;  // only dynamic bodies move in a rewind
                 if (isDynamic(b.flags)) bodyMark[j] = 1;
             }
@@ -1801,8 +1797,11 @@ VXD Q4 orientationAt(const Mass& m, const Q4& start, const V3& L, float elapsed)
 
 // Full rewind logic for one oriented pair on the current state. Returns true
 // when the pair was rewound.
+// `cached`: the probe's end-state gap for this pair when neither body has
+// moved since the probe (else null: computed here).
 __device__ __noinline__ bool caRewind(BodyArrays& B, const Soup& soup, uint32_t i, uint32_t j, float dt,
-                                      const float4* prevPos, const float4* prevRot, uint32_t* gapQueries) {
+                                      const float4* prevPos, const float4* prevRot, uint32_t* gapQueries,
+                                      const float4* cached) {
     BodyView a = loadViewCoherent(B, i), b = loadViewCoherent(B, j);
     if (!caEligible(a, b, B, i)) return false;
     if (shapeOf(b.flags) != kPlane) {
@@ -1811,7 +1810,13 @@ __device__ __noinline__ bool caRewind(BodyArrays& B, const Soup& soup, uint32_t 
                             coreExtent(shapeOf(b.flags), b.half, b.radius, b.hh) + 1e-3f;
         if (lengthSq(a.p - b.p) > reach * reach) return false;
     }
-    const GapProbe end = gapAt(a, b, soup);
+    GapProbe end;
+    if (cached) {
+        const float4 g = *cached;
+        end = GapProbe{g.x, V3{g.y, g.z, g.w}};
+    } else {
+        end = gapAt(a, b, soup);
+    }
     if (end.gap >= -8e-3f) return false;
     const bool bStatic = isStaticBody(b.flags), bDyn = isDynamic(b.flags);
     const V3 pa0 = f3(prevPos[i]), da = a.p - pa0;
@@ -1876,110 +1881,86 @@ VXD uint64_t globalTimerNs() {
     return t;
 }
 
-// Rewind pass over the candidate pairs in wavefronts. A candidate's
+// Rewind pass over the candidate pairs as a dataflow. A candidate's
 // predecessors are the latest earlier candidates sharing one of its dynamic
-// bodies; it runs in the first round after both have run. Candidates of one
-// round share no dynamic body, and each sees exactly the body states and
-// rewound marks that the reference's single ordered loop would show it, as
-// long as no rewind moves a body outside the marked set; that case is flagged
-// and the caller widens the set and replays the pass from a snapshot.
-// Cooperative launch; every wait is bounded (gridSync).
+// bodies; it becomes ready when both have finished and is then evaluated
+// exactly as the reference's single ordered loop would evaluate it: it sees
+// the same body states and rewound marks, as long as no rewind moves a body
+// outside the marked set (that case is flagged; the caller widens the set and
+// replays the pass from a snapshot). One worker per warp (lane 0) takes ready
+// candidates from a queue, so independent chains never wait for one another.
+// Cooperative launch (all workers resident); every wait is bounded.
 constexpr uint32_t kNoPred = 0xffffffffu;
 constexpr int kCaWidenLimit = 8;  // replays with a widened marked set before the serial loop
 
-__global__ void __launch_bounds__(256) caWaveKernel(BodyArrays B, Soup soup, const uint64_t* pairKeys,
-                                                    const uint32_t* flags, const uint32_t* cand, uint32_t ncand,
-                                                    const uint32_t* pred, uint32_t* doneRound, uint32_t* queue,
-                                                    const uint32_t* bodyMark, uint32_t* rewound, float dt,
-                                                    const float4* prevPos, const float4* prevRot, Counters* C,
-                                                    CoopState* st) {
+__global__ void __launch_bounds__(256) caFlowKernel(BodyArrays B, Soup soup, const uint64_t* pairKeys,
+                                                    const uint32_t* flags, const float4* endGap,
+                                                    const uint32_t* cand, uint32_t ncand, const uint32_t* succ,
+                                                    uint32_t* pending, uint32_t* queue, uint32_t* depth,
+                                                    uint32_t* crit, const uint32_t* bodyMark, uint32_t* rewound,
+                                                    float dt, const float4* prevPos, const float4* prevRot,
+                                                    Counters* C, CoopState* st) {
     const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
-    const uint32_t lane = threadIdx.x & 31u;
-    const uint32_t warp = tid >> 5, warps = stride >> 5;
-    uint32_t finished = 0;
-    uint64_t scanNs = 0, evalNs = 0, t0 = tid == 0 ? globalTimerNs() : 0;
-    for (uint32_t round = 1; round <= ncand; ++round) {
-        const uint32_t slot = round % 3;
-        if (tid == 0) {  // counters of the next round (last read two rounds ago)
-            st->changed[(round + 1) % 3] = 0u;
-            st->queued[(round + 1) % 3] = 0u;
+    uint32_t* tail = &st->queued[0];
+    uint32_t* head = &st->queued[1];
+    for (uint32_t k = tid; k < ncand; k += stride)  // roots
+        if (pending[k] == 0u) {
+            const uint32_t t = atomicAdd(tail, 1u);
+            if (t < ncand) __stcg(queue + t, k);
+            else atomicOr(&st->spill, 4u);  // pushed twice: inconsistent links
         }
-        // Phase 1: ready candidates. Skips (not flagged, neither body rewound
-        // so far) finish now; the others join this round's queue.
-        uint32_t ran = 0;
-        for (uint32_t k = tid; k < ncand; k += stride) {
-            if (__ldcg(doneRound + k)) continue;  // phase 2 may have written it from another SM
-            const uint32_t p0 = pred[2 * k], p1 = pred[2 * k + 1];
-            if (p0 != kNoPred) {
-                const uint32_t d = __ldcg(doneRound + p0);
-                if (d == 0u || d == round) continue;
+    if ((threadIdx.x & 31u) != 0u) return;
+    uint32_t rewinds = 0, maxDepth = 0, maxCrit = 0;
+    for (;;) {
+        const uint32_t h = atomicAdd(head, 1u);
+        if (h >= ncand) break;
+        uint32_t k, spins = 0;
+        while ((k = __ldcg(queue + h)) == kNoPred) {  // claimed before it was filled
+            if (++spins > kSpinLimit || __ldcg(&st->timeout)) {
+                atomicOr(&st->timeout, 1u);
+                return;
             }
-            if (p1 != kNoPred) {
-                const uint32_t d = __ldcg(doneRound + p1);
-                if (d == 0u || d == round) continue;
-            }
-            const uint32_t r = cand[k];
-            const uint64_t key = pairKeys[r];
-            const uint32_t ri = (uint32_t)(key >> 32), rj = (uint32_t)key;
-            if (flags[r] || __ldcg(rewound + ri) || __ldcg(rewound + rj)) {
-                queue[atomicAdd(&st->queued[slot], 1u)] = k;
-            } else {
-                __stcg(doneRound + k, round);
-                ++ran;
-            }
+            __nanosleep(64);
         }
-        if (ran) atomicAdd(&st->changed[slot], ran);
-        if (!gridSync(&st->bar, &st->timeout)) return;
-        if (tid == 0) { const uint64_t t = globalTimerNs(); scanNs += t - t0; t0 = t; }
-        // Phase 2: the queue. A short queue runs one candidate per warp
-        // (lane 0), so no two evaluations share a warp and serialise on
-        // divergence; a long one runs one per thread for throughput.
-        const uint32_t queued = __ldcg(&st->queued[slot]);
-        const bool perWarp = queued <= warps;
-        uint32_t rewinds = 0, evaluated = 0;
-        if (!perWarp || lane == 0) {
-            const uint32_t first = perWarp ? warp : tid, step = perWarp ? warps : stride;
-            for (uint32_t q = first; q < queued; q += step) {
-                const uint32_t k = __ldcg(queue + q);
-                uint32_t i, j;
-                orientPair(B, pairKeys[cand[k]], i, j);
-                if (caRewind(B, soup, i, j, dt, prevPos, prevRot, &C->caGapQueries)) {
-                    ++rewinds;
-                    const bool jDyn = isDynamic(B.filt[j].x);
-                    __stcg(rewound + i, 1u);
-                    if (jDyn) __stcg(rewound + j, 1u);
-                    if (!bodyMark[i] || (jDyn && !bodyMark[j])) atomicOr(&C->caOverflow, 1u);
-                }
-                __stcg(doneRound + k, round);
-                ++evaluated;
+        __threadfence();  // acquire the predecessors' writes
+        const uint64_t t0 = globalTimerNs();
+        const uint32_t r = cand[k];
+        const uint64_t key = pairKeys[r];
+        const uint32_t ri = (uint32_t)(key >> 32), rj = (uint32_t)key;
+        const bool touched = __ldcg(rewound + ri) || __ldcg(rewound + rj);
+        if (flags[r] || touched) {
+            uint32_t i, j;
+            orientPair(B, key, i, j);
+            if (caRewind(B, soup, i, j, dt, prevPos, prevRot, &C->caGapQueries,
+                         flags[r] && !touched ? endGap + r : nullptr)) {
+                ++rewinds;
+                const bool jDyn = isDynamic(B.filt[j].x);
+                __stcg(rewound + i, 1u);
+                if (jDyn) __stcg(rewound + j, 1u);
+                if (!bodyMark[i] || (jDyn && !bodyMark[j])) atomicOr(&C->caOverflow, 1u);
             }
         }
-        if (evaluated) atomicAdd(&st->changed[slot], evaluated);
-        if (rewinds) atomicAdd(&C->rewinds, rewinds);
-        if (!gridSync(&st->bar, &st->timeout)) return;
-        if (tid == 0) {
-            const uint64_t t = globalTimerNs();
-            evalNs += t - t0;
-            t0 = t;
-            if (round % 8 == 0 || __ldcg(&st->changed[slot]) + finished >= ncand) {  // publish as we go
-                atomicAdd(&C->caScanMicros, (uint32_t)(scanNs / 1000));
-                atomicAdd(&C->caEvalMicros, (uint32_t)(evalNs / 1000));
-                scanNs -= scanNs / 1000 * 1000;
-                evalNs -= evalNs / 1000 * 1000;
+        const uint32_t d = __ldcg(depth + k) + 1u;
+        const uint64_t elapsed = globalTimerNs() - t0;
+        const uint32_t ck = __ldcg(crit + k) + (uint32_t)(elapsed < 0x7fffffffull ? elapsed : 0x7fffffffull);
+        maxDepth = max(maxDepth, d);
+        maxCrit = max(maxCrit, ck);
+        __threadfence();  // release this evaluation's writes before the successors can run
+        for (int side = 0; side < 2; ++side) {
+            const uint32_t sk = succ[2 * k + side];
+            if (sk == kNoPred) continue;
+            atomicMax(depth + sk, d);
+            atomicMax(crit + sk, ck);
+            if (atomicSub(pending + sk, 1u) == 1u) {
+                const uint32_t t = atomicAdd(tail, 1u);
+                if (t < ncand) __stcg(queue + t, sk);
+                else atomicOr(&st->spill, 4u);
             }
-        }
-        const uint32_t now = __ldcg(&st->changed[slot]);
-        if (now == 0u) {  // nothing ready: impossible while predecessors precede
-            if (tid == 0) atomicOr(&st->spill, 2u);
-            return;
-        }
-        finished += now;
-        if (finished >= ncand) {
-            if (tid == 0) st->rounds = round;
-            return;
         }
     }
-    if (tid == 0) atomicOr(&st->spill, 2u);
+    if (rewinds) atomicAdd(&C->rewinds, rewinds);
+    atomicMax(&st->rounds, maxDepth);
+    atomicMax(&C->caCritMicros, maxCrit / 1000u);
 }
 
 // Entries (dynamic body, 2k + side) of the candidates; other endpoints sort last.
@@ -1995,12 +1976,16 @@ __global__ void caEntryKernel(const BodyArrays B, const uint64_t* pairKeys, cons
     }
 }
 
-// Entries sorted stably by body: the previous entry of the same body is the predecessor.
-__global__ void caPredKernel(const uint64_t* keys, const uint32_t* vals, uint32_t entries, uint32_t n,
-                             uint32_t* pred) {
+// Entries sorted stably by body: consecutive entries of one body link a
+// candidate to its successor on that body (pending counts its predecessors).
+__global__ void caLinkKernel(const uint64_t* keys, const uint32_t* vals, uint32_t entries, uint32_t n,
+                             uint32_t* succ, uint32_t* pending) {
     for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < entries; p += gridDim.x * blockDim.x) {
-        const bool chained = p > 0 && keys[p] != (uint64_t)n && keys[p - 1] == keys[p];
-        pred[vals[p]] = chained ? (vals[p - 1] >> 1) : kNoPred;
+        const uint64_t key = keys[p];
+        const bool body = key != (uint64_t)n;
+        const bool next = body && p + 1 < entries && keys[p + 1] == key;
+        succ[vals[p]] = next ? (vals[p + 1] >> 1) : kNoPred;
+        if (body && p > 0 && keys[p - 1] == key) atomicAdd(pending + (vals[p] >> 1), 1u);
     }
 }
 
@@ -2031,7 +2016,7 @@ __global__ void caFullSerialKernel(BodyArrays B, Soup soup, const uint64_t* pair
         if (!(flags[r] || rewound[ri] || rewound[rj])) continue;
         uint32_t i, j;
         orientPair(B, key, i, j);
-        if (caRewind(B, soup, i, j, dt, prevPos, prevRot, &C->caGapQueries)) {
+        if (caRewind(B, soup, i, j, dt, prevPos, prevRot, &C->caGapQueries, nullptr)) {
             ++rewinds;
             rewound[i] = 1;
             if (isDynamic(B.filt[j].x)) rewound[j] = 1;
@@ -2610,23 +2595,26 @@ static int positionCorrection(Context& c, vx_contact* cs, const IslandPlan& plan
 static int conservativeAdvancement(Context& c, uint32_t npairs, float dt) {
     if (npairs == 0) return VXB_OK;
     const uint32_t n = c.n;
-    VXB_TRY(ensure(c, c.caFlagBuf, (size_t)npairs * 8 + 16));
+    VXB_TRY(ensure(c, c.caFlagBuf, (size_t)npairs * 24 + 64));
     VXB_TRY(ensure(c, c.caBodyMarkBuf, (size_t)n * 8 + 16));
-    VXB_TRY(ensure(c, c.caCandBuf, (size_t)npairs * 20 + 16));
-    uint32_t* flags = P<uint32_t>(c.caFlagBuf);
+    VXB_TRY(ensure(c, c.caCandBuf, (size_t)npairs * 28 + 64));
+    float4* endGap = P<float4>(c.caFlagBuf);
+    uint32_t* flags = reinterpret_cast<uint32_t*>(endGap + npairs);
     uint32_t* candFlags = flags + npairs;
     uint32_t* bodyMark = P<uint32_t>(c.caBodyMarkBuf);
     uint32_t* rewound = bodyMark + n;
-    uint32_t* ranks = P<uint32_t>(c.caCandBuf);
-    uint32_t* candIndex = ranks + npairs;
-    uint32_t* pred = candIndex + npairs;  // two per candidate
-    uint32_t* doneRound = pred + 2 * (size_t)npairs;
+    uint32_t* queue = P<uint32_t>(c.caCandBuf);  // exclusive-scan ranks first, then the ready queue
+    uint32_t* candIndex = queue + npairs;
+    uint32_t* succ = candIndex + npairs;          // two per candidate
+    uint32_t* pending = succ + 2 * (size_t)npairs;
+    uint32_t* depth = pending + npairs;
+    uint32_t* crit = depth + npairs;
     VXB_CUDA(c, cudaMemsetAsync(bodyMark, 0, (size_t)n * 8, c.stream));
     const uint64_t* pk = P<uint64_t>(c.pairKeyBuf);
     const float4* prevPos = P<float4>(c.prevPoseBuf);
     const float4* prevRot = prevPos + n;
     LAUNCH(c, caProbeKernel, std::min<uint32_t>(blocksFor(npairs, 128), (uint32_t)c.smCount * 16), 128, c.B, soupOf(c),
-           pk, npairs, flags, bodyMark);
+           pk, npairs, flags, bodyMark, endGap);
     VXB_TRY(ensure(c, c.snapBuf, (size_t)n * 64));
     VXB_TRY(ensure(c, c.coopBuf, sizeof(CoopState)));
     CoopState* st = P<CoopState>(c.coopBuf);
@@ -2635,37 +2623,39 @@ static int conservativeAdvancement(Context& c, uint32_t npairs, float dt) {
         if (pass == kCaWidenLimit) { serial = true; break; }
         LAUNCH(c, caCandidateKernel, blocksFor(npairs, 256), 256, c.B, pk, npairs, flags, bodyMark, candFlags,
                c.dCounters);
-        VXB_TRY(exclusiveScan(c, candFlags, ranks, npairs, &c.dCounters->caCandidates));
+        VXB_TRY(exclusiveScan(c, candFlags, queue, npairs, &c.dCounters->caCandidates));
         VXB_TRY(readCounters(c));
         const uint32_t ncand = c.hostCounters.caCandidates;
         if (ncand == 0) return VXB_OK;
-        LAUNCH(c, compactKernel, blocksFor(npairs, 256), 256, candFlags, ranks, npairs, candIndex);
-        // predecessors through shared dynamic bodies
+        LAUNCH(c, compactKernel, blocksFor(npairs, 256), 256, candFlags, queue, npairs, candIndex);
+        // successors and predecessor counts through shared dynamic bodies
         const size_t valsOffset = ((size_t)ncand * 16 + 255) & ~(size_t)255;  // both arrays 256-byte aligned
         VXB_TRY(ensure(c, c.islandInfoBuf, valsOffset + (size_t)ncand * 8 + 16));
         uint64_t* ekeys = P<uint64_t>(c.islandInfoBuf);
         uint32_t* evals = reinterpret_cast<uint32_t*>(P<char>(c.islandInfoBuf) + valsOffset);
         LAUNCH(c, caEntryKernel, blocksFor(ncand, 256), 256, c.B, pk, candIndex, ncand, n, ekeys, evals);
         VXB_TRY(sortPairs(c, ekeys, evals, 2 * ncand, bitsFor(n)));
-        LAUNCH(c, caPredKernel, blocksFor(2 * ncand, 256), 256, ekeys, evals, 2 * ncand, n, pred);
+        VXB_CUDA(c, cudaMemsetAsync(pending, 0, (size_t)ncand * 4, c.stream));
+        VXB_CUDA(c, cudaMemsetAsync(depth, 0, (size_t)ncand * 8, c.stream));  // depth and crit
+        LAUNCH(c, caLinkKernel, blocksFor(2 * ncand, 256), 256, ekeys, evals, 2 * ncand, n, succ, pending);
         if (!snapped) {
             LAUNCH(c, copyStateKernel, blocksFor(n, 256), 256, c.B, n, P<float4>(c.snapBuf), 0);
             snapped = true;
         }
-        VXB_CUDA(c, cudaMemsetAsync(doneRound, 0, (size_t)ncand * 4, c.stream));
+        VXB_CUDA(c, cudaMemsetAsync(queue, 0xff, (size_t)ncand * 4, c.stream));
         VXB_CUDA(c, cudaMemsetAsync(st, 0, sizeof(CoopState), c.stream));
-        const int rc = launchCooperative(c, caWaveKernel, 256, c.B, soupOf(c), pk, (const uint32_t*)flags,
-                                         (const uint32_t*)candIndex, ncand, (const uint32_t*)pred, doneRound,
-                                         ranks /* free after compaction: the work queue */,
+        const int rc = launchCooperative(c, caFlowKernel, 256, c.B, soupOf(c), pk, (const uint32_t*)flags,
+                                         (const float4*)endGap, (const uint32_t*)candIndex, ncand,
+                                         (const uint32_t*)succ, pending, queue, depth, crit,
                                          (const uint32_t*)bodyMark, rewound, dt, prevPos, prevRot, c.dCounters, st);
         if (rc == VXB_ERR_UNSUPPORTED) { serial = true; break; }
         VXB_TRY(rc);
         CoopState host;
         VXB_CUDA(c, cudaMemcpyAsync(&host, st, sizeof(host), cudaMemcpyDeviceToHost, c.stream));
         VXB_TRY(readCounters(c));
-        if (host.timeout) return fail(c, VXB_ERR_TIMEOUT, "grid barrier timed out in the rewind pass");
+        if (host.timeout) return fail(c, VXB_ERR_TIMEOUT, "a wait timed out in the rewind pass");
+        if (host.spill) return fail(c, VXB_ERR_INTERNAL, "inconsistent candidate links in the rewind pass");
         c.caRounds += host.rounds;
-        if (host.spill) { serial = true; break; }
         if (!c.hostCounters.caOverflow) return VXB_OK;
         // a rewind reached an unmarked body: widen the marked set and replay from the snapshot
         LAUNCH(c, copyStateKernel, blocksFor(n, 256), 256, c.B, n, P<float4>(c.snapBuf), 1);
@@ -2742,8 +2732,7 @@ static int stepOnce(Context& c) {
     c.stats.rewindRounds = c.caRounds;
     c.stats.rewindReplays = c.caWidenings;
     c.stats.rewindGapQueries = c.hostCounters.caGapQueries;
-    c.stats.rewindScanMicros = c.hostCounters.caScanMicros;
-    c.stats.rewindEvalMicros = c.hostCounters.caEvalMicros;
+    c.stats.rewindCriticalMicros = c.hostCounters.caCritMicros;
     c.stats.warmStarted = c.hostCounters.warmStarted;
     c.stats.velocityIterations = (uint32_t)(2 * cfg.solver.velocityIterations * substeps);
     if (c.hostCounters.timeout) return fail(c, VXB_ERR_TIMEOUT, "a bounded device wait gave up");
