@@ -1892,6 +1892,7 @@ VXD uint64_t globalTimerNs() {
 // Cooperative launch (all workers resident); every wait is bounded.
 constexpr uint32_t kNoPred = 0xffffffffu;
 constexpr int kCaWidenLimit = 8;  // replays with a widened marked set before the serial loop
+constexpr int kCaWidenHops = 2;   // hops of widening per replay
 
 __global__ void __launch_bounds__(256) caFlowKernel(BodyArrays B, Soup soup, const uint64_t* pairKeys,
                                                     const uint32_t* flags, const float4* endGap,
@@ -1989,17 +1990,17 @@ __global__ void caLinkKernel(const uint64_t* keys, const uint32_t* vals, uint32_
     }
 }
 
-// Widen the marked set after a failed pass: the bodies it rewound and their
-// dynamic neighbours through candidate pairs (one hop ahead of the cascade,
-// so a long cascade needs fewer replays).
+// Widen the marked set after a failed pass, one hop per launch: both dynamic
+// endpoints of every pair touching a frontier body (the first frontier is
+// the set of bodies the pass rewound); bodies marked here form the next one.
+// Marking ahead of the cascade means fewer replays.
 __global__ void caWidenKernel(const BodyArrays B, const uint64_t* pairKeys, uint32_t npairs, uint32_t* bodyMark,
-                              const uint32_t* rewound) {
+                              const uint32_t* frontier, uint32_t* next) {
     for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < npairs; r += gridDim.x * blockDim.x) {
         const uint32_t i = (uint32_t)(pairKeys[r] >> 32), j = (uint32_t)pairKeys[r];
-        const bool ri = rewound[i] != 0u, rj = rewound[j] != 0u;
-        if (!ri && !rj) continue;
-        if (isDynamic(B.filt[i].x)) bodyMark[i] = 1u;
-        if (isDynamic(B.filt[j].x)) bodyMark[j] = 1u;
+        if (!frontier[i] && !frontier[j]) continue;
+        if (isDynamic(B.filt[i].x) && atomicExch(bodyMark + i, 1u) == 0u) next[i] = 1u;
+        if (isDynamic(B.filt[j].x) && atomicExch(bodyMark + j, 1u) == 0u) next[j] = 1u;
     }
 }
 
@@ -2596,13 +2597,14 @@ static int conservativeAdvancement(Context& c, uint32_t npairs, float dt) {
     if (npairs == 0) return VXB_OK;
     const uint32_t n = c.n;
     VXB_TRY(ensure(c, c.caFlagBuf, (size_t)npairs * 24 + 64));
-    VXB_TRY(ensure(c, c.caBodyMarkBuf, (size_t)n * 8 + 16));
+    VXB_TRY(ensure(c, c.caBodyMarkBuf, (size_t)n * 16 + 16));
     VXB_TRY(ensure(c, c.caCandBuf, (size_t)npairs * 28 + 64));
     float4* endGap = P<float4>(c.caFlagBuf);
     uint32_t* flags = reinterpret_cast<uint32_t*>(endGap + npairs);
     uint32_t* candFlags = flags + npairs;
     uint32_t* bodyMark = P<uint32_t>(c.caBodyMarkBuf);
     uint32_t* rewound = bodyMark + n;
+    uint32_t* front[2] = {rewound + n, rewound + 2 * (size_t)n};  // widening frontiers
     uint32_t* queue = P<uint32_t>(c.caCandBuf);  // exclusive-scan ranks first, then the ready queue
     uint32_t* candIndex = queue + npairs;
     uint32_t* succ = candIndex + npairs;          // two per candidate
@@ -2636,7 +2638,8 @@ static int conservativeAdvancement(Context& c, uint32_t npairs, float dt) {
         LAUNCH(c, caEntryKernel, blocksFor(ncand, 256), 256, c.B, pk, candIndex, ncand, n, ekeys, evals);
         VXB_TRY(sortPairs(c, ekeys, evals, 2 * ncand, bitsFor(n)));
         VXB_CUDA(c, cudaMemsetAsync(pending, 0, (size_t)ncand * 4, c.stream));
-        VXB_CUDA(c, cudaMemsetAsync(depth, 0, (size_t)ncand * 8, c.stream));  // depth and crit
+        VXB_CUDA(c, cudaMemsetAsync(depth, 0, (size_t)ncand * 4, c.stream));
+        VXB_CUDA(c, cudaMemsetAsync(crit, 0, (size_t)ncand * 4, c.stream));
         LAUNCH(c, caLinkKernel, blocksFor(2 * ncand, 256), 256, ekeys, evals, 2 * ncand, n, succ, pending);
         if (!snapped) {
             LAUNCH(c, copyStateKernel, blocksFor(n, 256), 256, c.B, n, P<float4>(c.snapBuf), 0);
@@ -2659,7 +2662,15 @@ static int conservativeAdvancement(Context& c, uint32_t npairs, float dt) {
         if (!c.hostCounters.caOverflow) return VXB_OK;
         // a rewind reached an unmarked body: widen the marked set and replay from the snapshot
         LAUNCH(c, copyStateKernel, blocksFor(n, 256), 256, c.B, n, P<float4>(c.snapBuf), 1);
-        LAUNCH(c, caWidenKernel, blocksFor(npairs, 256), 256, c.B, pk, npairs, bodyMark, (const uint32_t*)rewound);
+        {
+            const uint32_t* frontier = rewound;
+            for (int hop = 0; hop < kCaWidenHops; ++hop) {
+                uint32_t* next = front[hop & 1];
+                VXB_CUDA(c, cudaMemsetAsync(next, 0, (size_t)n * 4, c.stream));
+                LAUNCH(c, caWidenKernel, blocksFor(npairs, 256), 256, c.B, pk, npairs, bodyMark, frontier, next);
+                frontier = next;
+            }
+        }
         VXB_CUDA(c, cudaMemsetAsync(rewound, 0, (size_t)n * 4, c.stream));
         VXB_CUDA(c, cudaMemsetAsync(&c.dCounters->rewinds, 0, 4, c.stream));
         VXB_CUDA(c, cudaMemsetAsync(&c.dCounters->caOverflow, 0, 4, c.stream));
