@@ -89,3 +89,32 @@ def test_world_step_matches_reference_cuda_semantics(ref, kind, size, substeps):
     st = ctx.stats()
     assert st["contacts"] > 0
     ctx.close()
+
+
+def test_coloring_past_64_colours_in_a_large_island(ctx, ref):
+    # 50 overlapping big spheres in a row, each crowded by 90 small ones: one
+    # island of more than 4096 contacts (parallel colouring) needing > 64 colours
+    rng = np.random.default_rng(5)
+    spec = velox_b200.binding.SPEC
+    specs = np.zeros(50 + 50 * 90, spec)
+    specs["orientation"] = (0, 0, 0, 1)
+    specs["mass"] = 1.0
+    specs["friction"] = 0.5
+    specs["planeNormal"] = (0, 1, 0)
+    specs["radius"][:50] = 2.0
+    specs["position"][:50, 0] = 3.5 * np.arange(50)
+    d = rng.normal(size=(50 * 90, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    centres = np.repeat(specs["position"][:50], 90, axis=0)
+    specs["radius"][50:] = 0.3
+    specs["position"][50:] = centres + 2.0 * d
+    bodies, _, _ = velox_b200.bodies_from_specs(specs, np.zeros((1, 3), np.float32))
+    soup = velox_b200.make_soup(np.zeros((1, 3), np.float32), np.zeros(1, np.uint32))
+    pairs = ref.candidate_pairs(bodies, DT)
+    contacts, _ = ref.collide_pairs(bodies, soup, pairs, DT)
+    contacts = ref.sort_contacts(contacts)
+    theirs, tn = ref.color_contacts(bodies, contacts)
+    mine, mn = ctx.color(bodies, contacts)
+    assert len(contacts) > 4096 and tn > 64
+    assert mn == tn
+    assert np.array_equal(mine, theirs)

@@ -885,9 +885,10 @@ __global__ void islandMaxKernel(const uint32_t* islandStart, Counters* C) {
 }
 
 // Parallel greedy colouring of large islands. The greedy colour of a contact
-// is the first colour unused by the earlier contacts (island order) that
-// share one of its dynamic bodies; that is the unique fixed point of
-//   colour[k] = first colour not in { colour[j] : j < k, j shares a body with k }
+// is the first colour below 64 unused by the earlier contacts (island order)
+// that share one of its dynamic bodies (past that, one more than their
+// highest colour): the unique fixed point of
+//   colour[k] = rule({ colour[j] : j < k, j shares a body with k })
 // reached by iterating the rule from all-zero colours (a contact is final
 // once every earlier neighbour is). Every round runs over all contacts of the
 // large islands in parallel; a round without changes is the fixed point.
@@ -934,8 +935,11 @@ __global__ void colorFixedPointKernel(const uint64_t* keys, const uint32_t* vals
         for (uint32_t k = tid; k < m; k += stride) {
             const uint32_t isl = islandIdx[k];
             if (islandStart[isl + 1] - islandStart[isl] <= kSerialColorLimit) continue;
+            // Past 64 colours the greedy rule continues from a per-body
+            // counter: one past the highest colour (>= 64) of the body's
+            // earlier contacts, 64 when there is none.
             unsigned long long used = 0ull;
-            bool over = false;
+            uint32_t high = 63u;
             for (int side = 0; side < 2; ++side) {
                 const uint32_t e = slot[2 * k + side];
                 if (e == 0xffffffffu) continue;
@@ -943,11 +947,10 @@ __global__ void colorFixedPointKernel(const uint64_t* keys, const uint32_t* vals
                 for (uint32_t f = runStart[body]; f < e; ++f) {
                     const uint32_t cq = __ldcg(color + (vals[f] >> 1));
                     if (cq < 64u) used |= 1ull << cq;
-                    else over = true;
+                    else high = max(high, cq);
                 }
             }
-            if (over || ~used == 0ull) { atomicOr(&st->spill, 1u); continue; }
-            const uint32_t next = (uint32_t)(__ffsll((long long)~used) - 1);
+            const uint32_t next = ~used != 0ull ? (uint32_t)(__ffsll((long long)~used) - 1) : high + 1u;
             if (next != __ldcg(color + k)) {
                 __stcg(color + k, next);
                 ++local;
@@ -973,7 +976,7 @@ __global__ void colorFinishKernel(const uint32_t* order, uint32_t m, const uint3
         if (size <= kSerialColorLimit) continue;
         const uint32_t c = color[k];
         colorOf[order[k]] = c;
-        colorKeys[k] = ((uint64_t)isl << 16) | c;
+        colorKeys[k] = ((uint64_t)isl << 16) | (c < 65535u ? c : 65535u);
         mx = max(mx, c + 1);
         if (k == islandStart[isl]) atomicMax(&C->largestIsland, size);
     }
