@@ -91,6 +91,8 @@ struct Context {
     int cooperative = 0;  // cudaDevAttrCooperativeLaunch
     uint32_t caRounds = 0;     // rewind dependency depth of the last step (all passes)
     uint32_t caWidenings = 0;  // rewind replays with a widened body set (last step)
+    uint32_t planContacts = 0; // contacts of the current island plan
+    bool giantLinked = false;  // dataflow links of the plan's giant islands are built
     cudaStream_t ownStream = nullptr;
     cudaStream_t stream = nullptr;
     std::string lastError;

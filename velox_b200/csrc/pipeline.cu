@@ -1635,10 +1635,59 @@ VXD void giantIntegrateTransform(const SolveArgs& A, uint32_t i) {
 }
 
 // Cooperative launch over the giant islands listed in `giants`, one after the
-// other, with the block path's schedule (solveIslandGlobal) and a grid barrier
-// wherever that path has a block barrier.
+// other. Body phases (integration, inertia frames) and the row preparation are
+// separated by grid barriers; the sweeps run as a dataflow instead of one
+// barrier per colour: a row may run its sweep u once the previous row on each
+// of its dynamic bodies (colour order; the body's last row of sweep u - 1 for
+// its first row) has finished. That is the order the colour-by-colour sweep
+// imposes on every body, so the results are the same, but independent parts
+// of the island run ahead instead of waiting for the slowest colour. Rows go
+// to warps in groups of 32 of one colour; a warp takes its groups in
+// (sweep, colour, group) order, which keeps the earliest unfinished group
+// runnable. Every wait is bounded.
+constexpr uint32_t kNoPred = 0xffffffffu;  // no predecessor / empty queue slot
+constexpr uint32_t kWrap = 0x80000000u;    // predecessor from the previous sweep
+
+// Runs `units` dataflow sweeps (op as giantRow) over rows [s0, s1); false on timeout.
+VXD bool giantFlow(const SolveArgs& A, uint32_t s0, uint32_t g0, uint32_t g1, int units, int warmUnits, int op,
+                   const uint32_t* pred, uint32_t* done, CoopState* st) {
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t lane = threadIdx.x & 31u, warp = tid >> 5, warps = (gridDim.x * blockDim.x) >> 5;
+    for (int u = 0; u < units; ++u) {
+        const int rowOp = op == 1 && u < warmUnits ? 0 : op;
+        for (uint32_t g = g0; g < g1; ++g) {
+            const uint32_t r0 = A.segStart[g], r1 = A.segStart[g + 1];
+            const uint32_t groups = (r1 - r0 + 31u) >> 5;
+            const uint32_t rot = ((r0 - s0) >> 5) % warps;
+            for (uint32_t j = (warp + warps - rot) % warps; j < groups; j += warps) {
+                const uint32_t k = r0 + (j << 5) + lane;
+                const bool active = k < r1;
+                uint32_t p0 = kNoPred, p1 = kNoPred;
+                if (active) { p0 = pred[2 * k]; p1 = pred[2 * k + 1]; }
+                const uint32_t need0 = (p0 & kWrap) ? (uint32_t)u : (uint32_t)u + 1u;
+                const uint32_t need1 = (p1 & kWrap) ? (uint32_t)u : (uint32_t)u + 1u;
+                for (uint32_t spins = 0;; ++spins) {
+                    const bool ready = (p0 == kNoPred || __ldcg(done + (p0 & ~kWrap)) >= need0) &&
+                                       (p1 == kNoPred || __ldcg(done + (p1 & ~kWrap)) >= need1);
+                    if (__all_sync(0xffffffffu, ready)) break;
+                    if (spins > kSpinLimit || __ldcg(&st->timeout)) {
+                        if (lane == 0) atomicOr(&st->timeout, 1u);
+                        return false;
+                    }
+                    __nanosleep(32);
+                }
+                __threadfence();  // acquire the predecessors' writes
+                if (active) giantRow(A, k, rowOp);
+                __threadfence();  // release this row's writes before it is marked done
+                if (active) __stcg(done + k, (uint32_t)u + 1u);
+            }
+        }
+    }
+    return true;
+}
+
 __global__ void __launch_bounds__(256) solveGiantKernel(SolveArgs A, const uint32_t* giants, uint32_t count,
-                                                        CoopState* st) {
+                                                        const uint32_t* pred, uint32_t* done, CoopState* st) {
     const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
     for (uint32_t gi = 0; gi < count; ++gi) {
         const uint32_t isl = giants[gi];
@@ -1647,11 +1696,10 @@ __global__ void __launch_bounds__(256) solveGiantKernel(SolveArgs A, const uint3
         const uint32_t b0 = isl < A.realIslands ? A.bodyStart[isl] : 0u;
         const uint32_t b1 = isl < A.realIslands ? A.bodyStart[isl + 1] : 0u;
         if (A.positionIterations > 0) {
-            for (int it = 0; it < A.positionIterations; ++it)
-                for (uint32_t g = g0; g < g1; ++g) {
-                    for (uint32_t k = A.segStart[g] + tid; k < A.segStart[g + 1]; k += stride) giantRow(A, k, 2);
-                    if (!gridSync(&st->bar, &st->timeout)) return;
-                }
+            for (uint32_t k = s0 + tid; k < s1; k += stride) __stcg(done + k, 0u);
+            if (!gridSync(&st->bar, &st->timeout)) return;
+            if (!giantFlow(A, s0, g0, g1, A.positionIterations, 0, 2, pred, done, st)) return;
+            if (!gridSync(&st->bar, &st->timeout)) return;
             continue;
         }
         for (int s = 0; s < A.substeps; ++s) {
@@ -1661,18 +1709,14 @@ __global__ void __launch_bounds__(256) solveGiantKernel(SolveArgs A, const uint3
                 __stcg(A.frames + id, pack(inertiaFrameAt(loadMass(A.B, id), q4(ldcg4(A.B.rot + id)))));
             }
             if (!gridSync(&st->bar, &st->timeout)) return;
-            for (uint32_t k = s0 + tid; k < s1; k += stride) giantRow(A, k, 3);
+            for (uint32_t k = s0 + tid; k < s1; k += stride) {
+                giantRow(A, k, 3);
+                __stcg(done + k, 0u);
+            }
             if (!gridSync(&st->bar, &st->timeout)) return;
-            if (A.warmStart && s == 0)
-                for (uint32_t g = g0; g < g1; ++g) {
-                    for (uint32_t k = A.segStart[g] + tid; k < A.segStart[g + 1]; k += stride) giantRow(A, k, 0);
-                    if (!gridSync(&st->bar, &st->timeout)) return;
-                }
-            for (int it = 0; it < A.sweeps; ++it)
-                for (uint32_t g = g0; g < g1; ++g) {
-                    for (uint32_t k = A.segStart[g] + tid; k < A.segStart[g + 1]; k += stride) giantRow(A, k, 1);
-                    if (!gridSync(&st->bar, &st->timeout)) return;
-                }
+            const int warmUnits = A.warmStart && s == 0 ? 1 : 0;
+            if (!giantFlow(A, s0, g0, g1, warmUnits + A.sweeps, warmUnits, 1, pred, done, st)) return;
+            if (!gridSync(&st->bar, &st->timeout)) return;
             if (A.integrate) {
                 for (uint32_t k = b0 + tid; k < b1; k += stride) giantIntegrateTransform(A, A.bodyOrder[k]);
                 if (!gridSync(&st->bar, &st->timeout)) return;
@@ -1681,11 +1725,49 @@ __global__ void __launch_bounds__(256) solveGiantKernel(SolveArgs A, const uint3
     }
 }
 
+// Dataflow links of the giant islands' rows: entries (dynamic body, 2k + side)
+// of every row of a giant island, other endpoints keyed n (no link).
+__global__ void giantEntryKernel(SolveArgs A, const uint32_t* islandOf, uint32_t m, uint32_t n, uint64_t* keys,
+                                 uint32_t* vals);
+// For each body run of the sorted entries, the position of its last entry.
+__global__ void giantLastKernel(const uint64_t* keys, uint32_t entries, uint32_t n, uint32_t* lastOf) {
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < entries; p += gridDim.x * blockDim.x) {
+        const uint64_t key = keys[p];
+        if (key != (uint64_t)n && (p + 1 == entries || keys[p + 1] != key)) lastOf[key] = p;
+    }
+}
+// pred[2k + side]: the previous row on that body in colour order, or (kWrap |
+// the body's last row) for its first row; kNoPred for no dynamic body.
+__global__ void giantPredKernel(const uint64_t* keys, const uint32_t* vals, uint32_t entries, uint32_t n,
+                                const uint32_t* lastOf, uint32_t* pred) {
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < entries; p += gridDim.x * blockDim.x) {
+        const uint64_t key = keys[p];
+        uint32_t v = kNoPred;
+        if (key != (uint64_t)n)
+            v = p > 0 && keys[p - 1] == key ? (vals[p - 1] >> 1) : (kWrap | (vals[lastOf[key]] >> 1));
+        pred[vals[p]] = v;
+    }
+}
+
 // The block kernel's complement among the islands above tinyLimit.
 VXD bool isGiant(const SolveArgs& A, uint32_t isl) {
     const uint32_t rows = A.islandStart[isl + 1] - A.islandStart[isl];
     const uint32_t nb = isl < A.realIslands ? A.bodyStart[isl + 1] - A.bodyStart[isl] : 0u;
     return rows > A.tinyLimit && (nb > (uint32_t)kBlockBodies || rows > (uint32_t)kBlockRows);
+}
+
+__global__ void giantEntryKernel(SolveArgs A, const uint32_t* islandOf, uint32_t m, uint32_t n, uint64_t* keys,
+                                 uint32_t* vals) {
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < m; k += gridDim.x * blockDim.x) {
+        const bool giant = isGiant(A, islandOf[k]);
+        const vx_contact& c = A.contacts[A.order[k]];
+        const uint32_t fa = A.B.filt[c.a].x, fb = A.B.filt[c.b].x;
+        const bool solved = giant && solvedContact(fa, fb);
+        keys[2 * k] = solved && isDynamic(fa) ? c.a : n;
+        keys[2 * k + 1] = solved && isDynamic(fb) ? c.b : n;
+        vals[2 * k] = 2 * k;
+        vals[2 * k + 1] = 2 * k + 1;
+    }
 }
 
 __global__ void giantListKernel(SolveArgs A, uint32_t* list, uint32_t* count) {
@@ -1893,7 +1975,6 @@ VXD uint64_t globalTimerNs() {
 // replays the pass from a snapshot). One worker per warp (lane 0) takes ready
 // candidates from a queue, so independent chains never wait for one another.
 // Cooperative launch (all workers resident); every wait is bounded.
-constexpr uint32_t kNoPred = 0xffffffffu;
 constexpr int kCaWidenLimit = 8;  // replays with a widened marked set before the serial loop
 constexpr int kCaWidenHops = 2;   // hops of widening per replay
 
@@ -2405,6 +2486,8 @@ static int parallelColor(Context& c, const vx_contact* cs, const uint32_t* order
 static int buildIslands(Context& c, const vx_contact* cs, uint32_t m, IslandPlan& plan, uint32_t* colorOut) {
     const uint32_t n = c.n;
     plan.contacts = m;
+    c.planContacts = m;
+    c.giantLinked = false;
     VXB_TRY(ensure(c, c.parentBuf, (size_t)n * 4));
     VXB_TRY(ensure(c, c.islandOfBodyBuf, (size_t)n * 4));
     VXB_TRY(ensure(c, c.maskBuf, (size_t)n * 8));
@@ -2545,8 +2628,28 @@ static int launchSolve(Context& c, const SolveArgs& A) {
     VXB_CUDA(c, cudaStreamSynchronize(c.stream));
     if (!giants) return VXB_OK;
     c.stats.giantIslands = std::max(c.stats.giantIslands, giants);
+    // dataflow links of the giant islands' rows (once per island plan)
+    const uint32_t m = c.planContacts;
+    VXB_TRY(ensure(c, c.fpKeyBuf, (size_t)m * 16 + 64));
+    VXB_TRY(ensure(c, c.fpValBuf, (size_t)m * 8 + 64));
+    VXB_TRY(ensure(c, c.fpSlotBuf, (size_t)m * 8 + 64));
+    VXB_TRY(ensure(c, c.fpColorBuf, (size_t)m * 4 + 64));
+    VXB_TRY(ensure(c, c.fpRunStartBuf, (size_t)c.n * 4 + 64));
+    uint32_t* pred = P<uint32_t>(c.fpSlotBuf);
+    uint32_t* done = P<uint32_t>(c.fpColorBuf);
+    if (!c.giantLinked) {
+        uint64_t* keys = P<uint64_t>(c.fpKeyBuf);
+        uint32_t* vals = P<uint32_t>(c.fpValBuf);
+        LAUNCH(c, giantEntryKernel, blocksFor(m, 256), 256, A, P<uint32_t>(c.fpIslandBuf), m, c.n, keys, vals);
+        VXB_TRY(sortPairs(c, keys, vals, 2 * m, bitsFor(c.n)));
+        LAUNCH(c, giantLastKernel, blocksFor(2 * m, 256), 256, keys, 2 * m, c.n, P<uint32_t>(c.fpRunStartBuf));
+        LAUNCH(c, giantPredKernel, blocksFor(2 * m, 256), 256, keys, vals, 2 * m, c.n,
+               P<uint32_t>(c.fpRunStartBuf), pred);
+        c.giantLinked = true;
+    }
     VXB_CUDA(c, cudaMemsetAsync(st, 0, sizeof(CoopState), c.stream));
-    const int rc = launchCooperative(c, solveGiantKernel, 256, A, (const uint32_t*)list, giants, st);
+    const int rc = launchCooperative(c, solveGiantKernel, 256, A, (const uint32_t*)list, giants,
+                                     (const uint32_t*)pred, done, st);
     if (rc == VXB_ERR_UNSUPPORTED) {
         LAUNCH(c, solveGiantBlockKernel, giants, kBlockThreads, A, (const uint32_t*)list);
         return VXB_OK;
