@@ -156,6 +156,7 @@ struct Context {
     DevBuf fpKeyBuf, fpValBuf, fpSlotBuf, fpColorBuf, fpRunStartBuf, fpIslandBuf;  // parallel colouring
     DevBuf coopBuf;                     // CoopState of cooperative launches
     DevBuf giantBuf;                    // giant island list (solve)
+    DevBuf classKeyBuf, classValBuf;    // convex pairs grouped by shape combination (narrow phase)
 
     DevBuf countersBuf;
     Counters* dCounters = nullptr;

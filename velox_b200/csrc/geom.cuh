@@ -1361,7 +1361,7 @@ VXD bool isConvexVolume(uint32_t s) {
 static __device__ __noinline__ void convexConvex(const BodyView& a, const BodyView& b, uint32_t ia, uint32_t ib,
                                           const Soup& soup, float dt, vx_contact* out, int cap, int& n) {
     const Convex ca = makeConvex(a, soup), cb = makeConvex(b, soup);
-    const GjkResult r = gjkDistance(ca, cb);
+    const GjkResult r = gjkDistanceQuick(ca, cb);  // gjkDistance's result
     const uint32_t sa = shapeOf(a.flags), sb = shapeOf(b.flags);
     if (r.distance < 0.05f && (sa == kBox || sa == kHull) && (sb == kBox || sb == kHull)) {
         V3 manifoldNormal = r.normal;

@@ -494,19 +494,22 @@ VXD bool pointLess(const vx_contact& x, const vx_contact& y) {
 // light kernel (high occupancy), convex pairs to the GJK/EPA kernel.
 enum PairClass : int { kAnyPairs = 0, kPlanePairs = 1, kConvexPairs = 2 };
 
+// `order` (optional): the pairs in the order to process them (convex pairs
+// grouped by shape combination so that a warp runs one code path).
 template <int Class>
 __global__ void __launch_bounds__(128) collideKernel(BodyArrays B, Soup soup, const uint64_t* pairs,
-                                                     uint32_t npairs, float dt, int mode, int bodyBits,
-                                                     vx_contact* tmp, uint32_t contactCap, uint64_t* recKeys,
-                                                     uint32_t* recVals, uint2* recInfo, uint32_t recCap,
-                                                     Counters* C) {
+                                                     const uint32_t* order, uint32_t npairs, float dt, int mode,
+                                                     int bodyBits, vx_contact* tmp, uint32_t contactCap,
+                                                     uint64_t* recKeys, uint32_t* recVals, uint2* recInfo,
+                                                     uint32_t recCap, Counters* C) {
     const uint32_t stride = gridDim.x * blockDim.x;
     const uint32_t rounded = (npairs + 31u) & ~31u;
     for (uint32_t base = blockIdx.x * blockDim.x; base < rounded; base += stride) {
-        const uint32_t p = base + threadIdx.x;
+        const uint32_t slot = base + threadIdx.x;
+        const uint32_t p = slot < npairs && order ? order[slot] : slot;
         vx_contact buf[kMaxContactsPerPair];
         int count = 0;
-        if (p < npairs) {
+        if (slot < npairs) {
             const uint64_t pr = pairs[p];
             const uint32_t i = (uint32_t)(pr >> 32), j = (uint32_t)pr;
             const BodyView a = loadView(B, i);
@@ -561,6 +564,17 @@ __global__ void __launch_bounds__(128) collideKernel(BodyArrays B, Soup soup, co
 __global__ void gatherCountsKernel(const uint32_t* recVals, const uint2* recInfo, uint32_t nrec, uint32_t* counts) {
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < nrec; k += gridDim.x * blockDim.x)
         counts[k] = recInfo[recVals[k]].y;
+}
+
+// Shape combination of each convex pair (the processing-order sort key).
+__global__ void pairClassKernel(const BodyArrays B, const uint64_t* pairs, uint32_t npairs, uint64_t* keys,
+                                uint32_t* vals) {
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < npairs; p += gridDim.x * blockDim.x) {
+        const uint64_t pr = pairs[p];
+        const uint32_t sa = shapeOf(B.filt[(uint32_t)(pr >> 32)].x), sb = shapeOf(B.filt[(uint32_t)pr].x);
+        keys[p] = (uint64_t)(sa * 16u + sb);
+        vals[p] = p;
+    }
 }
 
 // Copies each record's contacts to their sorted position.
@@ -2381,20 +2395,31 @@ static int narrowPhase(Context& c, const uint64_t* pairs, uint32_t npairs, float
         stageBegin(c, kStageNarrowphase);
         if (npairs && convexSplit <= npairs) {
             const uint32_t np = npairs - convexSplit;
-            if (convexSplit)
+            if (convexSplit) {
+                // group the convex pairs by shape combination (records are keyed by body pair, so
+                // the processing order does not change the result)
+                VXB_TRY(ensure(c, c.classKeyBuf, (size_t)convexSplit * 8 + 64));
+                VXB_TRY(ensure(c, c.classValBuf, (size_t)convexSplit * 4 + 64));
+                if (attempt == 0) {
+                    LAUNCH(c, pairClassKernel, blocksFor(convexSplit, 256), 256, c.B, pairs, convexSplit,
+                           P<uint64_t>(c.classKeyBuf), P<uint32_t>(c.classValBuf));
+                    VXB_TRY(sortPairs(c, P<uint64_t>(c.classKeyBuf), P<uint32_t>(c.classValBuf), convexSplit, 8));
+                }
                 LAUNCH(c, collideKernel<kConvexPairs>, std::min<uint32_t>(blocksFor(convexSplit, 128), (uint32_t)c.smCount * 16),
-                       128, c.B, soupOf(c), pairs, convexSplit, dt, mode, bodyBits, P<vx_contact>(c.contactTmpBuf),
-                       c.contactCap, P<uint64_t>(c.recKeyBuf), P<uint32_t>(c.recValBuf), P<uint2>(c.recInfoBuf),
-                       c.recCap, c.dCounters);
+                       128, c.B, soupOf(c), pairs, (const uint32_t*)P<uint32_t>(c.classValBuf), convexSplit, dt, mode,
+                       bodyBits, P<vx_contact>(c.contactTmpBuf), c.contactCap, P<uint64_t>(c.recKeyBuf),
+                       P<uint32_t>(c.recValBuf), P<uint2>(c.recInfoBuf), c.recCap, c.dCounters);
+            }
             if (np)
                 LAUNCH(c, collideKernel<kPlanePairs>, std::min<uint32_t>(blocksFor(np, 128), (uint32_t)c.smCount * 16),
-                       128, c.B, soupOf(c), planePairs, np, dt, mode, bodyBits,
+                       128, c.B, soupOf(c), planePairs, (const uint32_t*)nullptr, np, dt, mode, bodyBits,
                        P<vx_contact>(c.contactTmpBuf), c.contactCap, P<uint64_t>(c.recKeyBuf),
                        P<uint32_t>(c.recValBuf), P<uint2>(c.recInfoBuf), c.recCap, c.dCounters);
         } else if (npairs) {
             LAUNCH(c, collideKernel<kAnyPairs>, std::min<uint32_t>(blocksFor(npairs, 128), (uint32_t)c.smCount * 16), 128,
-                   c.B, soupOf(c), pairs, npairs, dt, mode, bodyBits, P<vx_contact>(c.contactTmpBuf), c.contactCap,
-                   P<uint64_t>(c.recKeyBuf), P<uint32_t>(c.recValBuf), P<uint2>(c.recInfoBuf), c.recCap, c.dCounters);
+                   c.B, soupOf(c), pairs, (const uint32_t*)nullptr, npairs, dt, mode, bodyBits,
+                   P<vx_contact>(c.contactTmpBuf), c.contactCap, P<uint64_t>(c.recKeyBuf), P<uint32_t>(c.recValBuf),
+                   P<uint2>(c.recInfoBuf), c.recCap, c.dCounters);
         }
         stageEnd(c, kStageNarrowphase);
         VXB_TRY(readCounters(c));
