@@ -267,7 +267,7 @@ def main():
     rewind_ms, rewind_calls = stage["rewind"]
     rewind_bytes = gap_queries_total * REWIND_BYTES_PER_QUERY
     rewind_gbs = rewind_bytes / (rewind_ms / 1e3) / 1e9 if rewind_ms > 0 else 0.0
-    rewind_roofline = {"bound": "hbm", "kernel": "caProbeKernel+caWaveKernel (rewind pass)",
+    rewind_roofline = {"bound": "hbm", "kernel": "caProbeKernel+caFlowKernel (rewind pass)",
                        "achieved": rewind_gbs, "peak": peak, "unit": "GB/s", "frac": rewind_gbs / peak,
                        "peak_source": peak_kind, "traffic": None,
                        "algorithmic_bytes_per_launch": rewind_bytes / max(rewind_calls, 1),
