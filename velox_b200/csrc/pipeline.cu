@@ -1990,7 +1990,8 @@ VXD uint64_t globalTimerNs() {
 // candidates from a queue, so independent chains never wait for one another.
 // Cooperative launch (all workers resident); every wait is bounded.
 constexpr int kCaWidenLimit = 8;  // replays with a widened marked set before the serial loop
-constexpr int kCaWidenHops = 2;   // hops of widening per replay
+constexpr int kCaWidenHops = 8;   // hops of widening per replay
+constexpr int kCaInitialHops = 8; // hops of widening before the first pass
 
 __global__ void __launch_bounds__(256) caFlowKernel(BodyArrays B, Soup soup, const uint64_t* pairKeys,
                                                     const uint32_t* flags, const float4* endGap,
@@ -2748,6 +2749,16 @@ static int conservativeAdvancement(Context& c, uint32_t npairs, float dt) {
     const float4* prevRot = prevPos + n;
     LAUNCH(c, caProbeKernel, std::min<uint32_t>(blocksFor(npairs, 128), (uint32_t)c.smCount * 16), 128, c.B, soupOf(c),
            pk, npairs, flags, bodyMark, endGap);
+    // mark ahead of the cascade before the first pass too (fewer replays)
+    {
+        const uint32_t* frontier = bodyMark;
+        for (int hop = 0; hop < kCaInitialHops; ++hop) {
+            uint32_t* next = front[hop & 1];
+            VXB_CUDA(c, cudaMemsetAsync(next, 0, (size_t)n * 4, c.stream));
+            LAUNCH(c, caWidenKernel, blocksFor(npairs, 256), 256, c.B, pk, npairs, bodyMark, frontier, next);
+            frontier = next;
+        }
+    }
     VXB_TRY(ensure(c, c.snapBuf, (size_t)n * 64));
     VXB_TRY(ensure(c, c.coopBuf, sizeof(CoopState)));
     CoopState* st = P<CoopState>(c.coopBuf);
