@@ -105,7 +105,8 @@ void vxb_context_destroy(vxb_context* ctx) {
                            &c.bodyValBuf, &c.islandBodyStartBuf, &c.caFlagBuf, &c.caBodyMarkBuf, &c.caCandBuf,
                            &c.localIdxBuf, &c.prepBuf, &c.frameBuf, &c.fpKeyBuf, &c.fpValBuf,
                            &c.fpSlotBuf, &c.fpColorBuf, &c.fpRunStartBuf, &c.fpIslandBuf, &c.coopBuf,
-                           &c.giantBuf, &c.classKeyBuf, &c.classValBuf, &c.countersBuf};
+                           &c.giantBuf, &c.classKeyBuf, &c.classValBuf, &c.rowBodyBuf,
+                           &c.countersBuf};
     for (vxb::DevBuf* b : bufs)
         if (b->ptr) cudaFree(b->ptr);
     if (c.ownStream) cudaStreamDestroy(c.ownStream);

@@ -157,6 +157,7 @@ struct Context {
     DevBuf coopBuf;                     // CoopState of cooperative launches
     DevBuf giantBuf;                    // giant island list (solve)
     DevBuf classKeyBuf, classValBuf;    // convex pairs grouped by shape combination (narrow phase)
+    DevBuf rowBodyBuf;                  // (a, b) per solve-order row (giant islands)
 
     DevBuf countersBuf;
     Counters* dCounters = nullptr;

@@ -1072,6 +1072,7 @@ struct SolveArgs {
     int stackStabilization;
     float stackStiffness, stackDamping;
     uint32_t* fault;         // set when the island plan is inconsistent (Counters::planFault)
+    const uint2* rowBodies;  // per solve-order row: (a, b) of its contact (giant islands)
 };
 
 VXD void warmRow(const SolveArgs& A, uint32_t ci) {
@@ -1535,6 +1536,17 @@ __global__ void __launch_bounds__(kBlockThreads) solveBlockKernel(SolveArgs A, u
 
 VXD float4 ldcg4(const float4* p) { return __ldcg(p); }
 
+// Acquire load / release store at GPU scope: the dataflow's flag handoff
+// without a full fence on either side.
+VXD uint32_t ldAcquire(const uint32_t* p) {
+    uint32_t v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+VXD void stRelease(uint32_t* p, uint32_t v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
 VXD SolverBody coherentBody(const SolveArgs& A, uint32_t id) {
     SolverBody b;
     b.p = f3(ldcg4(A.B.pos + id));
@@ -1572,10 +1584,11 @@ VXD void coherentPrep(const RowPrep* p, RowPrep& P) {
 
 // op: 0 warm start, 1 velocity sweep, 2 position row, 3 prepare
 VXD void giantRow(const SolveArgs& A, uint32_t pos, int op) {
+    const uint2 ab = A.rowBodies[pos];  // issued with the contact load, not after it
     vx_contact* cp = A.contacts + A.order[pos];
     alignas(16) vx_contact cc;
     loadContactCoherent(cp, cc);
-    SolverBody a = coherentBody(A, cc.a), b = coherentBody(A, cc.b);
+    SolverBody a = coherentBody(A, ab.x), b = coherentBody(A, ab.y);
     if (!solvedContact(a.m.flags, b.m.flags)) return;
     RowContact r;
     loadRow(cc, r);
@@ -1592,9 +1605,9 @@ VXD void giantRow(const SolveArgs& A, uint32_t pos, int op) {
             resolve += 0.2f * (A.stackStiffness / 1000.0f) / (1.0f + A.stackDamping * A.h);
         const float push = -resolve * (gap + 1e-3f) / invMassSum;
         if (isDynamic(a.m.flags) && !isAsleep(a.m.flags))
-            __stcg(A.B.pos + cc.a, pack(a.p + r.normal * (push * ima), 0.0f));
+            __stcg(A.B.pos + ab.x, pack(a.p + r.normal * (push * ima), 0.0f));
         if (isDynamic(b.m.flags) && !isAsleep(b.m.flags))
-            __stcg(A.B.pos + cc.b, pack(b.p - r.normal * (push * imb), 0.0f));
+            __stcg(A.B.pos + ab.y, pack(b.p - r.normal * (push * imb), 0.0f));
         return;
     }
     RowPrep* Pg = A.prep + pos;
@@ -1610,8 +1623,8 @@ VXD void giantRow(const SolveArgs& A, uint32_t pos, int op) {
     coherentPrep(Pg, P);
     if (op == 0) warmPrepRow(a, b, r, P);
     else sweepRow(a, b, r, P, A.coneBlock != 0);
-    if (isDynamic(a.m.flags)) { __stcg(A.B.vel + cc.a, pack(a.v, 0.0f)); __stcg(A.B.ang + cc.a, pack(a.w, 0.0f)); }
-    if (isDynamic(b.m.flags)) { __stcg(A.B.vel + cc.b, pack(b.v, 0.0f)); __stcg(A.B.ang + cc.b, pack(b.w, 0.0f)); }
+    if (isDynamic(a.m.flags)) { __stcg(A.B.vel + ab.x, pack(a.v, 0.0f)); __stcg(A.B.ang + ab.x, pack(a.w, 0.0f)); }
+    if (isDynamic(b.m.flags)) { __stcg(A.B.vel + ab.y, pack(b.v, 0.0f)); __stcg(A.B.ang + ab.y, pack(b.w, 0.0f)); }
     storeRow(cc, r);
     storeContactCoherent(cp, cc);
 }
@@ -1681,8 +1694,8 @@ VXD bool giantFlow(const SolveArgs& A, uint32_t s0, uint32_t g0, uint32_t g1, in
                 const uint32_t need0 = (p0 & kWrap) ? (uint32_t)u : (uint32_t)u + 1u;
                 const uint32_t need1 = (p1 & kWrap) ? (uint32_t)u : (uint32_t)u + 1u;
                 for (uint32_t spins = 0;; ++spins) {
-                    const bool ready = (p0 == kNoPred || __ldcg(done + (p0 & ~kWrap)) >= need0) &&
-                                       (p1 == kNoPred || __ldcg(done + (p1 & ~kWrap)) >= need1);
+                    const bool ready = (p0 == kNoPred || ldAcquire(done + (p0 & ~kWrap)) >= need0) &&
+                                       (p1 == kNoPred || ldAcquire(done + (p1 & ~kWrap)) >= need1);
                     if (__all_sync(0xffffffffu, ready)) break;
                     if (spins > kSpinLimit || __ldcg(&st->timeout)) {
                         if (lane == 0) atomicOr(&st->timeout, 1u);
@@ -1690,10 +1703,10 @@ VXD bool giantFlow(const SolveArgs& A, uint32_t s0, uint32_t g0, uint32_t g1, in
                     }
                     __nanosleep(32);
                 }
-                __threadfence();  // acquire the predecessors' writes
-                if (active) giantRow(A, k, rowOp);
-                __threadfence();  // release this row's writes before it is marked done
-                if (active) __stcg(done + k, (uint32_t)u + 1u);
+                if (active) {
+                    giantRow(A, k, rowOp);
+                    stRelease(done + k, (uint32_t)u + 1u);  // publishes this row's writes
+                }
             }
         }
     }
@@ -1742,7 +1755,7 @@ __global__ void __launch_bounds__(256) solveGiantKernel(SolveArgs A, const uint3
 // Dataflow links of the giant islands' rows: entries (dynamic body, 2k + side)
 // of every row of a giant island, other endpoints keyed n (no link).
 __global__ void giantEntryKernel(SolveArgs A, const uint32_t* islandOf, uint32_t m, uint32_t n, uint64_t* keys,
-                                 uint32_t* vals);
+                                 uint32_t* vals, uint2* rowBodies);
 // For each body run of the sorted entries, the position of its last entry.
 __global__ void giantLastKernel(const uint64_t* keys, uint32_t entries, uint32_t n, uint32_t* lastOf) {
     for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < entries; p += gridDim.x * blockDim.x) {
@@ -1771,10 +1784,11 @@ VXD bool isGiant(const SolveArgs& A, uint32_t isl) {
 }
 
 __global__ void giantEntryKernel(SolveArgs A, const uint32_t* islandOf, uint32_t m, uint32_t n, uint64_t* keys,
-                                 uint32_t* vals) {
+                                 uint32_t* vals, uint2* rowBodies) {
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < m; k += gridDim.x * blockDim.x) {
         const bool giant = isGiant(A, islandOf[k]);
         const vx_contact& c = A.contacts[A.order[k]];
+        rowBodies[k] = make_uint2(c.a, c.b);
         const uint32_t fa = A.B.filt[c.a].x, fb = A.B.filt[c.b].x;
         const bool solved = giant && solvedContact(fa, fb);
         keys[2 * k] = solved && isDynamic(fa) ? c.a : n;
@@ -2661,12 +2675,14 @@ static int launchSolve(Context& c, const SolveArgs& A) {
     VXB_TRY(ensure(c, c.fpSlotBuf, (size_t)m * 8 + 64));
     VXB_TRY(ensure(c, c.fpColorBuf, (size_t)m * 4 + 64));
     VXB_TRY(ensure(c, c.fpRunStartBuf, (size_t)c.n * 4 + 64));
+    VXB_TRY(ensure(c, c.rowBodyBuf, (size_t)m * 8 + 64));
     uint32_t* pred = P<uint32_t>(c.fpSlotBuf);
     uint32_t* done = P<uint32_t>(c.fpColorBuf);
     if (!c.giantLinked) {
         uint64_t* keys = P<uint64_t>(c.fpKeyBuf);
         uint32_t* vals = P<uint32_t>(c.fpValBuf);
-        LAUNCH(c, giantEntryKernel, blocksFor(m, 256), 256, A, P<uint32_t>(c.fpIslandBuf), m, c.n, keys, vals);
+        LAUNCH(c, giantEntryKernel, blocksFor(m, 256), 256, A, P<uint32_t>(c.fpIslandBuf), m, c.n, keys, vals,
+               P<uint2>(c.rowBodyBuf));
         VXB_TRY(sortPairs(c, keys, vals, 2 * m, bitsFor(c.n)));
         LAUNCH(c, giantLastKernel, blocksFor(2 * m, 256), 256, keys, 2 * m, c.n, P<uint32_t>(c.fpRunStartBuf));
         LAUNCH(c, giantPredKernel, blocksFor(2 * m, 256), 256, keys, vals, 2 * m, c.n,
@@ -2674,7 +2690,9 @@ static int launchSolve(Context& c, const SolveArgs& A) {
         c.giantLinked = true;
     }
     VXB_CUDA(c, cudaMemsetAsync(st, 0, sizeof(CoopState), c.stream));
-    const int rc = launchCooperative(c, solveGiantKernel, 256, A, (const uint32_t*)list, giants,
+    SolveArgs G = A;
+    G.rowBodies = P<uint2>(c.rowBodyBuf);
+    const int rc = launchCooperative(c, solveGiantKernel, 256, G, (const uint32_t*)list, giants,
                                      (const uint32_t*)pred, done, st);
     if (rc == VXB_ERR_UNSUPPORTED) {
         LAUNCH(c, solveGiantBlockKernel, giants, kBlockThreads, A, (const uint32_t*)list);
