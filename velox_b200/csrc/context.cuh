@@ -93,6 +93,8 @@ struct Context {
     uint32_t caWidenings = 0;  // rewind replays with a widened body set (last step)
     uint32_t planContacts = 0; // contacts of the current island plan
     bool giantLinked = false;  // dataflow links of the plan's giant islands are built
+    bool clusterBuilt = false; // spatial clusters of the plan's (single) giant island are built
+    uint32_t clusterInfo[8] = {};  // island, rows [s0, s1), segments [g0, g1), bodies [b0, b1)
     cudaStream_t ownStream = nullptr;
     cudaStream_t stream = nullptr;
     std::string lastError;
@@ -158,6 +160,8 @@ struct Context {
     DevBuf giantBuf;                    // giant island list (solve)
     DevBuf classKeyBuf, classValBuf;    // convex pairs grouped by shape combination (narrow phase)
     DevBuf rowBodyBuf;                  // (a, b) per solve-order row (giant islands)
+    DevBuf clusterInfoBuf, clusterKeyBuf, clusterValBuf, clusterOfBuf, clusterCountBuf, clusterStartBuf,
+        clusterRowsBuf;                 // spatial clusters of a giant island
 
     DevBuf countersBuf;
     Counters* dCounters = nullptr;

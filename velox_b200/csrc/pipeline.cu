@@ -1776,6 +1776,170 @@ __global__ void giantPredKernel(const uint64_t* keys, const uint32_t* vals, uint
     }
 }
 
+// ---- one giant island in spatial clusters -------------------------------
+//
+// The same dataflow with coarser, local steps: the island's bodies are cut
+// into as many spatial clusters (Morton order) as the grid has blocks, each
+// row belongs to the cluster of its first dynamic body, and block c runs its
+// cluster's rows colour by colour with a block barrier between colours. Rows
+// whose predecessor on a body lies in another cluster wait for that row's
+// sweep counter; all others are ordered by the block barrier. Most chain steps
+// therefore stay inside a block. A block takes its (sweep, colour) steps in
+// order, which keeps the earliest unfinished step runnable; waits are bounded.
+
+VXD uint32_t spreadBits10(uint32_t v) {  // 10 bits -> every third bit
+    v &= 0x3ffu;
+    v = (v | (v << 16)) & 0x030000ffu;
+    v = (v | (v << 8)) & 0x0300f00fu;
+    v = (v | (v << 4)) & 0x030c30c3u;
+    v = (v | (v << 2)) & 0x09249249u;
+    return v;
+}
+
+__global__ void clusterBodyKeyKernel(SolveArgs A, uint32_t b0, uint32_t b1, const Counters* C, uint64_t* keys,
+                                     uint32_t* vals) {
+    const float lo[3] = {fromOrdered(C->cellMinBits[0]), fromOrdered(C->cellMinBits[1]), fromOrdered(C->cellMinBits[2])};
+    const float hi[3] = {fromOrdered(C->cellMaxBits[0]), fromOrdered(C->cellMaxBits[1]), fromOrdered(C->cellMaxBits[2])};
+    for (uint32_t k = b0 + blockIdx.x * blockDim.x + threadIdx.x; k < b1; k += gridDim.x * blockDim.x) {
+        const uint32_t id = A.bodyOrder[k];
+        const float4 p = A.B.pos[id];
+        const float x[3] = {p.x, p.y, p.z};
+        uint32_t code = 0;
+        for (int a = 0; a < 3; ++a) {
+            const float span = fmaxf(hi[a] - lo[a], 1e-6f);
+            float t = (x[a] - lo[a]) / span;
+            t = t >= 0.0f ? fminf(t, 1.0f) : 0.0f;  // NaN (no bounds) -> 0
+            code |= spreadBits10((uint32_t)(t * 1023.0f)) << a;
+        }
+        keys[k - b0] = code;
+        vals[k - b0] = id;
+    }
+}
+
+// Cluster of each island body (Morton rank chunked into `clusters`), per row
+// the owner cluster and its colour: counts per (cluster, colour).
+__global__ void clusterOfBodyKernel(const uint32_t* sortedIds, uint32_t nb, uint32_t clusters, uint32_t* clusterOf) {
+    for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < nb; r += gridDim.x * blockDim.x)
+        clusterOf[sortedIds[r]] = (uint32_t)(((uint64_t)r * clusters) / nb);
+}
+
+VXD uint32_t segmentOf(const uint32_t* segStart, uint32_t g0, uint32_t g1, uint32_t k) {
+    uint32_t lo = g0, hi = g1;  // last g with segStart[g] <= k
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (segStart[mid] <= k) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+VXD uint32_t rowCluster(const SolveArgs& A, uint32_t k, const uint32_t* clusterOf) {
+    const uint2 ab = A.rowBodies[k];
+    return clusterOf[isDynamic(A.B.filt[ab.x].x) ? ab.x : ab.y];
+}
+
+__global__ void clusterCountKernel(SolveArgs A, uint32_t s0, uint32_t s1, uint32_t g0, uint32_t g1,
+                                   const uint32_t* clusterOf, uint32_t* counts) {
+    const uint32_t G = g1 - g0;
+    for (uint32_t k = s0 + blockIdx.x * blockDim.x + threadIdx.x; k < s1; k += gridDim.x * blockDim.x)
+        atomicAdd(counts + rowCluster(A, k, clusterOf) * G + (segmentOf(A.segStart, g0, g1, k) - g0), 1u);
+}
+
+__global__ void clusterScatterKernel(SolveArgs A, uint32_t s0, uint32_t s1, uint32_t g0, uint32_t g1,
+                                     const uint32_t* clusterOf, const uint32_t* start, uint32_t* fill,
+                                     uint32_t* rows) {
+    const uint32_t G = g1 - g0;
+    for (uint32_t k = s0 + blockIdx.x * blockDim.x + threadIdx.x; k < s1; k += gridDim.x * blockDim.x) {
+        const uint32_t cell = rowCluster(A, k, clusterOf) * G + (segmentOf(A.segStart, g0, g1, k) - g0);
+        rows[start[cell] + atomicAdd(fill + cell, 1u)] = k;
+    }
+}
+
+// One unit (sweep) step of block c's cluster for colour slot gl; false = abort.
+VXD bool clusterStep(const SolveArgs& A, const uint32_t* start, const uint32_t* rows, uint32_t cell, int u, int op,
+                     const uint32_t* pred, uint32_t* done, CoopState* st, int* abortFlag) {
+    for (uint32_t idx = start[cell] + threadIdx.x; idx < start[cell + 1]; idx += blockDim.x) {
+        const uint32_t k = rows[idx];
+        const uint32_t p0 = pred[2 * k], p1 = pred[2 * k + 1];
+        const uint32_t need0 = (p0 & kWrap) ? (uint32_t)u : (uint32_t)u + 1u;
+        const uint32_t need1 = (p1 & kWrap) ? (uint32_t)u : (uint32_t)u + 1u;
+        bool ok = true;
+        for (uint32_t spins = 0;; ++spins) {
+            if ((p0 == kNoPred || ldAcquire(done + (p0 & ~kWrap)) >= need0) &&
+                (p1 == kNoPred || ldAcquire(done + (p1 & ~kWrap)) >= need1))
+                break;
+            if (spins > kSpinLimit || ((spins & 63u) == 63u && __ldcg(&st->timeout))) {
+                atomicOr(&st->timeout, 1u);
+                ok = false;
+                break;
+            }
+            __nanosleep(32);
+        }
+        if (!ok) { *abortFlag = 1; break; }
+        giantRow(A, k, op);
+        stRelease(done + k, (uint32_t)u + 1u);
+    }
+    __syncthreads();
+    return *abortFlag == 0;
+}
+
+__global__ void giantInfoKernel(SolveArgs A, const uint32_t* giants, uint32_t* info) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        const uint32_t isl = giants[0];
+        info[0] = isl;
+        info[1] = A.islandStart[isl];
+        info[2] = A.islandStart[isl + 1];
+        info[3] = A.islandSeg[isl];
+        info[4] = A.islandSeg[isl + 1];
+        info[5] = isl < A.realIslands ? A.bodyStart[isl] : 0u;
+        info[6] = isl < A.realIslands ? A.bodyStart[isl + 1] : 0u;
+    }
+}
+
+__global__ void __launch_bounds__(256) solveClusterKernel(SolveArgs A, uint32_t isl, uint32_t G,
+                                                          const uint32_t* start, const uint32_t* rows,
+                                                          const uint32_t* pred, uint32_t* done, CoopState* st) {
+    __shared__ int abortFlag;
+    if (threadIdx.x == 0) abortFlag = 0;
+    __syncthreads();
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+    const uint32_t s0 = A.islandStart[isl], s1 = A.islandStart[isl + 1];
+    const uint32_t b0 = isl < A.realIslands ? A.bodyStart[isl] : 0u;
+    const uint32_t b1 = isl < A.realIslands ? A.bodyStart[isl + 1] : 0u;
+    const uint32_t base = blockIdx.x * G;
+    if (A.positionIterations > 0) {
+        for (uint32_t k = s0 + tid; k < s1; k += stride) __stcg(done + k, 0u);
+        if (!gridSync(&st->bar, &st->timeout)) return;
+        for (int u = 0; u < A.positionIterations; ++u)
+            for (uint32_t gl = 0; gl < G; ++gl)
+                if (!clusterStep(A, start, rows, base + gl, u, 2, pred, done, st, &abortFlag)) return;
+        gridSync(&st->bar, &st->timeout);
+        return;
+    }
+    for (int s = 0; s < A.substeps; ++s) {
+        for (uint32_t k = b0 + tid; k < b1; k += stride) {
+            const uint32_t id = A.bodyOrder[k];
+            if (A.integrate && s > 0) giantIntegrateVelocity(A, id);
+            __stcg(A.frames + id, pack(inertiaFrameAt(loadMass(A.B, id), q4(ldcg4(A.B.rot + id)))));
+        }
+        if (!gridSync(&st->bar, &st->timeout)) return;
+        for (uint32_t k = s0 + tid; k < s1; k += stride) {
+            giantRow(A, k, 3);
+            __stcg(done + k, 0u);
+        }
+        if (!gridSync(&st->bar, &st->timeout)) return;
+        const int warmUnits = A.warmStart && s == 0 ? 1 : 0;
+        for (int u = 0; u < warmUnits + A.sweeps; ++u)
+            for (uint32_t gl = 0; gl < G; ++gl)
+                if (!clusterStep(A, start, rows, base + gl, u, u < warmUnits ? 0 : 1, pred, done, st, &abortFlag))
+                    return;
+        if (!gridSync(&st->bar, &st->timeout)) return;
+        if (A.integrate) {
+            for (uint32_t k = b0 + tid; k < b1; k += stride) giantIntegrateTransform(A, A.bodyOrder[k]);
+            if (!gridSync(&st->bar, &st->timeout)) return;
+        }
+    }
+}
+
 // The block kernel's complement among the islands above tinyLimit.
 VXD bool isGiant(const SolveArgs& A, uint32_t isl) {
     const uint32_t rows = A.islandStart[isl + 1] - A.islandStart[isl];
@@ -2528,6 +2692,7 @@ static int buildIslands(Context& c, const vx_contact* cs, uint32_t m, IslandPlan
     plan.contacts = m;
     c.planContacts = m;
     c.giantLinked = false;
+    c.clusterBuilt = false;
     VXB_TRY(ensure(c, c.parentBuf, (size_t)n * 4));
     VXB_TRY(ensure(c, c.islandOfBodyBuf, (size_t)n * 4));
     VXB_TRY(ensure(c, c.maskBuf, (size_t)n * 8));
@@ -2689,9 +2854,66 @@ static int launchSolve(Context& c, const SolveArgs& A) {
                P<uint32_t>(c.fpRunStartBuf), pred);
         c.giantLinked = true;
     }
-    VXB_CUDA(c, cudaMemsetAsync(st, 0, sizeof(CoopState), c.stream));
     SolveArgs G = A;
     G.rowBodies = P<uint2>(c.rowBodyBuf);
+    if (giants == 1 && c.cooperative) {
+        // one giant island: spatial clusters, one per block of the cooperative grid
+        int perSm = 0;
+        VXB_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, solveClusterKernel, 256, 0));
+        const uint32_t clusters = (uint32_t)(perSm * c.smCount);
+        if (clusters > 0) {
+            VXB_TRY(ensure(c, c.clusterInfoBuf, 64));
+            uint32_t* info = P<uint32_t>(c.clusterInfoBuf);
+            if (!c.clusterBuilt) {
+                LAUNCH(c, giantInfoKernel, 1, 32, G, (const uint32_t*)list, info);
+                VXB_CUDA(c, cudaMemcpyAsync(c.clusterInfo, info, sizeof(c.clusterInfo), cudaMemcpyDeviceToHost,
+                                            c.stream));
+                VXB_CUDA(c, cudaStreamSynchronize(c.stream));
+            }
+            const uint32_t isl = c.clusterInfo[0], s0 = c.clusterInfo[1], s1 = c.clusterInfo[2];
+            const uint32_t g0 = c.clusterInfo[3], g1 = c.clusterInfo[4], b0 = c.clusterInfo[5], b1 = c.clusterInfo[6];
+            const uint32_t nb = b1 - b0, cells = clusters * (g1 - g0);
+            VXB_TRY(ensure(c, c.clusterStartBuf, ((size_t)cells + 1) * 4 + 64));
+            VXB_TRY(ensure(c, c.clusterRowsBuf, (size_t)(s1 - s0) * 4 + 64));
+            uint32_t* start = P<uint32_t>(c.clusterStartBuf);
+            uint32_t* rows = P<uint32_t>(c.clusterRowsBuf);
+            if (!c.clusterBuilt && nb > 0 && s1 > s0) {
+                VXB_TRY(ensure(c, c.clusterKeyBuf, (size_t)nb * 8 + 64));
+                VXB_TRY(ensure(c, c.clusterValBuf, (size_t)nb * 4 + 64));
+                VXB_TRY(ensure(c, c.clusterOfBuf, (size_t)c.n * 4 + 64));
+                VXB_TRY(ensure(c, c.clusterCountBuf, (size_t)cells * 8 + 64));
+                uint32_t* counts = P<uint32_t>(c.clusterCountBuf);
+                uint32_t* fill = counts + cells;
+                LAUNCH(c, clusterBodyKeyKernel, blocksFor(nb, 256), 256, G, b0, b1, (const Counters*)c.dCounters,
+                       P<uint64_t>(c.clusterKeyBuf), P<uint32_t>(c.clusterValBuf));
+                VXB_TRY(sortPairs(c, P<uint64_t>(c.clusterKeyBuf), P<uint32_t>(c.clusterValBuf), nb, 30));
+                LAUNCH(c, clusterOfBodyKernel, blocksFor(nb, 256), 256, (const uint32_t*)P<uint32_t>(c.clusterValBuf),
+                       nb, clusters, P<uint32_t>(c.clusterOfBuf));
+                VXB_CUDA(c, cudaMemsetAsync(counts, 0, (size_t)cells * 8, c.stream));
+                LAUNCH(c, clusterCountKernel, blocksFor(s1 - s0, 256), 256, G, s0, s1, g0, g1,
+                       (const uint32_t*)P<uint32_t>(c.clusterOfBuf), counts);
+                VXB_TRY(exclusiveScan(c, counts, start, cells, start + cells));
+                LAUNCH(c, clusterScatterKernel, blocksFor(s1 - s0, 256), 256, G, s0, s1, g0, g1,
+                       (const uint32_t*)P<uint32_t>(c.clusterOfBuf), (const uint32_t*)start, fill, rows);
+                c.clusterBuilt = true;
+            }
+            if (c.clusterBuilt) {
+                VXB_CUDA(c, cudaMemsetAsync(st, 0, sizeof(CoopState), c.stream));
+                const int rcc = launchCooperative(c, solveClusterKernel, 256, G, isl, g1 - g0,
+                                                  (const uint32_t*)start, (const uint32_t*)rows,
+                                                  (const uint32_t*)pred, done, st);
+                if (rcc != VXB_ERR_UNSUPPORTED) {
+                    VXB_TRY(rcc);
+                    uint32_t timeout = 0;
+                    VXB_CUDA(c, cudaMemcpyAsync(&timeout, &st->timeout, 4, cudaMemcpyDeviceToHost, c.stream));
+                    VXB_CUDA(c, cudaStreamSynchronize(c.stream));
+                    if (timeout) return fail(c, VXB_ERR_TIMEOUT, "a wait timed out in the giant-island solve");
+                    return VXB_OK;
+                }
+            }
+        }
+    }
+    VXB_CUDA(c, cudaMemsetAsync(st, 0, sizeof(CoopState), c.stream));
     const int rc = launchCooperative(c, solveGiantKernel, 256, G, (const uint32_t*)list, giants,
                                      (const uint32_t*)pred, done, st);
     if (rc == VXB_ERR_UNSUPPORTED) {
