@@ -259,7 +259,7 @@ def main():
     rows = contacts_total * 2 * 8 * SUBSTEPS  # sweeps * substeps per step
     solve_bytes = rows * SOLVER_BYTES_PER_ROW
     solve_gbs = solve_bytes / (solve_ms / 1e3) / 1e9 if solve_ms > 0 else 0.0
-    solve_roofline = {"bound": "hbm", "kernel": "solveTinyKernel+solveBlockKernel+solveGiantKernel (substep solve)",
+    solve_roofline = {"bound": "hbm", "kernel": "solveTinyKernel+solveBlockKernel+solveClusterKernel (substep solve)",
                       "achieved": solve_gbs, "peak": peak, "unit": "GB/s", "frac": solve_gbs / peak,
                       "peak_source": peak_kind, "traffic": None,
                       "algorithmic_bytes_per_launch": solve_bytes / max(solve_calls, 1),
