@@ -4,6 +4,7 @@ mixed-shape scene (spheres, boxes, capsules, cylinders, 16-vertex hulls in a
 data.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+    python bench.py --workload batched [--steps K] ...   (4096 independent worlds)
 
 b200 arm: one process per GPU (torchrun for N > 1); every rank steps its own
 replica of the world ("replicas only": a single world does not shard), the
@@ -168,6 +169,207 @@ def run_reference(args):
     return 0
 
 
+BATCH_CONFIG = 4      # independent worlds: plane + log-uniform [8, 512] spheres/boxes/capsules each
+PLAIN_SAMPLE = 48     # worlds stepped one at a time for the plain comparison
+CPU_SAMPLE = 48       # worlds stepped by the reference CPU backend
+
+
+def run_batched(args):
+    """world-steps/s of 4096 independent worlds packed into one context (world
+    id in the cell-key high bits, islands never cross worlds), next to the
+    same worlds stepped one world per context (the plain single-world path:
+    a sample of worlds spread over the size distribution, scaled by their
+    share of the batch) and the reference CPU backend on a sample of worlds.
+    Under torchrun the worlds are split across ranks (strong scaling, no
+    data-path collective)."""
+    import torch
+    import velox_b200 as vb
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    nworlds = args.size if args.size != 100000 else 4096
+    specs, pool = vb.generate_scene(BATCH_CONFIG, seed=BATCH_CONFIG, size=nworlds)
+    lo, hi = nworlds * rank // world, nworlds * (rank + 1) // world
+    mine = specs[(specs["world"] >= lo) & (specs["world"] < hi)].copy()
+    mine["world"] -= lo
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        return run_batched_reference(args, specs, pool, nworlds)
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    bodies, hull, faces = vb.bodies_from_specs(mine, pool)
+    soup = vb.make_soup(hull, faces)
+    worlds_here = hi - lo
+    stream = torch.cuda.Stream()
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def timed(ctx, steps, host=None):
+        events = []
+        with torch.cuda.stream(stream):
+            for _ in range(steps):
+                flush.fill_(1)
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                if host:
+                    ctx.write_forces(host[0])
+                ctx.step(1)
+                if host:
+                    ctx.read_poses(host[1])
+                e1.record(stream)
+                events.append((e0, e1))
+        torch.cuda.synchronize()
+        return sum(a.elapsed_time(b) for a, b in events)
+
+    # batched
+    ctx = vb.Context(local)
+    ctx.set_stream(stream.cuda_stream)
+    ctx.load(bodies, soup, world_of=mine["world"])
+    ctx.configure(dt=DT, substeps=SUBSTEPS)
+    ctx.step(max(args.warmup, 3))
+    sampler = ClockSampler(local)
+    sampler.start()
+    barrier()
+    launches0 = ctx.launches
+    ctx.enable_timing(True)
+    ms = timed(ctx, args.steps)
+    barrier()
+    clocks = sampler.stop()
+    launches = ctx.launches - launches0
+    stage = ctx.stage_times()
+    last = ctx.stats()
+    ctx.close()
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = nworlds * args.steps / (ms / 1e3)
+
+    # e2e: a fresh batched world through the C ABI with host buffers every step
+    ctx = vb.Context(local)
+    ctx.set_stream(stream.cuda_stream)
+    ctx.load(bodies, soup, world_of=mine["world"])
+    ctx.configure(dt=DT, substeps=SUBSTEPS)
+    ctx.step(max(args.warmup, 3))
+    n = len(bodies)
+    forces = torch.zeros((n, 6), dtype=torch.float32).pin_memory()
+    poses = torch.zeros((n, 7), dtype=torch.float32).pin_memory()
+    barrier()
+    e2e_ms = timed(ctx, args.steps, (forces.numpy(), poses.numpy()))
+    ctx.close()
+    if dist:
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+
+    # plain: sampled worlds one per context, scaled by their body share
+    plain = None
+    if rank == 0:
+        counts = np.bincount(specs["world"], minlength=nworlds)
+        order = np.argsort(counts, kind="stable")
+        sample = order[np.linspace(0, nworlds - 1, min(PLAIN_SAMPLE, nworlds)).astype(int)]
+        total_ms = 0.0
+        for w in sample:
+            one = specs[specs["world"] == w].copy()
+            one["world"] = 0
+            b1, h1, f1 = vb.bodies_from_specs(one, pool)
+            c1 = vb.Context(local)
+            c1.set_stream(stream.cuda_stream)
+            c1.load(b1, vb.make_soup(h1, f1))
+            c1.configure(dt=DT, substeps=SUBSTEPS)
+            c1.step(max(args.warmup, 3))
+            total_ms += timed(c1, args.steps)
+            c1.close()
+        per_world_ms = total_ms / len(sample) / args.steps
+        plain = {"value": 1e3 / per_world_ms, "unit": "world-steps/s",
+                 "sample": f"{len(sample)} worlds spread over the body-count distribution, each in its own context, "
+                           f"{args.steps} device-timed steps after {max(args.warmup, 3)} warm-up steps; "
+                           f"one world at a time on this GPU"}
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        try:
+            cpu = batched_cpu_baseline(specs, pool, nworlds, min(args.steps, 20))
+        except Exception as exc:  # reported, not fatal
+            cpu = {"error": str(exc)}
+    if dist:
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    bodies_total = int(len(specs))
+    line = {"metric": f"world-steps/s @{nworlds} worlds", "value": value, "unit": "world-steps/s",
+            "n_gpus": world, "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded)",
+            "config": {"workload": f"{nworlds} independent worlds, plane + log-uniform [8,512] spheres/boxes/capsules "
+                                   f"each ({bodies_total} bodies), dt 1/60 s, {SUBSTEPS} substeps",
+                       "worlds": nworlds, "bodies": bodies_total, "parallelism": f"worlds split over {world} GPU(s)",
+                       "l2": "flushed (256 MiB write) before every timed step, outside the step's events"},
+            "body_steps_per_s": bodies_total * args.steps / (ms / 1e3),
+            "plain": plain, "vs_plain": value / plain["value"] if plain else None,
+            "last_step": last, "stage_ms_per_step": {k: v[0] / args.steps for k, v in stage.items()},
+            "cpu_baseline": cpu,
+            "e2e": {"value": nworlds * args.steps / (e2e_ms / 1e3), "unit": "world-steps/s",
+                    "h2d_bytes_per_step": int(forces.numel() * 4), "d2h_bytes_per_step": int(poses.numel() * 4)},
+            "clocks": clocks, "gpu_launches": int(launches)}
+    print(json.dumps(line))
+    return 0
+
+
+def batched_cpu_baseline(specs, pool, nworlds, steps):
+    """Reference CPU backend (Release build, all host threads) on sampled worlds."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref
+    if not ref.available(strict=False):
+        return None
+    counts = np.bincount(specs["world"], minlength=nworlds)
+    order = np.argsort(counts, kind="stable")
+    sample = order[np.linspace(0, nworlds - 1, min(CPU_SAMPLE, nworlds)).astype(int)]
+    total = 0.0
+    workers = 0
+    for w in sample:
+        one = specs[specs["world"] == w].copy()
+        one["world"] = 0
+        rw = ref.RefWorld(one, pool, backend=ref.BACKEND_CPU, strict=False)
+        rw.configure(substeps=SUBSTEPS, workers=0)
+        workers = int(rw.L.ref_world_worker_count(rw.h))
+        rw.step(DT, 3)
+        for _ in range(steps):
+            total += rw.step(DT, 1) / 1000.0
+        rw.close()
+    value = len(sample) * steps / total
+    return {"value": value, "unit": "world-steps/s", "cores": workers, "kind": "reference",
+            "sample": f"{len(sample)} worlds spread over the body-count distribution, {steps} steps each after 3 "
+                      f"warm-up steps, one world at a time; reference CPU backend (Release build), {workers} worker "
+                      f"threads on {os.cpu_count()} host cores"}
+
+
+def run_batched_reference(args, specs, pool, nworlds):
+    cpu = batched_cpu_baseline(specs, pool, nworlds, min(args.steps, 20))
+    if cpu is None:
+        print(json.dumps({"impl": "reference", "unavailable": "reference CPU build (oracle/_ref) missing"}))
+        return 0
+    line = {"metric": f"world-steps/s @{nworlds} worlds", "value": cpu["value"], "unit": "world-steps/s",
+            "impl": "reference", "n_gpus": 0, "steps": min(args.steps, 20), "warmup": 3, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+            "config": {"workload": f"{nworlds} independent worlds (sampled)", "worlds": nworlds},
+            "cpu_baseline": cpu,
+            "e2e": {"value": cpu["value"], "unit": "world-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -178,7 +380,11 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile", action="store_true",
                     help="bracket the timed steps with cudaProfilerStart/Stop (ncu --profile-from-start off)")
+    ap.add_argument("--workload", default="single", choices=["single", "batched"],
+                    help="single: the 100k-body world (default); batched: 4096 independent worlds in one context")
     args = ap.parse_args()
+    if args.workload == "batched":
+        return run_batched(args)
     if args.impl == "reference":
         return run_reference(args)
 
