@@ -244,7 +244,11 @@ def run_batched(args):
     barrier()
     launches0 = ctx.launches
     ctx.enable_timing(True)
+    if args.profile:
+        torch.cuda.cudart().cudaProfilerStart()
     ms = timed(ctx, args.steps)
+    if args.profile:
+        torch.cuda.cudart().cudaProfilerStop()
     barrier()
     clocks = sampler.stop()
     launches = ctx.launches - launches0
@@ -276,7 +280,7 @@ def run_batched(args):
 
     # plain: sampled worlds one per context, scaled by their body share
     plain = None
-    if rank == 0:
+    if rank == 0 and not args.profile:
         counts = np.bincount(specs["world"], minlength=nworlds)
         order = np.argsort(counts, kind="stable")
         sample = order[np.linspace(0, nworlds - 1, min(PLAIN_SAMPLE, nworlds)).astype(int)]
@@ -298,7 +302,7 @@ def run_batched(args):
                            f"{args.steps} device-timed steps after {max(args.warmup, 3)} warm-up steps; "
                            f"one world at a time on this GPU"}
     cpu = None
-    if rank == 0 and not args.no_cpu_baseline:
+    if rank == 0 and not args.no_cpu_baseline and not args.profile:
         try:
             cpu = batched_cpu_baseline(specs, pool, nworlds, min(args.steps, 20))
         except Exception as exc:  # reported, not fatal
