@@ -1275,8 +1275,18 @@ __global__ void __launch_bounds__(64) solveTinyKernel(SolveArgs A) {
 constexpr int kBlockThreads = 256;
 constexpr int kBlockBodies = 512;
 constexpr int kBlockRows = 3072;
-constexpr size_t kBlockSmem = (size_t)kBlockBodies * (7 * sizeof(float4) + sizeof(uint32_t)) +
-                              (size_t)kBlockRows * sizeof(int2);
+// Islands of up to kSmallBodies bodies and kSmallRows contacts run on one warp
+// each, many per SM (a colour of a small island has a few rows; a 256-thread
+// block would leave most of its threads idle and hold a whole SM's share of
+// shared memory).
+constexpr int kSmallThreads = 32;
+constexpr int kSmallBodies = 64;
+constexpr int kSmallRows = 256;
+constexpr size_t blockSmem(int bodies, int rows) {
+    return (size_t)bodies * (7 * sizeof(float4) + sizeof(uint32_t)) + (size_t)rows * sizeof(int2);
+}
+constexpr size_t kBlockSmem = blockSmem(kBlockBodies, kBlockRows);
+constexpr size_t kSmallSmem = blockSmem(kSmallBodies, kSmallRows);
 
 struct SharedBodies {
     float4 *p, *q, *v, *w, *inertia, *iq, *frame;
@@ -1284,17 +1294,18 @@ struct SharedBodies {
     int2* rowIdx;  // per island row: local index of a / b, -1 = read-only global body
 };
 
+template <int Bodies>
 VXD SharedBodies carve(float4* base) {
     SharedBodies S;
     S.p = base;
-    S.q = S.p + kBlockBodies;
-    S.v = S.q + kBlockBodies;
-    S.w = S.v + kBlockBodies;
-    S.inertia = S.w + kBlockBodies;
-    S.iq = S.inertia + kBlockBodies;
-    S.frame = S.iq + kBlockBodies;
-    S.flags = reinterpret_cast<uint32_t*>(S.frame + kBlockBodies);
-    S.rowIdx = reinterpret_cast<int2*>(S.flags + kBlockBodies);
+    S.q = S.p + Bodies;
+    S.v = S.q + Bodies;
+    S.w = S.v + Bodies;
+    S.inertia = S.w + Bodies;
+    S.iq = S.inertia + Bodies;
+    S.frame = S.iq + Bodies;
+    S.flags = reinterpret_cast<uint32_t*>(S.frame + Bodies);
+    S.rowIdx = reinterpret_cast<int2*>(S.flags + Bodies);
     return S;
 }
 
@@ -1448,16 +1459,21 @@ __device__ void solveIslandGlobal(const SolveArgs& A, uint32_t isl) {
     }
 }
 
-__global__ void __launch_bounds__(kBlockThreads) solveBlockKernel(SolveArgs A, uint32_t* localIdx) {
+// Small = the island fits the one-warp variant.
+VXD bool smallIsland(uint32_t nb, uint32_t rows) { return nb <= (uint32_t)kSmallBodies && rows <= (uint32_t)kSmallRows; }
+
+template <int Threads, int Bodies, int Rows, bool Small>
+__global__ void __launch_bounds__(Threads) solveBlockKernel(SolveArgs A, uint32_t* localIdx) {
     extern __shared__ float4 smemRaw[];
-    const SharedBodies S = carve(smemRaw);
+    const SharedBodies S = carve<Bodies>(smemRaw);
     for (uint32_t isl = blockIdx.x; isl < A.islands; isl += gridDim.x) {
         const uint32_t s0 = A.islandStart[isl], s1 = A.islandStart[isl + 1];
         if (s1 - s0 <= A.tinyLimit) continue;
         const uint32_t b0 = isl < A.realIslands ? A.bodyStart[isl] : 0u;
         const uint32_t b1 = isl < A.realIslands ? A.bodyStart[isl + 1] : 0u;
         const uint32_t nb = b1 - b0, rows = s1 - s0;
-        if (nb > (uint32_t)kBlockBodies || rows > (uint32_t)kBlockRows) continue;  // solveGiantKernel
+        if (nb > (uint32_t)Bodies || rows > (uint32_t)Rows) continue;  // a giant island
+        if (!Small && smallIsland(nb, rows)) continue;                 // the one-warp variant's
         for (uint32_t k = threadIdx.x; k < nb; k += blockDim.x) {
             const uint32_t id = A.bodyOrder[b0 + k];
             S.p[k] = A.B.pos[id]; S.q[k] = A.B.rot[id]; S.v[k] = A.B.vel[id]; S.w[k] = A.B.ang[id];
@@ -2811,13 +2827,21 @@ static int prepareSegments(Context& c, const IslandPlan& plan) {
 static int launchSolve(Context& c, const SolveArgs& A) {
     if (A.islands == 0) return VXB_OK;
     LAUNCH(c, solveTinyKernel, blocksFor(A.islands, 64), 64, A);
-    static bool configured = false;
-    if (!configured) {
-        cudaFuncSetAttribute(solveBlockKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBlockSmem);
-        configured = true;
+    auto* large = solveBlockKernel<kBlockThreads, kBlockBodies, kBlockRows, false>;
+    auto* small = solveBlockKernel<kSmallThreads, kSmallBodies, kSmallRows, true>;
+    static int smallPerSm = 0;
+    if (!smallPerSm) {
+        cudaFuncSetAttribute(large, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBlockSmem);
+        cudaFuncSetAttribute(small, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmallSmem);
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&smallPerSm, small, kSmallThreads, kSmallSmem) != cudaSuccess ||
+            smallPerSm <= 0)
+            smallPerSm = 8;
     }
-    ensure(c, c.localIdxBuf, (size_t)c.n * 4 + 16);
-    solveBlockKernel<<<std::min<uint32_t>(A.islands, (uint32_t)c.smCount * 2), kBlockThreads, kBlockSmem, c.stream>>>(
+    VXB_TRY(ensure(c, c.localIdxBuf, (size_t)c.n * 4 + 16));
+    small<<<std::min<uint32_t>(A.islands, (uint32_t)(c.smCount * smallPerSm)), kSmallThreads, kSmallSmem, c.stream>>>(
+        A, P<uint32_t>(c.localIdxBuf));
+    ++c.launches;
+    large<<<std::min<uint32_t>(A.islands, (uint32_t)c.smCount * 2), kBlockThreads, kBlockSmem, c.stream>>>(
         A, P<uint32_t>(c.localIdxBuf));
     ++c.launches;
     // giant islands: list them, then one cooperative launch over all of them
