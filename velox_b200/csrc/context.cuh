@@ -68,7 +68,9 @@ struct Counters {
     uint32_t planFault;      // a solve kernel found an inconsistent island plan
     uint32_t caGapQueries;   // distance queries of the rewind passes
     uint32_t caCritMicros;   // rewind: evaluation time along the longest dependency chain
-    uint32_t pad[4];
+    uint32_t tinyIslands;    // islands of at most tinyLimit contacts (packed solve)
+    uint32_t tinyPacks;      // warps they were packed into
+    uint32_t pad[2];
 };
 
 // Pipeline stages timed with CUDA events when timing is enabled.
@@ -94,6 +96,8 @@ struct Context {
     uint32_t planContacts = 0; // contacts of the current island plan
     bool giantLinked = false;  // dataflow links of the plan's giant islands are built
     bool clusterBuilt = false; // spatial clusters of the plan's (single) giant island are built
+    bool tinyPacked = false;   // the plan's tiny islands are packed into warps
+    uint32_t tinyCount = 0, tinyPackCount = 0;
     uint32_t clusterInfo[8] = {};  // island, rows [s0, s1), segments [g0, g1), bodies [b0, b1)
     cudaStream_t ownStream = nullptr;
     cudaStream_t stream = nullptr;
@@ -160,6 +164,7 @@ struct Context {
     DevBuf giantBuf;                    // giant island list (solve)
     DevBuf classKeyBuf, classValBuf;    // convex pairs grouped by shape combination (narrow phase)
     DevBuf rowBodyBuf;                  // (a, b) per solve-order row (giant islands)
+    DevBuf tinyBuf;                     // tiny-island flags, ranks, list, pack counts/bases/firsts
     DevBuf clusterInfoBuf, clusterKeyBuf, clusterValBuf, clusterOfBuf, clusterCountBuf, clusterStartBuf,
         clusterRowsBuf;                 // spatial clusters of a giant island
 

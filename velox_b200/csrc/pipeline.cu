@@ -1542,6 +1542,224 @@ __global__ void __launch_bounds__(Threads) solveBlockKernel(SolveArgs A, uint32_
     }
 }
 
+// ---- tiny islands packed into warps -----------------------------------------
+//
+// Islands of at most tinyLimit (16) contacts are packed, in island order, into
+// warps of at most 32 rows and 64 bodies. Each lane owns one row and keeps its
+// contact terms and per-substep pose terms in registers; the pack's bodies live
+// in shared memory. A step runs colour slot c of every island in the pack at
+// once (rows of different islands share no body; rows of one colour share no
+// dynamic body), so each body sees its rows in colour order, as in the serial
+// per-island loop. A pack needs (largest colour count) x sweeps x substeps
+// warp steps instead of (rows x sweeps x substeps) thread steps, with no
+// per-thread arrays in local memory.
+constexpr int kPackRows = 32;
+constexpr int kPackBodies = 64;
+constexpr int kPackChunk = 512;     // tiny islands per packing thread
+constexpr int kPackWarps = 4;       // warps (packs) per block
+
+__global__ void tinyFlagKernel(SolveArgs A, uint32_t* flags) {
+    for (uint32_t isl = blockIdx.x * blockDim.x + threadIdx.x; isl < A.islands; isl += gridDim.x * blockDim.x) {
+        const uint32_t rows = A.islandStart[isl + 1] - A.islandStart[isl];
+        flags[isl] = rows > 0 && rows <= A.tinyLimit ? 1u : 0u;
+    }
+}
+
+VXD uint32_t islandBodies(const SolveArgs& A, uint32_t isl) {
+    return isl < A.realIslands ? A.bodyStart[isl + 1] - A.bodyStart[isl] : 0u;
+}
+
+// Greedy packing of each chunk of the tiny-island list: pass 0 counts the
+// packs of a chunk, pass 1 writes each pack's first list index.
+__global__ void tinyPackKernel(SolveArgs A, const uint32_t* list, uint32_t count, int pass, uint32_t* packCount,
+                               const uint32_t* packBase, uint32_t* packFirst) {
+    const uint32_t chunks = (count + kPackChunk - 1) / kPackChunk;
+    for (uint32_t ch = blockIdx.x * blockDim.x + threadIdx.x; ch < chunks; ch += gridDim.x * blockDim.x) {
+        const uint32_t t0 = ch * kPackChunk, t1 = min(count, t0 + kPackChunk);
+        uint32_t packs = 0, rows = 0, bodies = 0;
+        for (uint32_t t = t0; t < t1; ++t) {
+            const uint32_t isl = list[t];
+            const uint32_t r = A.islandStart[isl + 1] - A.islandStart[isl], b = islandBodies(A, isl);
+            if (t == t0 || rows + r > (uint32_t)kPackRows || bodies + b > (uint32_t)kPackBodies) {
+                if (pass == 1) packFirst[packBase[ch] + packs] = t;
+                ++packs;
+                rows = 0;
+                bodies = 0;
+            }
+            rows += r;
+            bodies += b;
+        }
+        if (pass == 0) packCount[ch] = packs;
+    }
+}
+
+// Per-warp shared memory of the pack kernel: the bodies and their ids.
+constexpr size_t kPackBodySmem = blockSmem(kPackBodies, 0);
+constexpr size_t kPackWarpSmem = (kPackBodySmem + kPackBodies * sizeof(uint32_t) + 15) / 16 * 16;
+
+__global__ void __launch_bounds__(32 * kPackWarps) solveTinyPackKernel(SolveArgs A, const uint32_t* list,
+                                                                        const uint32_t* packFirst, uint32_t packs,
+                                                                        uint32_t listCount, uint32_t* localIdx) {
+    extern __shared__ float4 smemRaw[];
+    const uint32_t warpInBlock = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+    float4* base = smemRaw + warpInBlock * (kPackWarpSmem / sizeof(float4));
+    const SharedBodies S = carve<kPackBodies>(base);
+    uint32_t* ids = reinterpret_cast<uint32_t*>(base + kPackBodySmem / sizeof(float4));
+    const uint32_t packIdx = blockIdx.x * kPackWarps + warpInBlock;
+    if (packIdx >= packs) return;  // the whole warp
+    const uint32_t first = packFirst[packIdx];
+    const uint32_t last = packIdx + 1 < packs ? packFirst[packIdx + 1] : listCount;
+    const uint32_t count = last - first;  // islands in this pack (1..32)
+    uint32_t isl = 0, r = 0, nb = 0, colours = 0;
+    if (lane < count) {
+        isl = list[first + lane];
+        r = A.islandStart[isl + 1] - A.islandStart[isl];
+        nb = islandBodies(A, isl);
+        colours = A.islandSeg[isl + 1] - A.islandSeg[isl];
+    }
+    // inclusive prefix sums of rows and bodies over the pack's islands, largest colour count
+    uint32_t rp = r, bp = nb, maxC = colours;
+    for (int off = 1; off < 32; off <<= 1) {
+        const uint32_t x = __shfl_up_sync(0xffffffffu, rp, off), y = __shfl_up_sync(0xffffffffu, bp, off);
+        if ((int)lane >= off) { rp += x; bp += y; }
+    }
+    for (int off = 16; off > 0; off >>= 1) maxC = max(maxC, __shfl_xor_sync(0xffffffffu, maxC, off));
+    rp -= r;  // exclusive
+    bp -= nb;
+    const uint32_t totalBodies = __shfl_sync(0xffffffffu, bp + nb, 31);
+    // bodies into shared memory: island j's bodies at slots [bp_j, bp_j + nb_j)
+    for (uint32_t j = 0; j < count; ++j) {
+        const uint32_t jIsl = __shfl_sync(0xffffffffu, isl, j), jB = __shfl_sync(0xffffffffu, nb, j);
+        const uint32_t jBase = __shfl_sync(0xffffffffu, bp, j);
+        for (uint32_t k = lane; k < jB; k += 32) {
+            const uint32_t id = A.bodyOrder[A.bodyStart[jIsl] + k], t = jBase + k;
+            S.p[t] = A.B.pos[id]; S.q[t] = A.B.rot[id]; S.v[t] = A.B.vel[id]; S.w[t] = A.B.ang[id];
+            S.inertia[t] = A.B.inertia[id]; S.iq[t] = A.B.iq[id]; S.flags[t] = A.B.filt[id].x;
+            ids[t] = id;
+            localIdx[id] = t;
+        }
+    }
+    __syncwarp();
+    // this lane's row: the island j with rp_j <= lane < rp_j + r_j
+    bool has = false;
+    uint32_t row = 0, myIsl = 0, myBase = 0, myNb = 0;
+    for (uint32_t j = 0; j < count; ++j) {
+        const uint32_t jr = __shfl_sync(0xffffffffu, r, j), jrp = __shfl_sync(0xffffffffu, rp, j);
+        const uint32_t jIsl = __shfl_sync(0xffffffffu, isl, j), jBase = __shfl_sync(0xffffffffu, bp, j);
+        const uint32_t jNb = __shfl_sync(0xffffffffu, nb, j);
+        if (lane >= jrp && lane < jrp + jr) {
+            has = true;
+            myIsl = jIsl;
+            row = A.islandStart[jIsl] + (lane - jrp);
+            myBase = jBase;
+            myNb = jNb;
+        }
+    }
+    vx_contact* cp = nullptr;
+    RowContact rc;
+    RowPrep P;
+    int la = -1, lb = -1;
+    uint32_t ida = 0, idb = 0, myC = 0;
+    bool live = false;
+    if (has) {
+        cp = A.contacts + A.order[row];
+        loadRow(*cp, rc);
+        ida = cp->a;
+        idb = cp->b;
+        const uint32_t fa = A.B.filt[ida].x, fb = A.B.filt[idb].x;
+        live = solvedContact(fa, fb);
+        if (isDynamic(fa)) la = (int)localIdx[ida];
+        if (isDynamic(fb)) lb = (int)localIdx[idb];
+        // a dynamic body outside its island's slots means an inconsistent plan: report it, never index smem
+        if (la >= 0 && ((uint32_t)la < myBase || (uint32_t)la >= myBase + myNb || ids[la] != ida)) {
+            atomicOr(A.fault, 1u);
+            la = -1;
+        }
+        if (lb >= 0 && ((uint32_t)lb < myBase || (uint32_t)lb >= myBase + myNb || ids[lb] != idb)) {
+            atomicOr(A.fault, 1u);
+            lb = -1;
+        }
+        const uint32_t g0 = A.islandSeg[myIsl], g1 = A.islandSeg[myIsl + 1];
+        uint32_t g = g0;
+        while (g + 1 < g1 && A.segStart[g + 1] <= row) ++g;
+        myC = g - g0;
+    }
+    if (A.positionIterations > 0) {
+        for (int it = 0; it < A.positionIterations; ++it)
+            for (uint32_t c = 0; c < maxC; ++c) {
+                if (live && myC == c) {
+                    const SolverBody a = la >= 0 ? sharedBody(S, la) : globalBody(A.B, ida);
+                    const SolverBody b = lb >= 0 ? sharedBody(S, lb) : globalBody(A.B, idb);
+                    const float ima = solverInvMass(a.m), imb = solverInvMass(b.m);
+                    const float invMassSum = ima + imb;
+                    if (invMassSum > 0.0f) {
+                        const V3 wa = anchorWorld(a.sphere, a.p, a.q, rc.la);
+                        const V3 wb = anchorWorld(b.sphere, b.p, b.q, rc.lb);
+                        const float gap = rc.bias0 + dot(rc.normal, wa - wb);
+                        if (gap < -1e-3f) {
+                            float resolve = 0.6f;
+                            if (A.stackStabilization && lengthSq(a.v - b.v) < 1e-4f)
+                                resolve += 0.2f * (A.stackStiffness / 1000.0f) / (1.0f + A.stackDamping * A.h);
+                            const float push = -resolve * (gap + 1e-3f) / invMassSum;
+                            if (isDynamic(a.m.flags) && !isAsleep(a.m.flags) && la >= 0)
+                                S.p[la] = pack(a.p + rc.normal * (push * ima), 0.0f);
+                            if (isDynamic(b.m.flags) && !isAsleep(b.m.flags) && lb >= 0)
+                                S.p[lb] = pack(b.p - rc.normal * (push * imb), 0.0f);
+                        }
+                    }
+                }
+                __syncwarp();
+            }
+        for (uint32_t t = lane; t < totalBodies; t += 32)
+            if (isDynamic(S.flags[t])) A.B.pos[ids[t]] = S.p[t];
+        return;
+    }
+    for (int s = 0; s < A.substeps; ++s) {
+        for (uint32_t t = lane; t < totalBodies; t += 32) {
+            if (A.integrate && s > 0) sharedIntegrateVelocity(A, S, (int)t, ids[t]);
+            Mass m;
+            const float4 in = S.inertia[t];
+            m.invI = V3{in.x, in.y, in.z};
+            m.invMass = in.w;
+            m.iq = q4(S.iq[t]);
+            m.flags = S.flags[t];
+            S.frame[t] = pack(inertiaFrameAt(m, q4(S.q[t])));
+        }
+        __syncwarp();
+        if (live) {
+            const SolverBody a = la >= 0 ? sharedBody(S, la) : globalBody(A.B, ida);
+            const SolverBody b = lb >= 0 ? sharedBody(S, lb) : globalBody(A.B, idb);
+            prepRow(a, b, rc, A.h, A.coneBlock != 0, P);
+        }
+        __syncwarp();
+        const int units = (A.warmStart && s == 0 ? 1 : 0) + A.sweeps;
+        for (int u = 0; u < units; ++u) {
+            const bool warm = A.warmStart && s == 0 && u == 0;
+            for (uint32_t c = 0; c < maxC; ++c) {
+                if (live && myC == c) {
+                    SolverBody a = la >= 0 ? sharedBody(S, la) : globalBody(A.B, ida);
+                    SolverBody b = lb >= 0 ? sharedBody(S, lb) : globalBody(A.B, idb);
+                    if (warm) warmPrepRow(a, b, rc, P);
+                    else sweepRow(a, b, rc, P, A.coneBlock != 0);
+                    if (la >= 0 && isDynamic(a.m.flags)) { S.v[la] = pack(a.v, 0.0f); S.w[la] = pack(a.w, 0.0f); }
+                    if (lb >= 0 && isDynamic(b.m.flags)) { S.v[lb] = pack(b.v, 0.0f); S.w[lb] = pack(b.w, 0.0f); }
+                }
+                __syncwarp();
+            }
+        }
+        if (A.integrate) {
+            for (uint32_t t = lane; t < totalBodies; t += 32) sharedIntegrateTransform(A, S, (int)t);
+            __syncwarp();
+        }
+    }
+    for (uint32_t t = lane; t < totalBodies; t += 32) {
+        if (!isDynamic(S.flags[t])) continue;
+        const uint32_t id = ids[t];
+        A.B.pos[id] = S.p[t]; A.B.rot[id] = S.q[t]; A.B.vel[id] = S.v[t]; A.B.ang[id] = S.w[t];
+    }
+    if (has) storeRow(*cp, rc);
+}
+
 // ---- giant islands: the whole grid on one island ----------------------------
 //
 // Islands too large for one block's shared memory run on every block of a
@@ -2709,6 +2927,7 @@ static int buildIslands(Context& c, const vx_contact* cs, uint32_t m, IslandPlan
     c.planContacts = m;
     c.giantLinked = false;
     c.clusterBuilt = false;
+    c.tinyPacked = false;
     VXB_TRY(ensure(c, c.parentBuf, (size_t)n * 4));
     VXB_TRY(ensure(c, c.islandOfBodyBuf, (size_t)n * 4));
     VXB_TRY(ensure(c, c.maskBuf, (size_t)n * 8));
@@ -2826,7 +3045,48 @@ static int prepareSegments(Context& c, const IslandPlan& plan) {
 
 static int launchSolve(Context& c, const SolveArgs& A) {
     if (A.islands == 0) return VXB_OK;
-    LAUNCH(c, solveTinyKernel, blocksFor(A.islands, 64), 64, A);
+    // tiny islands: pack them into warps once per island plan
+    const uint32_t islands = A.islands, chunksCap = (islands + kPackChunk - 1) / kPackChunk + 1;
+    VXB_TRY(ensure(c, c.tinyBuf, ((size_t)islands * 4 + (size_t)chunksCap * 2 + 64) * 4));
+    uint32_t* tFlags = P<uint32_t>(c.tinyBuf);
+    uint32_t* tRanks = tFlags + islands + 16;
+    uint32_t* tList = tRanks + islands + 16;
+    uint32_t* tFirst = tList + islands + 16;
+    uint32_t* tChunkCount = tFirst + islands + 16;
+    uint32_t* tChunkBase = tChunkCount + chunksCap;
+    if (!c.tinyPacked) {
+        LAUNCH(c, tinyFlagKernel, blocksFor(islands, 256), 256, A, tFlags);
+        VXB_TRY(exclusiveScan(c, tFlags, tRanks, islands, &c.dCounters->tinyIslands));
+        LAUNCH(c, compactKernel, blocksFor(islands, 256), 256, tFlags, tRanks, islands, tList);
+        VXB_TRY(readCounters(c));
+        c.tinyCount = c.hostCounters.tinyIslands;
+        c.tinyPackCount = 0;
+        if (c.tinyCount) {
+            const uint32_t chunks = (c.tinyCount + kPackChunk - 1) / kPackChunk;
+            LAUNCH(c, tinyPackKernel, blocksFor(chunks, 128), 128, A, (const uint32_t*)tList, c.tinyCount, 0,
+                   tChunkCount, (const uint32_t*)tChunkBase, tFirst);
+            VXB_TRY(exclusiveScan(c, tChunkCount, tChunkBase, chunks, &c.dCounters->tinyPacks));
+            LAUNCH(c, tinyPackKernel, blocksFor(chunks, 128), 128, A, (const uint32_t*)tList, c.tinyCount, 1,
+                   tChunkCount, (const uint32_t*)tChunkBase, tFirst);
+            VXB_TRY(readCounters(c));
+            c.tinyPackCount = c.hostCounters.tinyPacks;
+        }
+        c.tinyPacked = true;
+    }
+    VXB_TRY(ensure(c, c.localIdxBuf, (size_t)c.n * 4 + 16));
+    if (c.tinyPackCount) {
+        static bool packConfigured = false;
+        if (!packConfigured) {
+            cudaFuncSetAttribute(solveTinyPackKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(kPackWarpSmem * kPackWarps));
+            packConfigured = true;
+        }
+        solveTinyPackKernel<<<(c.tinyPackCount + kPackWarps - 1) / kPackWarps, 32 * kPackWarps,
+                              kPackWarpSmem * kPackWarps, c.stream>>>(A, (const uint32_t*)tList,
+                                                                      (const uint32_t*)tFirst, c.tinyPackCount,
+                                                                      c.tinyCount, P<uint32_t>(c.localIdxBuf));
+        ++c.launches;
+    }
     auto* large = solveBlockKernel<kBlockThreads, kBlockBodies, kBlockRows, false>;
     auto* small = solveBlockKernel<kSmallThreads, kSmallBodies, kSmallRows, true>;
     static int smallPerSm = 0;
@@ -2837,7 +3097,6 @@ static int launchSolve(Context& c, const SolveArgs& A) {
             smallPerSm <= 0)
             smallPerSm = 8;
     }
-    VXB_TRY(ensure(c, c.localIdxBuf, (size_t)c.n * 4 + 16));
     small<<<std::min<uint32_t>(A.islands, (uint32_t)(c.smCount * smallPerSm)), kSmallThreads, kSmallSmem, c.stream>>>(
         A, P<uint32_t>(c.localIdxBuf));
     ++c.launches;
