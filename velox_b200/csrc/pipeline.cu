@@ -1075,33 +1075,6 @@ struct SolveArgs {
     const uint2* rowBodies;  // per solve-order row: (a, b) of its contact (giant islands)
 };
 
-VXD void warmRow(const SolveArgs& A, uint32_t ci) {
-    vx_contact& cc = A.contacts[ci];
-    const uint32_t fa = A.B.filt[cc.a].x, fb = A.B.filt[cc.b].x;
-    if (!solvedContact(fa, fb)) return;
-    RowContact r;
-    loadRow(cc, r);
-    SolverBody a = loadSolverBody(A.B, cc.a), b = loadSolverBody(A.B, cc.b);
-    warmStartRow(a, b, r);
-    if (isDynamic(fa)) { A.B.vel[cc.a] = pack(a.v, 0.0f); A.B.ang[cc.a] = pack(a.w, 0.0f); }
-    if (isDynamic(fb)) { A.B.vel[cc.b] = pack(b.v, 0.0f); A.B.ang[cc.b] = pack(b.w, 0.0f); }
-    storeRow(cc, r);
-}
-
-VXD void solveRowAt(const SolveArgs& A, uint32_t ci) {
-    vx_contact& cc = A.contacts[ci];
-    const uint32_t fa = A.B.filt[cc.a].x, fb = A.B.filt[cc.b].x;
-    if (!solvedContact(fa, fb)) return;
-    RowContact r;
-    loadRow(cc, r);
-    SolverBody a = loadSolverBody(A.B, cc.a), b = loadSolverBody(A.B, cc.b);
-    solveRow(a, b, r, A.h, A.coneBlock != 0);
-    if (isDynamic(fa)) { A.B.vel[cc.a] = pack(a.v, 0.0f); A.B.ang[cc.a] = pack(a.w, 0.0f); }
-    if (isDynamic(fb)) { A.B.vel[cc.b] = pack(b.v, 0.0f); A.B.ang[cc.b] = pack(b.w, 0.0f); }
-    storeRow(cc, r);
-}
-
-// Split-impulse position correction row (src/world.cpp:4370-4397).
 VXD void positionRow(const SolveArgs& A, uint32_t ci) {
     const vx_contact& cc = A.contacts[ci];
     const uint32_t fa = A.B.filt[cc.a].x, fb = A.B.filt[cc.b].x;
@@ -1132,141 +1105,7 @@ VXD void positionRow(const SolveArgs& A, uint32_t ci) {
     if (isDynamic(fb) && !isAsleep(fb)) { pb -= n * (push * imb); A.B.pos[cc.b] = pack(pb, 0.0f); }
 }
 
-VXD uint32_t islandSize(const SolveArgs& A, uint32_t isl) { return A.islandStart[isl + 1] - A.islandStart[isl]; }
 
-// Sequential island processing (one thread).
-VXD void solveIslandSerial(const SolveArgs& A, uint32_t isl) {
-    const uint32_t s0 = A.islandStart[isl], s1 = A.islandStart[isl + 1];
-    if (A.positionIterations > 0) {
-        for (int it = 0; it < A.positionIterations; ++it)
-            for (uint32_t k = s0; k < s1; ++k) positionRow(A, A.order[k]);
-        return;
-    }
-    const uint32_t b0 = isl < A.realIslands ? A.bodyStart[isl] : 0u;
-    const uint32_t b1 = isl < A.realIslands ? A.bodyStart[isl + 1] : 0u;
-    for (int s = 0; s < A.substeps; ++s) {
-        if (A.integrate && s > 0)
-            for (uint32_t k = b0; k < b1; ++k) integrateVelocity(A.B, A.bodyOrder[k], A.gravity, A.h);
-        if (A.warmStart && s == 0)
-            for (uint32_t k = s0; k < s1; ++k) warmRow(A, A.order[k]);
-        for (int it = 0; it < A.sweeps; ++it)
-            for (uint32_t k = s0; k < s1; ++k) solveRowAt(A, A.order[k]);
-        if (A.integrate)
-            for (uint32_t k = b0; k < b1; ++k) integrateTransform(A.B, A.bodyOrder[k], A.h);
-    }
-}
-
-// Tiny islands (at most kTinyContacts contacts): one thread gathers the
-// island's bodies and contacts into local arrays once, runs the whole substep
-// loop on them (same row order as the coloured sweeps: colour-major) and
-// writes the results back. Static endpoints are local read-only copies.
-constexpr int kTinyContacts = 16;
-constexpr int kTinyBodies = 2 * kTinyContacts;
-
-struct LocalBody {
-    SolverBody s;
-    float gs, ld, ad;  // gravityScale, linear / angular damping
-    V3 force, torque;
-    uint32_t id;
-};
-
-VXD void localIntegrateVelocity(LocalBody& b, const V3& g, float dt) {
-    const Mass& m = b.s.m;
-    if (!isDynamic(m.flags) || isLocked(m.flags) || isAsleep(m.flags)) return;
-    b.s.v += (g * b.gs + b.force * solverInvMass(m)) * dt;
-    b.s.w += invInertiaMulAt(m, b.torque, b.s.q) * dt;
-    b.s.v *= 1.0f / (1.0f + b.ld * dt);
-    b.s.w *= 1.0f / (1.0f + b.ad * dt);
-}
-
-VXD void localIntegrateTransform(LocalBody& b, float dt) {
-    const Mass& m = b.s.m;
-    if (isStaticBody(m.flags) || isLocked(m.flags) || isAsleep(m.flags)) return;
-    advanceTransform(m, b.s.p, b.s.q, b.s.v, b.s.w, dt);
-}
-
-__global__ void __launch_bounds__(64) solveTinyKernel(SolveArgs A) {
-    for (uint32_t isl = blockIdx.x * blockDim.x + threadIdx.x; isl < A.islands; isl += gridDim.x * blockDim.x) {
-        const uint32_t s0 = A.islandStart[isl], s1 = A.islandStart[isl + 1];
-        const uint32_t count = s1 - s0;
-        if (count > A.tinyLimit) continue;
-        if (count > (uint32_t)kTinyContacts) { solveIslandSerial(A, isl); continue; }
-        LocalBody bodies[kTinyBodies];
-        RowContact rows[kTinyContacts];
-        uint8_t ra[kTinyContacts], rb[kTinyContacts];
-        bool live[kTinyContacts];
-        int nb = 0;
-        auto slot = [&](uint32_t id) -> int {
-            for (int i = 0; i < nb; ++i)
-                if (bodies[i].id == id) return i;
-            LocalBody& b = bodies[nb];
-            b.s = loadSolverBody(A.B, id);
-            const float4 ex = A.B.extra[id];
-            b.gs = ex.y; b.ld = ex.z; b.ad = ex.w;
-            b.force = f3(A.B.force[id]);
-            b.torque = f3(A.B.torque[id]);
-            b.id = id;
-            return nb++;
-        };
-        for (uint32_t k = 0; k < count; ++k) {
-            const vx_contact& cc = A.contacts[A.order[s0 + k]];
-            loadRow(cc, rows[k]);
-            ra[k] = (uint8_t)slot(cc.a);
-            rb[k] = (uint8_t)slot(cc.b);
-            live[k] = solvedContact(bodies[ra[k]].s.m.flags, bodies[rb[k]].s.m.flags);
-        }
-        if (A.positionIterations > 0) {
-            for (int it = 0; it < A.positionIterations; ++it)
-                for (uint32_t k = 0; k < count; ++k) {
-                    if (!live[k]) continue;
-                    SolverBody& a = bodies[ra[k]].s;
-                    SolverBody& b = bodies[rb[k]].s;
-                    const float ima = solverInvMass(a.m), imb = solverInvMass(b.m);
-                    const float invMassSum = ima + imb;
-                    if (invMassSum <= 0.0f) continue;
-                    const RowContact& r = rows[k];
-                    const V3 wa = anchorWorld(a.sphere, a.p, a.q, r.la);
-                    const V3 wb = anchorWorld(b.sphere, b.p, b.q, r.lb);
-                    const float gap = r.bias0 + dot(r.normal, wa - wb);
-                    if (gap >= -1e-3f) continue;
-                    float resolve = 0.6f;
-                    if (A.stackStabilization && lengthSq(a.v - b.v) < 1e-4f)
-                        resolve += 0.2f * (A.stackStiffness / 1000.0f) / (1.0f + A.stackDamping * A.h);
-                    const float push = -resolve * (gap + 1e-3f) / invMassSum;
-                    if (isDynamic(a.m.flags) && !isAsleep(a.m.flags)) a.p += r.normal * (push * ima);
-                    if (isDynamic(b.m.flags) && !isAsleep(b.m.flags)) b.p -= r.normal * (push * imb);
-                }
-            for (int i = 0; i < nb; ++i)
-                if (isDynamic(bodies[i].s.m.flags)) A.B.pos[bodies[i].id] = pack(bodies[i].s.p, 0.0f);
-            continue;
-        }
-        RowPrep prep[kTinyContacts];
-        for (int s = 0; s < A.substeps; ++s) {
-            if (A.integrate && s > 0)
-                for (int i = 0; i < nb; ++i) localIntegrateVelocity(bodies[i], A.gravity, A.h);
-            for (int i = 0; i < nb; ++i) cacheFrame(bodies[i].s);
-            for (uint32_t k = 0; k < count; ++k)
-                if (live[k]) prepRow(bodies[ra[k]].s, bodies[rb[k]].s, rows[k], A.h, A.coneBlock != 0, prep[k]);
-            if (A.warmStart && s == 0)
-                for (uint32_t k = 0; k < count; ++k)
-                    if (live[k]) warmPrepRow(bodies[ra[k]].s, bodies[rb[k]].s, rows[k], prep[k]);
-            for (int it = 0; it < A.sweeps; ++it)
-                for (uint32_t k = 0; k < count; ++k)
-                    if (live[k]) sweepRow(bodies[ra[k]].s, bodies[rb[k]].s, rows[k], prep[k], A.coneBlock != 0);
-            if (A.integrate)
-                for (int i = 0; i < nb; ++i) localIntegrateTransform(bodies[i], A.h);
-        }
-        for (int i = 0; i < nb; ++i) {
-            const LocalBody& b = bodies[i];
-            if (!isDynamic(b.s.m.flags)) continue;
-            A.B.pos[b.id] = pack(b.s.p, 0.0f);
-            A.B.rot[b.id] = pack(b.s.q);
-            A.B.vel[b.id] = pack(b.s.v, 0.0f);
-            A.B.ang[b.id] = pack(b.s.w, 0.0f);
-        }
-        for (uint32_t k = 0; k < count; ++k) storeRow(A.contacts[A.order[s0 + k]], rows[k]);
-    }
-}
 
 // Block-cooperative island processing: contacts of one colour in parallel,
 // a block barrier between colours. The island's dynamic bodies live in shared
