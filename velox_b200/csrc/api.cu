@@ -105,7 +105,7 @@ void vxb_context_destroy(vxb_context* ctx) {
                            &c.bodyValBuf, &c.islandBodyStartBuf, &c.caFlagBuf, &c.caBodyMarkBuf, &c.caCandBuf,
                            &c.localIdxBuf, &c.prepBuf, &c.frameBuf, &c.fpKeyBuf, &c.fpValBuf,
                            &c.fpSlotBuf, &c.fpColorBuf, &c.fpRunStartBuf, &c.fpIslandBuf, &c.coopBuf,
-                           &c.giantBuf, &c.classKeyBuf, &c.classValBuf, &c.rowBodyBuf, &c.tinyBuf, &c.clusterInfoBuf, &c.clusterKeyBuf,
+                           &c.giantBuf, &c.classKeyBuf, &c.classValBuf, &c.rowBodyBuf, &c.tinyBuf, &c.tinyKeyBuf, &c.clusterInfoBuf, &c.clusterKeyBuf,
                            &c.clusterValBuf, &c.clusterOfBuf, &c.clusterCountBuf, &c.clusterStartBuf,
                            &c.clusterRowsBuf,
                            &c.countersBuf};

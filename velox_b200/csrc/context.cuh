@@ -165,6 +165,7 @@ struct Context {
     DevBuf classKeyBuf, classValBuf;    // convex pairs grouped by shape combination (narrow phase)
     DevBuf rowBodyBuf;                  // (a, b) per solve-order row (giant islands)
     DevBuf tinyBuf;                     // tiny-island flags, ranks, list, pack counts/bases/firsts
+    DevBuf tinyKeyBuf;                  // tiny islands' colour counts (pack order sort)
     DevBuf clusterInfoBuf, clusterKeyBuf, clusterValBuf, clusterOfBuf, clusterCountBuf, clusterStartBuf,
         clusterRowsBuf;                 // spatial clusters of a giant island
 

@@ -1397,6 +1397,16 @@ constexpr int kPackBodies = 64;
 constexpr int kPackChunk = 512;     // tiny islands per packing thread
 constexpr int kPackWarps = 4;       // warps (packs) per block
 
+// Sort key of a tiny island: its colour count (a pack runs as many colour
+// slots per sweep as its most coloured island, so similar islands share packs).
+__global__ void tinyKeyKernel(SolveArgs A, const uint32_t* list, uint32_t count, uint64_t* keys, uint32_t* vals) {
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < count; t += gridDim.x * blockDim.x) {
+        const uint32_t isl = list[t];
+        keys[t] = A.islandSeg[isl + 1] - A.islandSeg[isl];
+        vals[t] = isl;
+    }
+}
+
 __global__ void tinyFlagKernel(SolveArgs A, uint32_t* flags) {
     for (uint32_t isl = blockIdx.x * blockDim.x + threadIdx.x; isl < A.islands; isl += gridDim.x * blockDim.x) {
         const uint32_t rows = A.islandStart[isl + 1] - A.islandStart[isl];
@@ -2900,6 +2910,12 @@ static int launchSolve(Context& c, const SolveArgs& A) {
         VXB_TRY(readCounters(c));
         c.tinyCount = c.hostCounters.tinyIslands;
         c.tinyPackCount = 0;
+        if (c.tinyCount > 1) {
+            VXB_TRY(ensure(c, c.tinyKeyBuf, (size_t)c.tinyCount * 8 + 64));
+            LAUNCH(c, tinyKeyKernel, blocksFor(c.tinyCount, 256), 256, A, (const uint32_t*)tList, c.tinyCount,
+                   P<uint64_t>(c.tinyKeyBuf), tList);
+            VXB_TRY(sortPairs(c, P<uint64_t>(c.tinyKeyBuf), tList, c.tinyCount, 8));
+        }
         if (c.tinyCount) {
             const uint32_t chunks = (c.tinyCount + kPackChunk - 1) / kPackChunk;
             LAUNCH(c, tinyPackKernel, blocksFor(chunks, 128), 128, A, (const uint32_t*)tList, c.tinyCount, 0,
