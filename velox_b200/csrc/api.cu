@@ -102,7 +102,7 @@ void vxb_context_destroy(vxb_context* ctx) {
                            &c.parentBuf, &c.islandOfBodyBuf, &c.islandKeyBuf, &c.islandValBuf, &c.colorBuf,
                            &c.colorKeyBuf, &c.maskBuf, &c.nextColorBuf, &c.islandStartBuf, &c.islandInfoBuf,
                            &c.flagBuf, &c.scanBuf, &c.scanTmp, &c.segStartBuf, &c.islandSegBuf, &c.bodyKeyBuf,
-                           &c.bodyValBuf, &c.islandBodyStartBuf, &c.caFlagBuf, &c.caBodyMarkBuf, &c.caCandBuf,
+                           &c.bodyValBuf, &c.islandBodyStartBuf, &c.caFlagBuf, &c.caBodyMarkBuf, &c.caCandBuf, &c.caSpecBuf,
                            &c.localIdxBuf, &c.prepBuf, &c.frameBuf, &c.fpKeyBuf, &c.fpValBuf,
                            &c.fpSlotBuf, &c.fpColorBuf, &c.fpRunStartBuf, &c.fpIslandBuf, &c.coopBuf,
                            &c.giantBuf, &c.classKeyBuf, &c.classValBuf, &c.rowBodyBuf, &c.tinyBuf, &c.tinyKeyBuf, &c.clusterInfoBuf, &c.clusterKeyBuf,

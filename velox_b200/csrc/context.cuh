@@ -70,7 +70,8 @@ struct Counters {
     uint32_t caCritMicros;   // rewind: evaluation time along the longest dependency chain
     uint32_t tinyIslands;    // islands of at most tinyLimit contacts (packed solve)
     uint32_t tinyPacks;      // warps they were packed into
-    uint32_t pad[2];
+    uint32_t caFlagged;      // pairs the rewind probe flagged
+    uint32_t pad[1];
 };
 
 // Pipeline stages timed with CUDA events when timing is enabled.
@@ -156,7 +157,7 @@ struct Context {
     DevBuf flagBuf, scanBuf, scanTmp;
     DevBuf segStartBuf, islandSegBuf;
     DevBuf bodyKeyBuf, bodyValBuf, islandBodyStartBuf;
-    DevBuf caFlagBuf, caBodyMarkBuf, caCandBuf;
+    DevBuf caFlagBuf, caBodyMarkBuf, caCandBuf, caSpecBuf;
     DevBuf localIdxBuf;                 // island-local body index (block solve)
     DevBuf prepBuf, frameBuf;           // per-row pose terms / per-body inertia frames (solve)
     DevBuf fpKeyBuf, fpValBuf, fpSlotBuf, fpColorBuf, fpRunStartBuf, fpIslandBuf;  // parallel colouring

@@ -2158,10 +2158,11 @@ VXD Q4 orientationAt(const Mass& m, const Q4& start, const V3& L, float elapsed)
 // Full rewind logic for one oriented pair on the current state. Returns true
 // when the pair was rewound.
 // `cached`: the probe's end-state gap for this pair when neither body has
-// moved since the probe (else null: computed here).
+// moved since the probe (else null: computed here). `spec` (optional): write
+// the rewound states there (a: pos, rot, vel, ang; then b) instead of into B.
 __device__ __noinline__ bool caRewind(BodyArrays& B, const Soup& soup, uint32_t i, uint32_t j, float dt,
                                       const float4* prevPos, const float4* prevRot, uint32_t* gapQueries,
-                                      const float4* cached) {
+                                      const float4* cached, float4* spec = nullptr) {
     BodyView a = loadViewCoherent(B, i), b = loadViewCoherent(B, j);
     if (!caEligible(a, b, B, i)) return false;
     if (shapeOf(b.flags) != kPlane) {
@@ -2228,11 +2229,33 @@ __device__ __noinline__ bool caRewind(BodyArrays& B, const Soup& soup, uint32_t 
     const float remaining = dt * (1.0f - t);
     advanceTransform(ma, a.p, a.q, a.v, a.w, remaining);
     if (bDyn) advanceTransform(mb, b.p, b.q, b.v, b.w, remaining);
+    if (spec) {
+        spec[0] = pack(a.p, 0.0f); spec[1] = pack(a.q); spec[2] = pack(a.v, 0.0f); spec[3] = pack(a.w, 0.0f);
+        spec[4] = pack(b.p, 0.0f); spec[5] = pack(b.q); spec[6] = pack(b.v, 0.0f); spec[7] = pack(b.w, 0.0f);
+        return true;
+    }
     B.pos[i] = pack(a.p, 0.0f); B.rot[i] = pack(a.q); B.vel[i] = pack(a.v, 0.0f); B.ang[i] = pack(a.w, 0.0f);
     if (bDyn) {
         B.pos[j] = pack(b.p, 0.0f); B.rot[j] = pack(b.q); B.vel[j] = pack(b.v, 0.0f); B.ang[j] = pack(b.w, 0.0f);
     }
     return true;
+}
+
+// Every flagged pair evaluated in parallel on the probe's state (read-only):
+// in the ordered pass, a flagged pair whose bodies no earlier rewind has moved
+// sees exactly this state, so its outcome can be taken from here.
+__global__ void caSpeculateKernel(BodyArrays B, Soup soup, const uint64_t* pairKeys, uint32_t npairs,
+                                  const uint32_t* flags, const uint32_t* flagRank, const float4* endGap, float dt,
+                                  const float4* prevPos, const float4* prevRot, float4* specState,
+                                  uint32_t* specResult, Counters* C) {
+    for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < npairs; r += gridDim.x * blockDim.x) {
+        if (!flags[r]) continue;
+        const uint32_t k = flagRank[r];
+        uint32_t i, j;
+        orientPair(B, pairKeys[r], i, j);
+        specResult[k] = caRewind(B, soup, i, j, dt, prevPos, prevRot, &C->caGapQueries, endGap + r,
+                                 specState + 8 * (size_t)k) ? 1u : 0u;
+    }
 }
 
 VXD uint64_t globalTimerNs() {
@@ -2255,7 +2278,8 @@ constexpr int kCaWidenHops = 8;   // hops of widening per replay
 constexpr int kCaInitialHops = 8; // hops of widening before the first pass
 
 __global__ void __launch_bounds__(256) caFlowKernel(BodyArrays B, Soup soup, const uint64_t* pairKeys,
-                                                    const uint32_t* flags, const float4* endGap,
+                                                    const uint32_t* flags, const uint32_t* flagRank,
+                                                    const float4* specState, const uint32_t* specResult,
                                                     const uint32_t* cand, uint32_t ncand, const uint32_t* succ,
                                                     uint32_t* pending, uint32_t* queue, uint32_t* depth,
                                                     uint32_t* crit, const uint32_t* bodyMark, uint32_t* rewound,
@@ -2292,8 +2316,22 @@ __global__ void __launch_bounds__(256) caFlowKernel(BodyArrays B, Soup soup, con
         if (flags[r] || touched) {
             uint32_t i, j;
             orientPair(B, key, i, j);
-            if (caRewind(B, soup, i, j, dt, prevPos, prevRot, &C->caGapQueries,
-                         flags[r] && !touched ? endGap + r : nullptr)) {
+            bool rewoundPair;
+            if (!touched) {  // flagged, bodies as the probe saw them: the speculative outcome holds
+                const uint32_t sk = flagRank[r];
+                rewoundPair = specResult[sk] != 0u;
+                if (rewoundPair) {
+                    const float4* st4 = specState + 8 * (size_t)sk;
+                    __stcg(B.pos + i, st4[0]); __stcg(B.rot + i, st4[1]); __stcg(B.vel + i, st4[2]); __stcg(B.ang + i, st4[3]);
+                    if (isDynamic(B.filt[j].x)) {
+                        __stcg(B.pos + j, st4[4]); __stcg(B.rot + j, st4[5]); __stcg(B.vel + j, st4[6]);
+                        __stcg(B.ang + j, st4[7]);
+                    }
+                }
+            } else {
+                rewoundPair = caRewind(B, soup, i, j, dt, prevPos, prevRot, &C->caGapQueries, nullptr);
+            }
+            if (rewoundPair) {
                 ++rewinds;
                 const bool jDyn = isDynamic(B.filt[j].x);
                 __stcg(rewound + i, 1u);
@@ -3106,12 +3144,13 @@ static int positionCorrection(Context& c, vx_contact* cs, const IslandPlan& plan
 static int conservativeAdvancement(Context& c, uint32_t npairs, float dt) {
     if (npairs == 0) return VXB_OK;
     const uint32_t n = c.n;
-    VXB_TRY(ensure(c, c.caFlagBuf, (size_t)npairs * 24 + 64));
+    VXB_TRY(ensure(c, c.caFlagBuf, (size_t)npairs * 28 + 64));
     VXB_TRY(ensure(c, c.caBodyMarkBuf, (size_t)n * 16 + 16));
     VXB_TRY(ensure(c, c.caCandBuf, (size_t)npairs * 28 + 64));
     float4* endGap = P<float4>(c.caFlagBuf);
     uint32_t* flags = reinterpret_cast<uint32_t*>(endGap + npairs);
     uint32_t* candFlags = flags + npairs;
+    uint32_t* flagRank = candFlags + npairs;
     uint32_t* bodyMark = P<uint32_t>(c.caBodyMarkBuf);
     uint32_t* rewound = bodyMark + n;
     uint32_t* front[2] = {rewound + n, rewound + 2 * (size_t)n};  // widening frontiers
@@ -3127,6 +3166,17 @@ static int conservativeAdvancement(Context& c, uint32_t npairs, float dt) {
     const float4* prevRot = prevPos + n;
     LAUNCH(c, caProbeKernel, std::min<uint32_t>(blocksFor(npairs, 128), (uint32_t)c.smCount * 16), 128, c.B, soupOf(c),
            pk, npairs, flags, bodyMark, endGap);
+    // speculative outcomes of the flagged pairs on the probe's state
+    VXB_TRY(exclusiveScan(c, flags, flagRank, npairs, &c.dCounters->caFlagged));
+    VXB_TRY(readCounters(c));
+    const uint32_t flagged = c.hostCounters.caFlagged;
+    if (flagged == 0) return VXB_OK;  // nothing flagged: no pair is examined, nothing moves
+    VXB_TRY(ensure(c, c.caSpecBuf, (size_t)flagged * (8 * sizeof(float4) + 4) + 64));
+    float4* specState = P<float4>(c.caSpecBuf);
+    uint32_t* specResult = reinterpret_cast<uint32_t*>(specState + 8 * (size_t)flagged);
+    LAUNCH(c, caSpeculateKernel, std::min<uint32_t>(blocksFor(npairs, 128), (uint32_t)c.smCount * 16), 128, c.B,
+           soupOf(c), pk, npairs, (const uint32_t*)flags, (const uint32_t*)flagRank, (const float4*)endGap, dt, prevPos,
+           prevRot, specState, specResult, c.dCounters);
     // mark ahead of the cascade before the first pass too (fewer replays)
     {
         const uint32_t* frontier = bodyMark;
@@ -3168,7 +3218,8 @@ static int conservativeAdvancement(Context& c, uint32_t npairs, float dt) {
         VXB_CUDA(c, cudaMemsetAsync(queue, 0xff, (size_t)ncand * 4, c.stream));
         VXB_CUDA(c, cudaMemsetAsync(st, 0, sizeof(CoopState), c.stream));
         const int rc = launchCooperative(c, caFlowKernel, 256, c.B, soupOf(c), pk, (const uint32_t*)flags,
-                                         (const float4*)endGap, (const uint32_t*)candIndex, ncand,
+                                         (const uint32_t*)flagRank, (const float4*)specState,
+                                         (const uint32_t*)specResult, (const uint32_t*)candIndex, ncand,
                                          (const uint32_t*)succ, pending, queue, depth, crit,
                                          (const uint32_t*)bodyMark, rewound, dt, prevPos, prevRot, c.dCounters, st);
         if (rc == VXB_ERR_UNSUPPORTED) { serial = true; break; }
