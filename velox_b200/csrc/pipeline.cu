@@ -2244,13 +2244,11 @@ __device__ __noinline__ bool caRewind(BodyArrays& B, const Soup& soup, uint32_t 
 // Every flagged pair evaluated in parallel on the probe's state (read-only):
 // in the ordered pass, a flagged pair whose bodies no earlier rewind has moved
 // sees exactly this state, so its outcome can be taken from here.
-__global__ void caSpeculateKernel(BodyArrays B, Soup soup, const uint64_t* pairKeys, uint32_t npairs,
-                                  const uint32_t* flags, const uint32_t* flagRank, const float4* endGap, float dt,
-                                  const float4* prevPos, const float4* prevRot, float4* specState,
-                                  uint32_t* specResult, Counters* C) {
-    for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < npairs; r += gridDim.x * blockDim.x) {
-        if (!flags[r]) continue;
-        const uint32_t k = flagRank[r];
+__global__ void caSpeculateKernel(BodyArrays B, Soup soup, const uint64_t* pairKeys, const uint32_t* flaggedList,
+                                  uint32_t flagged, const float4* endGap, float dt, const float4* prevPos,
+                                  const float4* prevRot, float4* specState, uint32_t* specResult, Counters* C) {
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < flagged; k += gridDim.x * blockDim.x) {
+        const uint32_t r = flaggedList[k];
         uint32_t i, j;
         orientPair(B, pairKeys[r], i, j);
         specResult[k] = caRewind(B, soup, i, j, dt, prevPos, prevRot, &C->caGapQueries, endGap + r,
@@ -3171,12 +3169,13 @@ static int conservativeAdvancement(Context& c, uint32_t npairs, float dt) {
     VXB_TRY(readCounters(c));
     const uint32_t flagged = c.hostCounters.caFlagged;
     if (flagged == 0) return VXB_OK;  // nothing flagged: no pair is examined, nothing moves
-    VXB_TRY(ensure(c, c.caSpecBuf, (size_t)flagged * (8 * sizeof(float4) + 4) + 64));
+    VXB_TRY(ensure(c, c.caSpecBuf, (size_t)flagged * (8 * sizeof(float4) + 8) + 64));
     float4* specState = P<float4>(c.caSpecBuf);
     uint32_t* specResult = reinterpret_cast<uint32_t*>(specState + 8 * (size_t)flagged);
-    LAUNCH(c, caSpeculateKernel, std::min<uint32_t>(blocksFor(npairs, 128), (uint32_t)c.smCount * 16), 128, c.B,
-           soupOf(c), pk, npairs, (const uint32_t*)flags, (const uint32_t*)flagRank, (const float4*)endGap, dt, prevPos,
-           prevRot, specState, specResult, c.dCounters);
+    uint32_t* flaggedList = specResult + flagged;
+    LAUNCH(c, compactKernel, blocksFor(npairs, 256), 256, flags, flagRank, npairs, flaggedList);
+    LAUNCH(c, caSpeculateKernel, blocksFor(flagged, 64), 64, c.B, soupOf(c), pk, (const uint32_t*)flaggedList, flagged,
+           (const float4*)endGap, dt, prevPos, prevRot, specState, specResult, c.dCounters);
     // mark ahead of the cascade before the first pass too (fewer replays)
     {
         const uint32_t* frontier = bodyMark;
