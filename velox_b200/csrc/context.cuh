@@ -71,7 +71,10 @@ struct Counters {
     uint32_t tinyIslands;    // islands of at most tinyLimit contacts (packed solve)
     uint32_t tinyPacks;      // warps they were packed into
     uint32_t caFlagged;      // pairs the rewind probe flagged
-    uint32_t pad[1];
+    uint32_t clusterBodies;  // bodies of the giant islands (clustered solve)
+    uint32_t clusterRows;    // their rows
+    uint32_t clusterColours; // most colours of a giant island
+    uint32_t pad[2];
 };
 
 // Pipeline stages timed with CUDA events when timing is enabled.
@@ -99,7 +102,7 @@ struct Context {
     bool clusterBuilt = false; // spatial clusters of the plan's (single) giant island are built
     bool tinyPacked = false;   // the plan's tiny islands are packed into warps
     uint32_t tinyCount = 0, tinyPackCount = 0;
-    uint32_t clusterInfo[8] = {};  // island, rows [s0, s1), segments [g0, g1), bodies [b0, b1)
+    uint32_t clusterNB = 0, clusterR = 0, clusterG = 0;  // giant bodies, rows, most colours (clustered solve)
     cudaStream_t ownStream = nullptr;
     cudaStream_t stream = nullptr;
     std::string lastError;

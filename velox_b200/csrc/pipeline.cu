@@ -1879,12 +1879,12 @@ VXD uint32_t spreadBits10(uint32_t v) {  // 10 bits -> every third bit
     return v;
 }
 
-__global__ void clusterBodyKeyKernel(SolveArgs A, uint32_t b0, uint32_t b1, const Counters* C, uint64_t* keys,
-                                     uint32_t* vals) {
+__global__ void clusterBodyKeyKernel(SolveArgs A, const uint32_t* bodyPos, uint32_t nb, const Counters* C,
+                                     uint64_t* keys, uint32_t* vals) {
     const float lo[3] = {fromOrdered(C->cellMinBits[0]), fromOrdered(C->cellMinBits[1]), fromOrdered(C->cellMinBits[2])};
     const float hi[3] = {fromOrdered(C->cellMaxBits[0]), fromOrdered(C->cellMaxBits[1]), fromOrdered(C->cellMaxBits[2])};
-    for (uint32_t k = b0 + blockIdx.x * blockDim.x + threadIdx.x; k < b1; k += gridDim.x * blockDim.x) {
-        const uint32_t id = A.bodyOrder[k];
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < nb; k += gridDim.x * blockDim.x) {
+        const uint32_t id = A.bodyOrder[bodyPos[k]];
         const float4 p = A.B.pos[id];
         const float x[3] = {p.x, p.y, p.z};
         uint32_t code = 0;
@@ -1894,13 +1894,12 @@ __global__ void clusterBodyKeyKernel(SolveArgs A, uint32_t b0, uint32_t b1, cons
             t = t >= 0.0f ? fminf(t, 1.0f) : 0.0f;  // NaN (no bounds) -> 0
             code |= spreadBits10((uint32_t)(t * 1023.0f)) << a;
         }
-        keys[k - b0] = code;
-        vals[k - b0] = id;
+        keys[k] = code;
+        vals[k] = id;
     }
 }
 
-// Cluster of each island body (Morton rank chunked into `clusters`), per row
-// the owner cluster and its colour: counts per (cluster, colour).
+// Cluster of each giant-island body: its Morton rank chunked into `clusters`.
 __global__ void clusterOfBodyKernel(const uint32_t* sortedIds, uint32_t nb, uint32_t clusters, uint32_t* clusterOf) {
     for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < nb; r += gridDim.x * blockDim.x)
         clusterOf[sortedIds[r]] = (uint32_t)(((uint64_t)r * clusters) / nb);
@@ -1920,19 +1919,29 @@ VXD uint32_t rowCluster(const SolveArgs& A, uint32_t k, const uint32_t* clusterO
     return clusterOf[isDynamic(A.B.filt[ab.x].x) ? ab.x : ab.y];
 }
 
-__global__ void clusterCountKernel(SolveArgs A, uint32_t s0, uint32_t s1, uint32_t g0, uint32_t g1,
-                                   const uint32_t* clusterOf, uint32_t* counts) {
-    const uint32_t G = g1 - g0;
-    for (uint32_t k = s0 + blockIdx.x * blockDim.x + threadIdx.x; k < s1; k += gridDim.x * blockDim.x)
-        atomicAdd(counts + rowCluster(A, k, clusterOf) * G + (segmentOf(A.segStart, g0, g1, k) - g0), 1u);
+// (cluster, colour slot) cell of a giant row: colour slot = colour within its
+// island. Rows of the null island (no dynamic body of their own island) go to
+// cluster 0: they are never solved and link to nothing.
+VXD uint32_t rowCell(const SolveArgs& A, uint32_t k, const uint32_t* islandOf, const uint32_t* clusterOf,
+                     uint32_t G) {
+    const uint32_t isl = islandOf[k];
+    const uint32_t g0 = A.islandSeg[isl], g1 = A.islandSeg[isl + 1];
+    const uint32_t cluster = isl < A.realIslands ? rowCluster(A, k, clusterOf) : 0u;
+    return cluster * G + (segmentOf(A.segStart, g0, g1, k) - g0);
 }
 
-__global__ void clusterScatterKernel(SolveArgs A, uint32_t s0, uint32_t s1, uint32_t g0, uint32_t g1,
-                                     const uint32_t* clusterOf, const uint32_t* start, uint32_t* fill,
+__global__ void clusterCountKernel(SolveArgs A, const uint32_t* rowList, uint32_t R, const uint32_t* islandOf,
+                                   const uint32_t* clusterOf, uint32_t G, uint32_t* counts) {
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < R; t += gridDim.x * blockDim.x)
+        atomicAdd(counts + rowCell(A, rowList[t], islandOf, clusterOf, G), 1u);
+}
+
+__global__ void clusterScatterKernel(SolveArgs A, const uint32_t* rowList, uint32_t R, const uint32_t* islandOf,
+                                     const uint32_t* clusterOf, uint32_t G, const uint32_t* start, uint32_t* fill,
                                      uint32_t* rows) {
-    const uint32_t G = g1 - g0;
-    for (uint32_t k = s0 + blockIdx.x * blockDim.x + threadIdx.x; k < s1; k += gridDim.x * blockDim.x) {
-        const uint32_t cell = rowCluster(A, k, clusterOf) * G + (segmentOf(A.segStart, g0, g1, k) - g0);
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < R; t += gridDim.x * blockDim.x) {
+        const uint32_t k = rowList[t];
+        const uint32_t cell = rowCell(A, k, islandOf, clusterOf, G);
         rows[start[cell] + atomicAdd(fill + cell, 1u)] = k;
     }
 }
@@ -1965,32 +1974,17 @@ VXD bool clusterStep(const SolveArgs& A, const uint32_t* start, const uint32_t* 
     return *abortFlag == 0;
 }
 
-__global__ void giantInfoKernel(SolveArgs A, const uint32_t* giants, uint32_t* info) {
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        const uint32_t isl = giants[0];
-        info[0] = isl;
-        info[1] = A.islandStart[isl];
-        info[2] = A.islandStart[isl + 1];
-        info[3] = A.islandSeg[isl];
-        info[4] = A.islandSeg[isl + 1];
-        info[5] = isl < A.realIslands ? A.bodyStart[isl] : 0u;
-        info[6] = isl < A.realIslands ? A.bodyStart[isl + 1] : 0u;
-    }
-}
-
-__global__ void __launch_bounds__(256) solveClusterKernel(SolveArgs A, uint32_t isl, uint32_t G,
-                                                          const uint32_t* start, const uint32_t* rows,
-                                                          const uint32_t* pred, uint32_t* done, CoopState* st) {
+__global__ void __launch_bounds__(256) solveClusterKernel(SolveArgs A, uint32_t G, const uint32_t* start,
+                                                          const uint32_t* rows, const uint32_t* rowList, uint32_t R,
+                                                          const uint32_t* bodyIds, uint32_t NB, const uint32_t* pred,
+                                                          uint32_t* done, CoopState* st) {
     __shared__ int abortFlag;
     if (threadIdx.x == 0) abortFlag = 0;
     __syncthreads();
     const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
-    const uint32_t s0 = A.islandStart[isl], s1 = A.islandStart[isl + 1];
-    const uint32_t b0 = isl < A.realIslands ? A.bodyStart[isl] : 0u;
-    const uint32_t b1 = isl < A.realIslands ? A.bodyStart[isl + 1] : 0u;
     const uint32_t base = blockIdx.x * G;
     if (A.positionIterations > 0) {
-        for (uint32_t k = s0 + tid; k < s1; k += stride) __stcg(done + k, 0u);
+        for (uint32_t t = tid; t < R; t += stride) __stcg(done + rowList[t], 0u);
         if (!gridSync(&st->bar, &st->timeout)) return;
         for (int u = 0; u < A.positionIterations; ++u)
             for (uint32_t gl = 0; gl < G; ++gl)
@@ -1999,13 +1993,14 @@ __global__ void __launch_bounds__(256) solveClusterKernel(SolveArgs A, uint32_t 
         return;
     }
     for (int s = 0; s < A.substeps; ++s) {
-        for (uint32_t k = b0 + tid; k < b1; k += stride) {
-            const uint32_t id = A.bodyOrder[k];
+        for (uint32_t t = tid; t < NB; t += stride) {
+            const uint32_t id = bodyIds[t];
             if (A.integrate && s > 0) giantIntegrateVelocity(A, id);
             __stcg(A.frames + id, pack(inertiaFrameAt(loadMass(A.B, id), q4(ldcg4(A.B.rot + id)))));
         }
         if (!gridSync(&st->bar, &st->timeout)) return;
-        for (uint32_t k = s0 + tid; k < s1; k += stride) {
+        for (uint32_t t = tid; t < R; t += stride) {
+            const uint32_t k = rowList[t];
             giantRow(A, k, 3);
             __stcg(done + k, 0u);
         }
@@ -2017,7 +2012,7 @@ __global__ void __launch_bounds__(256) solveClusterKernel(SolveArgs A, uint32_t 
                     return;
         if (!gridSync(&st->bar, &st->timeout)) return;
         if (A.integrate) {
-            for (uint32_t k = b0 + tid; k < b1; k += stride) giantIntegrateTransform(A, A.bodyOrder[k]);
+            for (uint32_t t = tid; t < NB; t += stride) giantIntegrateTransform(A, bodyIds[t]);
             if (!gridSync(&st->bar, &st->timeout)) return;
         }
     }
@@ -2048,6 +2043,23 @@ __global__ void giantEntryKernel(SolveArgs A, const uint32_t* islandOf, uint32_t
 __global__ void giantListKernel(SolveArgs A, uint32_t* list, uint32_t* count) {
     for (uint32_t isl = blockIdx.x * blockDim.x + threadIdx.x; isl < A.islands; isl += gridDim.x * blockDim.x)
         if (isGiant(A, isl)) list[atomicAdd(count, 1u)] = isl;
+}
+
+// Giant-island membership of the sorted body positions and of the solve
+// positions (flags for compaction), and the largest colour count of a giant.
+__global__ void giantMemberKernel(SolveArgs A, const uint64_t* bodyKeys, uint32_t n, const uint32_t* islandOf,
+                                  uint32_t m, uint32_t* bodyFlags, uint32_t* rowFlags, Counters* C) {
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) {
+        const uint64_t isl = bodyKeys[k];
+        bodyFlags[k] = isl < A.realIslands && isGiant(A, (uint32_t)isl) ? 1u : 0u;
+    }
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < m; k += stride) {
+        const uint32_t isl = islandOf[k];
+        const bool g = isGiant(A, isl);
+        rowFlags[k] = g ? 1u : 0u;
+        if (g && k == A.islandStart[isl]) atomicMax(&C->clusterColours, A.islandSeg[isl + 1] - A.islandSeg[isl]);
+    }
 }
 
 // Fallback when the device cannot run a cooperative grid: one block per giant island.
@@ -3030,60 +3042,72 @@ static int launchSolve(Context& c, const SolveArgs& A) {
     }
     SolveArgs G = A;
     G.rowBodies = P<uint2>(c.rowBodyBuf);
-    if (giants == 1 && c.cooperative) {
-        // one giant island: spatial clusters, one per block of the cooperative grid
+    if (c.cooperative) {
+        // the giant islands in spatial clusters, one per block of the cooperative grid
         int perSm = 0;
         VXB_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, solveClusterKernel, 256, 0));
         const uint32_t clusters = (uint32_t)(perSm * c.smCount);
-        if (clusters > 0) {
-            VXB_TRY(ensure(c, c.clusterInfoBuf, 64));
-            uint32_t* info = P<uint32_t>(c.clusterInfoBuf);
-            if (!c.clusterBuilt) {
-                LAUNCH(c, giantInfoKernel, 1, 32, G, (const uint32_t*)list, info);
-                VXB_CUDA(c, cudaMemcpyAsync(c.clusterInfo, info, sizeof(c.clusterInfo), cudaMemcpyDeviceToHost,
-                                            c.stream));
-                VXB_CUDA(c, cudaStreamSynchronize(c.stream));
-            }
-            const uint32_t isl = c.clusterInfo[0], s0 = c.clusterInfo[1], s1 = c.clusterInfo[2];
-            const uint32_t g0 = c.clusterInfo[3], g1 = c.clusterInfo[4], b0 = c.clusterInfo[5], b1 = c.clusterInfo[6];
-            const uint32_t nb = b1 - b0, cells = clusters * (g1 - g0);
-            VXB_TRY(ensure(c, c.clusterStartBuf, ((size_t)cells + 1) * 4 + 64));
-            VXB_TRY(ensure(c, c.clusterRowsBuf, (size_t)(s1 - s0) * 4 + 64));
-            uint32_t* start = P<uint32_t>(c.clusterStartBuf);
-            uint32_t* rows = P<uint32_t>(c.clusterRowsBuf);
-            if (!c.clusterBuilt && nb > 0 && s1 > s0) {
+        const uint32_t n = c.n;
+        VXB_TRY(ensure(c, c.clusterInfoBuf, ((size_t)n * 3 + (size_t)m * 3 + 64) * 4));
+        uint32_t* bodyFlags = P<uint32_t>(c.clusterInfoBuf);
+        uint32_t* bodyRank = bodyFlags + n + 16;
+        uint32_t* bodyPos = bodyRank + n + 16;
+        uint32_t* rowFlags = bodyPos + n + 16;
+        uint32_t* rowRank = rowFlags + m + 16;
+        uint32_t* rowList = rowRank + m + 16;
+        if (clusters > 0 && !c.clusterBuilt) {
+            VXB_CUDA(c, cudaMemsetAsync(&c.dCounters->clusterColours, 0, 4, c.stream));
+            LAUNCH(c, giantMemberKernel, blocksFor(std::max(n, m), 256), 256, G, P<uint64_t>(c.bodyKeyBuf), n,
+                   (const uint32_t*)P<uint32_t>(c.fpIslandBuf), m, bodyFlags, rowFlags, c.dCounters);
+            VXB_TRY(exclusiveScan(c, bodyFlags, bodyRank, n, &c.dCounters->clusterBodies));
+            VXB_TRY(exclusiveScan(c, rowFlags, rowRank, m, &c.dCounters->clusterRows));
+            LAUNCH(c, compactKernel, blocksFor(n, 256), 256, bodyFlags, bodyRank, n, bodyPos);
+            LAUNCH(c, compactKernel, blocksFor(m, 256), 256, rowFlags, rowRank, m, rowList);
+            VXB_TRY(readCounters(c));
+            c.clusterNB = c.hostCounters.clusterBodies;
+            c.clusterR = c.hostCounters.clusterRows;
+            c.clusterG = c.hostCounters.clusterColours;
+            const uint32_t nb = c.clusterNB, R = c.clusterR, Gc = c.clusterG, cells = clusters * Gc;
+            if (nb > 0 && R > 0 && Gc > 0) {
                 VXB_TRY(ensure(c, c.clusterKeyBuf, (size_t)nb * 8 + 64));
                 VXB_TRY(ensure(c, c.clusterValBuf, (size_t)nb * 4 + 64));
-                VXB_TRY(ensure(c, c.clusterOfBuf, (size_t)c.n * 4 + 64));
+                VXB_TRY(ensure(c, c.clusterOfBuf, (size_t)n * 4 + 64));
                 VXB_TRY(ensure(c, c.clusterCountBuf, (size_t)cells * 8 + 64));
+                VXB_TRY(ensure(c, c.clusterStartBuf, ((size_t)cells + 1) * 4 + 64));
+                VXB_TRY(ensure(c, c.clusterRowsBuf, (size_t)R * 4 + 64));
                 uint32_t* counts = P<uint32_t>(c.clusterCountBuf);
                 uint32_t* fill = counts + cells;
-                LAUNCH(c, clusterBodyKeyKernel, blocksFor(nb, 256), 256, G, b0, b1, (const Counters*)c.dCounters,
-                       P<uint64_t>(c.clusterKeyBuf), P<uint32_t>(c.clusterValBuf));
+                uint32_t* start = P<uint32_t>(c.clusterStartBuf);
+                LAUNCH(c, clusterBodyKeyKernel, blocksFor(nb, 256), 256, G, (const uint32_t*)bodyPos, nb,
+                       (const Counters*)c.dCounters, P<uint64_t>(c.clusterKeyBuf), P<uint32_t>(c.clusterValBuf));
                 VXB_TRY(sortPairs(c, P<uint64_t>(c.clusterKeyBuf), P<uint32_t>(c.clusterValBuf), nb, 30));
                 LAUNCH(c, clusterOfBodyKernel, blocksFor(nb, 256), 256, (const uint32_t*)P<uint32_t>(c.clusterValBuf),
                        nb, clusters, P<uint32_t>(c.clusterOfBuf));
                 VXB_CUDA(c, cudaMemsetAsync(counts, 0, (size_t)cells * 8, c.stream));
-                LAUNCH(c, clusterCountKernel, blocksFor(s1 - s0, 256), 256, G, s0, s1, g0, g1,
-                       (const uint32_t*)P<uint32_t>(c.clusterOfBuf), counts);
+                LAUNCH(c, clusterCountKernel, blocksFor(R, 256), 256, G, (const uint32_t*)rowList, R,
+                       (const uint32_t*)P<uint32_t>(c.fpIslandBuf), (const uint32_t*)P<uint32_t>(c.clusterOfBuf), Gc,
+                       counts);
                 VXB_TRY(exclusiveScan(c, counts, start, cells, start + cells));
-                LAUNCH(c, clusterScatterKernel, blocksFor(s1 - s0, 256), 256, G, s0, s1, g0, g1,
-                       (const uint32_t*)P<uint32_t>(c.clusterOfBuf), (const uint32_t*)start, fill, rows);
+                LAUNCH(c, clusterScatterKernel, blocksFor(R, 256), 256, G, (const uint32_t*)rowList, R,
+                       (const uint32_t*)P<uint32_t>(c.fpIslandBuf), (const uint32_t*)P<uint32_t>(c.clusterOfBuf), Gc,
+                       (const uint32_t*)start, fill, P<uint32_t>(c.clusterRowsBuf));
                 c.clusterBuilt = true;
             }
-            if (c.clusterBuilt) {
-                VXB_CUDA(c, cudaMemsetAsync(st, 0, sizeof(CoopState), c.stream));
-                const int rcc = launchCooperative(c, solveClusterKernel, 256, G, isl, g1 - g0,
-                                                  (const uint32_t*)start, (const uint32_t*)rows,
-                                                  (const uint32_t*)pred, done, st);
-                if (rcc != VXB_ERR_UNSUPPORTED) {
-                    VXB_TRY(rcc);
-                    uint32_t timeout = 0;
-                    VXB_CUDA(c, cudaMemcpyAsync(&timeout, &st->timeout, 4, cudaMemcpyDeviceToHost, c.stream));
-                    VXB_CUDA(c, cudaStreamSynchronize(c.stream));
-                    if (timeout) return fail(c, VXB_ERR_TIMEOUT, "a wait timed out in the giant-island solve");
-                    return VXB_OK;
-                }
+        }
+        if (clusters > 0 && c.clusterBuilt) {
+            VXB_CUDA(c, cudaMemsetAsync(st, 0, sizeof(CoopState), c.stream));
+            const int rcc = launchCooperative(c, solveClusterKernel, 256, G, c.clusterG,
+                                              (const uint32_t*)P<uint32_t>(c.clusterStartBuf),
+                                              (const uint32_t*)P<uint32_t>(c.clusterRowsBuf), (const uint32_t*)rowList,
+                                              c.clusterR, (const uint32_t*)P<uint32_t>(c.clusterValBuf), c.clusterNB,
+                                              (const uint32_t*)pred, done, st);
+            if (rcc != VXB_ERR_UNSUPPORTED) {
+                VXB_TRY(rcc);
+                uint32_t timeout = 0;
+                VXB_CUDA(c, cudaMemcpyAsync(&timeout, &st->timeout, 4, cudaMemcpyDeviceToHost, c.stream));
+                VXB_CUDA(c, cudaStreamSynchronize(c.stream));
+                if (timeout) return fail(c, VXB_ERR_TIMEOUT, "a wait timed out in the giant-island solve");
+                return VXB_OK;
             }
         }
     }
