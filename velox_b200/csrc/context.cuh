@@ -74,7 +74,8 @@ struct Counters {
     uint32_t clusterBodies;  // bodies of the giant islands (clustered solve)
     uint32_t clusterRows;    // their rows
     uint32_t clusterColours; // most colours of a giant island
-    uint32_t pad[2];
+    uint32_t giantCount;     // islands the block kernels cannot hold
+    uint32_t pad[1];
 };
 
 // Pipeline stages timed with CUDA events when timing is enabled.
@@ -98,6 +99,7 @@ struct Context {
     uint32_t caRounds = 0;     // rewind dependency depth of the last step (all passes)
     uint32_t caWidenings = 0;  // rewind replays with a widened body set (last step)
     uint32_t planContacts = 0; // contacts of the current island plan
+    uint32_t planGiants = 0;   // giant islands of the current plan
     bool giantLinked = false;  // dataflow links of the plan's giant islands are built
     bool clusterBuilt = false; // spatial clusters of the plan's (single) giant island are built
     bool tinyPacked = false;   // the plan's tiny islands are packed into warps

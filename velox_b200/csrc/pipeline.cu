@@ -1035,6 +1035,23 @@ __global__ void bodyStartKernel(const uint64_t* keys, uint32_t n, uint32_t* body
     }
 }
 
+// Islands the block kernels cannot hold (solveGiantKernel's / solveClusterKernel's
+// share), counted for the host's single read of the plan.
+constexpr uint32_t kTinyLimit = 16;   // islands of at most this many contacts: packed tiny solve
+constexpr int kBlockBodies = 512;     // islands beyond these sizes: the whole grid (giant islands)
+constexpr int kBlockRows = 3072;
+__global__ void giantCountKernel(const uint32_t* islandStart, const uint32_t* bodyStart, uint32_t islands,
+                                 uint32_t realIslands, Counters* C) {
+    uint32_t count = 0;
+    for (uint32_t isl = blockIdx.x * blockDim.x + threadIdx.x; isl < islands; isl += gridDim.x * blockDim.x) {
+        const uint32_t rows = islandStart[isl + 1] - islandStart[isl];
+        const uint32_t nb = isl < realIslands ? bodyStart[isl + 1] - bodyStart[isl] : 0u;
+        if (rows > kTinyLimit && (nb > (uint32_t)kBlockBodies || rows > (uint32_t)kBlockRows)) ++count;
+    }
+    for (int off = 16; off > 0; off >>= 1) count += __shfl_xor_sync(0xffffffffu, count, off);
+    if ((threadIdx.x & 31) == 0 && count) atomicAdd(&C->giantCount, count);
+}
+
 // Contact-free bodies: the last two bodyStart entries, for the host's single read.
 __global__ void freeRangeKernel(const uint32_t* bodyStart, uint32_t entries, Counters* C) {
     if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -1112,8 +1129,6 @@ VXD void positionRow(const SolveArgs& A, uint32_t ci) {
 // memory for the whole substep loop (islands of up to kBlockBodies bodies and
 // kBlockRows contacts); larger islands run the same schedule on global memory.
 constexpr int kBlockThreads = 256;
-constexpr int kBlockBodies = 512;
-constexpr int kBlockRows = 3072;
 // Islands of up to kSmallBodies bodies and kSmallRows contacts run on one warp
 // each, many per SM (a colour of a small island has a few rows; a 256-thread
 // block would leave most of its threads idle and hold a whole SM's share of
@@ -1399,11 +1414,19 @@ constexpr int kPackWarps = 4;       // warps (packs) per block
 
 // Sort key of a tiny island: its colour count (a pack runs as many colour
 // slots per sweep as its most coloured island, so similar islands share packs).
-__global__ void tinyKeyKernel(SolveArgs A, const uint32_t* list, uint32_t count, uint64_t* keys, uint32_t* vals) {
-    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < count; t += gridDim.x * blockDim.x) {
-        const uint32_t isl = list[t];
-        keys[t] = A.islandSeg[isl + 1] - A.islandSeg[isl];
-        vals[t] = isl;
+// Over `cap` slots (an upper bound); slots past the device-side count sort last.
+__global__ void tinyKeyKernel(SolveArgs A, const uint32_t* list, const uint32_t* countPtr, uint32_t cap,
+                              uint64_t* keys, uint32_t* vals) {
+    const uint32_t count = *countPtr;
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < cap; t += gridDim.x * blockDim.x) {
+        if (t < count) {
+            const uint32_t isl = list[t];
+            keys[t] = A.islandSeg[isl + 1] - A.islandSeg[isl];
+            vals[t] = isl;
+        } else {
+            keys[t] = 0xffu;
+            vals[t] = 0xffffffffu;
+        }
     }
 }
 
@@ -1420,10 +1443,14 @@ VXD uint32_t islandBodies(const SolveArgs& A, uint32_t isl) {
 
 // Greedy packing of each chunk of the tiny-island list: pass 0 counts the
 // packs of a chunk, pass 1 writes each pack's first list index.
-__global__ void tinyPackKernel(SolveArgs A, const uint32_t* list, uint32_t count, int pass, uint32_t* packCount,
-                               const uint32_t* packBase, uint32_t* packFirst) {
-    const uint32_t chunks = (count + kPackChunk - 1) / kPackChunk;
-    for (uint32_t ch = blockIdx.x * blockDim.x + threadIdx.x; ch < chunks; ch += gridDim.x * blockDim.x) {
+__global__ void tinyPackKernel(SolveArgs A, const uint32_t* list, const uint32_t* countPtr, uint32_t chunksCap,
+                               int pass, uint32_t* packCount, const uint32_t* packBase, uint32_t* packFirst) {
+    const uint32_t count = *countPtr;
+    for (uint32_t ch = blockIdx.x * blockDim.x + threadIdx.x; ch < chunksCap; ch += gridDim.x * blockDim.x) {
+        if (ch * kPackChunk >= count) {  // past the list: no packs
+            if (pass == 0) packCount[ch] = 0;
+            continue;
+        }
         const uint32_t t0 = ch * kPackChunk, t1 = min(count, t0 + kPackChunk);
         uint32_t packs = 0, rows = 0, bodies = 0;
         for (uint32_t t = t0; t < t1; ++t) {
@@ -1446,16 +1473,29 @@ __global__ void tinyPackKernel(SolveArgs A, const uint32_t* list, uint32_t count
 constexpr size_t kPackBodySmem = blockSmem(kPackBodies, 0);
 constexpr size_t kPackWarpSmem = (kPackBodySmem + kPackBodies * sizeof(uint32_t) + 15) / 16 * 16;
 
+VXD void solveTinyPack(const SolveArgs& A, const uint32_t* list, const uint32_t* packFirst, uint32_t packs,
+                       uint32_t listCount, uint32_t* localIdx, const SharedBodies& S, uint32_t* ids,
+                       uint32_t packIdx, uint32_t lane);
+
+// Packs come from device-side counts (no host read); warps stride over them.
 __global__ void __launch_bounds__(32 * kPackWarps) solveTinyPackKernel(SolveArgs A, const uint32_t* list,
-                                                                        const uint32_t* packFirst, uint32_t packs,
-                                                                        uint32_t listCount, uint32_t* localIdx) {
+                                                                        const uint32_t* packFirst,
+                                                                        const Counters* C, uint32_t* localIdx) {
     extern __shared__ float4 smemRaw[];
     const uint32_t warpInBlock = threadIdx.x >> 5, lane = threadIdx.x & 31u;
     float4* base = smemRaw + warpInBlock * (kPackWarpSmem / sizeof(float4));
     const SharedBodies S = carve<kPackBodies>(base);
     uint32_t* ids = reinterpret_cast<uint32_t*>(base + kPackBodySmem / sizeof(float4));
-    const uint32_t packIdx = blockIdx.x * kPackWarps + warpInBlock;
-    if (packIdx >= packs) return;  // the whole warp
+    const uint32_t packs = C->tinyPacks, listCount = C->tinyIslands;
+    for (uint32_t packIdx = blockIdx.x * kPackWarps + warpInBlock; packIdx < packs; packIdx += gridDim.x * kPackWarps) {
+        solveTinyPack(A, list, packFirst, packs, listCount, localIdx, S, ids, packIdx, lane);
+        __syncwarp();
+    }
+}
+
+VXD void solveTinyPack(const SolveArgs& A, const uint32_t* list, const uint32_t* packFirst, uint32_t packs,
+                       uint32_t listCount, uint32_t* localIdx, const SharedBodies& S, uint32_t* ids,
+                       uint32_t packIdx, uint32_t lane) {
     const uint32_t first = packFirst[packIdx];
     const uint32_t last = packIdx + 1 < packs ? packFirst[packIdx + 1] : listCount;
     const uint32_t count = last - first;  // islands in this pack (1..32)
@@ -2038,6 +2078,10 @@ __global__ void giantEntryKernel(SolveArgs A, const uint32_t* islandOf, uint32_t
         vals[2 * k] = 2 * k;
         vals[2 * k + 1] = 2 * k + 1;
     }
+}
+
+__global__ void coopTimeoutKernel(const CoopState* st, Counters* C) {
+    if (blockIdx.x == 0 && threadIdx.x == 0 && st->timeout) atomicOr(&C->timeout, 1u);
 }
 
 __global__ void giantListKernel(SolveArgs A, uint32_t* list, uint32_t* count) {
@@ -2900,10 +2944,16 @@ static int buildIslands(Context& c, const vx_contact* cs, uint32_t m, IslandPlan
     LAUNCH(c, bodyStartKernel, blocksFor(n, 256), 256, P<uint64_t>(c.bodyKeyBuf), n, P<uint32_t>(c.islandBodyStartBuf),
            plan.realIslands + 2);
     LAUNCH(c, freeRangeKernel, 1, 32, P<uint32_t>(c.islandBodyStartBuf), plan.realIslands + 2, c.dCounters);
-    VXB_TRY(readCounters(c));  // one read for the segment count and the free-body range
+    VXB_CUDA(c, cudaMemsetAsync(&c.dCounters->giantCount, 0, 4, c.stream));
+    if (m)
+        LAUNCH(c, giantCountKernel, std::min<uint32_t>(blocksFor(plan.islands, 256), (uint32_t)c.smCount * 4), 256,
+               (const uint32_t*)P<uint32_t>(c.islandStartBuf), (const uint32_t*)P<uint32_t>(c.islandBodyStartBuf),
+               plan.islands, plan.realIslands, c.dCounters);
+    VXB_TRY(readCounters(c));  // one read for the segment count, the free-body range and the giants
     plan.segments = m ? c.hostCounters.segments : 0;
     plan.freeFrom = c.hostCounters.freeFrom;
     plan.freeTo = c.hostCounters.freeTo;
+    c.planGiants = m ? c.hostCounters.giantCount : 0u;
     return VXB_OK;
 }
 
@@ -2926,7 +2976,7 @@ static SolveArgs solveArgs(Context& c, vx_contact* cs, const IslandPlan& plan) {
     A.bodyStart = P<uint32_t>(c.islandBodyStartBuf);
     A.islands = plan.islands;
     A.realIslands = plan.realIslands;
-    A.tinyLimit = 16;
+    A.tinyLimit = kTinyLimit;
     A.fault = &c.dCounters->planFault;
     A.prep = P<RowPrep>(c.prepBuf);
     A.frames = P<float4>(c.frameBuf);
@@ -2951,43 +3001,34 @@ static int launchSolve(Context& c, const SolveArgs& A) {
     uint32_t* tFirst = tList + islands + 16;
     uint32_t* tChunkCount = tFirst + islands + 16;
     uint32_t* tChunkBase = tChunkCount + chunksCap;
+    // (counts stay on the device: sizes below are upper bounds, kernels read the counts)
+    const uint32_t chunks = (islands + kPackChunk - 1) / kPackChunk;
     if (!c.tinyPacked) {
         LAUNCH(c, tinyFlagKernel, blocksFor(islands, 256), 256, A, tFlags);
         VXB_TRY(exclusiveScan(c, tFlags, tRanks, islands, &c.dCounters->tinyIslands));
         LAUNCH(c, compactKernel, blocksFor(islands, 256), 256, tFlags, tRanks, islands, tList);
-        VXB_TRY(readCounters(c));
-        c.tinyCount = c.hostCounters.tinyIslands;
-        c.tinyPackCount = 0;
-        if (c.tinyCount > 1) {
-            VXB_TRY(ensure(c, c.tinyKeyBuf, (size_t)c.tinyCount * 8 + 64));
-            LAUNCH(c, tinyKeyKernel, blocksFor(c.tinyCount, 256), 256, A, (const uint32_t*)tList, c.tinyCount,
-                   P<uint64_t>(c.tinyKeyBuf), tList);
-            VXB_TRY(sortPairs(c, P<uint64_t>(c.tinyKeyBuf), tList, c.tinyCount, 8));
-        }
-        if (c.tinyCount) {
-            const uint32_t chunks = (c.tinyCount + kPackChunk - 1) / kPackChunk;
-            LAUNCH(c, tinyPackKernel, blocksFor(chunks, 128), 128, A, (const uint32_t*)tList, c.tinyCount, 0,
-                   tChunkCount, (const uint32_t*)tChunkBase, tFirst);
-            VXB_TRY(exclusiveScan(c, tChunkCount, tChunkBase, chunks, &c.dCounters->tinyPacks));
-            LAUNCH(c, tinyPackKernel, blocksFor(chunks, 128), 128, A, (const uint32_t*)tList, c.tinyCount, 1,
-                   tChunkCount, (const uint32_t*)tChunkBase, tFirst);
-            VXB_TRY(readCounters(c));
-            c.tinyPackCount = c.hostCounters.tinyPacks;
-        }
+        VXB_TRY(ensure(c, c.tinyKeyBuf, (size_t)islands * 8 + 64));
+        LAUNCH(c, tinyKeyKernel, blocksFor(islands, 256), 256, A, (const uint32_t*)tList,
+               (const uint32_t*)&c.dCounters->tinyIslands, islands, P<uint64_t>(c.tinyKeyBuf), tList);
+        VXB_TRY(sortPairs(c, P<uint64_t>(c.tinyKeyBuf), tList, islands, 8));
+        LAUNCH(c, tinyPackKernel, blocksFor(chunks, 128), 128, A, (const uint32_t*)tList,
+               (const uint32_t*)&c.dCounters->tinyIslands, chunks, 0, tChunkCount, (const uint32_t*)tChunkBase, tFirst);
+        VXB_TRY(exclusiveScan(c, tChunkCount, tChunkBase, chunks, &c.dCounters->tinyPacks));
+        LAUNCH(c, tinyPackKernel, blocksFor(chunks, 128), 128, A, (const uint32_t*)tList,
+               (const uint32_t*)&c.dCounters->tinyIslands, chunks, 1, tChunkCount, (const uint32_t*)tChunkBase, tFirst);
         c.tinyPacked = true;
     }
     VXB_TRY(ensure(c, c.localIdxBuf, (size_t)c.n * 4 + 16));
-    if (c.tinyPackCount) {
+    {
         static bool packConfigured = false;
         if (!packConfigured) {
             cudaFuncSetAttribute(solveTinyPackKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)(kPackWarpSmem * kPackWarps));
             packConfigured = true;
         }
-        solveTinyPackKernel<<<(c.tinyPackCount + kPackWarps - 1) / kPackWarps, 32 * kPackWarps,
-                              kPackWarpSmem * kPackWarps, c.stream>>>(A, (const uint32_t*)tList,
-                                                                      (const uint32_t*)tFirst, c.tinyPackCount,
-                                                                      c.tinyCount, P<uint32_t>(c.localIdxBuf));
+        const uint32_t grid = std::min<uint32_t>((islands + kPackWarps - 1) / kPackWarps, (uint32_t)c.smCount * 8);
+        solveTinyPackKernel<<<grid, 32 * kPackWarps, kPackWarpSmem * kPackWarps, c.stream>>>(
+            A, (const uint32_t*)tList, (const uint32_t*)tFirst, (const Counters*)c.dCounters, P<uint32_t>(c.localIdxBuf));
         ++c.launches;
     }
     auto* large = solveBlockKernel<kBlockThreads, kBlockBodies, kBlockRows, false>;
@@ -3012,12 +3053,10 @@ static int launchSolve(Context& c, const SolveArgs& A) {
     CoopState* st = P<CoopState>(c.coopBuf);
     uint32_t* list = P<uint32_t>(c.giantBuf);
     VXB_CUDA(c, cudaMemsetAsync(st, 0, sizeof(CoopState), c.stream));
+    const uint32_t giants = c.planGiants;  // counted with the island plan
+    if (!giants) return VXB_OK;
     LAUNCH(c, giantListKernel, std::min<uint32_t>(blocksFor(A.islands, 256), (uint32_t)c.smCount * 4), 256, A, list,
            &st->rounds);
-    uint32_t giants = 0;
-    VXB_CUDA(c, cudaMemcpyAsync(&giants, &st->rounds, 4, cudaMemcpyDeviceToHost, c.stream));
-    VXB_CUDA(c, cudaStreamSynchronize(c.stream));
-    if (!giants) return VXB_OK;
     c.stats.giantIslands = std::max(c.stats.giantIslands, giants);
     // dataflow links of the giant islands' rows (once per island plan)
     const uint32_t m = c.planContacts;
@@ -3103,10 +3142,8 @@ static int launchSolve(Context& c, const SolveArgs& A) {
                                               (const uint32_t*)pred, done, st);
             if (rcc != VXB_ERR_UNSUPPORTED) {
                 VXB_TRY(rcc);
-                uint32_t timeout = 0;
-                VXB_CUDA(c, cudaMemcpyAsync(&timeout, &st->timeout, 4, cudaMemcpyDeviceToHost, c.stream));
-                VXB_CUDA(c, cudaStreamSynchronize(c.stream));
-                if (timeout) return fail(c, VXB_ERR_TIMEOUT, "a wait timed out in the giant-island solve");
+                // a timed-out wait reaches the host with the step's final counter read
+                LAUNCH(c, coopTimeoutKernel, 1, 32, (const CoopState*)st, c.dCounters);
                 return VXB_OK;
             }
         }
