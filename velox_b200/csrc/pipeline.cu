@@ -1035,8 +1035,8 @@ __global__ void bodyStartKernel(const uint64_t* keys, uint32_t n, uint32_t* body
     }
 }
 
-// Islands the block kernels cannot hold (solveGiantKernel's / solveClusterKernel's
-// share), counted for the host's single read of the plan.
+// Islands the block kernels cannot hold (solveClusterKernel's share), counted
+// for the host's single read of the plan.
 constexpr uint32_t kTinyLimit = 16;   // islands of at most this many contacts: packed tiny solve
 constexpr int kBlockBodies = 512;     // islands beyond these sizes: the whole grid (giant islands)
 constexpr int kBlockRows = 3072;
@@ -1784,96 +1784,13 @@ VXD void giantIntegrateTransform(const SolveArgs& A, uint32_t i) {
     __stcg(A.B.ang + i, pack(w, 0.0f));
 }
 
-// Cooperative launch over the giant islands listed in `giants`, one after the
-// other. Body phases (integration, inertia frames) and the row preparation are
-// separated by grid barriers; the sweeps run as a dataflow instead of one
-// barrier per colour: a row may run its sweep u once the previous row on each
-// of its dynamic bodies (colour order; the body's last row of sweep u - 1 for
-// its first row) has finished. That is the order the colour-by-colour sweep
-// imposes on every body, so the results are the same, but independent parts
-// of the island run ahead instead of waiting for the slowest colour. Rows go
-// to warps in groups of 32 of one colour; a warp takes its groups in
-// (sweep, colour, group) order, which keeps the earliest unfinished group
-// runnable. Every wait is bounded.
+// Giant islands: every row is linked to the previous row on each of its
+// dynamic bodies (colour order; the body's last row of the previous sweep for
+// its first row). A row may run sweep u once those predecessors have
+// published sweep u (u - 1 across the wrap): the order the colour-by-colour
+// sweep imposes on every body, without a barrier per colour.
 constexpr uint32_t kNoPred = 0xffffffffu;  // no predecessor / empty queue slot
 constexpr uint32_t kWrap = 0x80000000u;    // predecessor from the previous sweep
-
-// Runs `units` dataflow sweeps (op as giantRow) over rows [s0, s1); false on timeout.
-VXD bool giantFlow(const SolveArgs& A, uint32_t s0, uint32_t g0, uint32_t g1, int units, int warmUnits, int op,
-                   const uint32_t* pred, uint32_t* done, CoopState* st) {
-    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t lane = threadIdx.x & 31u, warp = tid >> 5, warps = (gridDim.x * blockDim.x) >> 5;
-    for (int u = 0; u < units; ++u) {
-        const int rowOp = op == 1 && u < warmUnits ? 0 : op;
-        for (uint32_t g = g0; g < g1; ++g) {
-            const uint32_t r0 = A.segStart[g], r1 = A.segStart[g + 1];
-            const uint32_t groups = (r1 - r0 + 31u) >> 5;
-            const uint32_t rot = ((r0 - s0) >> 5) % warps;
-            for (uint32_t j = (warp + warps - rot) % warps; j < groups; j += warps) {
-                const uint32_t k = r0 + (j << 5) + lane;
-                const bool active = k < r1;
-                uint32_t p0 = kNoPred, p1 = kNoPred;
-                if (active) { p0 = pred[2 * k]; p1 = pred[2 * k + 1]; }
-                const uint32_t need0 = (p0 & kWrap) ? (uint32_t)u : (uint32_t)u + 1u;
-                const uint32_t need1 = (p1 & kWrap) ? (uint32_t)u : (uint32_t)u + 1u;
-                for (uint32_t spins = 0;; ++spins) {
-                    const bool ready = (p0 == kNoPred || ldAcquire(done + (p0 & ~kWrap)) >= need0) &&
-                                       (p1 == kNoPred || ldAcquire(done + (p1 & ~kWrap)) >= need1);
-                    if (__all_sync(0xffffffffu, ready)) break;
-                    if (spins > kSpinLimit || __ldcg(&st->timeout)) {
-                        if (lane == 0) atomicOr(&st->timeout, 1u);
-                        return false;
-                    }
-                    __nanosleep(32);
-                }
-                if (active) {
-                    giantRow(A, k, rowOp);
-                    stRelease(done + k, (uint32_t)u + 1u);  // publishes this row's writes
-                }
-            }
-        }
-    }
-    return true;
-}
-
-__global__ void __launch_bounds__(256) solveGiantKernel(SolveArgs A, const uint32_t* giants, uint32_t count,
-                                                        const uint32_t* pred, uint32_t* done, CoopState* st) {
-    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
-    for (uint32_t gi = 0; gi < count; ++gi) {
-        const uint32_t isl = giants[gi];
-        const uint32_t s0 = A.islandStart[isl], s1 = A.islandStart[isl + 1];
-        const uint32_t g0 = A.islandSeg[isl], g1 = A.islandSeg[isl + 1];
-        const uint32_t b0 = isl < A.realIslands ? A.bodyStart[isl] : 0u;
-        const uint32_t b1 = isl < A.realIslands ? A.bodyStart[isl + 1] : 0u;
-        if (A.positionIterations > 0) {
-            for (uint32_t k = s0 + tid; k < s1; k += stride) __stcg(done + k, 0u);
-            if (!gridSync(&st->bar, &st->timeout)) return;
-            if (!giantFlow(A, s0, g0, g1, A.positionIterations, 0, 2, pred, done, st)) return;
-            if (!gridSync(&st->bar, &st->timeout)) return;
-            continue;
-        }
-        for (int s = 0; s < A.substeps; ++s) {
-            for (uint32_t k = b0 + tid; k < b1; k += stride) {
-                const uint32_t id = A.bodyOrder[k];
-                if (A.integrate && s > 0) giantIntegrateVelocity(A, id);
-                __stcg(A.frames + id, pack(inertiaFrameAt(loadMass(A.B, id), q4(ldcg4(A.B.rot + id)))));
-            }
-            if (!gridSync(&st->bar, &st->timeout)) return;
-            for (uint32_t k = s0 + tid; k < s1; k += stride) {
-                giantRow(A, k, 3);
-                __stcg(done + k, 0u);
-            }
-            if (!gridSync(&st->bar, &st->timeout)) return;
-            const int warmUnits = A.warmStart && s == 0 ? 1 : 0;
-            if (!giantFlow(A, s0, g0, g1, warmUnits + A.sweeps, warmUnits, 1, pred, done, st)) return;
-            if (!gridSync(&st->bar, &st->timeout)) return;
-            if (A.integrate) {
-                for (uint32_t k = b0 + tid; k < b1; k += stride) giantIntegrateTransform(A, A.bodyOrder[k]);
-                if (!gridSync(&st->bar, &st->timeout)) return;
-            }
-        }
-    }
-}
 
 // Dataflow links of the giant islands' rows: entries (dynamic body, 2k + side)
 // of every row of a giant island, other endpoints keyed n (no link).
@@ -3148,18 +3065,8 @@ static int launchSolve(Context& c, const SolveArgs& A) {
             }
         }
     }
-    VXB_CUDA(c, cudaMemsetAsync(st, 0, sizeof(CoopState), c.stream));
-    const int rc = launchCooperative(c, solveGiantKernel, 256, G, (const uint32_t*)list, giants,
-                                     (const uint32_t*)pred, done, st);
-    if (rc == VXB_ERR_UNSUPPORTED) {
-        LAUNCH(c, solveGiantBlockKernel, giants, kBlockThreads, A, (const uint32_t*)list);
-        return VXB_OK;
-    }
-    VXB_TRY(rc);
-    uint32_t timeout = 0;
-    VXB_CUDA(c, cudaMemcpyAsync(&timeout, &st->timeout, 4, cudaMemcpyDeviceToHost, c.stream));
-    VXB_CUDA(c, cudaStreamSynchronize(c.stream));
-    if (timeout) return fail(c, VXB_ERR_TIMEOUT, "grid barrier timed out in the giant-island solve");
+    // no cooperative grid (or no solvable giant rows): one block per giant island
+    LAUNCH(c, solveGiantBlockKernel, giants, kBlockThreads, A, (const uint32_t*)list);
     return VXB_OK;
 }
 
