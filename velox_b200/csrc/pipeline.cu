@@ -2217,10 +2217,15 @@ __device__ __noinline__ bool caRewind(BodyArrays& B, const Soup& soup, uint32_t 
 // Every flagged pair evaluated in parallel on the probe's state (read-only):
 // in the ordered pass, a flagged pair whose bodies no earlier rewind has moved
 // sees exactly this state, so its outcome can be taken from here.
+// `spread`: threads per pair (one works), so that a few pairs still occupy
+// many SMs and share warps with few others (each is a long serial loop).
 __global__ void caSpeculateKernel(BodyArrays B, Soup soup, const uint64_t* pairKeys, const uint32_t* flaggedList,
-                                  uint32_t flagged, const float4* endGap, float dt, const float4* prevPos,
-                                  const float4* prevRot, float4* specState, uint32_t* specResult, Counters* C) {
-    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < flagged; k += gridDim.x * blockDim.x) {
+                                  uint32_t flagged, uint32_t spread, const float4* endGap, float dt,
+                                  const float4* prevPos, const float4* prevRot, float4* specState,
+                                  uint32_t* specResult, Counters* C) {
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid % spread) return;
+    for (uint32_t k = tid / spread; k < flagged; k += gridDim.x * blockDim.x / spread) {
         const uint32_t r = flaggedList[k];
         uint32_t i, j;
         orientPair(B, pairKeys[r], i, j);
@@ -3142,8 +3147,11 @@ static int conservativeAdvancement(Context& c, uint32_t npairs, float dt) {
     uint32_t* specResult = reinterpret_cast<uint32_t*>(specState + 8 * (size_t)flagged);
     uint32_t* flaggedList = specResult + flagged;
     LAUNCH(c, compactKernel, blocksFor(npairs, 256), 256, flags, flagRank, npairs, flaggedList);
-    LAUNCH(c, caSpeculateKernel, blocksFor(flagged, 64), 64, c.B, soupOf(c), pk, (const uint32_t*)flaggedList, flagged,
-           (const float4*)endGap, dt, prevPos, prevRot, specState, specResult, c.dCounters);
+    uint32_t spread = 1;
+    while (spread < 8 && (size_t)flagged * spread * 2 <= (size_t)c.smCount * 64) spread <<= 1;
+    LAUNCH(c, caSpeculateKernel, blocksFor((uint64_t)flagged * spread, 64), 64, c.B, soupOf(c), pk,
+           (const uint32_t*)flaggedList, flagged, spread, (const float4*)endGap, dt, prevPos, prevRot, specState,
+           specResult, c.dCounters);
     // mark ahead of the cascade before the first pass too (fewer replays)
     {
         const uint32_t* frontier = bodyMark;
