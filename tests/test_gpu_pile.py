@@ -50,3 +50,37 @@ def test_pile_step_matches_reference(ref):
     assert stats["giantIslands"] >= 1
     assert stats["colorRounds"] > 0
     assert stats["rewinds"] > 0
+
+
+def test_two_piles_in_two_worlds_match_reference(ref):
+    # the same 2,500-body scene in two worlds: two giant islands at once (the
+    # clustered solve over several islands), each world equal to the reference
+    specs, pool = velox_b200.generate_scene(2, size=2500)
+    w = ref.RefWorld(specs, pool)
+    start = w.bodies()
+    pts, faces = w.soup()
+    w.close()
+    soup = velox_b200.make_soup(pts, faces)
+    n = len(start)
+    both = np.concatenate([start, start])
+    world_of = np.repeat(np.arange(2, dtype=np.uint32), n)
+    ctx = velox_b200.Context(0)
+    ctx.load(both, soup, world_of=world_of)
+    ctx.configure(dt=DT, substeps=4)
+    ctx.step(220)
+    piles = ctx.read_bodies()
+    assert np.array_equal(_state(piles[:n]), _state(piles[n:]))
+    w = ref.RefWorld(specs, pool)
+    w.configure(substeps=4, workers=1)
+    w.set_bodies(piles[:n])
+    w.step(DT, 1)
+    ctx.step(1)
+    stats = ctx.stats()
+    out = ctx.read_bodies()
+    ctx.close()
+    theirs = _state(w.bodies())
+    w.close()
+    assert stats["giantIslands"] >= 2
+    for half in (out[:n], out[n:]):
+        err = np.abs(_state(half) - theirs) / np.maximum(1.0, np.abs(theirs))
+        assert err.max() <= 1e-4, float(err.max())
