@@ -69,11 +69,16 @@ def test_two_piles_in_two_worlds_match_reference(ref):
     ctx.configure(dt=DT, substeps=4)
     ctx.step(220)
     piles = ctx.read_bodies()
+    ctx.close()
     assert np.array_equal(_state(piles[:n]), _state(piles[n:]))
+    # one step from the piles on both engines (fresh contact caches on both)
     w = ref.RefWorld(specs, pool)
     w.configure(substeps=4, workers=1)
     w.set_bodies(piles[:n])
     w.step(DT, 1)
+    ctx = velox_b200.Context(0)
+    ctx.load(piles, soup, world_of=world_of)
+    ctx.configure(dt=DT, substeps=4)
     ctx.step(1)
     stats = ctx.stats()
     out = ctx.read_bodies()
