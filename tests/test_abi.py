@@ -54,6 +54,27 @@ def test_record_sizes_match_reference_layout():
     assert ctypes.sizeof(binding.SolverOptions) == 24
 
 
+def test_records_restore_the_struct_layout():
+    # np.concatenate of padded records drops the padding: the binding re-lays
+    # such arrays field by field, and refuses them where the library writes back
+    a = np.zeros(3, binding.BODY)
+    a["position"] = np.arange(9, dtype=np.float32).reshape(3, 3)
+    a["motionType"] = [0, 2, 0]
+    both = np.concatenate([a, a])
+    assert both.dtype.itemsize != binding.BODY.itemsize
+    fixed = binding.records(both, binding.BODY)
+    assert fixed.dtype == binding.BODY and fixed.flags["C_CONTIGUOUS"]
+    assert np.array_equal(fixed["position"], both["position"])
+    assert list(fixed["motionType"]) == [0, 2, 0, 0, 2, 0]
+    assert binding.records(a, binding.BODY) is a
+    try:
+        binding.records(both, binding.BODY, inout=True)
+    except ValueError:
+        pass
+    else:
+        raise AssertionError("an in/out array in another layout was accepted")
+
+
 def test_scene_generation_is_seeded_and_sized():
     a, pa = velox_b200.generate_scene(2, size=500)
     b, pb = velox_b200.generate_scene(2, size=500)

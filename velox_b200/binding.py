@@ -122,6 +122,21 @@ def ptr(a):
     return ctypes.c_void_p(a.ctypes.data) if a is not None and a.size else ctypes.c_void_p(0)
 
 
+def records(a, dtype, inout=False):
+    """`a` as contiguous records in the C struct layout `dtype`. A structured
+    array with the same fields but another layout (np.concatenate of padded
+    records drops the padding) is copied field by field; an array the library
+    writes into must already be in the layout, else ValueError."""
+    if a.dtype == dtype and a.flags["C_CONTIGUOUS"]:
+        return a
+    if inout or a.dtype.names is None or set(a.dtype.names) != set(dtype.names):
+        raise ValueError(f"expected a C-contiguous array of {len(dtype.names)}-field records, itemsize {dtype.itemsize}")
+    out = np.zeros(len(a), dtype)
+    for name in dtype.names:
+        out[name] = a[name]
+    return out
+
+
 _lib = None
 
 
@@ -270,6 +285,7 @@ class Context:
 
     # ---- device world
     def load(self, bodies, soup, world_of=None):
+        bodies = records(bodies, BODY)
         self.bodies_n = len(bodies)
         wo = None if world_of is None else np.ascontiguousarray(world_of, np.uint32)
         self._check(self.L.vxb_world_load(self.h, ptr(bodies), len(bodies), ctypes.byref(soup), ptr(wo)))
@@ -309,6 +325,7 @@ class Context:
 
     # ---- stages
     def pairs(self, bodies, dt):
+        bodies = records(bodies, BODY)
         cnt = ctypes.c_uint32()
         self._check(self.L.vxb_stage_pairs(self.h, ptr(bodies), len(bodies), dt, None, 0, ctypes.byref(cnt)))
         out = np.zeros(max(cnt.value, 1), np.uint64)
@@ -317,6 +334,7 @@ class Context:
         return out[:cnt.value]
 
     def collide(self, bodies, soup, pairs, dt, cap=None):
+        bodies = records(bodies, BODY)
         pairs = np.ascontiguousarray(pairs, np.uint64)
         cap = cap or max(12 * len(pairs), 1)
         out = np.zeros(cap, CONTACT)
@@ -329,6 +347,7 @@ class Context:
     def distance(self, bodies, soup, pairs, path=0):
         """gjkDistance per pair: (npairs, 11) float32 rows (distance, normal,
         pointA, pointB, overlapping)."""
+        bodies = records(bodies, BODY)
         pairs = np.ascontiguousarray(pairs, np.uint64)
         out = np.zeros((max(len(pairs), 1), 11), np.float32)
         self._check(self.L.vxb_stage_distance(self.h, ptr(bodies), len(bodies), ctypes.byref(soup), ptr(pairs),
@@ -336,6 +355,7 @@ class Context:
         return out[:len(pairs)]
 
     def color(self, bodies, contacts):
+        bodies, contacts = records(bodies, BODY), records(contacts, CONTACT)
         colors = np.zeros(max(len(contacts), 1), np.int32)
         nc = ctypes.c_uint32()
         self._check(self.L.vxb_stage_color(self.h, ptr(bodies), len(bodies), ptr(contacts), len(contacts),
@@ -344,9 +364,11 @@ class Context:
 
     # ---- Backend interface
     def backend_integrate(self, bodies, gravity, dt):
+        bodies = records(bodies, BODY, inout=True)
         self._check(self.L.vxb_backend_integrate(self.h, ptr(bodies), len(bodies), Vec3(*gravity), dt))
 
     def backend_find_contacts(self, bodies, soup, dt):
+        bodies = records(bodies, BODY)
         cnt = ctypes.c_uint32()
         self._check(self.L.vxb_backend_find_contacts(self.h, ptr(bodies), len(bodies), ctypes.byref(soup), dt,
                                                      ctypes.byref(cnt)))
@@ -355,6 +377,8 @@ class Context:
         return out
 
     def backend_advance_substeps(self, bodies, contacts, gravity, h, substeps, solver=None):
+        bodies = records(bodies, BODY, inout=True)
+        contacts = records(contacts, CONTACT, inout=True)
         adv = ctypes.c_int()
         it = ctypes.c_uint32()
         opts = solver or SolverOptions.default()
@@ -364,4 +388,5 @@ class Context:
         return bool(adv.value), it.value
 
     def backend_fetch_impulses(self, contacts):
+        contacts = records(contacts, CONTACT, inout=True)
         self._check(self.L.vxb_backend_fetch_impulses(self.h, ptr(contacts), len(contacts)))
