@@ -101,7 +101,7 @@ struct Context {
     uint32_t planContacts = 0; // contacts of the current island plan
     uint32_t planGiants = 0;   // giant islands of the current plan
     bool giantLinked = false;  // dataflow links of the plan's giant islands are built
-    bool clusterBuilt = false; // spatial clusters of the plan's (single) giant island are built
+    bool clusterBuilt = false; // spatial clusters of the plan's giant islands are built
     bool tinyPacked = false;   // the plan's tiny islands are packed into warps
     uint32_t tinyCount = 0, tinyPackCount = 0;
     uint32_t clusterNB = 0, clusterR = 0, clusterG = 0;  // giant bodies, rows, most colours (clustered solve)
@@ -174,6 +174,7 @@ struct Context {
     DevBuf tinyKeyBuf;                  // tiny islands' colour counts (pack order sort)
     DevBuf clusterInfoBuf, clusterKeyBuf, clusterValBuf, clusterOfBuf, clusterCountBuf, clusterStartBuf,
         clusterRowsBuf;                 // spatial clusters of a giant island
+    DevBuf clusterLinkBuf;              // cross-cluster predecessor links + remote-successor flags
 
     DevBuf countersBuf;
     Counters* dCounters = nullptr;

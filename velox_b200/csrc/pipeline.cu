@@ -1705,12 +1705,28 @@ VXD void coherentPrep(const RowPrep* p, RowPrep& P) {
     for (int i = 0; i < (int)(sizeof(RowPrep) / 4); ++i) d[i] = __ldcg(s + i);
 }
 
-// op: 0 warm start, 1 velocity sweep, 2 position row, 3 prepare
-VXD void giantRow(const SolveArgs& A, uint32_t pos, int op) {
-    const uint2 ab = A.rowBodies[pos];  // issued with the contact load, not after it
-    vx_contact* cp = A.contacts + A.order[pos];
+// Inputs of one giant row that only the row itself writes (its contact
+// record and its prepared terms; the body ids are fixed): a row fetches them
+// before it waits for its predecessors, so their latency overlaps the wait.
+struct GiantRowIn {
+    uint2 ab;
+    vx_contact* cp;
     alignas(16) vx_contact cc;
-    loadContactCoherent(cp, cc);
+    RowPrep P;
+};
+
+VXD void giantRowFetch(const SolveArgs& A, uint32_t pos, int op, GiantRowIn& in) {
+    in.ab = A.rowBodies[pos];
+    in.cp = A.contacts + A.order[pos];
+    loadContactCoherent(in.cp, in.cc);
+    if (op == 0 || op == 1) coherentPrep(A.prep + pos, in.P);
+}
+
+// op: 0 warm start, 1 velocity sweep, 2 position row, 3 prepare
+VXD void giantRowRun(const SolveArgs& A, uint32_t pos, int op, GiantRowIn& in) {
+    const uint2 ab = in.ab;
+    vx_contact* cp = in.cp;
+    vx_contact& cc = in.cc;
     SolverBody a = coherentBody(A, ab.x), b = coherentBody(A, ab.y);
     if (!solvedContact(a.m.flags, b.m.flags)) return;
     RowContact r;
@@ -1733,23 +1749,27 @@ VXD void giantRow(const SolveArgs& A, uint32_t pos, int op) {
             __stcg(A.B.pos + ab.y, pack(b.p - r.normal * (push * imb), 0.0f));
         return;
     }
-    RowPrep* Pg = A.prep + pos;
-    RowPrep P;
+    RowPrep& P = in.P;
     if (op == 3) {
         prepRow(a, b, r, A.h, A.coneBlock != 0, P);
         const float* src = reinterpret_cast<const float*>(&P);
-        float* dst = reinterpret_cast<float*>(Pg);
+        float* dst = reinterpret_cast<float*>(A.prep + pos);
 #pragma unroll
         for (int i = 0; i < (int)(sizeof(RowPrep) / 4); ++i) __stcg(dst + i, src[i]);
         return;
     }
-    coherentPrep(Pg, P);
     if (op == 0) warmPrepRow(a, b, r, P);
     else sweepRow(a, b, r, P, A.coneBlock != 0);
     if (isDynamic(a.m.flags)) { __stcg(A.B.vel + ab.x, pack(a.v, 0.0f)); __stcg(A.B.ang + ab.x, pack(a.w, 0.0f)); }
     if (isDynamic(b.m.flags)) { __stcg(A.B.vel + ab.y, pack(b.v, 0.0f)); __stcg(A.B.ang + ab.y, pack(b.w, 0.0f)); }
     storeRow(cc, r);
     storeContactCoherent(cp, cc);
+}
+
+VXD void giantRow(const SolveArgs& A, uint32_t pos, int op) {
+    GiantRowIn in;
+    giantRowFetch(A, pos, op, in);
+    giantRowRun(A, pos, op, in);
 }
 
 // integrateKernel semantics (src/backend_cuda.cu:80-89) on coherent loads.
@@ -1879,12 +1899,39 @@ VXD uint32_t rowCluster(const SolveArgs& A, uint32_t k, const uint32_t* clusterO
 // (cluster, colour slot) cell of a giant row: colour slot = colour within its
 // island. Rows of the null island (no dynamic body of their own island) go to
 // cluster 0: they are never solved and link to nothing.
+VXD uint32_t rowBlock(const SolveArgs& A, uint32_t k, const uint32_t* islandOf, const uint32_t* clusterOf) {
+    return islandOf[k] < A.realIslands ? rowCluster(A, k, clusterOf) : 0u;
+}
+
 VXD uint32_t rowCell(const SolveArgs& A, uint32_t k, const uint32_t* islandOf, const uint32_t* clusterOf,
                      uint32_t G) {
     const uint32_t isl = islandOf[k];
     const uint32_t g0 = A.islandSeg[isl], g1 = A.islandSeg[isl + 1];
-    const uint32_t cluster = isl < A.realIslands ? rowCluster(A, k, clusterOf) : 0u;
-    return cluster * G + (segmentOf(A.segStart, g0, g1, k) - g0);
+    return rowBlock(A, k, islandOf, clusterOf) * G + (segmentOf(A.segStart, g0, g1, k) - g0);
+}
+
+// Links the clustered solve waits on. A predecessor in the row's own cluster
+// ran in the same block, in an earlier (sweep, colour) step: a same-sweep
+// predecessor has a lower colour of the same island, a wrapped one belongs to
+// the previous sweep, and the block barrier after every step orders it. Only
+// predecessors in other clusters stay linked (clusterPred), and only rows that
+// such a link names publish their sweep counter (remote = 1).
+__global__ void clusterLinkKernel(SolveArgs A, const uint32_t* rowList, uint32_t R, const uint32_t* islandOf,
+                                  const uint32_t* clusterOf, const uint32_t* pred, uint32_t* clusterPred,
+                                  uint32_t* remote) {
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < R; t += gridDim.x * blockDim.x) {
+        const uint32_t k = rowList[t];
+        const uint32_t own = rowBlock(A, k, islandOf, clusterOf);
+        for (int side = 0; side < 2; ++side) {
+            const uint32_t p = pred[2 * k + side];
+            uint32_t link = kNoPred;
+            if (p != kNoPred && rowBlock(A, p & ~kWrap, islandOf, clusterOf) != own) {
+                link = p;
+                remote[p & ~kWrap] = 1u;
+            }
+            clusterPred[2 * k + side] = link;
+        }
+    }
 }
 
 __global__ void clusterCountKernel(SolveArgs A, const uint32_t* rowList, uint32_t R, const uint32_t* islandOf,
@@ -1904,28 +1951,34 @@ __global__ void clusterScatterKernel(SolveArgs A, const uint32_t* rowList, uint3
 }
 
 // One unit (sweep) step of block c's cluster for colour slot gl; false = abort.
+// `pred`: the cross-cluster links (clusterLinkKernel); `remote`: rows that
+// publish their sweep counter.
 VXD bool clusterStep(const SolveArgs& A, const uint32_t* start, const uint32_t* rows, uint32_t cell, int u, int op,
-                     const uint32_t* pred, uint32_t* done, CoopState* st, int* abortFlag) {
+                     const uint32_t* pred, const uint32_t* remote, uint32_t* done, CoopState* st, int* abortFlag) {
     for (uint32_t idx = start[cell] + threadIdx.x; idx < start[cell + 1]; idx += blockDim.x) {
         const uint32_t k = rows[idx];
+        GiantRowIn in;
+        giantRowFetch(A, k, op, in);
         const uint32_t p0 = pred[2 * k], p1 = pred[2 * k + 1];
-        const uint32_t need0 = (p0 & kWrap) ? (uint32_t)u : (uint32_t)u + 1u;
-        const uint32_t need1 = (p1 & kWrap) ? (uint32_t)u : (uint32_t)u + 1u;
-        bool ok = true;
-        for (uint32_t spins = 0;; ++spins) {
-            if ((p0 == kNoPred || ldAcquire(done + (p0 & ~kWrap)) >= need0) &&
-                (p1 == kNoPred || ldAcquire(done + (p1 & ~kWrap)) >= need1))
-                break;
-            if (spins > kSpinLimit || ((spins & 63u) == 63u && __ldcg(&st->timeout))) {
-                atomicOr(&st->timeout, 1u);
-                ok = false;
-                break;
+        if (p0 != kNoPred || p1 != kNoPred) {
+            const uint32_t need0 = (p0 & kWrap) ? (uint32_t)u : (uint32_t)u + 1u;
+            const uint32_t need1 = (p1 & kWrap) ? (uint32_t)u : (uint32_t)u + 1u;
+            bool ok = true;
+            for (uint32_t spins = 0;; ++spins) {
+                const uint32_t d0 = p0 == kNoPred ? 0xffffffffu : ldAcquire(done + (p0 & ~kWrap));
+                const uint32_t d1 = p1 == kNoPred ? 0xffffffffu : ldAcquire(done + (p1 & ~kWrap));
+                if (d0 >= need0 && d1 >= need1) break;
+                if (spins > kSpinLimit || ((spins & 63u) == 63u && __ldcg(&st->timeout))) {
+                    atomicOr(&st->timeout, 1u);
+                    ok = false;
+                    break;
+                }
+                __nanosleep(32);
             }
-            __nanosleep(32);
+            if (!ok) { *abortFlag = 1; break; }
         }
-        if (!ok) { *abortFlag = 1; break; }
-        giantRow(A, k, op);
-        stRelease(done + k, (uint32_t)u + 1u);
+        giantRowRun(A, k, op, in);
+        if (remote[k]) stRelease(done + k, (uint32_t)u + 1u);
     }
     __syncthreads();
     return *abortFlag == 0;
@@ -1934,7 +1987,7 @@ VXD bool clusterStep(const SolveArgs& A, const uint32_t* start, const uint32_t* 
 __global__ void __launch_bounds__(256) solveClusterKernel(SolveArgs A, uint32_t G, const uint32_t* start,
                                                           const uint32_t* rows, const uint32_t* rowList, uint32_t R,
                                                           const uint32_t* bodyIds, uint32_t NB, const uint32_t* pred,
-                                                          uint32_t* done, CoopState* st) {
+                                                          const uint32_t* remote, uint32_t* done, CoopState* st) {
     __shared__ int abortFlag;
     if (threadIdx.x == 0) abortFlag = 0;
     __syncthreads();
@@ -1945,7 +1998,7 @@ __global__ void __launch_bounds__(256) solveClusterKernel(SolveArgs A, uint32_t 
         if (!gridSync(&st->bar, &st->timeout)) return;
         for (int u = 0; u < A.positionIterations; ++u)
             for (uint32_t gl = 0; gl < G; ++gl)
-                if (!clusterStep(A, start, rows, base + gl, u, 2, pred, done, st, &abortFlag)) return;
+                if (!clusterStep(A, start, rows, base + gl, u, 2, pred, remote, done, st, &abortFlag)) return;
         gridSync(&st->bar, &st->timeout);
         return;
     }
@@ -1965,7 +2018,8 @@ __global__ void __launch_bounds__(256) solveClusterKernel(SolveArgs A, uint32_t 
         const int warmUnits = A.warmStart && s == 0 ? 1 : 0;
         for (int u = 0; u < warmUnits + A.sweeps; ++u)
             for (uint32_t gl = 0; gl < G; ++gl)
-                if (!clusterStep(A, start, rows, base + gl, u, u < warmUnits ? 0 : 1, pred, done, st, &abortFlag))
+                if (!clusterStep(A, start, rows, base + gl, u, u < warmUnits ? 0 : 1, pred, remote, done, st,
+                                 &abortFlag))
                     return;
         if (!gridSync(&st->bar, &st->timeout)) return;
         if (A.integrate) {
@@ -3052,6 +3106,12 @@ static int launchSolve(Context& c, const SolveArgs& A) {
                 LAUNCH(c, clusterScatterKernel, blocksFor(R, 256), 256, G, (const uint32_t*)rowList, R,
                        (const uint32_t*)P<uint32_t>(c.fpIslandBuf), (const uint32_t*)P<uint32_t>(c.clusterOfBuf), Gc,
                        (const uint32_t*)start, fill, P<uint32_t>(c.clusterRowsBuf));
+                VXB_TRY(ensure(c, c.clusterLinkBuf, (size_t)m * 12 + 64));
+                uint32_t* remote = P<uint32_t>(c.clusterLinkBuf) + 2 * (size_t)m;
+                VXB_CUDA(c, cudaMemsetAsync(remote, 0, (size_t)m * 4, c.stream));
+                LAUNCH(c, clusterLinkKernel, blocksFor(R, 256), 256, G, (const uint32_t*)rowList, R,
+                       (const uint32_t*)P<uint32_t>(c.fpIslandBuf), (const uint32_t*)P<uint32_t>(c.clusterOfBuf),
+                       (const uint32_t*)pred, P<uint32_t>(c.clusterLinkBuf), remote);
                 c.clusterBuilt = true;
             }
         }
@@ -3061,7 +3121,9 @@ static int launchSolve(Context& c, const SolveArgs& A) {
                                               (const uint32_t*)P<uint32_t>(c.clusterStartBuf),
                                               (const uint32_t*)P<uint32_t>(c.clusterRowsBuf), (const uint32_t*)rowList,
                                               c.clusterR, (const uint32_t*)P<uint32_t>(c.clusterValBuf), c.clusterNB,
-                                              (const uint32_t*)pred, done, st);
+                                              (const uint32_t*)P<uint32_t>(c.clusterLinkBuf),
+                                              (const uint32_t*)(P<uint32_t>(c.clusterLinkBuf) + 2 * (size_t)m), done,
+                                              st);
             if (rcc != VXB_ERR_UNSUPPORTED) {
                 VXB_TRY(rcc);
                 // a timed-out wait reaches the host with the step's final counter read
