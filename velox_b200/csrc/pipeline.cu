@@ -1711,7 +1711,7 @@ VXD void coherentPrep(const RowPrep* p, RowPrep& P) {
 struct GiantRowIn {
     uint2 ab;
     vx_contact* cp;
-    alignas(16) vx_contact cc;
+    vx_contact cc;
     RowPrep P;
 };
 
@@ -1964,6 +1964,7 @@ VXD bool clusterStep(const SolveArgs& A, const uint32_t* start, const uint32_t* 
             const uint32_t need0 = (p0 & kWrap) ? (uint32_t)u : (uint32_t)u + 1u;
             const uint32_t need1 = (p1 & kWrap) ? (uint32_t)u : (uint32_t)u + 1u;
             bool ok = true;
+            uint32_t nap = 16;
             for (uint32_t spins = 0;; ++spins) {
                 const uint32_t d0 = p0 == kNoPred ? 0xffffffffu : ldAcquire(done + (p0 & ~kWrap));
                 const uint32_t d1 = p1 == kNoPred ? 0xffffffffu : ldAcquire(done + (p1 & ~kWrap));
@@ -1973,7 +1974,8 @@ VXD bool clusterStep(const SolveArgs& A, const uint32_t* start, const uint32_t* 
                     ok = false;
                     break;
                 }
-                __nanosleep(32);
+                __nanosleep(nap);
+                if (nap < 256u) nap <<= 1;
             }
             if (!ok) { *abortFlag = 1; break; }
         }
@@ -2306,6 +2308,15 @@ VXD uint64_t globalTimerNs() {
 constexpr int kCaWidenLimit = 8;  // replays with a widened marked set before the serial loop
 constexpr int kCaWidenHops = 8;   // hops of widening per replay
 constexpr int kCaInitialHops = 8; // hops of widening before the first pass
+// Workers of the rewind pass: one block of kCaFlowThreads threads per SM, one
+// worker lane per warp. The workers of an SM share its query rate: on a
+// settled 100k-body pile a distance query took 18 us with 1 worker per SM,
+// 31 us with 2, 64 us with 4 and 127 us with 8, at about the same queries per
+// SM per second. The pass is bound by its longest dependency chain, so one
+// fast worker per SM wins (chain 5.0 ms, against 8.1 ms with 2 and 12.1 ms
+// with 8; the work of the pass, 24k evaluations, still fits beside it).
+constexpr int kCaFlowThreads = 32;
+constexpr int kCaFlowBlocksPerSm = 1;
 
 __global__ void __launch_bounds__(256) caFlowKernel(BodyArrays B, Soup soup, const uint64_t* pairKeys,
                                                     const uint32_t* flags, const uint32_t* flagRank,
@@ -2324,18 +2335,25 @@ __global__ void __launch_bounds__(256) caFlowKernel(BodyArrays B, Soup soup, con
             if (t < ncand) __stcg(queue + t, k);
             else atomicOr(&st->spill, 4u);  // pushed twice: inconsistent links
         }
+    // Every root is queued before any worker starts: a count that a finished
+    // candidate has taken to zero must not read as a root.
+    if (!gridSync(&st->bar, &st->timeout)) return;
     if ((threadIdx.x & 31u) != 0u) return;
     uint32_t rewinds = 0, maxDepth = 0, maxCrit = 0;
     for (;;) {
         const uint32_t h = atomicAdd(head, 1u);
         if (h >= ncand) break;
-        uint32_t k, spins = 0;
-        while ((k = __ldcg(queue + h)) == kNoPred) {  // claimed before it was filled
-            if (++spins > kSpinLimit || __ldcg(&st->timeout)) {
+        // Claimed before it was filled. Idle workers back off (up to ~1 us) and
+        // read the shared timeout word only every 16th poll: a thousand warps
+        // polling one L2 line at full rate slow the working lanes' own loads.
+        uint32_t k, spins = 0, nap = 32;
+        while ((k = __ldcg(queue + h)) == kNoPred) {
+            if (++spins > kSpinLimit || ((spins & 15u) == 0u && __ldcg(&st->timeout))) {
                 atomicOr(&st->timeout, 1u);
                 return;
             }
-            __nanosleep(64);
+            __nanosleep(nap);
+            if (nap < 1024u) nap <<= 1;
         }
         __threadfence();  // acquire the predecessors' writes
         const uint64_t t0 = globalTimerNs();
@@ -2785,18 +2803,25 @@ static int narrowPhase(Context& c, const uint64_t* pairs, uint32_t npairs, float
 // Groups the m contacts of `cs` into islands, colours them and builds the
 // solve order (island, colour, contact order) plus per-island body lists.
 // Cooperative launch of `kernel` with as many blocks as fit on the device at
-// once. VXB_ERR_UNSUPPORTED (nothing recorded) when the device cannot run it:
-// callers then take their serial path.
+// once (at most maxPerSm per SM when maxPerSm > 0). VXB_ERR_UNSUPPORTED
+// (nothing recorded) when the device cannot run it: callers then take their
+// serial path.
 template <class Kernel, class... Args>
-static int launchCooperative(Context& c, Kernel kernel, int threads, Args... args) {
+static int launchCooperativeCapped(Context& c, int maxPerSm, Kernel kernel, int threads, Args... args) {
     int perSm = 0;
     cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kernel, threads, 0);
     if (e != cudaSuccess) return cudaStatus(c, e, "cooperative occupancy");
     if (perSm <= 0 || !c.cooperative) return VXB_ERR_UNSUPPORTED;
+    if (maxPerSm > 0 && perSm > maxPerSm) perSm = maxPerSm;
     void* params[] = {&args...};
     e = cudaLaunchCooperativeKernel((const void*)kernel, dim3(perSm * c.smCount), dim3(threads), params, 0, c.stream);
     ++c.launches;
     return cudaStatus(c, e, "cudaLaunchCooperativeKernel");
+}
+
+template <class Kernel, class... Args>
+static int launchCooperative(Context& c, Kernel kernel, int threads, Args... args) {
+    return launchCooperativeCapped(c, 0, kernel, threads, args...);
 }
 
 // Colours of the islands above kSerialColorLimit contacts (colorOf, colour
@@ -3254,11 +3279,12 @@ static int conservativeAdvancement(Context& c, uint32_t npairs, float dt) {
         }
         VXB_CUDA(c, cudaMemsetAsync(queue, 0xff, (size_t)ncand * 4, c.stream));
         VXB_CUDA(c, cudaMemsetAsync(st, 0, sizeof(CoopState), c.stream));
-        const int rc = launchCooperative(c, caFlowKernel, 256, c.B, soupOf(c), pk, (const uint32_t*)flags,
-                                         (const uint32_t*)flagRank, (const float4*)specState,
-                                         (const uint32_t*)specResult, (const uint32_t*)candIndex, ncand,
-                                         (const uint32_t*)succ, pending, queue, depth, crit,
-                                         (const uint32_t*)bodyMark, rewound, dt, prevPos, prevRot, c.dCounters, st);
+        const int rc = launchCooperativeCapped(c, kCaFlowBlocksPerSm, caFlowKernel, kCaFlowThreads, c.B, soupOf(c), pk,
+                                               (const uint32_t*)flags, (const uint32_t*)flagRank,
+                                               (const float4*)specState, (const uint32_t*)specResult,
+                                               (const uint32_t*)candIndex, ncand, (const uint32_t*)succ, pending,
+                                               queue, depth, crit, (const uint32_t*)bodyMark, rewound, dt, prevPos,
+                                               prevRot, c.dCounters, st);
         if (rc == VXB_ERR_UNSUPPORTED) { serial = true; break; }
         VXB_TRY(rc);
         CoopState host;
