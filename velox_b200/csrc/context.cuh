@@ -175,6 +175,7 @@ struct Context {
     DevBuf clusterInfoBuf, clusterKeyBuf, clusterValBuf, clusterOfBuf, clusterCountBuf, clusterStartBuf,
         clusterRowsBuf;                 // spatial clusters of a giant island
     DevBuf clusterLinkBuf;              // cross-cluster predecessor links + remote-successor flags
+    DevBuf caInfoBuf;                   // rewind pass: one record per candidate
 
     DevBuf countersBuf;
     Counters* dCounters = nullptr;

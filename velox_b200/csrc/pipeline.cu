@@ -2273,15 +2273,19 @@ __device__ __noinline__ bool caRewind(BodyArrays& B, const Soup& soup, uint32_t 
 // Every flagged pair evaluated in parallel on the probe's state (read-only):
 // in the ordered pass, a flagged pair whose bodies no earlier rewind has moved
 // sees exactly this state, so its outcome can be taken from here.
-// `spread`: threads per pair (one works), so that a few pairs still occupy
-// many SMs and share warps with few others (each is a long serial loop).
+// `spread` (1, 2, 4 or 8): threads per pair, so that a few pairs still
+// occupy many SMs and share warps with few others (each is a long serial
+// loop). The working lanes are the first 32 / spread of each warp: local
+// memory interleaves the lanes' words, so contiguous lanes share L1 sectors
+// of their stack frames (lanes 0-7 use one sector of every line).
 __global__ void caSpeculateKernel(BodyArrays B, Soup soup, const uint64_t* pairKeys, const uint32_t* flaggedList,
                                   uint32_t flagged, uint32_t spread, const float4* endGap, float dt,
                                   const float4* prevPos, const float4* prevRot, float4* specState,
                                   uint32_t* specResult, Counters* C) {
-    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
-    if (tid % spread) return;
-    for (uint32_t k = tid / spread; k < flagged; k += gridDim.x * blockDim.x / spread) {
+    const uint32_t perWarp = 32u / spread, lane = threadIdx.x & 31u;
+    if (lane >= perWarp) return;
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, warps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t k = warp * perWarp + lane; k < flagged; k += warps * perWarp) {
         const uint32_t r = flaggedList[k];
         uint32_t i, j;
         orientPair(B, pairKeys[r], i, j);
@@ -2318,10 +2322,9 @@ constexpr int kCaInitialHops = 8; // hops of widening before the first pass
 constexpr int kCaFlowThreads = 32;
 constexpr int kCaFlowBlocksPerSm = 1;
 
-__global__ void __launch_bounds__(256) caFlowKernel(BodyArrays B, Soup soup, const uint64_t* pairKeys,
-                                                    const uint32_t* flags, const uint32_t* flagRank,
+__global__ void __launch_bounds__(256) caFlowKernel(BodyArrays B, Soup soup, const uint32_t* flagRank,
                                                     const float4* specState, const uint32_t* specResult,
-                                                    const uint32_t* cand, uint32_t ncand, const uint32_t* succ,
+                                                    const uint4* info, uint32_t ncand, const uint32_t* succ,
                                                     uint32_t* pending, uint32_t* queue, uint32_t* depth,
                                                     uint32_t* crit, const uint32_t* bodyMark, uint32_t* rewound,
                                                     float dt, const float4* prevPos, const float4* prevRot,
@@ -2357,21 +2360,24 @@ __global__ void __launch_bounds__(256) caFlowKernel(BodyArrays B, Soup soup, con
         }
         __threadfence();  // acquire the predecessors' writes
         const uint64_t t0 = globalTimerNs();
-        const uint32_t r = cand[k];
-        const uint64_t key = pairKeys[r];
-        const uint32_t ri = (uint32_t)(key >> 32), rj = (uint32_t)key;
-        const bool touched = __ldcg(rewound + ri) || __ldcg(rewound + rj);
-        if (flags[r] || touched) {
-            uint32_t i, j;
-            orientPair(B, key, i, j);
+        // record, successors and chain statistics in one round of loads (the
+        // predecessors raised depth and crit before they released this one)
+        const uint4 rec = info[k];
+        const uint2 next = reinterpret_cast<const uint2*>(succ)[k];
+        const uint32_t d = __ldcg(depth + k) + 1u;
+        const uint32_t crit0 = __ldcg(crit + k);
+        const uint32_t i = rec.y, j = rec.z;
+        const bool jDyn = (rec.w & 2u) != 0u;
+        const bool touched = __ldcg(rewound + i) || __ldcg(rewound + j);
+        if ((rec.w & 1u) || touched) {
             bool rewoundPair;
             if (!touched) {  // flagged, bodies as the probe saw them: the speculative outcome holds
-                const uint32_t sk = flagRank[r];
+                const uint32_t sk = flagRank[rec.x];
                 rewoundPair = specResult[sk] != 0u;
                 if (rewoundPair) {
                     const float4* st4 = specState + 8 * (size_t)sk;
                     __stcg(B.pos + i, st4[0]); __stcg(B.rot + i, st4[1]); __stcg(B.vel + i, st4[2]); __stcg(B.ang + i, st4[3]);
-                    if (isDynamic(B.filt[j].x)) {
+                    if (jDyn) {
                         __stcg(B.pos + j, st4[4]); __stcg(B.rot + j, st4[5]); __stcg(B.vel + j, st4[6]);
                         __stcg(B.ang + j, st4[7]);
                     }
@@ -2381,26 +2387,40 @@ __global__ void __launch_bounds__(256) caFlowKernel(BodyArrays B, Soup soup, con
             }
             if (rewoundPair) {
                 ++rewinds;
-                const bool jDyn = isDynamic(B.filt[j].x);
                 __stcg(rewound + i, 1u);
                 if (jDyn) __stcg(rewound + j, 1u);
                 if (!bodyMark[i] || (jDyn && !bodyMark[j])) atomicOr(&C->caOverflow, 1u);
             }
         }
-        const uint32_t d = __ldcg(depth + k) + 1u;
         const uint64_t elapsed = globalTimerNs() - t0;
-        const uint32_t ck = __ldcg(crit + k) + (uint32_t)(elapsed < 0x7fffffffull ? elapsed : 0x7fffffffull);
+        const uint32_t ck = crit0 + (uint32_t)(elapsed < 0x7fffffffull ? elapsed : 0x7fffffffull);
         maxDepth = max(maxDepth, d);
         maxCrit = max(maxCrit, ck);
         __threadfence();  // release this evaluation's writes before the successors can run
-        for (int side = 0; side < 2; ++side) {
-            const uint32_t sk = succ[2 * k + side];
-            if (sk == kNoPred) continue;
-            atomicMax(depth + sk, d);
-            atomicMax(crit + sk, ck);
-            if (atomicSub(pending + sk, 1u) == 1u) {
-                const uint32_t t = atomicAdd(tail, 1u);
-                if (t < ncand) __stcg(queue + t, sk);
+        // both successors' counts drop in one round; a count that reaches
+        // zero queues its candidate (the same one twice only if it follows
+        // this one on both bodies, and then only the second drop reaches zero)
+        uint32_t left0 = 0u, left1 = 0u;
+        if (next.x != kNoPred) {
+            atomicMax(depth + next.x, d);
+            atomicMax(crit + next.x, ck);
+            left0 = atomicSub(pending + next.x, 1u);
+        }
+        if (next.y != kNoPred) {
+            atomicMax(depth + next.y, d);
+            atomicMax(crit + next.y, ck);
+            left1 = atomicSub(pending + next.y, 1u);
+        }
+        const uint32_t ready = (left0 == 1u ? 1u : 0u) + (left1 == 1u ? 1u : 0u);
+        if (ready) {
+            uint32_t t = atomicAdd(tail, ready);
+            if (left0 == 1u) {
+                if (t < ncand) __stcg(queue + t, next.x);
+                else atomicOr(&st->spill, 4u);
+                ++t;
+            }
+            if (left1 == 1u) {
+                if (t < ncand) __stcg(queue + t, next.y);
                 else atomicOr(&st->spill, 4u);
             }
         }
@@ -2411,15 +2431,21 @@ __global__ void __launch_bounds__(256) caFlowKernel(BodyArrays B, Soup soup, con
 }
 
 // Entries (dynamic body, 2k + side) of the candidates; other endpoints sort last.
+// Also the candidate's record for the pass: (pair, oriented bodies i and j,
+// bit 0 flagged by the probe | bit 1 j dynamic), one load for the worker.
 __global__ void caEntryKernel(const BodyArrays B, const uint64_t* pairKeys, const uint32_t* cand, uint32_t ncand,
-                              uint32_t n, uint64_t* keys, uint32_t* vals) {
+                              uint32_t n, const uint32_t* flags, uint64_t* keys, uint32_t* vals, uint4* info) {
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < ncand; k += gridDim.x * blockDim.x) {
-        const uint64_t key = pairKeys[cand[k]];
+        const uint32_t r = cand[k];
+        const uint64_t key = pairKeys[r];
         const uint32_t a = (uint32_t)(key >> 32), b = (uint32_t)key;
         keys[2 * k] = isDynamic(B.filt[a].x) ? a : n;
         keys[2 * k + 1] = isDynamic(B.filt[b].x) ? b : n;
         vals[2 * k] = 2 * k;
         vals[2 * k + 1] = 2 * k + 1;
+        uint32_t i, j;
+        orientPair(B, key, i, j);
+        info[k] = make_uint4(r, i, j, (flags[r] ? 1u : 0u) | (isDynamic(B.filt[j].x) ? 2u : 0u));
     }
 }
 
@@ -3267,7 +3293,10 @@ static int conservativeAdvancement(Context& c, uint32_t npairs, float dt) {
         VXB_TRY(ensure(c, c.islandInfoBuf, valsOffset + (size_t)ncand * 8 + 16));
         uint64_t* ekeys = P<uint64_t>(c.islandInfoBuf);
         uint32_t* evals = reinterpret_cast<uint32_t*>(P<char>(c.islandInfoBuf) + valsOffset);
-        LAUNCH(c, caEntryKernel, blocksFor(ncand, 256), 256, c.B, pk, candIndex, ncand, n, ekeys, evals);
+        VXB_TRY(ensure(c, c.caInfoBuf, (size_t)ncand * 16 + 64));
+        uint4* info = P<uint4>(c.caInfoBuf);
+        LAUNCH(c, caEntryKernel, blocksFor(ncand, 256), 256, c.B, pk, (const uint32_t*)candIndex, ncand, n,
+               (const uint32_t*)flags, ekeys, evals, info);
         VXB_TRY(sortPairs(c, ekeys, evals, 2 * ncand, bitsFor(n)));
         VXB_CUDA(c, cudaMemsetAsync(pending, 0, (size_t)ncand * 4, c.stream));
         VXB_CUDA(c, cudaMemsetAsync(depth, 0, (size_t)ncand * 4, c.stream));
@@ -3279,12 +3308,12 @@ static int conservativeAdvancement(Context& c, uint32_t npairs, float dt) {
         }
         VXB_CUDA(c, cudaMemsetAsync(queue, 0xff, (size_t)ncand * 4, c.stream));
         VXB_CUDA(c, cudaMemsetAsync(st, 0, sizeof(CoopState), c.stream));
-        const int rc = launchCooperativeCapped(c, kCaFlowBlocksPerSm, caFlowKernel, kCaFlowThreads, c.B, soupOf(c), pk,
-                                               (const uint32_t*)flags, (const uint32_t*)flagRank,
-                                               (const float4*)specState, (const uint32_t*)specResult,
-                                               (const uint32_t*)candIndex, ncand, (const uint32_t*)succ, pending,
-                                               queue, depth, crit, (const uint32_t*)bodyMark, rewound, dt, prevPos,
-                                               prevRot, c.dCounters, st);
+        const int rc = launchCooperativeCapped(c, kCaFlowBlocksPerSm, caFlowKernel, kCaFlowThreads, c.B, soupOf(c),
+                                               (const uint32_t*)flagRank, (const float4*)specState,
+                                               (const uint32_t*)specResult, (const uint4*)info, ncand,
+                                               (const uint32_t*)succ, pending, queue, depth, crit,
+                                               (const uint32_t*)bodyMark, rewound, dt, prevPos, prevRot, c.dCounters,
+                                               st);
         if (rc == VXB_ERR_UNSUPPORTED) { serial = true; break; }
         VXB_TRY(rc);
         CoopState host;
