@@ -184,15 +184,14 @@ def run_batched(args):
     data-path collective)."""
     import torch
     import velox_b200 as vb
+    from velox_b200.ranks import max_over_ranks, shard_specs
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     nworlds = args.size if args.size != 100000 else 4096
     specs, pool = vb.generate_scene(BATCH_CONFIG, seed=BATCH_CONFIG, size=nworlds)
-    lo, hi = nworlds * rank // world, nworlds * (rank + 1) // world
-    mine = specs[(specs["world"] >= lo) & (specs["world"] < hi)].copy()
-    mine["world"] -= lo
+    mine, lo, hi = shard_specs(specs, nworlds, rank, world)
     if args.impl == "reference":
         if rank != 0:
             return 0
@@ -255,10 +254,7 @@ def run_batched(args):
     stage = ctx.stage_times()
     last = ctx.stats()
     ctx.close()
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, dist, "cuda")
     value = nworlds * args.steps / (ms / 1e3)
 
     # e2e: a fresh batched world through the C ABI with host buffers every step
@@ -273,10 +269,7 @@ def run_batched(args):
     barrier()
     e2e_ms = timed(ctx, args.steps, (forces.numpy(), poses.numpy()))
     ctx.close()
-    if dist:
-        t = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(e2e_ms, dist, "cuda")
 
     # plain: sampled worlds one per context, scaled by their body share
     plain = None
@@ -394,6 +387,7 @@ def main():
 
     import torch
     import velox_b200 as vb
+    from velox_b200.ranks import max_over_ranks
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -455,10 +449,7 @@ def main():
     stage = ctx.stage_times()
     ctx.enable_timing(False)
     ms = sum(a.elapsed_time(b) for a, b in events)
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, dist, "cuda")
     value = world * n * args.steps / (ms / 1e3)
 
     # Roofline. Island solve: memory-bound sweeps over contact rows.
@@ -512,10 +503,7 @@ def main():
     wall = time.perf_counter() - t0
     ctx2.close()
     e2e_ms = e0.elapsed_time(e1)
-    if dist:
-        t = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(e2e_ms, dist, "cuda")
     e2e = {"value": world * n * args.steps / (e2e_ms / 1e3), "unit": "body-steps/s",
            "h2d_bytes_per_step": int(forces.numel() * 4), "d2h_bytes_per_step": int(poses.numel() * 4),
            "steps": args.steps, "wall_s": wall}
