@@ -81,3 +81,49 @@ def test_oracle_warm_start_match_semantics(ref):
     cur3["point"][:, 1] += 10.0
     out3, warm3 = ref.oracle_warm_start(cur3, prev)
     assert warm3 == 0 and np.all(out3["normalImpulse"] == 0)
+
+
+def test_oracle_pairs_on_empty_and_single_body_inputs(ref):
+    w, specs, pool, bodies, soup = reference_scene(ref, "dense", 200)
+    plane = bodies[bodies["shape"] == 1]
+    one = bodies[bodies["shape"] != 1][:1]
+    for b in (bodies[:0], plane, one, np.concatenate([plane, one])):
+        b = np.ascontiguousarray(b)
+        mine, theirs = ref.oracle_pairs(b, DT), ref.candidate_pairs(b, DT)
+        assert np.array_equal(mine, theirs)
+    # one body resting on the plane pairs with it
+    assert len(ref.candidate_pairs(np.ascontiguousarray(np.concatenate([plane, one])), DT)) <= 1
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_oracle_pairs_under_filters_static_and_sleeping_bodies(ref, seed):
+    # collision groups, category/mask bits, static and sleeping bodies: the
+    # pair filter (Body::canCollideWith and the inert-pair rule) on both sides
+    w, specs, pool, bodies, soup = reference_scene(ref, "dense", 800)
+    rng = np.random.default_rng(seed)
+    b = bodies.copy()
+    dyn = np.flatnonzero(b["shape"] != 1)
+    b["groupIndex"][dyn] = rng.choice([0, 0, 0, 1, -1, 2, -2], len(dyn))
+    b["categoryBits"][dyn] = rng.choice([1, 2, 4, 0xffff], len(dyn))
+    b["maskBits"][dyn] = rng.choice([0xffff, 0xffff, 1 | 4, 2, 0], len(dyn))
+    b["motionType"][rng.choice(dyn, len(dyn) // 10, replace=False)] = 0  # static
+    b["asleep"][rng.choice(dyn, len(dyn) // 10, replace=False)] = 1
+    mine, theirs = ref.oracle_pairs(b, DT), ref.candidate_pairs(b, DT)
+    assert len(theirs) > 0 and np.array_equal(mine, theirs)
+    assert len(theirs) < len(ref.candidate_pairs(bodies, DT))  # the filters removed pairs
+
+
+def test_oracle_coloring_with_static_endpoints(ref):
+    # contacts against static bodies do not constrain colours; the restatement
+    # and the reference agree on which endpoints count
+    w, specs, pool, bodies, soup = reference_scene(ref, "dense", 1200)
+    contacts, _ = ref.collide_pairs(bodies, soup, ref.candidate_pairs(bodies, DT), DT)
+    contacts = ref.sort_contacts(contacts)
+    b = bodies.copy()
+    dyn = np.flatnonzero(b["shape"] != 1)
+    b["motionType"][np.random.default_rng(3).choice(dyn, len(dyn) // 4, replace=False)] = 0
+    c1, n1 = ref.oracle_color(b, contacts)
+    c2, n2 = ref.color_contacts(b, contacts)
+    assert n1 == n2 and np.array_equal(c1, c2)
+    full, nfull = ref.color_contacts(bodies, contacts)
+    assert n2 <= nfull
