@@ -118,3 +118,27 @@ def test_coloring_past_64_colours_in_a_large_island(ctx, ref):
     assert len(contacts) > 4096 and tn > 64
     assert mn == tn
     assert np.array_equal(mine, theirs)
+
+
+@pytest.mark.parametrize("seed", [0, 1])
+def test_pairs_and_colours_under_filters_static_and_sleeping_bodies(ctx, ref, seed):
+    # collision groups, category/mask bits, static and sleeping bodies: the
+    # device pair filter and the colouring's endpoints against the reference
+    w, specs, pool, bodies, soup = reference_scene(ref, "dense", 800)
+    rng = np.random.default_rng(seed)
+    b = bodies.copy()
+    dyn = np.flatnonzero(b["shape"] != 1)
+    b["groupIndex"][dyn] = rng.choice([0, 0, 0, 1, -1, 2, -2], len(dyn))
+    b["categoryBits"][dyn] = rng.choice([1, 2, 4, 0xffff], len(dyn))
+    b["maskBits"][dyn] = rng.choice([0xffff, 0xffff, 1 | 4, 2, 0], len(dyn))
+    b["motionType"][rng.choice(dyn, len(dyn) // 10, replace=False)] = 0  # static
+    b["asleep"][rng.choice(dyn, len(dyn) // 10, replace=False)] = 1
+    theirs = ref.candidate_pairs(b, DT)
+    assert len(theirs) > 0
+    assert np.array_equal(ctx.pairs(b, DT), theirs)
+    contacts, _ = ref.collide_pairs(b, soup, theirs, DT)
+    contacts = ref.sort_contacts(contacts)
+    tc, tn = ref.color_contacts(b, contacts)
+    mc, mn = ctx.color(b, contacts)
+    assert len(contacts) > 0 and mn == tn
+    assert np.array_equal(mc, tc)
