@@ -2306,19 +2306,22 @@ VXD uint64_t globalTimerNs() {
 // exactly as the reference's single ordered loop would evaluate it: it sees
 // the same body states and rewound marks, as long as no rewind moves a body
 // outside the marked set (that case is flagged; the caller widens the set and
-// replays the pass from a snapshot). One worker per warp (lane 0) takes ready
+// replays the pass from a snapshot). Workers (lane 0 of a warp) take ready
 // candidates from a queue, so independent chains never wait for one another.
 // Cooperative launch (all workers resident); every wait is bounded.
 constexpr int kCaWidenLimit = 8;  // replays with a widened marked set before the serial loop
 constexpr int kCaWidenHops = 8;   // hops of widening per replay
 constexpr int kCaInitialHops = 8; // hops of widening before the first pass
 // Workers of the rewind pass: one block of kCaFlowThreads threads per SM, one
-// worker lane per warp. The workers of an SM share its query rate: on a
-// settled 100k-body pile a distance query took 18 us with 1 worker per SM,
-// 31 us with 2, 64 us with 4 and 127 us with 8, at about the same queries per
-// SM per second. The pass is bound by its longest dependency chain, so one
-// fast worker per SM wins (chain 5.0 ms, against 8.1 ms with 2 and 12.1 ms
-// with 8; the work of the pass, 24k evaluations, still fits beside it).
+// worker lane per warp. A worker's distance queries keep a stack frame of
+// about 10 KB (simplex, EPA polytope) in local memory, where one active lane
+// takes a 32-byte L1 sector per 4-byte word: several workers on an SM evict
+// one another's frames. On a settled 100k-body pile a distance query took
+// 18 us with 1 worker per SM, 31 us with 2, 64 us with 4 and 127 us with 8,
+// at about the same queries per SM per second. The pass is bound by its
+// longest dependency chain, so one fast worker per SM wins (chain 5.0 ms,
+// against 8.1 ms with 2 and 12.1 ms with 8; the pass's 24k evaluations still
+// fit beside it).
 constexpr int kCaFlowThreads = 32;
 constexpr int kCaFlowBlocksPerSm = 1;
 
