@@ -124,27 +124,53 @@ def cpu_baseline(specs, pool, n_bodies, checkpoints, total_steps):
         w.step(DT, 1)
         est += (w.step(DT, 1) / 1000.0) * (total_steps / len(checkpoints))
     spent = time.perf_counter() - t0
+    single = one_worker_sample(w, n_bodies, budget_s=10.0, max_steps=2)
     w.close()
     value = n_bodies * total_steps / est
     return {"value": value, "unit": "body-steps/s", "cores": workers, "kind": "reference",
+            "single_worker": single,
             "sample": f"{len(checkpoints)} timed steps of the {n_bodies}-body scene, one from each of "
                       f"{len(checkpoints)} evenly spaced states of the {total_steps}-step device trajectory "
                       f"(each after one settling step), weighted equally; reference CPU backend (Release "
                       f"build), {workers} worker threads on {os.cpu_count()} host cores; {spent:.1f} s"}
 
 
+def single_config(n, world):
+    """The workload description both arms print (identical for the same N)."""
+    return {"workload": f"mixed-shape scene, {n} bodies (1 plane), dt 1/60 s, {SUBSTEPS} substeps",
+            "bodies": n, "parallelism": f"replicas x{world}",
+            "l2": "flushed (256 MiB write) before every timed step, outside the step's events"}
+
+
+def one_worker_sample(w, n, budget_s=20.0, max_steps=3):
+    """The reference CPU backend with setWorkerCount(1) on the world's current
+    state: up to `max_steps` steps within `budget_s`."""
+    w.configure(substeps=SUBSTEPS, workers=1)
+    steps, total = 0, 0.0
+    while steps < max_steps and total < budget_s:
+        total += w.step(DT, 1) / 1000.0
+        steps += 1
+    return {"value": n * steps / total, "unit": "body-steps/s", "cores": 1, "kind": "reference",
+            "sample": f"{steps} steps continuing the same trajectory, reference CPU backend (Release build), "
+                      f"setWorkerCount(1)"}
+
+
 def run_reference(args):
+    """The reference CPU backend (built from its sources into oracle/_ref) on
+    the same scene. The scene specs come from the generator compiled into that
+    build, so this process loads no library of this package."""
     rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
         return 0
-    specs, pool, bodies, soup = build_scene(args.size)
-    n = len(bodies)
     budget = float(os.environ.get("VXB_REFERENCE_BUDGET_S", "240"))
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import ref
     if not ref.available(strict=False):
         print(json.dumps({"impl": "reference", "unavailable": "reference CPU build (oracle/_ref) missing"}))
         return 0
+    specs, pool = ref.generate_scene(CONFIG, seed=CONFIG, size=args.size)
+    n = len(specs)
     w = ref.RefWorld(specs, pool, backend=ref.BACKEND_CPU, strict=False)
     w.configure(substeps=SUBSTEPS, workers=0)
     workers = int(w.L.ref_world_worker_count(w.h))
@@ -153,17 +179,18 @@ def run_reference(args):
     while steps < args.steps and total < budget:
         total += w.step(DT, 1) / 1000.0
         steps += 1
+    single = one_worker_sample(w, n)
     w.close()
     value = n * steps / total
     sample = (f"{steps} of {args.steps} requested steps (time budget {budget:.0f} s) of the {n}-body scene after "
-              f"{args.warmup} warm-up steps; reference CPU backend (Release build), {workers} worker threads")
+              f"{args.warmup} warm-up steps; reference CPU backend (Release build), {workers} worker threads on "
+              f"{os.cpu_count()} host cores")
     line = {"metric": METRIC, "value": value, "unit": "body-steps/s", "impl": "reference", "n_gpus": 0,
             "steps": steps, "warmup": args.warmup, "ms_per_step": total / steps * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
-            "config": {"workload": f"mixed-shape scene, {n} bodies (1 plane), dt 1/60 s, {SUBSTEPS} substeps",
-                       "bodies": n},
+            "config": single_config(n, world),
             "cpu_baseline": {"value": value, "unit": "body-steps/s", "cores": workers, "kind": "reference",
-                             "sample": sample},
+                             "sample": sample, "single_worker": single},
             "e2e": {"value": value, "unit": "body-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
@@ -182,20 +209,26 @@ def run_batched(args):
     share of the batch) and the reference CPU backend on a sample of worlds.
     Under torchrun the worlds are split across ranks (strong scaling, no
     data-path collective)."""
-    import torch
-    import velox_b200 as vb
-    from velox_b200.ranks import max_over_ranks, shard_specs
-
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     nworlds = args.size if args.size != 100000 else 4096
-    specs, pool = vb.generate_scene(BATCH_CONFIG, seed=BATCH_CONFIG, size=nworlds)
-    mine, lo, hi = shard_specs(specs, nworlds, rank, world)
     if args.impl == "reference":
         if rank != 0:
             return 0
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import ref
+        if not ref.available(strict=False):
+            print(json.dumps({"impl": "reference", "unavailable": "reference CPU build (oracle/_ref) missing"}))
+            return 0
+        specs, pool = ref.generate_scene(BATCH_CONFIG, seed=BATCH_CONFIG, size=nworlds)
         return run_batched_reference(args, specs, pool, nworlds)
+    import torch
+    import velox_b200 as vb
+    from velox_b200.ranks import max_over_ranks, shard_specs
+
+    specs, pool = vb.generate_scene(BATCH_CONFIG, seed=BATCH_CONFIG, size=nworlds)
+    mine, lo, hi = shard_specs(specs, nworlds, rank, world)
     torch.cuda.set_device(local)
     dist = None
     if world > 1:
@@ -524,9 +557,7 @@ def main():
     line = {"metric": METRIC, "value": value, "unit": "body-steps/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
-            "config": {"workload": f"mixed-shape scene, {n} bodies (1 plane), dt 1/60 s, {SUBSTEPS} substeps",
-                       "bodies": n, "parallelism": f"replicas x{world}",
-                       "l2": "flushed (256 MiB write) before every timed step, outside the step's events"},
+            "config": single_config(n, world),
             "contacts_per_s": contacts_total / (ms / 1e3), "last_step": stats,
             "stage_ms_per_step": {k: v[0] / args.steps for k, v in stage.items()},
             "roofline": roofline, "solve_roofline": solve_roofline, "rewind_roofline": rewind_roofline,

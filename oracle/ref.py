@@ -71,6 +71,8 @@ def lib(strict=True):
         "ref_solve_sequence": ([vp, vp, u32, f32, vp, i32, i32], None),
         "ref_integrate_velocities": ([vp, u32, f32, f32, f32, f32], None),
         "ref_integrate_transforms": ([vp, u32, f32], None),
+        "ref_scene_generate": ([i32, ctypes.c_uint64, u32, vp, u32, ctypes.POINTER(u32), vp, u32,
+                                ctypes.POINTER(u32)], i32),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -82,6 +84,25 @@ def lib(strict=True):
 
 def _p(a):
     return ctypes.c_void_p(a.ctypes.data) if a is not None and a.size else ctypes.c_void_p(0)
+
+
+def generate_scene(config, seed=None, size=0, strict=False):
+    """Specs + hull point pool of a benchmark workload, from the scene
+    generator compiled into the reference build (the same source and seeds as
+    the library's vxb_scene_generate). A process that only times the reference
+    builds its scene through this and loads no library of this package."""
+    from velox_b200.binding import SPEC  # record layout only (no library load)
+    L = lib(strict)
+    seed = config if seed is None else seed
+    count, npool = ctypes.c_uint32(), ctypes.c_uint32()
+    if L.ref_scene_generate(config, seed, size, None, 0, ctypes.byref(count), None, 0, ctypes.byref(npool)) != 0:
+        raise RuntimeError("scene generation failed")
+    specs = np.zeros(count.value, SPEC)
+    pts = np.zeros((max(npool.value, 1), 3), np.float32)
+    if L.ref_scene_generate(config, seed, size, _p(specs), count.value, ctypes.byref(count), _p(pts), npool.value,
+                            ctypes.byref(npool)) != 0:
+        raise RuntimeError("scene generation failed")
+    return specs, pts[:npool.value]
 
 
 class RefWorld:
