@@ -93,6 +93,15 @@ const char* vxb_context_last_error(const vxb_context* ctx);
 int vxb_context_set_stream(vxb_context* ctx, void* stream);
 /* Number of kernel launches this context issued since it was created. */
 uint64_t vxb_context_launch_count(const vxb_context* ctx);
+/* Polls after which any device-side wait of this context (grid barriers,
+ * dataflow waits of the cooperative solve and rewind kernels) gives up; the
+ * call then fails with VXB_ERR_TIMEOUT and the context stays usable. 0
+ * restores the default (2^24 polls of at least 32 ns, over a second). The
+ * environment variable VXB_WAIT_LIMIT sets it for contexts created after it.
+ * No counterpart in the reference (its CUDA backend has no device-side
+ * waits); it exists to bound and test the recovery path of
+ * src/world.cpp:3807-3828. */
+int vxb_context_set_wait_limit(vxb_context* ctx, uint32_t polls);
 
 /* Per-stage device timing with CUDA events recorded on the context's stream
  * (stages: 0 prepare, 1 broad phase, 2 cell-key sort, 3 narrow phase,
@@ -106,7 +115,10 @@ int vxb_context_stage_times(vxb_context* ctx, double* ms, uint64_t* calls, uint3
 /* ---- Backend interface over host arrays ------------------------------- */
 
 /* Backend::integrate (backend.h:116; CudaBackend::integrate,
- * src/backend_cuda.cu:393-403): first-substep velocity integration. */
+ * src/backend_cuda.cu:393-403): first-substep velocity integration. Honours
+ * the reference's test injection VELOX_CUDA_TEST_FAIL=oom|device-loss
+ * (src/backend_cuda.cu:69-78): VXB_ERR_OOM / VXB_ERR_DEVICE_LOST before any
+ * device work. */
 int vxb_backend_integrate(vxb_context* ctx, vx_body* bodies, uint32_t n, vx_vec3 gravity,
                           float dt);
 /* Backend::findContacts (backend.h:125-127; src/backend_cuda.cu:405-567):
@@ -186,14 +198,19 @@ int vxb_stage_color(vxb_context* ctx, const vx_body* bodies, uint32_t n,
  * nearly full device). No counterpart in the reference: it exists for such
  * callers only. Needs no context. All device memory it uses is one
  * library-owned array of about 4.3 MB, held on every device that loads the
- * library until exit; the call allocates nothing (device or host heap).
+ * library until exit; after the first call on a device the call allocates
+ * nothing (device or host heap). The first call on a device is its set-up: it
+ * resolves the array's device address and loads the kernels it launches
+ * (with CUDA's lazy module loading, loading may allocate device memory); make
+ * that first call before any stream capture. After a device reset do not call
+ * it again on that device.
  * Limits: n <= 4096 bodies, <= 32768 body-body and <= 8192 body-plane pairs;
  * beyond them it returns VXB_ERR_CAPACITY (*count still reports the pairs
- * found when the body limit was met). The first call on a device resolves
- * the array's device address; make that first call before any stream
- * capture. Every call shares the array, so calls that overlap on the GPU
- * (other threads or streams) race. Works on the current device and `stream`
- * (null = the default stream); returns after the pairs are in `out`. */
+ * found when the body limit was met; when only `cap` is too small, *count is
+ * the number of pairs, so a retry with cap = *count succeeds). Every call
+ * shares the array, so calls that overlap on the GPU (other threads or
+ * streams) race. Works on the current device and `stream` (null = the
+ * default stream); returns after the pairs are in `out`. */
 int vxb_stage_pairs_noalloc(const vx_body* bodies, uint32_t n, float dt, uint64_t* out, uint32_t cap,
                             uint32_t* count, void* stream);
 

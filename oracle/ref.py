@@ -15,6 +15,8 @@ STRICT = os.path.join(REF_DIR, "libvelox_ref_strict.so")
 FAST = os.path.join(REF_DIR, "libvelox_ref_fast.so")
 # The reference engine whose CUDA backend is velox_b200/dropin/b200_backend.cpp.
 DROPIN = os.path.join(REF_DIR, "libvelox_ref_dropin.so")
+# The same engine over a fake of the library's Backend entry points (no GPU).
+DROPIN_FAKE = os.path.join(REF_DIR, "libvelox_ref_dropin_fake.so")
 
 BACKEND_CPU = 1
 BACKEND_CUDA_EMULATED = 2
@@ -23,6 +25,8 @@ BACKEND_CUDA_EMULATED = 2
 def _path(strict):
     if strict == "dropin":
         return DROPIN
+    if strict == "dropin_fake":
+        return DROPIN_FAKE
     return STRICT if strict else FAST
 
 

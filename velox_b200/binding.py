@@ -158,6 +158,7 @@ def lib(path=LIB_PATH):
         "vxb_context_last_error": ([vp], ctypes.c_char_p),
         "vxb_context_set_stream": ([vp, vp], i32),
         "vxb_context_launch_count": ([vp], ctypes.c_uint64),
+        "vxb_context_set_wait_limit": ([vp, u32], i32),
         "vxb_context_enable_timing": ([vp, i32], i32),
         "vxb_context_stage_times": ([vp, vp, vp, u32], i32),
         "vxb_backend_integrate": ([vp, vp, u32, Vec3, f32], i32),
@@ -263,6 +264,10 @@ class Context:
 
     def _check(self, status):
         check(status, self.h)
+
+    def set_wait_limit(self, polls):
+        """Polls before a device-side wait gives up (0 = the default)."""
+        self._check(self.L.vxb_context_set_wait_limit(self.h, polls))
 
     @property
     def launches(self):

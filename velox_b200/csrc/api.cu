@@ -1,5 +1,6 @@
 // extern "C" entry points (include/velox_b200.h). Every function validates
 // its arguments, never throws, and maps failures to status codes.
+#include <cstdlib>
 #include <cstring>
 #include <new>
 
@@ -31,6 +32,21 @@ int guardContext(vxb_context* ctx) {
         int s_ = (expr);                   \
         if (s_ != VXB_OK) return s_;       \
     } while (0)
+
+// Failure injection for tests, read on every Backend::integrate call (the
+// first backend call of each World::step) like the reference's
+// injectCudaFailureForTesting (src/backend_cuda.cu:69-78, :394):
+// VELOX_CUDA_TEST_FAIL=oom reports an allocation failure, =device-loss a lost
+// device, before any device work. Nothing on the device is touched.
+int injectedFailure(Context& c) {
+    const char* mode = std::getenv("VELOX_CUDA_TEST_FAIL");
+    if (!mode || mode[0] == '\0') return VXB_OK;
+    if (std::strcmp(mode, "oom") == 0)
+        return vxb::fail(c, VXB_ERR_OOM, "test injection: allocation failure");
+    if (std::strcmp(mode, "device-loss") == 0)
+        return vxb::fail(c, VXB_ERR_DEVICE_LOST, "test injection: device loss");
+    return VXB_OK;
+}
 
 int ensureCounters(Context& c) {
     TRY(vxb::ensure(c, c.countersBuf, sizeof(vxb::Counters)));
@@ -73,6 +89,10 @@ int vxb_context_create(int device, vxb_context** out) {
     if (!ctx) return VXB_ERR_OOM;
     Context& c = ctx->impl;
     c.device = device;
+    if (const char* limit = std::getenv("VXB_WAIT_LIMIT")) {  // polls; 0 or unset = the default
+        const unsigned long v = std::strtoul(limit, nullptr, 10);
+        if (v > 0 && v <= vxb::kSpinLimit) c.waitLimit = (uint32_t)v;
+    }
     cudaDeviceGetAttribute(&c.smCount, cudaDevAttrMultiProcessorCount, device);
     cudaDeviceGetAttribute(&c.cooperative, cudaDevAttrCooperativeLaunch, device);
     if (cudaStreamCreateWithFlags(&c.ownStream, cudaStreamNonBlocking) != cudaSuccess) {
@@ -127,6 +147,12 @@ int vxb_context_set_stream(vxb_context* ctx, void* stream) {
 
 uint64_t vxb_context_launch_count(const vxb_context* ctx) { return ctx ? ctx->impl.launches : 0; }
 
+int vxb_context_set_wait_limit(vxb_context* ctx, uint32_t polls) {
+    if (!ctx || polls > vxb::kSpinLimit) return VXB_ERR_INVALID;
+    ctx->impl.waitLimit = polls ? polls : vxb::kSpinLimit;
+    return VXB_OK;
+}
+
 int vxb_context_enable_timing(vxb_context* ctx, int enable) {
     GUARD(ctx);
     Context& c = ctx->impl;
@@ -155,6 +181,7 @@ int vxb_context_stage_times(vxb_context* ctx, double* ms, uint64_t* calls, uint3
 
 int vxb_backend_integrate(vxb_context* ctx, vx_body* bodies, uint32_t n, vx_vec3 gravity, float dt) {
     GUARD(ctx);
+    TRY(injectedFailure(ctx->impl));
     if (n == 0) return VXB_OK;
     if (!bodies) return VXB_ERR_INVALID;
     Context& c = ctx->impl;

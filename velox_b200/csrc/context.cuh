@@ -24,7 +24,7 @@ struct IslandPlan {
     uint32_t freeFrom = 0, freeTo = 0;  // contact-free bodies (range in the island-sorted body order)
 };
 
-// State of one cooperative launch (zeroed before it).
+// State of one cooperative launch (zeroed before it, except spinLimit).
 struct CoopState {
     GridBarrier bar;
     uint32_t changed[3];  // per-round counters, rotated
@@ -32,7 +32,8 @@ struct CoopState {
     uint32_t rounds;      // rounds the kernel ran (or a count the launch returns)
     uint32_t timeout;     // a barrier wait gave up
     uint32_t queued[3];   // per-round work-queue lengths, rotated like changed[]
-    uint32_t pad[5];
+    uint32_t spinLimit;   // polls before any wait of the launch gives up (Context::waitLimit)
+    uint32_t pad[4];
 };
 
 // Grow-only device allocation.
@@ -105,6 +106,7 @@ struct Context {
     bool tinyPacked = false;   // the plan's tiny islands are packed into warps
     uint32_t tinyCount = 0, tinyPackCount = 0;
     uint32_t clusterNB = 0, clusterR = 0, clusterG = 0;  // giant bodies, rows, most colours (clustered solve)
+    uint32_t waitLimit = kSpinLimit;  // polls before a device wait gives up (vxb_context_set_wait_limit)
     cudaStream_t ownStream = nullptr;
     cudaStream_t stream = nullptr;
     std::string lastError;
@@ -207,6 +209,10 @@ int stageResolve(Context& c);
 // Records a failure on the context; returns the mapped status.
 int fail(Context& c, int status, const std::string& message);
 int cudaStatus(Context& c, cudaError_t e, const char* what);
+
+// Zeroes a cooperative launch's state on the context's stream and sets its
+// wait limit to the context's.
+int resetCoop(Context& c, CoopState* st);
 
 // Grow-only device allocation helper; returns VXB_OK or VXB_ERR_OOM.
 int ensure(Context& c, DevBuf& b, size_t bytes);

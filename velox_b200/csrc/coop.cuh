@@ -1,9 +1,10 @@
 // Grid-wide barrier for kernels launched with cudaLaunchCooperativeKernel
 // (all blocks co-resident). Arrival is an atomic counter; the last block to
 // arrive bumps a generation word that the others wait on. Every wait is
-// bounded: after kSpinLimit polls the block records a timeout in *timeout and
-// returns false, so a fault can never turn into a hung GPU; callers stop their
-// work when it returns false and the host reports VXB_ERR_TIMEOUT.
+// bounded: after `limit` polls (kSpinLimit unless the context sets another
+// limit) the block records a timeout in *timeout and returns false, so a fault
+// can never turn into a hung GPU; callers stop their work when it returns
+// false and the host reports VXB_ERR_TIMEOUT.
 #pragma once
 #include <cstdint>
 
@@ -21,7 +22,7 @@ __device__ __forceinline__ unsigned int loadVolatile(const unsigned int* p) {
 }
 
 // Returns false when the wait timed out (in this block or another one).
-__device__ __forceinline__ bool gridSync(GridBarrier* bar, unsigned int* timeout) {
+__device__ __forceinline__ bool gridSync(GridBarrier* bar, unsigned int* timeout, unsigned int limit) {
     __shared__ int ok;
     __syncthreads();
     if (threadIdx.x == 0) ok = loadVolatile(timeout) == 0u;
@@ -38,7 +39,7 @@ __device__ __forceinline__ bool gridSync(GridBarrier* bar, unsigned int* timeout
         } else {
             unsigned int spins = 0;
             while (loadVolatile(&bar->generation) == gen) {
-                if (++spins > kSpinLimit) {
+                if (++spins > limit) {
                     atomicOr(timeout, 1u);
                     ok = 0;
                     break;

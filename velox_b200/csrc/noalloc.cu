@@ -12,7 +12,17 @@
 // 8,192 body-plane pairs per call; larger requests are rejected with
 // VXB_ERR_CAPACITY before any device work. The array (about 4.3 MB) is held
 // on every device that loads the library until the process exits.
+//
+// The first call on a device is its set-up: it resolves the array's device
+// address and loads every kernel the entry point launches. With CUDA's lazy
+// module loading (the default) loading a module allocates device memory, so
+// that first call may allocate; calls after it on the same device do not.
+// Make the first call before any stream capture. A device reset
+// (cudaDeviceReset) discards the loaded module: do not call the entry point
+// on that device again in the same process.
+#include <atomic>
 #include <cstring>
+#include <mutex>
 
 #include "broadphase_kernels.cuh"
 
@@ -54,8 +64,11 @@ static __device__ __align__(256) unsigned char g_noallocScratch[kScratchBytes];
 
 // Device address of g_noallocScratch per device, resolved on the first call
 // made on that device (with it current). In host code the array's name is
-// only a host-side stand-in; kernels must get this address instead.
-unsigned char* g_scratchAddress[kMaxDevices] = {};
+// only a host-side stand-in; kernels must get this address instead. Host
+// threads may make first calls concurrently: the set-up runs under a mutex and
+// publishes the address atomically.
+std::atomic<unsigned char*> g_scratchAddress[kMaxDevices] = {};
+std::mutex g_setupMutex;
 
 // Pair (i, j) compressed to 24 bits for the output sort (i, j < 4096).
 __global__ void packPairKeysKernel(const uint64_t* convex, uint32_t nc, const uint64_t* plane, uint32_t np,
@@ -88,6 +101,31 @@ int cudaToStatus(cudaError_t e) {
         if (s_ != VXB_OK) return s_;                    \
     } while (0)
 
+// Set-up of one device (current): the array's address, and every kernel
+// this entry point launches loaded now rather than at its first launch.
+int setupDevice(int device, unsigned char** base) {
+    std::lock_guard<std::mutex> lock(g_setupMutex);
+    unsigned char* known = g_scratchAddress[device].load(std::memory_order_acquire);
+    if (known) {
+        *base = known;
+        return VXB_OK;
+    }
+    void* address = nullptr;
+    NA_CUDA(cudaGetSymbolAddress(&address, g_noallocScratch));
+    cudaFuncAttributes a;
+    NA_CUDA(cudaFuncGetAttributes(&a, packBodiesKernel));
+    NA_CUDA(cudaFuncGetAttributes(&a, aabbKernel));
+    NA_CUDA(cudaFuncGetAttributes(&a, keyKernel));
+    NA_CUDA(cudaFuncGetAttributes(&a, cellTableKernel));
+    NA_CUDA(cudaFuncGetAttributes(&a, pairKernel));
+    NA_CUDA(cudaFuncGetAttributes(&a, packPairKeysKernel));
+    NA_CUDA(cudaFuncGetAttributes(&a, unpackPairKeysKernel));
+    NA_CUDA(radixSortPreload());
+    *base = static_cast<unsigned char*>(address);
+    g_scratchAddress[device].store(*base, std::memory_order_release);
+    return VXB_OK;
+}
+
 }  // namespace
 }  // namespace vxb
 
@@ -110,12 +148,11 @@ extern "C" int vxb_stage_pairs_noalloc(const vx_body* bodies, uint32_t n, float 
     int device = 0;
     NA_CUDA(cudaGetDevice(&device));
     if (device < 0 || device >= (int)kMaxDevices) return VXB_ERR_INVALID;
-    if (!g_scratchAddress[device]) {
-        void* address = nullptr;
-        NA_CUDA(cudaGetSymbolAddress(&address, g_noallocScratch));
-        g_scratchAddress[device] = static_cast<unsigned char*>(address);
+    unsigned char* base = g_scratchAddress[device].load(std::memory_order_acquire);
+    if (!base) {
+        const int status = setupDevice(device, &base);
+        if (status != VXB_OK) return status;
     }
-    unsigned char* base = g_scratchAddress[device];
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
 
     vx_body* aos = reinterpret_cast<vx_body*>(base + kOffAos);

@@ -971,7 +971,7 @@ __global__ void colorFixedPointKernel(const uint64_t* keys, const uint32_t* vals
             }
         }
         if (local) atomicAdd(&st->changed[r % 3], local);
-        if (!gridSync(&st->bar, &st->timeout)) return;
+        if (!gridSync(&st->bar, &st->timeout, st->spinLimit)) return;
         if (__ldcg(&st->changed[r % 3]) == 0u || __ldcg(&st->spill) != 0u) {
             if (tid == 0) st->rounds = r + 1;
             return;
@@ -1969,7 +1969,7 @@ VXD bool clusterStep(const SolveArgs& A, const uint32_t* start, const uint32_t* 
                 const uint32_t d0 = p0 == kNoPred ? 0xffffffffu : ldAcquire(done + (p0 & ~kWrap));
                 const uint32_t d1 = p1 == kNoPred ? 0xffffffffu : ldAcquire(done + (p1 & ~kWrap));
                 if (d0 >= need0 && d1 >= need1) break;
-                if (spins > kSpinLimit || ((spins & 63u) == 63u && __ldcg(&st->timeout))) {
+                if (spins > st->spinLimit || ((spins & 63u) == 63u && __ldcg(&st->timeout))) {
                     atomicOr(&st->timeout, 1u);
                     ok = false;
                     break;
@@ -1997,11 +1997,11 @@ __global__ void __launch_bounds__(256) solveClusterKernel(SolveArgs A, uint32_t 
     const uint32_t base = blockIdx.x * G;
     if (A.positionIterations > 0) {
         for (uint32_t t = tid; t < R; t += stride) __stcg(done + rowList[t], 0u);
-        if (!gridSync(&st->bar, &st->timeout)) return;
+        if (!gridSync(&st->bar, &st->timeout, st->spinLimit)) return;
         for (int u = 0; u < A.positionIterations; ++u)
             for (uint32_t gl = 0; gl < G; ++gl)
                 if (!clusterStep(A, start, rows, base + gl, u, 2, pred, remote, done, st, &abortFlag)) return;
-        gridSync(&st->bar, &st->timeout);
+        gridSync(&st->bar, &st->timeout, st->spinLimit);
         return;
     }
     for (int s = 0; s < A.substeps; ++s) {
@@ -2010,23 +2010,23 @@ __global__ void __launch_bounds__(256) solveClusterKernel(SolveArgs A, uint32_t 
             if (A.integrate && s > 0) giantIntegrateVelocity(A, id);
             __stcg(A.frames + id, pack(inertiaFrameAt(loadMass(A.B, id), q4(ldcg4(A.B.rot + id)))));
         }
-        if (!gridSync(&st->bar, &st->timeout)) return;
+        if (!gridSync(&st->bar, &st->timeout, st->spinLimit)) return;
         for (uint32_t t = tid; t < R; t += stride) {
             const uint32_t k = rowList[t];
             giantRow(A, k, 3);
             __stcg(done + k, 0u);
         }
-        if (!gridSync(&st->bar, &st->timeout)) return;
+        if (!gridSync(&st->bar, &st->timeout, st->spinLimit)) return;
         const int warmUnits = A.warmStart && s == 0 ? 1 : 0;
         for (int u = 0; u < warmUnits + A.sweeps; ++u)
             for (uint32_t gl = 0; gl < G; ++gl)
                 if (!clusterStep(A, start, rows, base + gl, u, u < warmUnits ? 0 : 1, pred, remote, done, st,
                                  &abortFlag))
                     return;
-        if (!gridSync(&st->bar, &st->timeout)) return;
+        if (!gridSync(&st->bar, &st->timeout, st->spinLimit)) return;
         if (A.integrate) {
             for (uint32_t t = tid; t < NB; t += stride) giantIntegrateTransform(A, bodyIds[t]);
-            if (!gridSync(&st->bar, &st->timeout)) return;
+            if (!gridSync(&st->bar, &st->timeout, st->spinLimit)) return;
         }
     }
 }
@@ -2343,7 +2343,7 @@ __global__ void __launch_bounds__(256) caFlowKernel(BodyArrays B, Soup soup, con
         }
     // Every root is queued before any worker starts: a count that a finished
     // candidate has taken to zero must not read as a root.
-    if (!gridSync(&st->bar, &st->timeout)) return;
+    if (!gridSync(&st->bar, &st->timeout, st->spinLimit)) return;
     if ((threadIdx.x & 31u) != 0u) return;
     uint32_t rewinds = 0, maxDepth = 0, maxCrit = 0;
     for (;;) {
@@ -2354,7 +2354,7 @@ __global__ void __launch_bounds__(256) caFlowKernel(BodyArrays B, Soup soup, con
         // polling one L2 line at full rate slow the working lanes' own loads.
         uint32_t k, spins = 0, nap = 32;
         while ((k = __ldcg(queue + h)) == kNoPred) {
-            if (++spins > kSpinLimit || ((spins & 15u) == 0u && __ldcg(&st->timeout))) {
+            if (++spins > st->spinLimit || ((spins & 15u) == 0u && __ldcg(&st->timeout))) {
                 atomicOr(&st->timeout, 1u);
                 return;
             }
@@ -2551,6 +2551,14 @@ static int sortPairs(Context& c, uint64_t* keys, uint32_t* vals, uint32_t n, int
     cudaError_t e = cudaSuccess;
     c.launches += radixSortPairs(keys, vals, n, 0, bits, c.sortScratch, c.stream, &e);
     if (e != cudaSuccess) return cudaStatus(c, e, "radix sort");
+    return VXB_OK;
+}
+
+int resetCoop(Context& c, CoopState* st) {
+    CoopState init;
+    std::memset(&init, 0, sizeof(init));
+    init.spinLimit = c.waitLimit;
+    VXB_CUDA(c, cudaMemcpyAsync(st, &init, sizeof(init), cudaMemcpyHostToDevice, c.stream));
     return VXB_OK;
 }
 
@@ -2876,7 +2884,7 @@ static int parallelColor(Context& c, const vx_contact* cs, const uint32_t* order
     VXB_TRY(sortPairs(c, keys, vals, 2 * m, bitsFor(n)));
     LAUNCH(c, colorSlotKernel, blocksFor(2 * m, 256), 256, keys, vals, 2 * m, n, slot, runStart);
     VXB_CUDA(c, cudaMemsetAsync(color, 0, (size_t)m * 4, c.stream));
-    VXB_CUDA(c, cudaMemsetAsync(st, 0, sizeof(CoopState), c.stream));
+    VXB_TRY(resetCoop(c, st));
     const int rc = launchCooperative(c, colorFixedPointKernel, 256, (const uint64_t*)keys, (const uint32_t*)vals,
                                      (const uint32_t*)slot, (const uint32_t*)runStart, islandIdx,
                                      islandStart, m, color, st, 4096u);
@@ -3082,7 +3090,7 @@ static int launchSolve(Context& c, const SolveArgs& A) {
     VXB_TRY(ensure(c, c.coopBuf, sizeof(CoopState)));
     CoopState* st = P<CoopState>(c.coopBuf);
     uint32_t* list = P<uint32_t>(c.giantBuf);
-    VXB_CUDA(c, cudaMemsetAsync(st, 0, sizeof(CoopState), c.stream));
+    VXB_TRY(resetCoop(c, st));
     const uint32_t giants = c.planGiants;  // counted with the island plan
     if (!giants) return VXB_OK;
     LAUNCH(c, giantListKernel, std::min<uint32_t>(blocksFor(A.islands, 256), (uint32_t)c.smCount * 4), 256, A, list,
@@ -3170,7 +3178,7 @@ static int launchSolve(Context& c, const SolveArgs& A) {
             }
         }
         if (clusters > 0 && c.clusterBuilt) {
-            VXB_CUDA(c, cudaMemsetAsync(st, 0, sizeof(CoopState), c.stream));
+            VXB_TRY(resetCoop(c, st));
             const int rcc = launchCooperative(c, solveClusterKernel, 256, G, c.clusterG,
                                               (const uint32_t*)P<uint32_t>(c.clusterStartBuf),
                                               (const uint32_t*)P<uint32_t>(c.clusterRowsBuf), (const uint32_t*)rowList,
@@ -3310,7 +3318,7 @@ static int conservativeAdvancement(Context& c, uint32_t npairs, float dt) {
             snapped = true;
         }
         VXB_CUDA(c, cudaMemsetAsync(queue, 0xff, (size_t)ncand * 4, c.stream));
-        VXB_CUDA(c, cudaMemsetAsync(st, 0, sizeof(CoopState), c.stream));
+        VXB_TRY(resetCoop(c, st));
         const int rc = launchCooperativeCapped(c, kCaFlowBlocksPerSm, caFlowKernel, kCaFlowThreads, c.B, soupOf(c),
                                                (const uint32_t*)flagRank, (const float4*)specState,
                                                (const uint32_t*)specResult, (const uint4*)info, ncand,

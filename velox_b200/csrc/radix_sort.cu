@@ -138,6 +138,14 @@ __global__ void scatterKernel(const uint64_t* __restrict__ keysIn, const uint32_
 
 }  // namespace
 
+cudaError_t radixSortPreload() {
+    cudaFuncAttributes a;
+    cudaError_t e = cudaFuncGetAttributes(&a, histogramKernel);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&a, scanKernel);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&a, scatterKernel);
+    return e;
+}
+
 int radixSortPairs(uint64_t* keys, uint32_t* vals, uint32_t n, int beginBit, int endBit,
                    RadixScratch& s, cudaStream_t stream, cudaError_t* err) {
     int launches = 0;

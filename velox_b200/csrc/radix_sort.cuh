@@ -31,6 +31,11 @@ struct RadixScratch {
 int radixSortPairs(uint64_t* keys, uint32_t* vals, uint32_t n, int beginBit, int endBit,
                    RadixScratch& scratch, cudaStream_t stream, cudaError_t* err);
 
+// Loads the sort's kernels on the current device now (cudaFuncGetAttributes),
+// so that a later sort does not load them lazily (which allocates device
+// memory) on its first launch.
+cudaError_t radixSortPreload();
+
 // Bits needed to represent `maxKey`.
 inline int keyBits(uint64_t maxKey) {
     int b = 0;
