@@ -288,3 +288,70 @@ def oracle_warm_start(cur, prev):
     p = np.ascontiguousarray(prev)
     warm = oracle().vxo_warm_start_match(_p(c), len(c), _p(p), len(p))
     return c, warm
+
+
+# ---- the FP64 frozen-contact step and its adjoint (oracle/adjoint_ref.c) ------
+
+ADJREF = os.path.join(HERE, "_build", "libvelox_adjref.so")
+_adjref = None
+
+
+class AdjConfig(ctypes.Structure):
+    _fields_ = [("dt", ctypes.c_double), ("gx", ctypes.c_double), ("gy", ctypes.c_double), ("gz", ctypes.c_double),
+                ("substeps", ctypes.c_int), ("sweeps", ctypes.c_int), ("positionIterations", ctypes.c_int),
+                ("stackStabilization", ctypes.c_int), ("stackStiffness", ctypes.c_double),
+                ("stackDamping", ctypes.c_double)]
+
+    @classmethod
+    def make(cls, dt=1.0 / 60.0, gravity=(0.0, -9.81, 0.0), substeps=4, velocity_iterations=8,
+             position_iterations=3, stack_stabilization=0, stack_stiffness=1000.0, stack_damping=10.0):
+        return cls(dt, gravity[0], gravity[1], gravity[2], substeps, 2 * velocity_iterations, position_iterations,
+                   stack_stabilization, stack_stiffness, stack_damping)
+
+
+def adjref():
+    global _adjref
+    if _adjref is not None:
+        return _adjref
+    if not os.path.exists(ADJREF):
+        raise RuntimeError(f"adjoint restatement missing: {ADJREF} (run `make -C oracle oracle`)")
+    L = ctypes.CDLL(ADJREF)
+    vp = ctypes.c_void_p
+    L.adjref_run.argtypes = [ctypes.POINTER(AdjConfig), vp, ctypes.c_uint32, vp, vp, vp, vp, vp, vp, vp,
+                             ctypes.c_uint32, vp, vp, vp, vp, vp, ctypes.POINTER(ctypes.c_uint64)]
+    L.adjref_run.restype = ctypes.c_int
+    _adjref = L
+    return L
+
+
+def adjoint_reference(cfg, bodies, state0, inv_mass, inv_inertia, contacts, step_start, src, color, seed=None):
+    """FP64 frozen-contact rollout from state0 (n x 13: p, q, v, w) over the
+    recorded contacts of each step. Returns (final state, branch hash) and, with
+    a seed (dL/d final state), also (dL/d state0, dL/d invMass, dL/d invInertia)."""
+    from velox_b200.binding import BODY, CONTACT, records  # record layouts only (no library load)
+    L = adjref()
+    n = len(bodies)
+    bodies = records(bodies, BODY)
+    contacts = records(contacts, CONTACT)
+    state0 = np.ascontiguousarray(state0, np.float64)
+    inv_mass = np.ascontiguousarray(inv_mass, np.float64)
+    inv_inertia = np.ascontiguousarray(inv_inertia, np.float64)
+    step_start = np.ascontiguousarray(step_start, np.uint32)
+    src = np.ascontiguousarray(src, np.uint32)
+    color = np.ascontiguousarray(color, np.int32)
+    out = np.zeros((n, 13), np.float64)
+    h = ctypes.c_uint64()
+    grad = gim = gii = None
+    if seed is not None:
+        seed = np.ascontiguousarray(seed, np.float64)
+        grad = np.zeros((n, 13), np.float64)
+        gim = np.zeros(n, np.float64)
+        gii = np.zeros(n, np.float64)
+    rc = L.adjref_run(ctypes.byref(cfg), _p(bodies), n, _p(state0), _p(inv_mass),
+                      _p(inv_inertia), _p(contacts), _p(step_start), _p(src), _p(color), len(step_start) - 1,
+                      _p(out), _p(seed), _p(grad), _p(gim), _p(gii), ctypes.byref(h))
+    if rc != 0:
+        raise ValueError("adjoint restatement: anisotropic inverse inertia")
+    if seed is None:
+        return out, h.value
+    return out, h.value, grad, gim, gii
