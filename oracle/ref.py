@@ -17,6 +17,10 @@ FAST = os.path.join(REF_DIR, "libvelox_ref_fast.so")
 DROPIN = os.path.join(REF_DIR, "libvelox_ref_dropin.so")
 # The same engine over a fake of the library's Backend entry points (no GPU).
 DROPIN_FAKE = os.path.join(REF_DIR, "libvelox_ref_dropin_fake.so")
+# The reference engine with its own CUDA backend (src/backend_cuda.cu, sm_100a):
+# strict floating point (the GPU solver oracle) and the default build (timed).
+CUDA_STRICT = os.path.join(REF_DIR, "libvelox_ref_cuda_strict.so")
+CUDA_FAST = os.path.join(REF_DIR, "libvelox_ref_cuda_fast.so")
 
 BACKEND_CPU = 1
 BACKEND_CUDA_EMULATED = 2
@@ -27,6 +31,10 @@ def _path(strict):
         return DROPIN
     if strict == "dropin_fake":
         return DROPIN_FAKE
+    if strict == "cuda":
+        return CUDA_STRICT
+    if strict == "cuda_fast":
+        return CUDA_FAST
     return STRICT if strict else FAST
 
 

@@ -253,8 +253,9 @@ thread_local ColoredCpuBackend* g_lastEmulated = nullptr;
 }  // namespace
 
 // The drop-in build links velox_b200/dropin/b200_backend.cpp instead, whose
-// createCudaBackend() serves World(BackendType::Cuda) from libvelox_b200.so.
-#ifndef REF_SHIM_DROPIN
+// createCudaBackend() serves World(BackendType::Cuda) from libvelox_b200.so;
+// the CUDA build links the reference's own src/backend_cuda.cu.
+#if !defined(REF_SHIM_DROPIN) && !defined(REF_SHIM_CUDA)
 Backend* createCudaBackend() {
     auto* backend = new ColoredCpuBackend();
     g_lastEmulated = backend;
