@@ -168,6 +168,51 @@ int vxb_world_write_forces(vxb_context* ctx, const float* in, uint32_t n);
 int vxb_world_read_contacts(vxb_context* ctx, vx_contact* out, uint32_t cap, uint32_t* count);
 int vxb_world_stats(vxb_context* ctx, vxb_step_stats* out);
 
+/* ---- adjoint of the device world's step ---------------------------------------
+ * No counterpart in the reference (it has no differentiation). The adjoint
+ * differentiates the step as the device world runs it (src/world.cpp:4007-4397
+ * with the coloured solve of src/backend_cuda.cu:569-761): the warm start and
+ * solveContact sweeps (src/narrowphase.h:80-366), the integration
+ * (include/velox/body.h:266-321) and the position correction
+ * (src/world.cpp:4370-4397), with each step's contact set, feature matching,
+ * colours and clamp / friction-ellipse / correction active sets frozen from
+ * the forward pass. Scope: two-axis friction, isotropic inverse inertia, zero
+ * rolling and spinning friction, no forces written during the taped steps.
+ *
+ * Use: vxb_world_load + vxb_world_configure, vxb_tape_begin(steps, k), then
+ * vxb_world_step for those steps (they are recorded: contacts after matching,
+ * body checkpoints every k steps), then vxb_adjoint_backward. The backward
+ * pass recomputes each k-step segment from its checkpoint (bit-identical to
+ * the forward) and runs the reverse; one warp per world. */
+
+/* Per-world flags of a tape / backward pass. */
+#define VXB_ADJ_REWOUND 1u     /* a conservative-advancement rewind moved a body: not smooth */
+#define VXB_ADJ_DIVERGED 2u    /* the recomputed segment left the forward trajectory */
+#define VXB_ADJ_UNSUPPORTED 4u /* outside the reverse's scope (see above) */
+
+/* Starts recording the next `steps` steps of vxb_world_step, with a body
+ * checkpoint every `checkpointEvery` steps. Replaces any earlier tape. */
+int vxb_tape_begin(vxb_context* ctx, uint32_t steps, uint32_t checkpointEvery);
+/* Steps recorded so far, contacts recorded, checkpoint slots (incl. the final state). */
+int vxb_tape_info(vxb_context* ctx, uint32_t* recordedSteps, uint32_t* contacts, uint32_t* checkpoints);
+/* Copies the tape out (each pointer nullable): contacts after matching,
+ * stepStart[steps + 1], sources (2 per contact: the previous step's contact
+ * it inherited impulses / vn0 from, 0xffffffff = none), colours, checkpoints
+ * (slots x 4 x n float4: position, orientation, velocity, angular velocity),
+ * world flags. */
+int vxb_tape_read(vxb_context* ctx, vx_contact* contacts, uint32_t* stepStart, uint32_t* sources, int32_t* colors,
+                  float* checkpoints, uint32_t* worldFlags);
+/* Backward pass over a fully recorded tape. seed: dL/d(state after the last
+ * taped step), n x 13 floats per body (position 3, orientation 4, velocity 3,
+ * angular velocity 3), null = zero. Outputs (each nullable): grad = dL/d(state
+ * at the tape's first step), n x 13; gradInverseMass = dL/d(invMass) and
+ * dL/d(isotropic invInertia), n x 2; gradMass = dL/d(mass) for inertia that
+ * scales with mass, n; worldFlags (VXB_ADJ_*), one per world. */
+int vxb_adjoint_backward(vxb_context* ctx, const float* seed, float* grad, float* gradInverseMass,
+                         float* gradMass, uint32_t* worldFlags);
+/* Releases the tape. */
+int vxb_tape_end(vxb_context* ctx);
+
 /* ---- individual stages (parity testing) --------------------------------- */
 
 /* Candidate pairs (i<j) of the sorted-grid broad phase, returned sorted

@@ -184,6 +184,11 @@ def lib(path=LIB_PATH):
         "vxb_stage_distance": ([vp, vp, u32, ctypes.POINTER(Soup), vp, u32, i32, vp], i32),
         "vxb_stage_color": ([vp, vp, u32, vp, u32, vp, p_u32], i32),
         "vxb_stage_pairs_noalloc": ([vp, u32, f32, vp, u32, p_u32, vp], i32),
+        "vxb_tape_begin": ([vp, u32, u32], i32),
+        "vxb_tape_info": ([vp, p_u32, p_u32, p_u32], i32),
+        "vxb_tape_read": ([vp, vp, vp, vp, vp, vp, vp], i32),
+        "vxb_adjoint_backward": ([vp, vp, vp, vp, vp, vp], i32),
+        "vxb_tape_end": ([vp], i32),
         "vxb_scene_generate": ([i32, ctypes.c_uint64, u32, vp, u32, p_u32, vp, u32, p_u32], i32),
         "vxb_bodies_from_specs": ([vp, u32, vp, vp, vp, u32, p_u32, vp, u32, p_u32], i32),
     }
@@ -293,6 +298,7 @@ class Context:
         bodies = records(bodies, BODY)
         self.bodies_n = len(bodies)
         wo = None if world_of is None else np.ascontiguousarray(world_of, np.uint32)
+        self.worlds = 1 if wo is None or len(wo) == 0 else int(wo.max()) + 1
         self._check(self.L.vxb_world_load(self.h, ptr(bodies), len(bodies), ctypes.byref(soup), ptr(wo)))
 
     def configure(self, dt=1.0 / 60.0, substeps=4, gravity=(0.0, -9.81, 0.0), solver=None):
@@ -327,6 +333,50 @@ class Context:
         s = StepStats()
         self._check(self.L.vxb_world_stats(self.h, ctypes.byref(s)))
         return {k: getattr(s, k) for k, _ in StepStats._fields_}
+
+    # ---- adjoint
+    def tape_begin(self, steps, checkpoint_every=10):
+        """Record the next `steps` steps for vxb_adjoint_backward."""
+        self._check(self.L.vxb_tape_begin(self.h, steps, checkpoint_every))
+
+    def tape_info(self):
+        r, c, k = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()
+        self._check(self.L.vxb_tape_info(self.h, ctypes.byref(r), ctypes.byref(c), ctypes.byref(k)))
+        return {"recorded": r.value, "contacts": c.value, "checkpoints": k.value}
+
+    def tape_read(self):
+        """The recorded tape: contacts (after matching), step starts, sources
+        (impulse, vn0; 0xffffffff = none), colours, checkpoints (slots x 4 x n
+        x 4 floats: position, orientation, velocity, angular velocity), world flags."""
+        info = self.tape_info()
+        total, slots, n = info["contacts"], info["checkpoints"], self.bodies_n
+        contacts = np.zeros(max(total, 1), CONTACT)
+        starts = np.zeros(info["recorded"] + 1, np.uint32)
+        src = np.zeros((max(total, 1), 2), np.uint32)
+        colors = np.zeros(max(total, 1), np.int32)
+        ckpt = np.zeros((slots, 4, n, 4), np.float32)
+        flags = np.zeros(self.worlds, np.uint32)
+        self._check(self.L.vxb_tape_read(self.h, ptr(contacts), ptr(starts), ptr(src), ptr(colors), ptr(ckpt),
+                                         ptr(flags)))
+        return {"contacts": contacts[:total], "step_start": starts, "src": src[:total], "colors": colors[:total],
+                "checkpoints": ckpt, "flags": flags}
+
+    def adjoint_backward(self, seed=None):
+        """dL/d(state at the tape's first step) from dL/d(state after its last
+        step) (n x 13: position, orientation, velocity, angular velocity).
+        Returns (grad n x 13, dL/d(invMass, invInertia) n x 2, dL/dmass n,
+        world flags)."""
+        n = self.bodies_n
+        seed = None if seed is None else np.ascontiguousarray(seed, np.float32).reshape(n, 13)
+        grad = np.zeros((n, 13), np.float32)
+        ginv = np.zeros((n, 2), np.float32)
+        gmass = np.zeros(n, np.float32)
+        flags = np.zeros(self.worlds, np.uint32)
+        self._check(self.L.vxb_adjoint_backward(self.h, ptr(seed), ptr(grad), ptr(ginv), ptr(gmass), ptr(flags)))
+        return grad, ginv, gmass, flags
+
+    def tape_end(self):
+        self._check(self.L.vxb_tape_end(self.h))
 
     # ---- stages
     def pairs(self, bodies, dt):

@@ -114,6 +114,7 @@ void vxb_context_destroy(vxb_context* ctx) {
     Context& c = ctx->impl;
     cudaSetDevice(c.device);
     if (c.stream) cudaStreamSynchronize(c.stream);
+    vxb::tapeEnd(c);
     vxb::DevBuf* bufs[] = {&c.bodyBuf, &c.aosBuf, &c.worldOfBuf, &c.planeStartBuf, &c.planeListBuf, &c.prevPoseBuf,
                            &c.snapBuf, &c.hullPtsBuf, &c.facesBuf, &c.aabbBuf, &c.cellKeyBuf, &c.cellValBuf,
                            &c.sortKeysAlt, &c.sortValsAlt, &c.sortHist, &c.hashKeyBuf, &c.hashValBuf, &c.pairBuf,
@@ -270,6 +271,7 @@ int vxb_world_load(vxb_context* ctx, const vx_body* bodies, uint32_t n, const vx
     if (!bodies || n == 0) return VXB_ERR_INVALID;
     Context& c = ctx->impl;
     TRY(ensureCounters(c));
+    vxb::tapeEnd(c);  // a tape belongs to the world it recorded
     TRY(vxb::loadBodies(c, bodies, n, worldOfBody));
     TRY(vxb::loadSoup(c, soup));
     cudaError_t e = cudaStreamSynchronize(c.stream);
@@ -320,6 +322,43 @@ int vxb_world_stats(vxb_context* ctx, vxb_step_stats* out) {
     if (!ctx || !out) return VXB_ERR_INVALID;
     *out = ctx->impl.stats;
     return VXB_OK;
+}
+
+// ---- adjoint -----------------------------------------------------------------
+
+int vxb_tape_begin(vxb_context* ctx, uint32_t steps, uint32_t checkpointEvery) {
+    GUARD(ctx);
+    Context& c = ctx->impl;
+    if (!c.configured) return vxb::fail(c, VXB_ERR_INVALID, "vxb_world_configure was not called");
+    TRY(vxb::tapeEnd(c));
+    return vxb::tapeBegin(c, steps, checkpointEvery);
+}
+
+int vxb_tape_info(vxb_context* ctx, uint32_t* recordedSteps, uint32_t* contacts, uint32_t* checkpoints) {
+    if (!ctx) return VXB_ERR_INVALID;
+    const vxb::Tape& T = ctx->impl.tape;
+    if (recordedSteps) *recordedSteps = T.active ? T.recorded : 0u;
+    if (contacts) *contacts = T.active ? T.stepStart.back() : 0u;
+    if (checkpoints) *checkpoints = T.active ? (T.steps + T.every - 1) / T.every + 1 : 0u;
+    return VXB_OK;
+}
+
+int vxb_tape_read(vxb_context* ctx, vx_contact* contacts, uint32_t* stepStart, uint32_t* sources, int32_t* colors,
+                  float* checkpoints, uint32_t* worldFlags) {
+    GUARD(ctx);
+    if (!ctx->impl.tape.active) return vxb::fail(ctx->impl, VXB_ERR_INVALID, "no tape");
+    return vxb::tapeRead(ctx->impl, contacts, stepStart, sources, colors, checkpoints, worldFlags);
+}
+
+int vxb_adjoint_backward(vxb_context* ctx, const float* seed, float* grad, float* gradInverseMass, float* gradMass,
+                         uint32_t* worldFlags) {
+    GUARD(ctx);
+    return vxb::adjointBackward(ctx->impl, seed, grad, gradInverseMass, gradMass, worldFlags);
+}
+
+int vxb_tape_end(vxb_context* ctx) {
+    GUARD(ctx);
+    return vxb::tapeEnd(ctx->impl);
 }
 
 // ---- stages ----------------------------------------------------------------

@@ -42,6 +42,21 @@ struct DevBuf {
     size_t bytes = 0;
 };
 
+// Recording of the device world's steps for the adjoint (adjoint.cu).
+struct Tape {
+    bool active = false;
+    uint32_t steps = 0, every = 0, recorded = 0;
+    std::vector<uint32_t> stepStart{0u};  // first contact of each recorded step (+ total)
+    DevBuf contacts;    // vx_contact per contact, after warm-start matching
+    DevBuf src;         // uint2 per contact: impulse source, vn0 source (previous step's index)
+    DevBuf color;       // uint32 per contact
+    DevBuf worldStart;  // steps x (worlds + 1): first contact of each world within its step
+    DevBuf ckpt;        // (J + 1) x 4 x n float4: body state every k steps, then the final state
+    DevBuf flags;       // uint32 per world (VXB_ADJ_*)
+    DevBuf scratch;     // backward: per-world working memory
+    DevBuf host;        // backward: small device arrays (body ranges, seeds, gradients)
+};
+
 // Device-side counters and flags (one small allocation, read back once per call).
 struct Counters {
     uint32_t pairs;          // convex candidate pairs emitted (may exceed capacity)
@@ -199,6 +214,8 @@ struct Context {
     bool timing = false;
     StageTimer timer;
 
+    Tape tape;
+
     cudaError_t err = cudaSuccess;
 };
 
@@ -236,5 +253,20 @@ int backendFetchImpulses(Context& c, vx_contact* contacts, uint32_t m);
 int readPoses(Context& c, float* out, uint32_t n);
 int writeForces(Context& c, const float* in, uint32_t n);
 int readContacts(Context& c, vx_contact* out, uint32_t cap, uint32_t* count);
+
+// Adjoint (adjoint.cu): tape hooks of the device world's step, and the backward pass.
+int tapeBegin(Context& c, uint32_t steps, uint32_t every);
+int tapeEnd(Context& c);
+int tapeStepBegin(Context& c);
+int tapeBeforeMatch(Context& c, const vx_contact* cs, uint32_t m, const vx_contact* prev, const uint64_t* prevKeys,
+                    uint32_t mPrev);
+int tapeAfterMatch(Context& c, const vx_contact* cs, uint32_t m);
+int tapeAfterIslands(Context& c, const uint32_t* color, uint32_t m);
+int tapeAfterRewind(Context& c, const uint32_t* rewound);
+int tapeStepEnd(Context& c, uint32_t m);
+int tapeRead(Context& c, vx_contact* contacts, uint32_t* stepStart, uint32_t* src, int32_t* color, float* ckpt,
+             uint32_t* worldFlags);
+int adjointBackward(Context& c, const float* seed, float* grad, float* gradInv, float* gradMass,
+                    uint32_t* worldFlags);
 
 }  // namespace vxb

@@ -3374,6 +3374,7 @@ static int stepOnce(Context& c) {
     c.caWidenings = 0;
     VXB_TRY(ensure(c, c.prevPoseBuf, (size_t)n * 32));
     float4* prevPos = P<float4>(c.prevPoseBuf);
+    if (c.tape.active) VXB_TRY(tapeStepBegin(c));
     stageBegin(c, kStagePrepare);
     LAUNCH(c, prepareKernel, blocksFor(n, 256), 256, c.B, n, g, h, prevPos, prevPos + n, 1);
     stageEnd(c, kStagePrepare);
@@ -3384,20 +3385,26 @@ static int stepOnce(Context& c) {
                         P<uint64_t>(c.pairBuf) + c.pairCap));
     vx_contact* cs = P<vx_contact>(c.contactBuf[c.cur]);
     stageBegin(c, kStageWarmStart);
+    if (c.tape.active)
+        VXB_TRY(tapeBeforeMatch(c, cs, m, P<vx_contact>(c.contactBuf[c.cur ^ 1]), P<uint64_t>(c.prevKeyBuf),
+                                c.prevCount));
     if (c.prevCount && m)
         LAUNCH(c, matchKernel, blocksFor(m, 128), 128, cs, m, P<vx_contact>(c.contactBuf[c.cur ^ 1]),
                P<uint64_t>(c.prevKeyBuf), c.prevCount, c.dCounters);
+    if (c.tape.active) VXB_TRY(tapeAfterMatch(c, cs, m));
     stageEnd(c, kStageWarmStart);
     IslandPlan plan;
     stageBegin(c, kStageIslands);
     VXB_TRY(buildIslands(c, cs, m, plan, nullptr));
     VXB_TRY(prepareSegments(c, plan));
+    if (c.tape.active) VXB_TRY(tapeAfterIslands(c, P<uint32_t>(c.colorBuf), m));
     stageEnd(c, kStageIslands);
     stageBegin(c, kStageSolve);
     VXB_TRY(runSubsteps(c, cs, plan, g, h, substeps, cfg.solver, true, true));
     stageEnd(c, kStageSolve);
     stageBegin(c, kStageRewind);
     if (m) VXB_TRY(conservativeAdvancement(c, nrec, dt));
+    if (c.tape.active && m && nrec) VXB_TRY(tapeAfterRewind(c, P<uint32_t>(c.caBodyMarkBuf) + n));
     stageEnd(c, kStageRewind);
     stageBegin(c, kStagePositions);
     VXB_TRY(positionCorrection(c, cs, plan, cfg.solver, h));
@@ -3408,6 +3415,7 @@ static int stepOnce(Context& c) {
     if (m) LAUNCH(c, contactKeysKernel, blocksFor(m, 256), 256, cs, m, P<uint64_t>(c.prevKeyBuf));
     c.prevCount = m;
     c.cur ^= 1;
+    if (c.tape.active) VXB_TRY(tapeStepEnd(c, m));
     VXB_TRY(readCounters(c));
     c.stats.contacts = m;
     c.stats.islands = plan.realIslands;
