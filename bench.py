@@ -408,6 +408,9 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--size", type=int, default=100000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the reference CUDA backend and the batched, adjoint and stacking workloads "
+                         "reported beside the headline")
     ap.add_argument("--profile", action="store_true",
                     help="bracket the timed steps with cudaProfilerStart/Stop (ncu --profile-from-start off)")
     ap.add_argument("--workload", default="single", choices=["single", "batched"],
@@ -548,12 +551,24 @@ def main():
         except Exception as exc:  # reported, not fatal
             baseline = {"error": str(exc)}
 
+    plain_gpu = None
+    if rank == 0 and world == 1 and not args.no_extras and not args.profile:
+        try:
+            plain_gpu = reference_gpu(specs, pool, n, args.steps, max(args.warmup, 3))
+            if plain_gpu and "value" in plain_gpu:
+                plain_gpu["e2e_vs_plain_gpu"] = e2e["value"] / plain_gpu["value"]
+        except Exception as exc:  # reported, not fatal
+            plain_gpu = {"error": str(exc)}
+
     stats = ctx.stats()
     ctx.close()
     if dist:
         dist.destroy_process_group()
     if rank != 0:
         return 0
+    extra = {}
+    if world == 1 and not args.no_extras and not args.profile:
+        extra = run_extras(args, local, stream)
     line = {"metric": METRIC, "value": value, "unit": "body-steps/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
@@ -562,9 +577,238 @@ def main():
             "stage_ms_per_step": {k: v[0] / args.steps for k, v in stage.items()},
             "roofline": roofline, "solve_roofline": solve_roofline, "rewind_roofline": rewind_roofline,
             "cpu_baseline": baseline, "e2e": e2e, "clocks": clocks,
-            "gpu_launches": int(launches)}
+            "gpu_launches": int(launches), "plain_gpu": plain_gpu}
+    line.update(extra)
     print(json.dumps(line))
     return 0
+
+
+def reference_gpu(specs, pool, n, steps, warmup, budget_s=60.0):
+    """The reference's own CUDA backend (src/backend_cuda.cu built for sm_100a
+    with its default flags, World(BackendType::Cuda)) on the same scene and
+    this GPU: the plain single-world GPU path. Its World::step is blocking
+    (host copies every step), so the per-step time is the host wall time."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref
+    if not ref.available("cuda_fast"):
+        return None
+    w = ref.RefWorld(specs, pool, backend=ref.BACKEND_CUDA_EMULATED, strict="cuda_fast")
+    if w.L.ref_world_backend_name(w.h) != b"cuda":
+        w.close()
+        return {"error": "reference CUDA backend unavailable on this device"}
+    w.configure(substeps=SUBSTEPS, workers=0)
+    w.step(DT, warmup)
+    done, total = 0, 0.0
+    while done < steps and total < budget_s:
+        total += w.step(DT, 1) / 1000.0
+        done += 1
+    w.close()
+    return {"value": n * done / total, "unit": "body-steps/s", "steps": done, "ms_per_step": total / done * 1e3,
+            "kind": "reference CUDA backend (src/backend_cuda.cu, sm_100a, default flags) on this GPU",
+            "timing": "host wall time of World::step (blocking), after the same warm-up"}
+
+
+# ---- the other workloads, reported beside the headline -----------------------
+
+STACK_CONFIG = 3      # 256 twenty-row box pyramids, 8 substeps, 600 steps
+ADJOINT_CONFIG = 5    # 1024 worlds: 5-box stack + sphere projectile, 120 steps, checkpoints every 10
+
+
+def _timed_blocks(ctx, stream, flush, steps, block=1):
+    """Device time of `steps` steps in blocks of `block` (L2 flushed before each block)."""
+    import torch
+    events = []
+    with torch.cuda.stream(stream):
+        done = 0
+        while done < steps:
+            k = min(block, steps - done)
+            flush.fill_(1)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            ctx.step(k)
+            e1.record(stream)
+            events.append((e0, e1))
+            done += k
+    torch.cuda.synchronize()
+    return sum(a.elapsed_time(b) for a, b in events)
+
+
+def measure_batched(local, stream, nworlds, steps, warmup, plain_sample=PLAIN_SAMPLE):
+    """world-steps/s of `nworlds` independent worlds in one context, next to
+    the same worlds stepped one world at a time: in this library (one context
+    per world) and on the reference's own CUDA backend (one World per world)."""
+    import torch
+    import velox_b200 as vb
+    specs, pool = vb.generate_scene(BATCH_CONFIG, seed=BATCH_CONFIG, size=nworlds)
+    bodies, hull, faces = vb.bodies_from_specs(specs, pool)
+    soup = vb.make_soup(hull, faces)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+    ctx = vb.Context(local)
+    ctx.set_stream(stream.cuda_stream)
+    ctx.load(bodies, soup, world_of=specs["world"])
+    ctx.configure(dt=DT, substeps=SUBSTEPS)
+    ctx.step(max(warmup, 3))
+    torch.cuda.synchronize()
+    launches0 = ctx.launches
+    ms = _timed_blocks(ctx, stream, flush, steps)
+    launches = ctx.launches - launches0
+    ctx.close()
+    value = nworlds * steps / (ms / 1e3)
+    counts = np.bincount(specs["world"], minlength=nworlds)
+    order = np.argsort(counts, kind="stable")
+    sample = order[np.linspace(0, nworlds - 1, min(plain_sample, nworlds)).astype(int)]
+    total_ms = 0.0
+    for w in sample:
+        one = specs[specs["world"] == w].copy()
+        one["world"] = 0
+        b1, h1, f1 = vb.bodies_from_specs(one, pool)
+        c1 = vb.Context(local)
+        c1.set_stream(stream.cuda_stream)
+        c1.load(b1, vb.make_soup(h1, f1))
+        c1.configure(dt=DT, substeps=SUBSTEPS)
+        c1.step(max(warmup, 3))
+        torch.cuda.synchronize()
+        total_ms += _timed_blocks(c1, stream, flush, steps)
+        c1.close()
+    plain = 1e3 / (total_ms / len(sample) / steps)
+    plain_ref = None
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref
+    if ref.available("cuda_fast"):
+        ref_s, ref_steps = 0.0, 0
+        for w in sample:
+            one = specs[specs["world"] == w].copy()
+            one["world"] = 0
+            rw = ref.RefWorld(one, pool, backend=ref.BACKEND_CUDA_EMULATED, strict="cuda_fast")
+            rw.configure(substeps=SUBSTEPS, workers=0)
+            rw.step(DT, max(warmup, 3))
+            for _ in range(steps):
+                ref_s += rw.step(DT, 1) / 1000.0
+                ref_steps += 1
+            rw.close()
+        plain_ref = {"value": ref_steps / ref_s, "unit": "world-steps/s",
+                     "kind": "reference CUDA backend (src/backend_cuda.cu, sm_100a), one World per world, stepped "
+                             "one world at a time on this GPU (host wall time of the blocking World::step)",
+                     "sample": f"{len(sample)} worlds over the body-count distribution, {steps} steps each"}
+    return {"metric": f"world-steps/s @{nworlds} worlds", "value": value, "unit": "world-steps/s",
+            "steps": steps, "warmup": max(warmup, 3), "ms_per_step": ms / steps,
+            "bodies": int(len(specs)), "body_steps_per_s": len(specs) * steps / (ms / 1e3),
+            "workload": f"{nworlds} independent worlds, plane + log-uniform [8,512] spheres/boxes/capsules each "
+                        f"({len(specs)} bodies), dt 1/60 s, {SUBSTEPS} substeps",
+            "plain": {"value": plain, "unit": "world-steps/s",
+                      "sample": f"{len(sample)} worlds over the body-count distribution, one context per world, "
+                                f"one world at a time, {steps} device-timed steps each"},
+            "vs_plain": value / plain, "gpu_launches": int(launches),
+            "plain_reference_gpu": plain_ref,
+            "vs_plain_reference_gpu": value / plain_ref["value"] if plain_ref else None}
+
+
+def measure_adjoint(local, stream, nworlds=1024, steps=120, every=10):
+    """The differentiation workload: forward with the tape, and the backward
+    pass (vxb_adjoint_backward) over the same steps; adjoint/forward time."""
+    import torch
+    import velox_b200 as vb
+    specs, pool = vb.generate_scene(ADJOINT_CONFIG, seed=ADJOINT_CONFIG, size=nworlds)
+    bodies, hull, faces = vb.bodies_from_specs(specs, pool)
+    soup = vb.make_soup(hull, faces)
+    world_of = np.ascontiguousarray(specs["world"], np.uint32)
+    boxes = bodies["shape"] == vb.binding.SHAPE["box"]
+    rng = np.random.default_rng(ADJOINT_CONFIG)
+    target = np.zeros((len(bodies), 3), np.float32)
+    target[boxes] = rng.normal(scale=0.05, size=(int(boxes.sum()), 3))
+    ctx = vb.Context(local)
+    ctx.set_stream(stream.cuda_stream)
+
+    def forward(tape):
+        ctx.load(bodies, soup, world_of=world_of)
+        ctx.configure(dt=DT, substeps=SUBSTEPS)
+        if tape:
+            ctx.tape_begin(steps, every)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ctx.step(steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    forward(True)  # warm-up (allocations, module loading)
+    fwd_plain = forward(False)
+    fwd_tape = forward(True)
+    final = ctx.read_bodies()
+    d = final["position"] - bodies["position"] - target
+    seed = np.zeros((len(bodies), 13), np.float32)
+    seed[boxes, 0:3] = 2.0 * d[boxes]
+    ctx.adjoint_backward(seed)  # warm-up
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    t0 = time.perf_counter()
+    e0.record(stream)
+    grad, ginv, gmass, flags = ctx.adjoint_backward(seed)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    wall_ms = (time.perf_counter() - t0) * 1e3
+    bwd = e0.elapsed_time(e1)
+    ctx.close()
+    sphere = bodies["shape"] == vb.binding.SHAPE["sphere"]
+    return {"metric": "adjoint/forward time", "value": bwd / fwd_tape, "unit": "ratio", "higher_is_better": False,
+            "workload": f"{nworlds} worlds, 5-box stack + sphere projectile each ({len(bodies)} bodies), "
+                        f"{steps} steps, dt 1/60 s, {SUBSTEPS} substeps, checkpoints every {every} steps",
+            "forward_ms": fwd_tape, "forward_untaped_ms": fwd_plain, "backward_ms": bwd,
+            "backward_wall_ms": wall_ms, "vs_untaped_forward": bwd / fwd_plain,
+            "smooth_worlds": int(np.sum(flags == 0)), "worlds": nworlds,
+            "rewound_worlds": int(np.sum((flags & 1) != 0)), "diverged_worlds": int(np.sum((flags & 2) != 0)),
+            "loss": float(np.sum(d[boxes] ** 2)),
+            "grad_norm": {"sphere_velocity": float(np.linalg.norm(grad[sphere, 7:10])),
+                          "sphere_angular_velocity": float(np.linalg.norm(grad[sphere, 10:13])),
+                          "mass": float(np.linalg.norm(gmass))}}
+
+
+def measure_stacking(local, stream, pyramids=256, steps=600, block=100):
+    """Solver-heavy stacking: 256 twenty-row box pyramids (53,760 boxes),
+    8 substeps, 600 steps; pass = every pyramid standing and no contact deeper
+    than 5 mm (sampled every `block` steps)."""
+    import torch
+    import velox_b200 as vb
+    specs, pool = vb.generate_scene(STACK_CONFIG, seed=STACK_CONFIG, size=pyramids)
+    bodies, hull, faces = vb.bodies_from_specs(specs, pool)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+    ctx = vb.Context(local)
+    ctx.set_stream(stream.cuda_stream)
+    ctx.load(bodies, vb.make_soup(hull, faces))
+    ctx.configure(dt=DT, substeps=8)
+    start = bodies["position"].copy()
+    ms, deepest = 0.0, 0.0
+    for _ in range(steps // block):
+        ms += _timed_blocks(ctx, stream, flush, block, block)
+        contacts = ctx.read_contacts()
+        deepest = min(deepest, float(contacts["gap"].min()) if len(contacts) else 0.0)
+    end = ctx.read_bodies()["position"]
+    ctx.close()
+    drift = end[1:] - start[1:]
+    standing = bool(np.abs(drift[:, 1]).max() < 0.05 and np.linalg.norm(drift, axis=1).max() < 0.1)
+    n = len(bodies) - 1
+    return {"metric": f"body-steps/s @{n} stacked boxes", "value": n * steps / (ms / 1e3), "unit": "body-steps/s",
+            "workload": f"{pyramids} twenty-row box pyramids ({n} boxes), friction 0.6, dt 1/60 s, 8 substeps",
+            "steps": steps, "ms_per_step": ms / steps, "max_penetration_m": -deepest,
+            "max_drift_m": float(np.linalg.norm(drift, axis=1).max()), "all_standing": standing,
+            "pass": standing and deepest >= -5e-3,
+            "l2": f"flushed before every {block}-step block"}
+
+
+def run_extras(args, local, stream):
+    out = {}
+    for name, fn in [("batched", lambda: measure_batched(local, stream, 4096, min(args.steps, 20), args.warmup)),
+                     ("adjoint", lambda: measure_adjoint(local, stream)),
+                     ("stacking", lambda: measure_stacking(local, stream))]:
+        try:
+            out[name] = fn()
+        except Exception as exc:  # reported, not fatal
+            out[name] = {"error": f"{type(exc).__name__}: {exc}"}
+    return out
 
 
 if __name__ == "__main__":
