@@ -154,7 +154,12 @@ int vxb_backend_invalidate(vxb_context* ctx);
  * colouring, the substep loop, the conservative-advancement rewind,
  * split-impulse position correction and the previous-contact cache.
  * Batches: `worldOfBody` (nullable = one world) assigns each body to a world;
- * bodies of one world must be contiguous and worlds never interact. */
+ * bodies of one world must be contiguous and worlds never interact.
+ * Inputs are validated with the reference's per-step rules for public state
+ * (src/world.cpp:3855-3931): vxb_world_load rejects non-finite or out-of-range
+ * body state and invalid shape parameters ("body <i>: <reason>"),
+ * vxb_world_configure non-finite dt or gravity and invalid solver options,
+ * vxb_world_write_forces non-finite values; each with VXB_ERR_INVALID. */
 int vxb_world_load(vxb_context* ctx, const vx_body* bodies, uint32_t n, const vx_soup* soup,
                    const uint32_t* worldOfBody);
 int vxb_world_configure(vxb_context* ctx, const vxb_step_config* config);

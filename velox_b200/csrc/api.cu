@@ -1,8 +1,10 @@
 // extern "C" entry points (include/velox_b200.h). Every function validates
 // its arguments, never throws, and maps failures to status codes.
+#include <cmath>
 #include <cstdlib>
 #include <cstring>
 #include <new>
+#include <string>
 
 #include "context.cuh"
 
@@ -270,6 +272,13 @@ int vxb_world_load(vxb_context* ctx, const vx_body* bodies, uint32_t n, const vx
     GUARD(ctx);
     if (!bodies || n == 0) return VXB_ERR_INVALID;
     Context& c = ctx->impl;
+    {
+        std::string why;
+        const size_t hp = soup ? soup->hullPointCount : 0, fi = soup ? soup->hullFaceIndexCount : 0;
+        for (uint32_t i = 0; i < n; ++i)
+            if (!vxb::validBody(bodies[i], hp, fi, why))
+                return vxb::fail(c, VXB_ERR_INVALID, "body " + std::to_string(i) + ": " + why);
+    }
     TRY(ensureCounters(c));
     vxb::tapeEnd(c);  // a tape belongs to the world it recorded
     TRY(vxb::loadBodies(c, bodies, n, worldOfBody));
@@ -280,7 +289,14 @@ int vxb_world_load(vxb_context* ctx, const vx_body* bodies, uint32_t n, const vx
 
 int vxb_world_configure(vxb_context* ctx, const vxb_step_config* config) {
     GUARD(ctx);
-    if (!config || !(config->dt >= 0.0f) || config->substeps <= 0) return VXB_ERR_INVALID;
+    if (!config || !(config->dt >= 0.0f) || !std::isfinite(config->dt) || config->substeps <= 0)
+        return vxb::fail(ctx->impl, VXB_ERR_INVALID, "dt must be finite and >= 0, substeps > 0");
+    if (!std::isfinite(config->gravity.x) || !std::isfinite(config->gravity.y) || !std::isfinite(config->gravity.z))
+        return vxb::fail(ctx->impl, VXB_ERR_INVALID, "gravity must be finite");
+    {
+        std::string why;
+        if (!vxb::validSolverOptions(config->solver, why)) return vxb::fail(ctx->impl, VXB_ERR_INVALID, why);
+    }
     if (config->solver.iterationPolicy != 0)
         return vxb::fail(ctx->impl, VXB_ERR_UNSUPPORTED, "the adaptive iteration policy runs on the host");
     ctx->impl.config = *config;
@@ -310,6 +326,8 @@ int vxb_world_read_poses(vxb_context* ctx, float* out, uint32_t n) {
 int vxb_world_write_forces(vxb_context* ctx, const float* in, uint32_t n) {
     GUARD(ctx);
     if (!in) return VXB_ERR_INVALID;
+    if (!vxb::finiteValues(in, (size_t)n * 6))
+        return vxb::fail(ctx->impl, VXB_ERR_INVALID, "forces and torques must be finite");
     return vxb::writeForces(ctx->impl, in, n);
 }
 

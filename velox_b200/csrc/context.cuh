@@ -254,6 +254,11 @@ int readPoses(Context& c, float* out, uint32_t n);
 int writeForces(Context& c, const float* in, uint32_t n);
 int readContacts(Context& c, vx_contact* out, uint32_t cap, uint32_t* count);
 
+// Input validation (validate.cpp), the reference's per-step checks of public state.
+bool validBody(const vx_body& b, size_t hullPoints, size_t faceIndices, std::string& why);
+bool validSolverOptions(const vx_solver_options& o, std::string& why);
+bool finiteValues(const float* v, size_t count);
+
 // Adjoint (adjoint.cu): tape hooks of the device world's step, and the backward pass.
 int tapeBegin(Context& c, uint32_t steps, uint32_t every);
 int tapeEnd(Context& c);
