@@ -173,6 +173,24 @@ int vxb_world_write_forces(vxb_context* ctx, const float* in, uint32_t n);
 int vxb_world_read_contacts(vxb_context* ctx, vx_contact* out, uint32_t cap, uint32_t* count);
 int vxb_world_stats(vxb_context* ctx, vxb_step_stats* out);
 
+/* ---- snapshots of the device world ------------------------------------------
+ * World::saveSnapshot / restoreSnapshot (src/world.cpp:2038-2128) for the
+ * state this library keeps on the device: all body state, the previous step's
+ * contacts (the warm-start cache), the step configuration and the last step's
+ * statistics. A snapshot restores only into a world with the same body count
+ * and world partition (VXB_ERR_INVALID otherwise); restoring ends an adjoint
+ * tape. Stepping after a restore repeats the original steps bit for bit. */
+
+/* Device-memory snapshot slots 0..7 (copies stay on the device: rollback and
+ * replay without host round trips). */
+int vxb_world_snapshot_save(vxb_context* ctx, uint32_t slot);
+int vxb_world_snapshot_restore(vxb_context* ctx, uint32_t slot);
+/* The same state as a byte image in caller memory (files, other contexts):
+ * size, copy out (VXB_ERR_CAPACITY if `capacity` is too small), copy in. */
+int vxb_world_snapshot_bytes(vxb_context* ctx, uint64_t* bytes);
+int vxb_world_snapshot_read(vxb_context* ctx, void* out, uint64_t capacity);
+int vxb_world_snapshot_write(vxb_context* ctx, const void* in, uint64_t size);
+
 /* ---- adjoint of the device world's step ---------------------------------------
  * No counterpart in the reference (it has no differentiation). The adjoint
  * differentiates the step as the device world runs it (src/world.cpp:4007-4397

@@ -184,6 +184,11 @@ def lib(path=LIB_PATH):
         "vxb_stage_distance": ([vp, vp, u32, ctypes.POINTER(Soup), vp, u32, i32, vp], i32),
         "vxb_stage_color": ([vp, vp, u32, vp, u32, vp, p_u32], i32),
         "vxb_stage_pairs_noalloc": ([vp, u32, f32, vp, u32, p_u32, vp], i32),
+        "vxb_world_snapshot_save": ([vp, u32], i32),
+        "vxb_world_snapshot_restore": ([vp, u32], i32),
+        "vxb_world_snapshot_bytes": ([vp, ctypes.POINTER(ctypes.c_uint64)], i32),
+        "vxb_world_snapshot_read": ([vp, vp, ctypes.c_uint64], i32),
+        "vxb_world_snapshot_write": ([vp, vp, ctypes.c_uint64], i32),
         "vxb_tape_begin": ([vp, u32, u32], i32),
         "vxb_tape_info": ([vp, p_u32, p_u32, p_u32], i32),
         "vxb_tape_read": ([vp, vp, vp, vp, vp, vp, vp], i32),
@@ -333,6 +338,25 @@ class Context:
         s = StepStats()
         self._check(self.L.vxb_world_stats(self.h, ctypes.byref(s)))
         return {k: getattr(s, k) for k, _ in StepStats._fields_}
+
+    # ---- snapshots
+    def snapshot_save(self, slot=0):
+        self._check(self.L.vxb_world_snapshot_save(self.h, slot))
+
+    def snapshot_restore(self, slot=0):
+        self._check(self.L.vxb_world_snapshot_restore(self.h, slot))
+
+    def snapshot_bytes(self):
+        """The world's state as a byte image (numpy uint8)."""
+        size = ctypes.c_uint64()
+        self._check(self.L.vxb_world_snapshot_bytes(self.h, ctypes.byref(size)))
+        out = np.zeros(size.value, np.uint8)
+        self._check(self.L.vxb_world_snapshot_read(self.h, ptr(out), size.value))
+        return out
+
+    def snapshot_load(self, image):
+        image = np.ascontiguousarray(image, np.uint8)
+        self._check(self.L.vxb_world_snapshot_write(self.h, ptr(image), image.size))
 
     # ---- adjoint
     def tape_begin(self, steps, checkpoint_every=10):

@@ -117,6 +117,8 @@ void vxb_context_destroy(vxb_context* ctx) {
     cudaSetDevice(c.device);
     if (c.stream) cudaStreamSynchronize(c.stream);
     vxb::tapeEnd(c);
+    for (auto& snap : c.snapshots)
+        if (snap.buf.ptr) cudaFree(snap.buf.ptr);
     vxb::DevBuf* bufs[] = {&c.bodyBuf, &c.aosBuf, &c.worldOfBuf, &c.planeStartBuf, &c.planeListBuf, &c.prevPoseBuf,
                            &c.snapBuf, &c.hullPtsBuf, &c.facesBuf, &c.aabbBuf, &c.cellKeyBuf, &c.cellValBuf,
                            &c.sortKeysAlt, &c.sortValsAlt, &c.sortHist, &c.hashKeyBuf, &c.hashValBuf, &c.pairBuf,
@@ -340,6 +342,39 @@ int vxb_world_stats(vxb_context* ctx, vxb_step_stats* out) {
     if (!ctx || !out) return VXB_ERR_INVALID;
     *out = ctx->impl.stats;
     return VXB_OK;
+}
+
+// ---- snapshots ---------------------------------------------------------------
+
+int vxb_world_snapshot_save(vxb_context* ctx, uint32_t slot) {
+    GUARD(ctx);
+    return vxb::snapshotSave(ctx->impl, slot);
+}
+
+int vxb_world_snapshot_restore(vxb_context* ctx, uint32_t slot) {
+    GUARD(ctx);
+    return vxb::snapshotRestore(ctx->impl, slot);
+}
+
+int vxb_world_snapshot_bytes(vxb_context* ctx, uint64_t* bytes) {
+    GUARD(ctx);
+    if (!bytes) return VXB_ERR_INVALID;
+    size_t b = 0;
+    TRY(vxb::snapshotBytes(ctx->impl, &b));
+    *bytes = b;
+    return VXB_OK;
+}
+
+int vxb_world_snapshot_read(vxb_context* ctx, void* out, uint64_t capacity) {
+    GUARD(ctx);
+    if (!out) return VXB_ERR_INVALID;
+    return vxb::snapshotRead(ctx->impl, out, (size_t)capacity);
+}
+
+int vxb_world_snapshot_write(vxb_context* ctx, const void* in, uint64_t size) {
+    GUARD(ctx);
+    if (!in) return VXB_ERR_INVALID;
+    return vxb::snapshotWrite(ctx->impl, in, (size_t)size);
 }
 
 // ---- adjoint -----------------------------------------------------------------

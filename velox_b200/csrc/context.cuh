@@ -42,6 +42,14 @@ struct DevBuf {
     size_t bytes = 0;
 };
 
+// A snapshot of the device world kept in device memory (snapshot.cu).
+constexpr uint32_t kSnapshotSlots = 8;
+struct DeviceSnapshot {
+    DevBuf buf;                    // body arrays, previous contacts and their keys
+    alignas(8) char header[256];   // layout, configuration and statistics at save time
+    bool valid = false;
+};
+
 // Recording of the device world's steps for the adjoint (adjoint.cu).
 struct Tape {
     bool active = false;
@@ -215,6 +223,7 @@ struct Context {
     StageTimer timer;
 
     Tape tape;
+    DeviceSnapshot snapshots[kSnapshotSlots];
 
     cudaError_t err = cudaSuccess;
 };
@@ -253,6 +262,13 @@ int backendFetchImpulses(Context& c, vx_contact* contacts, uint32_t m);
 int readPoses(Context& c, float* out, uint32_t n);
 int writeForces(Context& c, const float* in, uint32_t n);
 int readContacts(Context& c, vx_contact* out, uint32_t cap, uint32_t* count);
+
+// Snapshots of the device world (snapshot.cu).
+int snapshotSave(Context& c, uint32_t slot);
+int snapshotRestore(Context& c, uint32_t slot);
+int snapshotBytes(Context& c, size_t* bytes);
+int snapshotRead(Context& c, void* out, size_t capacity);
+int snapshotWrite(Context& c, const void* in, size_t size);
 
 // Input validation (validate.cpp), the reference's per-step checks of public state.
 bool validBody(const vx_body& b, size_t hullPoints, size_t faceIndices, std::string& why);
