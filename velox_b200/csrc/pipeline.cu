@@ -1409,7 +1409,7 @@ __global__ void __launch_bounds__(Threads) solveBlockKernel(SolveArgs A, uint32_
 // per-thread arrays in local memory.
 constexpr int kPackRows = 32;
 constexpr int kPackBodies = 64;
-constexpr int kPackChunk = 512;     // tiny islands per packing thread
+constexpr int kPackChunk = 64;      // tiny islands per packing thread (a serial greedy scan each)
 constexpr int kPackWarps = 4;       // warps (packs) per block
 
 // Sort key of a tiny island: its colour count (a pack runs as many colour
@@ -2273,11 +2273,11 @@ __device__ __noinline__ bool caRewind(BodyArrays& B, const Soup& soup, uint32_t 
 // Every flagged pair evaluated in parallel on the probe's state (read-only):
 // in the ordered pass, a flagged pair whose bodies no earlier rewind has moved
 // sees exactly this state, so its outcome can be taken from here.
-// `spread` (1, 2, 4 or 8): threads per pair, so that a few pairs still
-// occupy many SMs and share warps with few others (each is a long serial
-// loop). The working lanes are the first 32 / spread of each warp: local
-// memory interleaves the lanes' words, so contiguous lanes share L1 sectors
-// of their stack frames (lanes 0-7 use one sector of every line).
+// `spread` (1..32): threads per pair, so that a few pairs occupy many SMs
+// and share warps with few others (each is a long serial loop). The working
+// lanes are the first 32 / spread of each warp: local memory interleaves the
+// lanes' words, so contiguous lanes share L1 sectors of their stack frames
+// (lanes 0-7 use one sector of every line).
 __global__ void caSpeculateKernel(BodyArrays B, Soup soup, const uint64_t* pairKeys, const uint32_t* flaggedList,
                                   uint32_t flagged, uint32_t spread, const float4* endGap, float dt,
                                   const float4* prevPos, const float4* prevRot, float4* specState,
@@ -3271,11 +3271,15 @@ static int conservativeAdvancement(Context& c, uint32_t npairs, float dt) {
     uint32_t* specResult = reinterpret_cast<uint32_t*>(specState + 8 * (size_t)flagged);
     uint32_t* flaggedList = specResult + flagged;
     LAUNCH(c, compactKernel, blocksFor(npairs, 256), 256, flags, flagRank, npairs, flaggedList);
-    uint32_t spread = 1;
-    while (spread < 8 && (size_t)flagged * spread * 2 <= (size_t)c.smCount * 64) spread <<= 1;
-    LAUNCH(c, caSpeculateKernel, blocksFor((uint64_t)flagged * spread, 64), 64, c.B, soupOf(c), pk,
-           (const uint32_t*)flaggedList, flagged, spread, (const float4*)endGap, dt, prevPos, prevRot, specState,
-           specResult, c.dCounters);
+    // Spread the flagged pairs evenly over all SMs, one single-warp block per
+    // group of `lanes` pairs: a distance query's latency grows with the number
+    // of stack frames live on its SM (local memory shares the SM's L1), so a
+    // few flagged pairs run one per SM rather than packed into a few warps.
+    uint32_t lanes = 1;
+    while (lanes < 32 && (size_t)lanes * c.smCount < flagged) lanes <<= 1;
+    const uint32_t spread = 32u / lanes;
+    LAUNCH(c, caSpeculateKernel, (flagged + lanes - 1) / lanes, 32, c.B, soupOf(c), pk, (const uint32_t*)flaggedList,
+           flagged, spread, (const float4*)endGap, dt, prevPos, prevRot, specState, specResult, c.dCounters);
     // mark ahead of the cascade before the first pass too (fewer replays)
     {
         const uint32_t* frontier = bodyMark;
