@@ -230,7 +230,8 @@ int vxb_tape_read(vxb_context* ctx, vx_contact* contacts, uint32_t* stepStart, u
  * angular velocity 3), null = zero. Outputs (each nullable): grad = dL/d(state
  * at the tape's first step), n x 13; gradInverseMass = dL/d(invMass) and
  * dL/d(isotropic invInertia), n x 2; gradMass = dL/d(mass) for inertia that
- * scales with mass, n; worldFlags (VXB_ADJ_*), one per world. */
+ * scales with mass, n; worldFlags (VXB_ADJ_*), one per world. Worlds with a
+ * flag get zero gradients. */
 int vxb_adjoint_backward(vxb_context* ctx, const float* seed, float* grad, float* gradInverseMass,
                          float* gradMass, uint32_t* worldFlags);
 /* Releases the tape. */

@@ -55,9 +55,9 @@ def test_injected_failure_falls_back_to_the_cpu(ref, monkeypatch, mode):
     cpu = ref.RefWorld(specs, pool, backend=ref.BACKEND_CPU, strict=True)
     for w in (dev, cpu):
         w.configure(substeps=4, workers=1)
-    dev.step(DT, 1)  # one frame on the device first
-    cpu.set_bodies(dev.bodies())
     assert dev.L.ref_world_backend_name(dev.h) == b"cuda"
+    # the first frame fails on the device and is re-run on the CPU, so it
+    # equals a CPU world's first frame (no warm-start history on either side)
     monkeypatch.setenv("VELOX_CUDA_TEST_FAIL", mode)
     dev.step(DT, 1)
     monkeypatch.delenv("VELOX_CUDA_TEST_FAIL")

@@ -1035,14 +1035,22 @@ __global__ void __launch_bounds__(128) adjointKernel(AdjArgs A) {
             R.reverseStep((uint32_t)t, start);
         }
     }
+    // Worlds outside the model (rewound, diverged, unsupported) get zero
+    // gradients rather than values of another trajectory.
+    __syncwarp();
+    const bool flagged = atomicOr(A.flags + w, 0u) != 0u;
     for (uint32_t li = R.lane; li < R.nb; li += 32) {
-        const BodyBar X = R.V.adj[li];
+        BodyBar X = R.V.adj[li];
+        float2 gm = R.V.gm[li];
+        if (flagged) {
+            X.p = X.q = X.v = X.w = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            gm = make_float2(0.0f, 0.0f);
+        }
         float* g = A.grad + (size_t)(R.b0 + li) * 13;
         g[0] = X.p.x; g[1] = X.p.y; g[2] = X.p.z;
         g[3] = X.q.x; g[4] = X.q.y; g[5] = X.q.z; g[6] = X.q.w;
         g[7] = X.v.x; g[8] = X.v.y; g[9] = X.v.z;
         g[10] = X.w.x; g[11] = X.w.y; g[12] = X.w.z;
-        const float2 gm = R.V.gm[li];
         const Mass m = R.mass(li);
         A.gradInv[2 * (R.b0 + li)] = gm.x;
         A.gradInv[2 * (R.b0 + li) + 1] = gm.y;
