@@ -171,6 +171,12 @@ int vxb_world_read_poses(vxb_context* ctx, float* out, uint32_t n);
  * next step like Body::force/torque. */
 int vxb_world_write_forces(vxb_context* ctx, const float* in, uint32_t n);
 int vxb_world_read_contacts(vxb_context* ctx, vx_contact* out, uint32_t cap, uint32_t* count);
+/* Replaces the warm-start cache (the previous step's contacts, what the next
+ * step matches against: World::prevContacts_, src/world.cpp:4496-4520 and
+ * 4133-4184). `contacts` must be sorted by (a, b) with a < b < n; within one
+ * pair the given order is kept (it decides exact ties of the nearest-point
+ * fallback). m = 0 empties the cache. Ends an adjoint tape. */
+int vxb_world_write_contacts(vxb_context* ctx, const vx_contact* contacts, uint32_t m);
 int vxb_world_stats(vxb_context* ctx, vxb_step_stats* out);
 
 /* ---- snapshots of the device world ------------------------------------------

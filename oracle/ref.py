@@ -73,6 +73,8 @@ def lib(strict=True):
         "ref_world_last_call_ms": ([vp], ctypes.c_double),
         "ref_world_stats": ([vp, vp], None),
         "ref_world_contacts": ([vp, vp, u32], u32),
+        "ref_world_prev_contacts": ([vp, vp, u32], u32),
+        "ref_world_fix_tie_order": ([vp, i32], None),
         "ref_world_found_contacts": ([vp, vp, u32], u32),
         "ref_candidate_pairs": ([vp, u32, f32, vp, u32], u32),
         "ref_body_aabb": ([vp, f32, vp], None),
@@ -120,7 +122,7 @@ def generate_scene(config, seed=None, size=0, strict=False):
 class RefWorld:
     """A reference World built from shape specs (dense index == spec index)."""
 
-    def __init__(self, specs, pool, backend=BACKEND_CUDA_EMULATED, strict=True):
+    def __init__(self, specs, pool, backend=BACKEND_CUDA_EMULATED, strict=True, fix_tie_order=True):
         from velox_b200.binding import BODY  # record layout only
         self._BODY = BODY
         self.L = lib(strict)
@@ -131,6 +133,9 @@ class RefWorld:
         if self.L.ref_world_build(self.h, _p(specs), len(specs), _p(pool)) != 0:
             raise RuntimeError(self.L.ref_last_error().decode())
         self.n = len(specs)
+        # the emulated backend's worlds fix the reference's unspecified
+        # within-pair order of the warm-start cache (no effect elsewhere)
+        self.fix_tie_order(fix_tie_order)
 
     def close(self):
         if self.h:
@@ -178,6 +183,31 @@ class RefWorld:
         m = self.L.ref_world_contacts(self.h, None, 0)
         out = np.zeros(m, CONTACT)
         self.L.ref_world_contacts(self.h, _p(out), m)
+        return out
+
+    def fix_tie_order(self, on=True):
+        """Before each step, order the warm-start cache within a pair by
+        (point, emission order): the reference leaves that order to an
+        unstable sort (emulated backend only)."""
+        self.L.ref_world_fix_tie_order(self.h, 1 if on else 0)
+
+    def found_contacts(self):
+        """The emulated backend's narrow-phase output of the last step (pair
+        order, emission order within a pair, before warm-start matching)."""
+        from velox_b200.binding import CONTACT
+        m = self.L.ref_world_found_contacts(self.h, None, 0)
+        out = np.zeros(m, CONTACT)
+        self.L.ref_world_found_contacts(self.h, _p(out), m)
+        return out
+
+    def prev_contacts(self):
+        """The world's warm-start cache (World::prevContacts_) in its order."""
+        from velox_b200.binding import CONTACT
+        m = self.L.ref_world_prev_contacts(self.h, None, 0)
+        if m == 0xffffffff:
+            raise RuntimeError("the reference's snapshot layout did not parse")
+        out = np.zeros(m, CONTACT)
+        self.L.ref_world_prev_contacts(self.h, _p(out), m)
         return out
 
 

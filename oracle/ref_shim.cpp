@@ -16,6 +16,7 @@
 #include "velox/world.h"
 #include "velox/backend.h"
 #include "velox/sleep.h"
+#include "velox/serialization.h"
 #include "narrowphase.h"
 #include "mass_properties.h"
 #include "velox_b200_types.h"
@@ -24,7 +25,9 @@
 #include <chrono>
 #include <cstring>
 #include <memory>
+#include <stdexcept>
 #include <string>
+#include <utility>
 #include <vector>
 
 static_assert(sizeof(velox::Body) == sizeof(vx_body), "Body layout");
@@ -185,7 +188,12 @@ public:
         const int m = (int)contacts.size();
         if (m == 0) return;
         if (warmStart) {
-            std::sort(contacts.begin(), contacts.end(), contactLess);
+            // backend_cuda.cu:587-595 std::sorts contacts that its kernel
+            // appended in atomic arrival order, so contacts that tie on
+            // (a, b, point) (a box vertex on another box's edge emits the same
+            // point under two feature keys) end in an unspecified order. The
+            // emulation fixes that order: pair order, then emission order.
+            std::stable_sort(contacts.begin(), contacts.end(), contactLess);
             colorOf_.resize(m);
             numColors_ = greedyColor(bodies, contacts.data(), m, colorOf_.data());
             colorStart_.assign(numColors_ + 1, 0);
@@ -276,7 +284,75 @@ struct RefWorld {
     std::vector<Vec3> soupPoints;
     std::vector<uint32_t> soupFaces;
     double lastStepMs = 0.0;
+    bool fixTieOrder = false;
 };
+
+// Offset and count of World::prevContacts_ inside the world's serialized
+// snapshot (SerializationAccess::encode, src/serialization.cpp:263-300: five
+// fixed-size fields, then vectors stored as element size, count and
+// elements; the sixth vector is prevContacts_). False when it does not parse.
+bool locatePrevContacts(const std::vector<uint8_t>& bytes, size_t* offset, uint64_t* count) {
+    size_t at = sizeof(Vec3) + sizeof(int) + sizeof(WorldCcdDefaults) + sizeof(WorldMultiToiSettings) +
+                sizeof(SolverOptions);
+    for (int v = 0; v < 6; ++v) {
+        uint64_t elem = 0, n = 0;
+        if (at + 16 > bytes.size()) return false;
+        std::memcpy(&elem, bytes.data() + at, 8);
+        std::memcpy(&n, bytes.data() + at + 8, 8);
+        at += 16;
+        if (at + elem * n > bytes.size()) return false;
+        if (v == 5) {
+            if (elem != sizeof(Contact)) return false;
+            *offset = at;
+            *count = n;
+            return true;
+        }
+        at += elem * n;
+    }
+    return false;
+}
+
+// World::prevContacts_ is std::sorted on the pair key alone
+// (src/world.cpp:4517-4520), which leaves the order of one pair's contacts
+// unspecified; the nearest-point warm-start fallback (src/world.cpp:4170-4181)
+// takes the first of equally near cached contacts, so contacts that share a
+// point under two feature keys make the result depend on that order. This
+// fixes it to (a, b, point, narrow-phase emission order) by rewriting the
+// cache through the world's own snapshot round trip.
+void fixPrevContactOrder(RefWorld* w) {
+    SerializedScene scene = serializeWorld(*w->world);
+    size_t off = 0;
+    uint64_t m = 0;
+    if (!locatePrevContacts(scene.data, &off, &m)) throw std::runtime_error("snapshot layout did not parse");
+    if (m < 2) return;
+    std::vector<Contact> prev(m);
+    std::memcpy(prev.data(), scene.data.data() + off, m * sizeof(Contact));
+    std::vector<std::pair<uint64_t, uint64_t>> emitted;  // (pair and feature key mix, emission index)
+    const std::vector<Contact>& found = w->emulated->lastFound;
+    auto tag = [](const Contact& c) {
+        return ((uint64_t)c.a << 32 | c.b) * 0x9e3779b97f4a7c15ull ^ c.featureKey;
+    };
+    emitted.reserve(found.size());
+    for (size_t k = 0; k < found.size(); ++k) emitted.push_back({tag(found[k]), (uint64_t)k});
+    std::sort(emitted.begin(), emitted.end());
+    auto rank = [&](const Contact& c) -> uint64_t {
+        auto it = std::lower_bound(emitted.begin(), emitted.end(), std::pair<uint64_t, uint64_t>(tag(c), 0));
+        return it != emitted.end() && it->first == tag(c) ? it->second : ~0ull;
+    };
+    std::vector<std::pair<uint64_t, size_t>> order(m);
+    for (size_t k = 0; k < m; ++k) order[k] = {rank(prev[k]), k};
+    std::stable_sort(order.begin(), order.end(), [&](const auto& x, const auto& y) {
+        const Contact& cx = prev[x.second];
+        const Contact& cy = prev[y.second];
+        if (contactLess(cx, cy)) return true;
+        if (contactLess(cy, cx)) return false;
+        return x.first < y.first;
+    });
+    std::vector<Contact> sorted(m);
+    for (size_t k = 0; k < m; ++k) sorted[k] = prev[order[k].second];
+    std::memcpy(scene.data.data() + off, sorted.data(), m * sizeof(Contact));
+    deserializeWorld(*w->world, scene);
+}
 
 Vec3 V(const vx_vec3& v) { return {v.x, v.y, v.z}; }
 Quat Q(const vx_quat& q) { return {q.x, q.y, q.z, q.w}; }
@@ -434,10 +510,15 @@ uint32_t ref_world_worker_count(void* handle) {
 int ref_world_step(void* handle, float dt, int steps) {
     auto* w = static_cast<RefWorld*>(handle);
     try {
-        auto t0 = std::chrono::steady_clock::now();
-        for (int s = 0; s < steps; ++s) w->world->step(dt);
-        auto t1 = std::chrono::steady_clock::now();
-        w->lastStepMs = std::chrono::duration<double, std::milli>(t1 - t0).count();
+        double ms = 0.0;
+        for (int s = 0; s < steps; ++s) {
+            if (w->fixTieOrder && w->emulated) fixPrevContactOrder(w);
+            auto t0 = std::chrono::steady_clock::now();
+            w->world->step(dt);
+            auto t1 = std::chrono::steady_clock::now();
+            ms += std::chrono::duration<double, std::milli>(t1 - t0).count();
+        }
+        w->lastStepMs = ms;
         return 0;
     } catch (const std::exception& e) {
         g_error = e.what();
@@ -468,6 +549,24 @@ uint32_t ref_world_contacts(void* handle, vx_contact* out, uint32_t cap) {
     if (out) std::memcpy(out, c.data(), std::min(m, cap) * sizeof(Contact));
     return m;
 }
+
+// The world's warm-start cache (World::prevContacts_, in the world's order:
+// sorted by (a, b) by src/world.cpp:4517-4520, within a pair as std::sort left
+// it), read from the world's own serialized snapshot. Returns the count, or
+// ~0u when the layout does not parse.
+uint32_t ref_world_prev_contacts(void* handle, vx_contact* out, uint32_t cap) {
+    auto* w = static_cast<RefWorld*>(handle);
+    const std::vector<uint8_t> bytes = serializeWorld(*w->world).data;
+    size_t off = 0;
+    uint64_t m = 0;
+    if (!locatePrevContacts(bytes, &off, &m)) return ~0u;
+    if (out) std::memcpy(out, bytes.data() + off, std::min<uint64_t>(m, cap) * sizeof(Contact));
+    return (uint32_t)m;
+}
+
+// Test switch (default off): before each step of an emulated-backend world,
+// fix the within-pair order of its warm-start cache (fixPrevContactOrder).
+void ref_world_fix_tie_order(void* handle, int on) { static_cast<RefWorld*>(handle)->fixTieOrder = on != 0; }
 
 // Contacts as the emulated backend's findContacts produced them in the last
 // step (pair order, before warm-start matching).

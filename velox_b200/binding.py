@@ -178,6 +178,7 @@ def lib(path=LIB_PATH):
         "vxb_world_read_poses": ([vp, vp, u32], i32),
         "vxb_world_write_forces": ([vp, vp, u32], i32),
         "vxb_world_read_contacts": ([vp, vp, u32, p_u32], i32),
+        "vxb_world_write_contacts": ([vp, vp, u32], i32),
         "vxb_world_stats": ([vp, ctypes.POINTER(StepStats)], i32),
         "vxb_stage_pairs": ([vp, vp, u32, f32, vp, u32, p_u32], i32),
         "vxb_stage_collide": ([vp, vp, u32, ctypes.POINTER(Soup), vp, u32, f32, vp, u32, vp, p_u32], i32),
@@ -333,6 +334,11 @@ class Context:
         out = np.zeros(cnt.value, CONTACT)
         self._check(self.L.vxb_world_read_contacts(self.h, ptr(out), cnt.value, ctypes.byref(cnt)))
         return out
+
+    def write_contacts(self, contacts):
+        """Replaces the warm-start cache with `contacts` (sorted by (a, b))."""
+        contacts = records(contacts, CONTACT)
+        self._check(self.L.vxb_world_write_contacts(self.h, ptr(contacts), len(contacts)))
 
     def stats(self):
         s = StepStats()

@@ -338,6 +338,21 @@ int vxb_world_read_contacts(vxb_context* ctx, vx_contact* out, uint32_t cap, uin
     return vxb::readContacts(ctx->impl, out, cap, count);
 }
 
+int vxb_world_write_contacts(vxb_context* ctx, const vx_contact* contacts, uint32_t m) {
+    GUARD(ctx);
+    vxb::Context& c = ctx->impl;
+    if (m && !contacts) return VXB_ERR_INVALID;
+    if (c.n == 0) return vxb::fail(c, VXB_ERR_INVALID, "no bodies loaded");
+    for (uint32_t k = 0; k < m; ++k) {
+        const vx_contact& x = contacts[k];
+        if (x.a >= x.b || x.b >= c.n)
+            return vxb::fail(c, VXB_ERR_INVALID, "contact " + std::to_string(k) + ": needs a < b < body count");
+        if (k && (((uint64_t)x.a << 32) | x.b) < (((uint64_t)contacts[k - 1].a << 32) | contacts[k - 1].b))
+            return vxb::fail(c, VXB_ERR_INVALID, "contacts must be sorted by (a, b)");
+    }
+    return vxb::writeContacts(c, contacts, m);
+}
+
 int vxb_world_stats(vxb_context* ctx, vxb_step_stats* out) {
     if (!ctx || !out) return VXB_ERR_INVALID;
     *out = ctx->impl.stats;

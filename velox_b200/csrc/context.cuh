@@ -262,6 +262,7 @@ int backendFetchImpulses(Context& c, vx_contact* contacts, uint32_t m);
 int readPoses(Context& c, float* out, uint32_t n);
 int writeForces(Context& c, const float* in, uint32_t n);
 int readContacts(Context& c, vx_contact* out, uint32_t cap, uint32_t* count);
+int writeContacts(Context& c, const vx_contact* contacts, uint32_t m);
 
 // Snapshots of the device world (snapshot.cu).
 int snapshotSave(Context& c, uint32_t slot);

@@ -18,11 +18,15 @@
 //   rewind       conservative advancement for deep end-of-step overlaps
 //   correction   split-impulse position correction, coloured per island
 #include <algorithm>
+#include <cstddef>
 #include <cstring>
 
 #include "context.cuh"
 
 namespace vxb {
+
+static_assert(sizeof(vx_contact) == 128 && offsetof(vx_contact, spinningImpulse) == 116,
+              "contact record: 120 bytes of fields, 8 of padding");
 
 // ---------------------------------------------------------------------------
 // host helpers
@@ -552,7 +556,12 @@ __global__ void __launch_bounds__(128) collideKernel(BodyArrays B, Soup soup, co
             if (off + (uint32_t)count > contactCap || rec >= recCap) {
                 atomicOr(&C->overflow, 2u);
             } else {
-                for (int x = 0; x < count; ++x) tmp[off + x] = buf[x];
+                for (int x = 0; x < count; ++x) {
+                    tmp[off + x] = buf[x];
+                    // the record's 8 tail bytes are padding: zero them so contact
+                    // images (snapshots, read-back) are deterministic bytes
+                    *reinterpret_cast<uint2*>(reinterpret_cast<char*>(tmp + off + x) + 120) = make_uint2(0u, 0u);
+                }
                 recKeys[rec] = mode == 0 ? (((uint64_t)buf[0].a << bodyBits) | buf[0].b) : (uint64_t)p;
                 recVals[rec] = rec;
                 recInfo[rec] = make_uint2(off, (uint32_t)count);
@@ -3456,6 +3465,21 @@ int readContacts(Context& c, vx_contact* out, uint32_t cap, uint32_t* count) {
                                     cudaMemcpyDeviceToHost, c.stream));
         VXB_CUDA(c, cudaStreamSynchronize(c.stream));
     }
+    return VXB_OK;
+}
+
+int writeContacts(Context& c, const vx_contact* contacts, uint32_t m) {
+    tapeEnd(c);
+    VXB_TRY(ensure(c, c.contactBuf[c.cur ^ 1], (size_t)m * sizeof(vx_contact) + 128));
+    VXB_TRY(ensure(c, c.prevKeyBuf, (size_t)m * 8 + 16));
+    if (m) {
+        VXB_CUDA(c, cudaMemcpyAsync(c.contactBuf[c.cur ^ 1].ptr, contacts, (size_t)m * sizeof(vx_contact),
+                                    cudaMemcpyHostToDevice, c.stream));
+        LAUNCH(c, contactKeysKernel, blocksFor(m, 256), 256, P<vx_contact>(c.contactBuf[c.cur ^ 1]), m,
+               P<uint64_t>(c.prevKeyBuf));
+    }
+    c.prevCount = m;
+    VXB_CUDA(c, cudaStreamSynchronize(c.stream));
     return VXB_OK;
 }
 
