@@ -240,6 +240,20 @@ int vxb_tape_read(vxb_context* ctx, vx_contact* contacts, uint32_t* stepStart, u
  * flag get zero gradients. */
 int vxb_adjoint_backward(vxb_context* ctx, const float* seed, float* grad, float* gradInverseMass,
                          float* gradMass, uint32_t* worldFlags);
+/* vxb_adjoint_backward that also reports the branch decisions the reverse
+ * differentiated (the piece of the piecewise-smooth step the forward took),
+ * one byte each, for checking against an independent adjoint. Layout: worlds
+ * x steps x blocks of *branchRows bytes (world-local contact index within the
+ * step): per substep the live gap's sign (1 = positive); the warm start's
+ * activity; per substep and sweep the row bits (1 restitution condition,
+ * 2 restitution target, 4 normal impulse unclamped, 8 friction rows,
+ * 16 / 32 first / second friction axis bounded, 64 ellipse projection,
+ * 128 row without normal mass); per position pass the push's activity.
+ * *branchBytes receives the size; a null or smaller buffer returns
+ * VXB_ERR_CAPACITY before the reverse runs. */
+int vxb_adjoint_backward_branches(vxb_context* ctx, const float* seed, float* grad, float* gradInverseMass,
+                                  float* gradMass, uint32_t* worldFlags, uint8_t* branches, size_t capacity,
+                                  size_t* branchBytes, uint32_t* branchRows);
 /* Releases the tape. */
 int vxb_tape_end(vxb_context* ctx);
 

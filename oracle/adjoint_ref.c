@@ -22,8 +22,9 @@
  * a contact inherits, world.cpp:4133-4184) and the restitution-reference
  * sources frozen from the forward pass. A contact's approach speed vn0 is its
  * relative normal velocity at its anchors at detection, or the frozen
- * source's vn0. The conservative-advancement rewind is not part of the model
- * (a world that rewound is not smooth).
+ * source's vn0; on the first step, a vn0 carried from before the recorded
+ * steps is the recorded constant. The conservative-advancement rewind is not
+ * part of the model (a world that rewound is not smooth).
  *
  * Everything is double precision; bodies must have isotropic inverse inertia.
  */
@@ -126,6 +127,8 @@ typedef struct {
 
 typedef struct { D3 p; D4 q; D3 v, w; } St;
 
+
+
 typedef struct {
     double dt, gx, gy, gz;
     int substeps, sweeps, positionIterations, stackStabilization;
@@ -153,12 +156,14 @@ typedef struct {
     int a, b, solved;
     D3 n, t1, t2, la, lb;
     double bias0, e, f1, f2;
+    double vn0;  /* as recorded (the constant a first-step carried vn0 takes) */
     int color;
 } Row;
 
 typedef struct {  /* pose terms of one row at one substep */
     D3 ra, rb, raxn, rbxn, raxt1, rbxt1, raxt2, rbxt2;
     double ma, mb, iA, iB, kN, k1, k2, gap, target0;
+    int gpos;  /* the live gap's branch: positive (speculative target) */
 } Prep;
 
 typedef struct {  /* adjoints of the pose terms */
@@ -200,7 +205,8 @@ static void prep(const Mass* M, const St* S, const Row* r, double h, Prep* P) {
     P->k1 = P->ma + P->mb + P->iA * dot(P->raxt1, P->raxt1) + P->iB * dot(P->rbxt1, P->rbxt1);
     P->k2 = P->ma + P->mb + P->iA * dot(P->raxt2, P->raxt2) + P->iB * dot(P->rbxt2, P->rbxt2);
     P->gap = r->bias0 + dot(r->n, sub(add(A->p, P->ra), add(B->p, P->rb)));
-    P->target0 = P->gap > 0.0 ? -P->gap / h : 0.0;
+    P->gpos = P->gap > 0.0;
+    P->target0 = P->gpos ? -P->gap / h : 0.0;
 }
 
 /* reverse of prep: pose-term adjoints -> state and mass adjoints */
@@ -225,7 +231,7 @@ static void prepRev(const Mass* M, const St* S, const Row* r, double h, const Pr
     acc(&Pb->rb, cross(r->t1, Pb->rbxt1));
     acc(&Pb->rb, cross(r->t2, Pb->rbxt2));
     /* live gap */
-    double gapb = P->gap > 0.0 ? -Pb->target0 / h : 0.0;
+    double gapb = P->gpos ? -Pb->target0 / h : 0.0;
     accs(&pb[a], r->n, gapb);
     accs(&Pb->ra, r->n, gapb);
     accs(&pb[b], r->n, -gapb);
@@ -246,8 +252,11 @@ static void applyImpulse(St* A, St* B, const Prep* P, D3 imp, D3 raxI, D3 rbxI, 
     if (dynB) { accs(&B->v, imp, -P->mb); accs(&B->w, rbxI, -P->iB); }
 }
 
-/* one solveContact sweep (two-axis friction) on prepared terms; lam[3] in/out */
-static void rowForward(const Mass* M, St* S, const Row* r, const Prep* P, double vn0, double* lam, RowIn* tape) {
+/* one solveContact sweep (two-axis friction) on prepared terms; lam[3] in/out.
+ * forced >= 0: take the branch decisions from those bits (BR_*) instead of
+ * deciding them (the piece another run took). */
+static void rowForward(const Mass* M, St* S, const Row* r, const Prep* P, double vn0, double* lam, RowIn* tape,
+                       int forced) {
     St* A = &S[r->a];
     St* B = &S[r->b];
     const int dynA = M->prop[r->a].dyn, dynB = M->prop[r->b].dyn;
@@ -256,18 +265,20 @@ static void rowForward(const Mass* M, St* S, const Row* r, const Prep* P, double
         tape->ln = lam[0]; tape->l1 = lam[1]; tape->l2 = lam[2]; tape->bits = 0;
     }
     if (P->kN <= 0.0) { if (tape) tape->bits = BR_SKIP; return; }
+    const int F = forced >= 0;
     int bits = 0;
     double vn = dot(r->n, sub(A->v, B->v)) + dot(P->raxn, A->w) - dot(P->rbxn, B->w);
     double target = P->target0;
-    if (vn0 < -1.0 && (P->gap <= 0.0 || vn > 0.0)) {
+    if (F ? (forced & BR_RESTITUTION) != 0 : (vn0 < -1.0 && (!P->gpos || vn > 0.0))) {
         bits |= BR_RESTITUTION;
         double rest = -r->e * vn0;
-        if (rest > target) { target = rest; bits |= BR_RESMAX; }
+        if (F ? (forced & BR_RESMAX) != 0 : rest > target) { target = rest; bits |= BR_RESMAX; }
     }
     double jn = (target - vn) / P->kN;
     double s = lam[0] + jn;
-    double lnp = s > 0.0 ? s : 0.0;
-    if (s > 0.0) bits |= BR_CLAMP;
+    const int clamp = F ? (forced & BR_CLAMP) != 0 : s > 0.0;
+    double lnp = clamp ? s : 0.0;
+    if (clamp) bits |= BR_CLAMP;
     double dn = lnp - lam[0];
     lam[0] = lnp;
     applyImpulse(A, B, P, mul(r->n, dn), mul(P->raxn, dn), mul(P->rbxn, dn), dynA, dynB);
@@ -277,10 +288,11 @@ static void rowForward(const Mass* M, St* S, const Row* r, const Prep* P, double
         double rv2 = dot(r->t2, sub(A->v, B->v)) + dot(P->raxt2, A->w) - dot(P->rbxt2, B->w);
         double u1 = lam[1] - rv1 / P->k1, u2 = lam[2] - rv2 / P->k2;
         double m1 = r->f1 * lnp, m2 = r->f2 * lnp;
-        if (m1 > 0.0) bits |= BR_M1; else u1 = 0.0;
-        if (m2 > 0.0) bits |= BR_M2; else u2 = 0.0;
-        double E = (m1 > 0.0 ? u1 * u1 / (m1 * m1) : 0.0) + (m2 > 0.0 ? u2 * u2 / (m2 * m2) : 0.0);
-        if (E > 1.0) {
+        const int on1 = F ? (forced & BR_M1) != 0 : m1 > 0.0, on2 = F ? (forced & BR_M2) != 0 : m2 > 0.0;
+        if (on1) bits |= BR_M1; else u1 = 0.0;
+        if (on2) bits |= BR_M2; else u2 = 0.0;
+        double E = (on1 ? u1 * u1 / (m1 * m1) : 0.0) + (on2 ? u2 * u2 / (m2 * m2) : 0.0);
+        if (F ? (forced & BR_ELLIPSE) != 0 : E > 1.0) {
             bits |= BR_ELLIPSE;
             double sc = 1.0 / sqrt(E);
             u1 *= sc; u2 *= sc;
@@ -421,16 +433,16 @@ static void rowReverse(const Mass* M, const Row* r, const Prep* P, double vn0, c
  * spinning impulses are zero in the model) */
 static int warmActive(const double* lam) { return !(lam[0] <= 0.0 && lam[1] == 0.0 && lam[2] == 0.0); }
 
-static void warmForward(const Mass* M, St* S, const Row* r, const Prep* P, const double* lam) {
-    if (!warmActive(lam)) return;
+static void warmForward(const Mass* M, St* S, const Row* r, const Prep* P, const double* lam, int active) {
+    if (!active) return;
     D3 imp = add(add(mul(r->n, lam[0]), mul(r->t1, lam[1])), mul(r->t2, lam[2]));
     applyImpulse(&S[r->a], &S[r->b], P, imp, cross(P->ra, imp), cross(P->rb, imp), M->prop[r->a].dyn,
                  M->prop[r->b].dyn);
 }
 
 static void warmReverse(const Mass* M, const Row* r, const Prep* P, const double* lam, D3* vbA, D3* wbA, D3* vbB,
-                        D3* wbB, double* lamb, PrepBar* Pb) {
-    if (!warmActive(lam)) return;
+                        D3* wbB, double* lamb, PrepBar* Pb, int active) {
+    if (!active) return;
     D3 imp = add(add(mul(r->n, lam[0]), mul(r->t1, lam[1])), mul(r->t2, lam[2]));
     D3 ib = d3(0, 0, 0);
     if (M->prop[r->a].dyn) {
@@ -503,6 +515,89 @@ static double rowVn0Own(const Model* m, const St* S, const Row* r) {
     return dot(r->n, sub(S[r->a].v, S[r->b].v)) + dot(cross(ra, r->n), S[r->a].w) - dot(cross(rb, r->n), S[r->b].w);
 }
 
+/* Branch decisions to follow instead of deciding (adjref_force_branches):
+ * per step, blocks of g_forcedRows bytes indexed by the step's row: per
+ * substep the live gap's sign, the warm start's activity, per substep and
+ * sweep the row bits (BR_*), per position pass the push's activity. */
+static const uint8_t* g_forced = NULL;
+static uint32_t g_forcedRows = 0;
+/* The same layout, written with the decisions a run takes (adjref_record_branches). */
+static uint8_t* g_record = NULL;
+static uint32_t g_recordRows = 0;
+
+static size_t branchBlocks(const adjref_config* c) {
+    return (size_t)c->substeps * (1 + c->sweeps) + 1 + (size_t)c->positionIterations;
+}
+
+static const uint8_t* forcedStep(const Model* m, int t) {
+    if (!g_forced) return NULL;
+    return g_forced + (size_t)t * branchBlocks(m->cfg) * g_forcedRows;
+}
+
+/* block `block`, row k of step t in the recording (NULL when not recording) */
+static uint8_t* recordAt(const Model* m, int t, size_t block, int k) {
+    if (!g_record) return NULL;
+    return g_record + ((size_t)t * branchBlocks(m->cfg) + block) * g_recordRows + (k - (int)m->stepStart[t]);
+}
+
+/* prep with the live gap's branch taken from the forced decisions */
+static void prepAt(const Model* m, const St* S, int t, int sub, int k, double h, Prep* P) {
+    prep(&m->M, S, &m->rows[k], h, P);
+    const uint8_t* f = forcedStep(m, t);
+    if (f) {
+        P->gpos = f[(size_t)sub * g_forcedRows + (k - (int)m->stepStart[t])] != 0;
+        P->target0 = P->gpos ? -P->gap / h : 0.0;
+    }
+    uint8_t* rec = recordAt(m, t, (size_t)sub, k);
+    if (rec) *rec = (uint8_t)P->gpos;
+}
+
+static int warmAt(const Model* m, int t, int k, const double* lam) {
+    const uint8_t* f = forcedStep(m, t);
+    const int active = f ? f[(size_t)m->cfg->substeps * g_forcedRows + (k - (int)m->stepStart[t])] != 0
+                         : warmActive(lam);
+    uint8_t* rec = recordAt(m, t, (size_t)m->cfg->substeps, k);
+    if (rec) *rec = (uint8_t)active;
+    return active;
+}
+
+static int rowForcedAt(const Model* m, int t, int sub, int sweep, int k) {
+    const uint8_t* f = forcedStep(m, t);
+    if (!f) return -1;
+    const size_t R = g_forcedRows, base = ((size_t)m->cfg->substeps + 1) * R;
+    return f[base + ((size_t)sub * m->cfg->sweeps + sweep) * R + (k - (int)m->stepStart[t])];
+}
+
+static int pushForcedAt(const Model* m, int t, int it, int k) {
+    const uint8_t* f = forcedStep(m, t);
+    if (!f) return -1;
+    const size_t R = g_forcedRows, base = ((size_t)m->cfg->substeps * (1 + m->cfg->sweeps) + 1) * R;
+    return f[base + (size_t)it * R + (k - (int)m->stepStart[t])];
+}
+
+/* Relative perturbation of every state component after each substep
+ * (adjref_set_state_noise): a deterministic function of (seed, step,
+ * substep, body, component), so repeated evaluations see the same run. It
+ * stands for an FP32 evaluation's per-substep rounding when estimating how
+ * far the problem's conditioning lets an FP32 gradient sit from this one. */
+static double g_noise = 0.0;
+static uint64_t g_noiseSeed = 0;
+
+static double noiseAt(int t, int s, int i, int c) {
+    uint64_t x = g_noiseSeed ^ ((uint64_t)t << 40) ^ ((uint64_t)s << 32) ^ ((uint64_t)i << 8) ^ (uint64_t)c;
+    x ^= x >> 33; x *= 0xff51afd7ed558ccdull; x ^= x >> 33; x *= 0xc4ceb9fe1a85ec53ull; x ^= x >> 33;
+    return ((double)(x >> 11) / 9007199254740992.0 * 2.0 - 1.0) * g_noise;
+}
+
+static void perturbState(St* S, int t, int s, int i) {
+    S->p.x *= 1.0 + noiseAt(t, s, i, 0); S->p.y *= 1.0 + noiseAt(t, s, i, 1); S->p.z *= 1.0 + noiseAt(t, s, i, 2);
+    S->q.x *= 1.0 + noiseAt(t, s, i, 3); S->q.y *= 1.0 + noiseAt(t, s, i, 4);
+    S->q.z *= 1.0 + noiseAt(t, s, i, 5); S->q.w *= 1.0 + noiseAt(t, s, i, 6);
+    S->v.x *= 1.0 + noiseAt(t, s, i, 7); S->v.y *= 1.0 + noiseAt(t, s, i, 8); S->v.z *= 1.0 + noiseAt(t, s, i, 9);
+    S->w.x *= 1.0 + noiseAt(t, s, i, 10); S->w.y *= 1.0 + noiseAt(t, s, i, 11);
+    S->w.z *= 1.0 + noiseAt(t, s, i, 12);
+}
+
 /* tape of one step */
 typedef struct {
     St* start;      /* state at step start (n) */
@@ -532,21 +627,22 @@ static void stepForward(Model* m, St* S, int t, Tape* T) {
         lam[3 * k] = from[0]; lam[3 * k + 1] = from[1]; lam[3 * k + 2] = from[2];
         if (T) memcpy(T->lamInit + 3 * (k - r0), from, sizeof(double) * 3);
         const int vs = m->vsrc[k];
-        m->vn0[k] = (t > 0 && vs >= 0) ? m->vn0[vs] : rowVn0Own(m, S, &m->rows[k]);
+        m->vn0[k] = vs < 0 ? rowVn0Own(m, S, &m->rows[k]) : t > 0 ? m->vn0[vs] : m->rows[k].vn0;
     }
     Prep* P = (Prep*)malloc(sizeof(Prep) * (R ? R : 1));
     for (int s = 0; s < S_; ++s) {
         if (s > 0) integrateVelocity(m, S, h);
         if (T) memcpy(T->sub + (size_t)s * m->n, S, sizeof(St) * m->n);
         for (int j = 0; j < R; ++j) {
-            prep(&m->M, S, &m->rows[ord[j]], h, &P[j]);
-            hashIn(m, (uint64_t)(P[j].gap > 0.0));
+            prepAt(m, S, t, s, ord[j], h, &P[j]);
+            hashIn(m, (uint64_t)P[j].gpos);
         }
         if (s == 0)
             for (int j = 0; j < R; ++j) {
                 const Row* r = &m->rows[ord[j]];
-                if (r->solved) warmForward(&m->M, S, r, &P[j], lam + 3 * ord[j]);
-                hashIn(m, (uint64_t)warmActive(lam + 3 * ord[j]));
+                const int active = warmAt(m, t, ord[j], lam + 3 * ord[j]);
+                if (r->solved) warmForward(&m->M, S, r, &P[j], lam + 3 * ord[j], active);
+                hashIn(m, (uint64_t)active);
             }
         for (int w = 0; w < W; ++w)
             for (int j = 0; j < R; ++j) {
@@ -555,7 +651,9 @@ static void stepForward(Model* m, St* S, int t, Tape* T) {
                 RowIn* tin = T ? &T->rin[((size_t)s * W + w) * R + j] : NULL;
                 if (!r->solved) { if (tin) tin->bits = BR_SKIP; continue; }
                 RowIn tmp;
-                rowForward(&m->M, S, r, &P[j], m->vn0[k], lam + 3 * k, tin ? tin : &tmp);
+                rowForward(&m->M, S, r, &P[j], m->vn0[k], lam + 3 * k, tin ? tin : &tmp, rowForcedAt(m, t, s, w, k));
+                uint8_t* rec = recordAt(m, t, (size_t)S_ + 1 + (size_t)s * W + w, k);
+                if (rec) *rec = (uint8_t)(tin ? tin->bits : tmp.bits);
                 hashIn(m, (uint64_t)(tin ? tin->bits : tmp.bits));
             }
         if (T) memcpy(T->end + (size_t)s * m->n, S, sizeof(St) * m->n);
@@ -564,6 +662,7 @@ static void stepForward(Model* m, St* S, int t, Tape* T) {
             S[i].p = add(S[i].p, mul(S[i].v, h));
             if (!m->prop[i].rotLocked) S[i].q = qintegrate(S[i].q, S[i].w, h);
             else S[i].w = d3(0, 0, 0);
+            if (g_noise > 0.0) perturbState(&S[i], t, s, i);
         }
     }
     if (T) memcpy(T->corr, S, sizeof(St) * m->n);
@@ -577,7 +676,8 @@ static void stepForward(Model* m, St* S, int t, Tape* T) {
                 D3 ra = anchorArm(&m->prop[r->a], S[r->a].q, r->la);
                 D3 rb = anchorArm(&m->prop[r->b], S[r->b].q, r->lb);
                 double g = r->bias0 + dot(r->n, sub(add(S[r->a].p, ra), add(S[r->b].p, rb)));
-                if (g < -1e-3) {
+                const int forced = pushForcedAt(m, t, it, ord[j]);
+                if (forced >= 0 ? forced != 0 : g < -1e-3) {
                     double resolve = 0.6;
                     if (cfg->stackStabilization) {
                         D3 rv = sub(S[r->a].v, S[r->b].v);
@@ -591,6 +691,8 @@ static void stepForward(Model* m, St* S, int t, Tape* T) {
                 }
             }
             hashIn(m, (uint64_t)active);
+            uint8_t* rec = recordAt(m, t, (size_t)S_ * (1 + W) + 1 + (size_t)it, ord[j]);
+            if (rec) *rec = (uint8_t)active;
             if (T) { T->push[(size_t)it * R + j] = push; T->pact[(size_t)it * R + j] = active; }
         }
     free(P);
@@ -664,7 +766,7 @@ static void stepReverse(Model* m, int t, Tape* T, D3* pb, D4* qb, D3* vb, D3* wb
             accs(&vb[i], pb[i], h);
         }
         memset(Pb, 0, sizeof(PrepBar) * (R ? R : 1));
-        for (int j = 0; j < R; ++j) prep(&m->M, Ss, &m->rows[ord[j]], h, &P[j]);
+        for (int j = 0; j < R; ++j) prepAt(m, Ss, t, s, ord[j], h, &P[j]);
         /* sweeps */
         for (int w = W - 1; w >= 0; --w)
             for (int j = R - 1; j >= 0; --j) {
@@ -681,7 +783,7 @@ static void stepReverse(Model* m, int t, Tape* T, D3* pb, D4* qb, D3* vb, D3* wb
                 const Row* r = &m->rows[k];
                 if (r->solved)
                     warmReverse(&m->M, r, &P[j], T->lamInit + 3 * (k - r0), &vb[r->a], &wb[r->a], &vb[r->b],
-                                &wb[r->b], lamb + 3 * k, &Pb[j]);
+                                &wb[r->b], lamb + 3 * k, &Pb[j], warmAt(m, t, k, T->lamInit + 3 * (k - r0)));
             }
             /* restitution references of this step: own detection or a source */
             for (int j = 0; j < R; ++j) {
@@ -690,7 +792,10 @@ static void stepReverse(Model* m, int t, Tape* T, D3* pb, D4* qb, D3* vb, D3* wb
                 const double g = rvn0b[j] + vn0b[k];
                 if (g == 0.0 || !r->solved) continue;
                 const int vs = m->vsrc[k];
-                if (t > 0 && vs >= 0) { vn0b[vs] += g; continue; }
+                if (vs >= 0) {  /* carried: to its source, or a constant from before the recorded steps */
+                    if (t > 0) vn0b[vs] += g;
+                    continue;
+                }
                 /* vn0 = n.(va - vb) + (ra x n).wa - (rb x n).wb at detection (= Ss for s == 0) */
                 accs(&vb[r->a], r->n, g);
                 accs(&vb[r->b], r->n, -g);
@@ -800,6 +905,7 @@ int adjref_run(const adjref_config* cfg, const vx_body* bodies, uint32_t n, cons
             tangents(r->n, &r->t1, &r->t2);
             r->la = fromf(c->localAnchorA); r->lb = fromf(c->localAnchorB);
             r->bias0 = c->bias0; r->e = c->restitution; r->f1 = c->friction1; r->f2 = c->friction2;
+            r->vn0 = c->vn0;
             r->color = color[k];
             const uint32_t prev0 = t > 0 ? stepStart[t - 1] : 0;
             m.src[k] = src[2 * k] == 0xffffffffu ? -1 : (int32_t)(prev0 + src[2 * k]);
@@ -872,4 +978,27 @@ int adjref_run(const adjref_config* cfg, const vx_body* bodies, uint32_t n, cons
     free(S); free(prop); free(gIm); free(gIi); free(m.rows); free(m.src); free(m.vsrc); free(m.lamRec);
     free(m.lamFin); free(m.vn0); free(m.order);
     return 0;
+}
+
+/* Follow the given branch decisions (layout at g_forced; rows = bytes per
+ * block) in the following adjref_run calls, instead of deciding them: the
+ * derivative of the piece another run took. Null stops it. */
+void adjref_force_branches(const uint8_t* bits, uint32_t rows) {
+    g_forced = bits;
+    g_forcedRows = rows;
+}
+
+/* Write the branch decisions of the following adjref_run calls to `out`
+ * (the layout adjref_force_branches reads; rows = bytes per block, at least
+ * the most rows of any step). Null stops it. */
+void adjref_record_branches(uint8_t* out, uint32_t rows) {
+    g_record = out;
+    g_recordRows = rows;
+}
+
+/* Perturb the state by up to `relative` after every substep of the following
+ * adjref_run calls (0 = off); `seed` picks the perturbation. */
+void adjref_set_state_noise(double relative, uint64_t seed) {
+    g_noise = relative;
+    g_noiseSeed = seed;
 }

@@ -358,14 +358,27 @@ def adjref():
     L.adjref_run.argtypes = [ctypes.POINTER(AdjConfig), vp, ctypes.c_uint32, vp, vp, vp, vp, vp, vp, vp,
                              ctypes.c_uint32, vp, vp, vp, vp, vp, ctypes.POINTER(ctypes.c_uint64)]
     L.adjref_run.restype = ctypes.c_int
+    L.adjref_force_branches.argtypes = [vp, ctypes.c_uint32]
+    L.adjref_force_branches.restype = None
+    L.adjref_record_branches.argtypes = [vp, ctypes.c_uint32]
+    L.adjref_record_branches.restype = None
+    L.adjref_set_state_noise.argtypes = [ctypes.c_double, ctypes.c_uint64]
+    L.adjref_set_state_noise.restype = None
     _adjref = L
     return L
 
 
-def adjoint_reference(cfg, bodies, state0, inv_mass, inv_inertia, contacts, step_start, src, color, seed=None):
+def adjoint_reference(cfg, bodies, state0, inv_mass, inv_inertia, contacts, step_start, src, color, seed=None,
+                      branches=None, record=None, noise=0.0, noise_seed=0):
     """FP64 frozen-contact rollout from state0 (n x 13: p, q, v, w) over the
     recorded contacts of each step. Returns (final state, branch hash) and, with
-    a seed (dL/d final state), also (dL/d state0, dL/d invMass, dL/d invInertia)."""
+    a seed (dL/d final state), also (dL/d state0, dL/d invMass, dL/d invInertia).
+    `branches` (steps x blocks x rows uint8, one world's slice of
+    Context.adjoint_backward_branches): follow those branch decisions instead
+    of deciding them. `record` (an array of that shape): receives the
+    decisions the run takes. `noise` > 0: perturb the state by up to that
+    relative amount after every substep (seeded by `noise_seed`), an FP32-like
+    evaluation for estimating the problem's conditioning."""
     from velox_b200.binding import BODY, CONTACT, records  # record layouts only (no library load)
     L = adjref()
     n = len(bodies)
@@ -385,9 +398,21 @@ def adjoint_reference(cfg, bodies, state0, inv_mass, inv_inertia, contacts, step
         grad = np.zeros((n, 13), np.float64)
         gim = np.zeros(n, np.float64)
         gii = np.zeros(n, np.float64)
-    rc = L.adjref_run(ctypes.byref(cfg), _p(bodies), n, _p(state0), _p(inv_mass),
-                      _p(inv_inertia), _p(contacts), _p(step_start), _p(src), _p(color), len(step_start) - 1,
-                      _p(out), _p(seed), _p(grad), _p(gim), _p(gii), ctypes.byref(h))
+    if branches is not None:
+        branches = np.ascontiguousarray(branches, np.uint8)
+        L.adjref_force_branches(_p(branches), branches.shape[-1])
+    if record is not None:
+        assert record.dtype == np.uint8 and record.flags["C_CONTIGUOUS"]
+        L.adjref_record_branches(_p(record), record.shape[-1])
+    L.adjref_set_state_noise(float(noise), int(noise_seed))
+    try:
+        rc = L.adjref_run(ctypes.byref(cfg), _p(bodies), n, _p(state0), _p(inv_mass),
+                          _p(inv_inertia), _p(contacts), _p(step_start), _p(src), _p(color), len(step_start) - 1,
+                          _p(out), _p(seed), _p(grad), _p(gim), _p(gii), ctypes.byref(h))
+    finally:
+        L.adjref_force_branches(None, 0)
+        L.adjref_record_branches(None, 0)
+        L.adjref_set_state_noise(0.0, 0)
     if rc != 0:
         raise ValueError("adjoint restatement: anisotropic inverse inertia")
     if seed is None:

@@ -130,3 +130,46 @@ def test_adjoint_restatement_per_parameter(ref):
             assert abs(fd - gim[i]) <= 1e-5 * max(1.0, abs(fd)), (i, fd, gim[i])
             checked += 1
     assert checked >= 10
+
+
+def _branch_blocks(cfg):
+    return cfg.substeps * (1 + cfg.sweeps) + 1 + cfg.positionIterations
+
+
+def test_forced_branches_reproduce_the_run_and_make_the_piece_smooth(ref):
+    # The decisions a run takes, fed back, reproduce it bit for bit; with the
+    # decisions held, central differences of the piece match the adjoint even
+    # where the free model sits on a kink (an exactly resting stack).
+    steps = 8
+    bodies, c, ss, src, col, state0 = _frozen_rollout_inputs(ref, steps)
+    cfg = ref.AdjConfig.make()
+    im = bodies["invMass"].astype(np.float64)
+    ii = bodies["invInertia"][:, 0].astype(np.float64)
+    rows = int(np.diff(ss).max())
+    rec = np.zeros((steps, _branch_blocks(cfg), rows), np.uint8)
+    seed = np.random.default_rng(4).normal(size=state0.shape)
+    seed[bodies["motionType"] != 2] = 0.0
+    out, h, grad, gim, gii = ref.adjoint_reference(cfg, bodies, state0, im, ii, c, ss, src, col, seed=seed,
+                                                   record=rec)
+    assert rec.any()
+    out2, h2, grad2, gim2, gii2 = ref.adjoint_reference(cfg, bodies, state0, im, ii, c, ss, src, col, seed=seed,
+                                                        branches=rec)
+    assert np.array_equal(out, out2) and np.array_equal(grad, grad2) and np.array_equal(gim, gim2)
+    # the stack at exact rest: the free model's hash changes under any perturbation
+    rest = state0.copy()
+    rest[1:5, 0:3] = np.round(rest[1:5, 0:3] * 2) / 2  # exact half-unit lattice: corners at zero gap
+    rest[1:5, 7:13] = 0.0
+    rest[1:5, 3:7] = (0.0, 0.0, 0.0, 1.0)
+    rec[:] = 0
+    _, h0, g0, _, _ = ref.adjoint_reference(cfg, bodies, rest, im, ii, c, ss, src, col, seed=seed, record=rec)
+    rng = np.random.default_rng(6)
+    eps = 1e-7  # the held piece bends sharply away from its own decisions: a tight stencil
+    for trial in range(6):
+        d = rng.normal(size=rest.shape)
+        d[bodies["motionType"] != 2] = 0.0
+        d[:, 3:7] = 0.0
+        lp, _ = ref.adjoint_reference(cfg, bodies, rest + eps * d, im, ii, c, ss, src, col, branches=rec)
+        lm, _ = ref.adjoint_reference(cfg, bodies, rest - eps * d, im, ii, c, ss, src, col, branches=rec)
+        fd = np.sum((lp - lm) * seed) / (2 * eps)
+        predicted = np.sum(g0 * d)
+        assert abs(fd - predicted) <= 1e-5 * max(1.0, abs(fd)), (trial, fd, predicted)

@@ -194,6 +194,7 @@ def lib(path=LIB_PATH):
         "vxb_tape_info": ([vp, p_u32, p_u32, p_u32], i32),
         "vxb_tape_read": ([vp, vp, vp, vp, vp, vp, vp], i32),
         "vxb_adjoint_backward": ([vp, vp, vp, vp, vp, vp], i32),
+        "vxb_adjoint_backward_branches": ([vp, vp, vp, vp, vp, vp, vp, ctypes.c_size_t, vp, vp], i32),
         "vxb_tape_end": ([vp], i32),
         "vxb_scene_generate": ([i32, ctypes.c_uint64, u32, vp, u32, p_u32, vp, u32, p_u32], i32),
         "vxb_bodies_from_specs": ([vp, u32, vp, vp, vp, u32, p_u32, vp, u32, p_u32], i32),
@@ -404,6 +405,30 @@ class Context:
         flags = np.zeros(self.worlds, np.uint32)
         self._check(self.L.vxb_adjoint_backward(self.h, ptr(seed), ptr(grad), ptr(ginv), ptr(gmass), ptr(flags)))
         return grad, ginv, gmass, flags
+
+    def adjoint_backward_branches(self, seed=None):
+        """adjoint_backward plus the branch decisions the reverse
+        differentiated: uint8 array (worlds, steps, blocks, rows) with blocks
+        [substeps live-gap signs, warm start, substeps x sweeps row bits,
+        position passes push activity] (vxb_adjoint_backward_branches)."""
+        n = self.bodies_n
+        seed = None if seed is None else np.ascontiguousarray(seed, np.float32).reshape(n, 13)
+        grad = np.zeros((n, 13), np.float32)
+        ginv = np.zeros((n, 2), np.float32)
+        gmass = np.zeros(n, np.float32)
+        flags = np.zeros(self.worlds, np.uint32)
+        need, rows = ctypes.c_size_t(), ctypes.c_uint32()
+        st = self.L.vxb_adjoint_backward_branches(self.h, ptr(seed), None, None, None, None, None, 0,
+                                                   ctypes.byref(need), ctypes.byref(rows))
+        if st != 5:  # VXB_ERR_CAPACITY: the size query
+            self._check(st)
+        bits = np.zeros(need.value, np.uint8)
+        self._check(self.L.vxb_adjoint_backward_branches(self.h, ptr(seed), ptr(grad), ptr(ginv), ptr(gmass),
+                                                         ptr(flags), ptr(bits), need.value, ctypes.byref(need),
+                                                         ctypes.byref(rows)))
+        steps = self.tape_info()["recorded"]
+        blocks = need.value // max(1, self.worlds * steps * rows.value)
+        return grad, ginv, gmass, flags, bits.reshape(self.worlds, steps, blocks, rows.value)
 
     def tape_end(self):
         self._check(self.L.vxb_tape_end(self.h))

@@ -59,6 +59,12 @@ namespace {
 template <class T> T* PT(DevBuf& b) { return reinterpret_cast<T*>(b.ptr); }
 
 constexpr uint32_t kNone = 0xffffffffu;
+// Row branch bits as the backward reports them (the FP64 restatement's
+// numbering): restitution condition, restitution target taken, normal impulse
+// unclamped, friction rows present, each friction axis bounded, ellipse
+// projection; kBrSkip for a row without normal mass.
+constexpr uint32_t kBrRestitution = 1, kBrResMax = 2, kBrClamp = 4, kBrFriction = 8, kBrM1 = 16, kBrM2 = 32,
+                   kBrEllipse = 64, kBrSkip = 128;
 constexpr uint32_t kNoColour = 0x7fffffffu;
 
 inline uint32_t gridFor(uint64_t items, int threads) {
@@ -266,6 +272,8 @@ struct AdjArgs {
     float* gradInv;                // n x 2 (invMass, isotropic invInertia)
     float* gradMass;               // n
     uint32_t* flags;               // worlds
+    uint8_t* branches;             // optional: branch decisions, worlds x steps x branchStep
+    size_t branchStep;             // (S + 1 + S*W + PI) * MR bytes per world and step
     char* scratch;
     size_t worldBytes;
     // offsets inside a world's slice
@@ -363,6 +371,13 @@ struct WorldRun {
     VXD void copyState(float4* dst, const float4* from) const {
         for (uint32_t k = lane; k < 4 * A.NB; k += 32) dst[k] = from[k];
         __syncwarp();
+    }
+
+    // Branch decisions of step t (null unless requested): per substep the live
+    // gap's sign, the warm start's activity, per substep and sweep the row bits,
+    // per position pass the push's activity; MR entries each, world-local rows.
+    VXD uint8_t* branchesOf(uint32_t t) const {
+        return A.branches ? A.branches + ((size_t)w * A.steps + t) * A.branchStep : nullptr;
     }
 
     VXD uint32_t rowsOf(uint32_t t, uint32_t& c0) const {
@@ -568,10 +583,15 @@ struct WorldRun {
     }
 
     // Reverse of one sweepRow (two-axis friction) from its recorded inputs.
-    VXD void rowReverse(uint32_t j, const vx_contact& cc, const float4* rec, const float4* poseState) {
+    VXD void rowReverse(uint32_t j, const vx_contact& cc, const float4* rec, const float4* poseState,
+                        uint8_t* bitsOut) {
         const uint32_t la = cc.a - b0, lb = cc.b - b0;
         const RowPrep& P = V.prep[j];
-        if (P.kNormal <= 0.0f) return;
+        if (P.kNormal <= 0.0f) {
+            if (bitsOut) *bitsOut = kBrSkip;
+            return;
+        }
+        uint32_t bits = 0;
         SolverBody a = body(poseState, la), b = body(poseState, lb);
         a.v = f3(rec[0]); a.w = f3(rec[1]); b.v = f3(rec[2]); b.w = f3(rec[3]);
         const float ln = rec[0].w, l1 = rec[1].w, l2 = rec[2].w;
@@ -583,12 +603,14 @@ struct WorldRun {
         float target = P.targetBase;
         bool resMax = false;
         if (cc.vn0 < -1.0f && (P.liveGap <= 0.0f || vn > 0.0f)) {
+            bits |= kBrRestitution;
             const float rest = -cc.restitution * cc.vn0;
-            if (rest > target) { target = rest; resMax = true; }
+            if (rest > target) { target = rest; resMax = true; bits |= kBrResMax; }
         }
         const float jn = (target - vn) / P.kNormal;
         const float s = ln + jn;
         const bool clampOn = s > 0.0f;  // vmax(s, 0) == s
+        if (clampOn) bits |= kBrClamp;
         const float lnp = vmax(s, 0.0f);
         const float dn = lnp - ln;
         const V3 ni = n * dn;
@@ -613,9 +635,11 @@ struct WorldRun {
             const float max1 = cc.friction1 * lnp;
             const float max2 = cc.friction2 * lnp;
             const bool m1on = max1 > 0.0f, m2on = max2 > 0.0f;
+            bits |= kBrFriction | (m1on ? kBrM1 : 0u) | (m2on ? kBrM2 : 0u);
             const float z1 = m1on ? next1 : 0.0f, z2 = m2on ? next2 : 0.0f;
             const float E = (m1on ? z1 * z1 / (max1 * max1) : 0.0f) + (m2on ? z2 * z2 / (max2 * max2) : 0.0f);
             const bool ell = E > 1.0f;
+            if (ell) bits |= kBrEllipse;
             const float sc = ell ? 1.0f / sqrtf(E) : 1.0f;
             const float y1 = z1 * sc, y2 = z2 * sc;
             const float d1 = y1 - l1, d2 = y2 - l2;
@@ -694,12 +718,15 @@ struct WorldRun {
         if (dynA) { A_.v = pack(VA, 0.0f); A_.w = pack(WA, 0.0f); addGm(la, mA, gImA, gIiA); }
         if (dynB) { B_.v = pack(VB, 0.0f); B_.w = pack(WB, 0.0f); addGm(lb, mB, gImB, gIiB); }
         V.lamb[0][j] = make_float4(lnb, l1b, l2b, lb4.w);
+        if (bitsOut) *bitsOut = (uint8_t)bits;
     }
 
     // Reverse of warmPrepRow (linear impulses; rolling and spinning are zero).
-    VXD void warmReverse(uint32_t j, const vx_contact& cc) {
+    VXD void warmReverse(uint32_t j, const vx_contact& cc, uint8_t* activeOut) {
         const float4 l = V.lamInit[j];
-        if (l.x <= 0.0f && l.y == 0.0f && l.z == 0.0f) return;
+        const bool active = !(l.x <= 0.0f && l.y == 0.0f && l.z == 0.0f);
+        if (activeOut) *activeOut = active ? 1u : 0u;
+        if (!active) return;
         const uint32_t la = cc.a - b0, lb = cc.b - b0;
         const RowPrep& P = V.prep[j];
         const Mass mA = mass(la), mB = mass(lb);
@@ -779,6 +806,8 @@ struct WorldRun {
         const uint32_t m = rowsOf(t, c0);
         const vx_contact* cs = A.contacts;
         const int S = A.substeps, W = A.sweeps;
+        uint8_t* br = branchesOf(t);
+        const size_t MR = A.MR, oWarm = (size_t)S * MR, oRows = oWarm + MR, oPush = oRows + (size_t)S * W * MR;
         // previous step's row adjoints start at zero; sources index the
         // previous step's contacts, whose world range starts at pbase
         uint32_t pc0 = 0, pm = 0, pbase = 0;
@@ -795,6 +824,7 @@ struct WorldRun {
                 for (uint32_t x = r0 + lane; x < r1; x += 32) {
                     const uint32_t j = V.order[x];
                     const float push = V.push[(size_t)it * A.MR + j];
+                    if (br) br[oPush + (size_t)it * MR + j] = push != 0.0f ? 1u : 0u;
                     if (push == 0.0f) continue;
                     const vx_contact& cc = cs[c0 + j];
                     const uint32_t la = cc.a - b0, lb = cc.b - b0;
@@ -866,6 +896,7 @@ struct WorldRun {
                 RowContact r;
                 loadRowContact(cc, V.lamInit[j], r);
                 prepRow(a, b, r, A.h, false, V.prep[j]);
+                if (br) br[(size_t)sub * MR + j] = V.prep[j].liveGap > 0.0f ? 1u : 0u;
                 PrepBar z = {};
                 V.pbar[j] = z;
             }
@@ -878,7 +909,7 @@ struct WorldRun {
                         const vx_contact& cc = cs[c0 + j];
                         if (!solved(cc)) continue;
                         const float4* rec = V.rin + (((size_t)sub * W + sweep) * A.MR + j) * 4;
-                        rowReverse(j, cc, rec, ss);
+                        rowReverse(j, cc, rec, ss, br ? br + oRows + ((size_t)sub * W + sweep) * MR + j : nullptr);
                     }
                     __syncwarp();
                 }
@@ -888,7 +919,7 @@ struct WorldRun {
                     for (uint32_t x = r0 + lane; x < r1; x += 32) {
                         const uint32_t j = V.order[x];
                         const vx_contact& cc = cs[c0 + j];
-                        if (solved(cc)) warmReverse(j, cc);
+                        if (solved(cc)) warmReverse(j, cc, br ? br + oWarm + j : nullptr);
                     }
                     __syncwarp();
                 }
@@ -902,7 +933,9 @@ struct WorldRun {
                         const float g = V.lamb[0][j].w;
                         if (g == 0.0f || !solved(cc)) continue;
                         const uint2 sr = A.src[c0 + j];
-                        if (t > 0 && sr.y != kNone) continue;  // carried: handled with the impulses below
+                        // carried: handled with the impulses below, or (first taped
+                        // step) a constant from before the tape
+                        if (sr.y != kNone) continue;
                         const uint32_t la = cc.a - b0, lb = cc.b - b0;
                         const Mass mA = mass(la), mB = mass(lb);
                         const V3 n{cc.normal.x, cc.normal.y, cc.normal.z};
@@ -1154,8 +1187,9 @@ int tapeEnd(Context& c) {
     T.active = false;
     T.recorded = 0;
     T.stepStart.assign(1, 0u);
-    if (T.contacts.ptr || T.ckpt.ptr || T.scratch.ptr) cudaStreamSynchronize(c.stream);
-    for (DevBuf* b : {&T.contacts, &T.src, &T.color, &T.worldStart, &T.ckpt, &T.flags, &T.scratch, &T.host}) {
+    if (T.contacts.ptr || T.ckpt.ptr || T.scratch.ptr || T.branches.ptr) cudaStreamSynchronize(c.stream);
+    for (DevBuf* b : {&T.contacts, &T.src, &T.color, &T.worldStart, &T.ckpt, &T.flags, &T.scratch, &T.host,
+                      &T.branches}) {
         if (b->ptr) cudaFree(b->ptr);
         b->ptr = nullptr;
         b->bytes = 0;
@@ -1188,7 +1222,8 @@ int tapeRead(Context& c, vx_contact* contacts, uint32_t* stepStart, uint32_t* sr
 }
 
 int adjointBackward(Context& c, const float* seed, float* grad, float* gradInv, float* gradMass,
-                    uint32_t* worldFlags) {
+                    uint32_t* worldFlags, uint8_t* branches, size_t branchCapacity, size_t* branchBytes,
+                    uint32_t* branchRows) {
     Tape& T = c.tape;
     if (!T.active || T.recorded != T.steps)
         return fail(c, VXB_ERR_INVALID, "adjoint: the tape has not recorded all of its steps");
@@ -1258,6 +1293,18 @@ int adjointBackward(Context& c, const float* seed, float* grad, float* gradInv, 
     A.gradInv = dGradInv;
     A.gradMass = dGradMass;
     A.flags = PT<uint32_t>(T.flags);
+    const bool wantBranches = branchBytes != nullptr || branches != nullptr;
+    if (wantBranches) {
+        A.branchStep = ((size_t)substeps * (1 + std::max(A.sweeps, 1)) + 1 + (size_t)std::max(A.posIters, 1)) * A.MR;
+        const size_t need = A.branchStep * steps * worlds;
+        if (branchBytes) *branchBytes = need;
+        if (branchRows) *branchRows = A.MR;
+        if (!branches || branchCapacity < need)
+            return fail(c, VXB_ERR_CAPACITY, "adjoint: branch buffer smaller than the reported size");
+        AD_TRY(ensure(c, T.branches, need));
+        AD_CUDA(c, cudaMemsetAsync(T.branches.ptr, 0, need, c.stream));
+        A.branches = PT<uint8_t>(T.branches);
+    }
     // per-world scratch layout
     auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
     const size_t NBs = A.NB, MRs = A.MR;
@@ -1290,6 +1337,9 @@ int adjointBackward(Context& c, const float* seed, float* grad, float* gradInv, 
     if (gradMass) AD_CUDA(c, cudaMemcpyAsync(gradMass, dGradMass, (size_t)n * 4, cudaMemcpyDeviceToHost, c.stream));
     if (worldFlags)
         AD_CUDA(c, cudaMemcpyAsync(worldFlags, T.flags.ptr, (size_t)worlds * 4, cudaMemcpyDeviceToHost, c.stream));
+    if (A.branches)
+        AD_CUDA(c, cudaMemcpyAsync(branches, A.branches, A.branchStep * steps * worlds, cudaMemcpyDeviceToHost,
+                                   c.stream));
     AD_CUDA(c, cudaStreamSynchronize(c.stream));
     return VXB_OK;
 }

@@ -424,6 +424,15 @@ int vxb_adjoint_backward(vxb_context* ctx, const float* seed, float* grad, float
     return vxb::adjointBackward(ctx->impl, seed, grad, gradInverseMass, gradMass, worldFlags);
 }
 
+int vxb_adjoint_backward_branches(vxb_context* ctx, const float* seed, float* grad, float* gradInverseMass,
+                                  float* gradMass, uint32_t* worldFlags, uint8_t* branches, size_t capacity,
+                                  size_t* branchBytes, uint32_t* branchRows) {
+    GUARD(ctx);
+    if (!branchBytes || !branchRows) return VXB_ERR_INVALID;
+    return vxb::adjointBackward(ctx->impl, seed, grad, gradInverseMass, gradMass, worldFlags, branches, capacity,
+                                branchBytes, branchRows);
+}
+
 int vxb_tape_end(vxb_context* ctx) {
     GUARD(ctx);
     return vxb::tapeEnd(ctx->impl);

@@ -63,6 +63,7 @@ struct Tape {
     DevBuf flags;       // uint32 per world (VXB_ADJ_*)
     DevBuf scratch;     // backward: per-world working memory
     DevBuf host;        // backward: small device arrays (body ranges, seeds, gradients)
+    DevBuf branches;    // backward: branch decisions, when requested
 };
 
 // Device-side counters and flags (one small allocation, read back once per call).
@@ -289,6 +290,7 @@ int tapeStepEnd(Context& c, uint32_t m);
 int tapeRead(Context& c, vx_contact* contacts, uint32_t* stepStart, uint32_t* src, int32_t* color, float* ckpt,
              uint32_t* worldFlags);
 int adjointBackward(Context& c, const float* seed, float* grad, float* gradInv, float* gradMass,
-                    uint32_t* worldFlags);
+                    uint32_t* worldFlags, uint8_t* branches = nullptr, size_t branchCapacity = 0,
+                    size_t* branchBytes = nullptr, uint32_t* branchRows = nullptr);
 
 }  // namespace vxb
