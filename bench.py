@@ -39,6 +39,15 @@ L2_FLUSH_BYTES = 256 << 20
 SOLVER_BYTES_PER_ROW = 328
 # Rewind: one distance query reads both bodies' 256-byte records.
 REWIND_BYTES_PER_QUERY = 512
+# Memory-bound stages: (stage, algorithmic bytes per body, per candidate pair).
+# prepare: velocity integration 60 + pose copy 56; broadphase: AABB 72, keys
+# 44, cell table 12, neighbour search 36 per body + 8 per emitted pair;
+# cell_sort: 4 passes x (8 + 4) B read and written per body.
+MEMORY_STAGE_BYTES = [("prepare", 116, 0), ("broadphase", 164, 8), ("cell_sort", 96, 0)]
+# DRAM bytes per step of the same stages on the 100,001-body scene: the sum of
+# their kernels' dram__bytes_read.sum + dram__bytes_write.sum per launch from
+# one ncu capture each (writes stay in L2 within a launch).
+MEMORY_STAGE_TRAFFIC = {"prepare": 16.02e6, "broadphase": 11.21e6 + 4.81e6 + 2.78e6 + 9.16e6}
 
 
 def measured_peaks():
@@ -459,6 +468,8 @@ def main():
     events = []
     contacts_total = 0
     gap_queries_total = 0
+    pairs_total = 0
+    chain_us = 0
     if args.profile:
         torch.cuda.cudart().cudaProfilerStart()
     checkpoints = []
@@ -477,6 +488,8 @@ def main():
             st = ctx.stats()
             contacts_total += st["contacts"]
             gap_queries_total += st["rewindGapQueries"]
+            pairs_total += st["candidatePairs"]
+            chain_us += st["rewindSpeculateMicros"] + st["rewindCriticalMicros"]
     if args.profile:
         torch.cuda.cudart().cudaProfilerStop()
     barrier()
@@ -509,7 +522,26 @@ def main():
                        "peak_source": peak_kind, "traffic": None,
                        "algorithmic_bytes_per_launch": rewind_bytes / max(rewind_calls, 1),
                        "avg_launch_ms": rewind_ms / max(rewind_calls, 1),
+                       # the pass's own dependency chain: the longest single pair's
+                       # conservative advancement (speculated in parallel) plus the
+                       # longest chain of the ordered pass
+                       "chain_ms_per_step": chain_us / 1e3 / args.steps,
+                       "chain_frac": (chain_us / 1e3) / rewind_ms if rewind_ms > 0 else None,
                        "note": "a chain of dependent distance queries: latency-bound, not bandwidth-bound"}
+    # Memory-bound stages: algorithmic bytes per step (the per-unit figures in
+    # MEMORY_STAGE_BYTES) over the stage's own CUDA-event time.
+    memory_rooflines = []
+    for name, per_body, per_pair in MEMORY_STAGE_BYTES:
+        st_ms, st_calls = stage[name]
+        if st_ms <= 0:
+            continue
+        algo = per_body * n * args.steps + per_pair * pairs_total
+        gbs = algo / (st_ms / 1e3) / 1e9
+        memory_rooflines.append({"stage": name, "bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s",
+                                 "frac": gbs / peak, "peak_source": peak_kind,
+                                 "algorithmic_bytes_per_step": algo / args.steps,
+                                 "ms_per_step": st_ms / args.steps,
+                                 "traffic": MEMORY_STAGE_TRAFFIC.get(name)})
     dominant = max(stage.items(), key=lambda kv: kv[1][0])[0]
     roofline = rewind_roofline if dominant == "rewind" else solve_roofline
     roofline = dict(roofline, stage=dominant)
@@ -576,6 +608,7 @@ def main():
             "contacts_per_s": contacts_total / (ms / 1e3), "last_step": stats,
             "stage_ms_per_step": {k: v[0] / args.steps for k, v in stage.items()},
             "roofline": roofline, "solve_roofline": solve_roofline, "rewind_roofline": rewind_roofline,
+            "memory_rooflines": memory_rooflines,
             "cpu_baseline": baseline, "e2e": e2e, "clocks": clocks,
             "gpu_launches": int(launches), "plain_gpu": plain_gpu}
     line.update(extra)

@@ -72,6 +72,8 @@ typedef struct vxb_step_stats {
     uint32_t rewindReplays;      /* rewind passes replayed with a widened body set */
     uint32_t rewindGapQueries;   /* distance queries of the rewind passes */
     uint32_t rewindCriticalMicros; /* evaluation time along the longest rewind dependency chain */
+    uint32_t rewindSpeculateMicros; /* the longest single pair's conservative advancement (speculated
+                                       in parallel before the ordered pass; part of that chain) */
 } vxb_step_stats;
 
 /* ---- library / context ------------------------------------------------ */

@@ -122,7 +122,8 @@ def generate_scene(config, seed=None, size=0, strict=False):
 class RefWorld:
     """A reference World built from shape specs (dense index == spec index)."""
 
-    def __init__(self, specs, pool, backend=BACKEND_CUDA_EMULATED, strict=True, fix_tie_order=True):
+    def __init__(self, specs, pool, backend=BACKEND_CUDA_EMULATED, strict=True, fix_tie_order=True,
+                 reverse_ties=False):
         from velox_b200.binding import BODY  # record layout only
         self._BODY = BODY
         self.L = lib(strict)
@@ -135,7 +136,7 @@ class RefWorld:
         self.n = len(specs)
         # the emulated backend's worlds fix the reference's unspecified
         # within-pair order of the warm-start cache (no effect elsewhere)
-        self.fix_tie_order(fix_tie_order)
+        self.fix_tie_order(fix_tie_order, reverse_ties)
 
     def close(self):
         if self.h:
@@ -185,11 +186,13 @@ class RefWorld:
         self.L.ref_world_contacts(self.h, _p(out), m)
         return out
 
-    def fix_tie_order(self, on=True):
+    def fix_tie_order(self, on=True, reverse=False):
         """Before each step, order the warm-start cache within a pair by
         (point, emission order): the reference leaves that order to an
-        unstable sort (emulated backend only)."""
-        self.L.ref_world_fix_tie_order(self.h, 1 if on else 0)
+        unstable sort (emulated backend only). reverse: ties in reverse
+        emission order there and in the contact sort (another order the
+        reference allows)."""
+        self.L.ref_world_fix_tie_order(self.h, (2 if reverse else 1) if on else 0)
 
     def found_contacts(self):
         """The emulated backend's narrow-phase output of the last step (pair

@@ -193,6 +193,7 @@ public:
             // (a, b, point) (a box vertex on another box's edge emits the same
             // point under two feature keys) end in an unspecified order. The
             // emulation fixes that order: pair order, then emission order.
+            if (reverseTies) std::reverse(contacts.begin(), contacts.end());
             std::stable_sort(contacts.begin(), contacts.end(), contactLess);
             colorOf_.resize(m);
             numColors_ = greedyColor(bodies, contacts.data(), m, colorOf_.data());
@@ -239,6 +240,7 @@ public:
 
     std::vector<Contact> solve_;
     std::vector<Contact> lastFound;
+    bool reverseTies = false;  // ties in reverse emission order (a second valid realisation)
     std::vector<uint64_t> lastPairs;
     std::vector<Vec3> soupPoints;
     std::vector<uint32_t> soupFaces;
@@ -284,7 +286,7 @@ struct RefWorld {
     std::vector<Vec3> soupPoints;
     std::vector<uint32_t> soupFaces;
     double lastStepMs = 0.0;
-    bool fixTieOrder = false;
+    int fixTieOrder = 0;  // 0 left to std::sort, 1 emission order, 2 reverse emission order
 };
 
 // Offset and count of World::prevContacts_ inside the world's serialized
@@ -340,7 +342,11 @@ void fixPrevContactOrder(RefWorld* w) {
         return it != emitted.end() && it->first == tag(c) ? it->second : ~0ull;
     };
     std::vector<std::pair<uint64_t, size_t>> order(m);
-    for (size_t k = 0; k < m; ++k) order[k] = {rank(prev[k]), k};
+    const bool reverse = w->fixTieOrder == 2;
+    for (size_t k = 0; k < m; ++k) {
+        const uint64_t r = rank(prev[k]);
+        order[k] = {reverse && r != ~0ull ? ~0ull - 1 - r : r, k};
+    }
     std::stable_sort(order.begin(), order.end(), [&](const auto& x, const auto& y) {
         const Contact& cx = prev[x.second];
         const Contact& cy = prev[y.second];
@@ -564,9 +570,16 @@ uint32_t ref_world_prev_contacts(void* handle, vx_contact* out, uint32_t cap) {
     return (uint32_t)m;
 }
 
-// Test switch (default off): before each step of an emulated-backend world,
-// fix the within-pair order of its warm-start cache (fixPrevContactOrder).
-void ref_world_fix_tie_order(void* handle, int on) { static_cast<RefWorld*>(handle)->fixTieOrder = on != 0; }
+// Test switch (default 0, off): before each step of an emulated-backend world,
+// fix the within-pair order of its warm-start cache (fixPrevContactOrder);
+// 1 = emission order (the order the device keeps), 2 = reverse emission order
+// for ties both there and in the backend's contact sort (another order the
+// reference allows, to find the steps that depend on it).
+void ref_world_fix_tie_order(void* handle, int mode) {
+    auto* w = static_cast<RefWorld*>(handle);
+    w->fixTieOrder = mode;
+    if (w->emulated) w->emulated->reverseTies = mode == 2;
+}
 
 // Contacts as the emulated backend's findContacts produced them in the last
 // step (pair order, before warm-start matching).

@@ -66,3 +66,21 @@ def test_pyramid_shares_points_and_depends_on_the_order(ref):
     assert differs_at is not None and differs_at >= 2
     plain.close()
     fixed.close()
+
+
+def test_the_two_tie_orders_agree_without_ties_and_differ_on_the_pyramid(ref):
+    for kind, size, substeps, differs in [("dense", 400, 4, False), (3, 1, 8, True)]:
+        w, specs, pool, bodies, soup = reference_scene(ref, kind, size)
+        w.close()
+        a = ref.RefWorld(specs, pool)
+        b = ref.RefWorld(specs, pool, reverse_ties=True)
+        for x in (a, b):
+            x.configure(substeps=substeps, workers=1)
+        seen = False
+        for _ in range(5):
+            a.step(DT, 1)
+            b.step(DT, 1)
+            seen |= not np.array_equal(_state(a.bodies()), _state(b.bodies()))
+        assert seen == differs, kind
+        a.close()
+        b.close()

@@ -115,7 +115,7 @@ class StepStats(ctypes.Structure):
                                                "largestIsland", "rewinds", "velocityIterations",
                                                "warmStarted", "colorRounds", "giantIslands",
                                                "rewindRounds", "rewindReplays", "rewindGapQueries",
-                                               "rewindCriticalMicros")]
+                                               "rewindCriticalMicros", "rewindSpeculateMicros")]
 
 
 def ptr(a):

@@ -93,6 +93,7 @@ struct Counters {
     uint32_t planFault;      // a solve kernel found an inconsistent island plan
     uint32_t caGapQueries;   // distance queries of the rewind passes
     uint32_t caCritMicros;   // rewind: evaluation time along the longest dependency chain
+    uint32_t caSpecMicros;   // rewind: the longest single speculated pair
     uint32_t tinyIslands;    // islands of at most tinyLimit contacts (packed solve)
     uint32_t tinyPacks;      // warps they were packed into
     uint32_t caFlagged;      // pairs the rewind probe flagged

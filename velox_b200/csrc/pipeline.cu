@@ -2279,6 +2279,12 @@ __device__ __noinline__ bool caRewind(BodyArrays& B, const Soup& soup, uint32_t 
     return true;
 }
 
+VXD uint64_t globalTimerNs() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
 // Every flagged pair evaluated in parallel on the probe's state (read-only):
 // in the ordered pass, a flagged pair whose bodies no earlier rewind has moved
 // sees exactly this state, so its outcome can be taken from here.
@@ -2298,15 +2304,11 @@ __global__ void caSpeculateKernel(BodyArrays B, Soup soup, const uint64_t* pairK
         const uint32_t r = flaggedList[k];
         uint32_t i, j;
         orientPair(B, pairKeys[r], i, j);
+        const uint64_t t0 = globalTimerNs();
         specResult[k] = caRewind(B, soup, i, j, dt, prevPos, prevRot, &C->caGapQueries, endGap + r,
                                  specState + 8 * (size_t)k) ? 1u : 0u;
+        atomicMax(&C->caSpecMicros, (uint32_t)((globalTimerNs() - t0) / 1000u));
     }
-}
-
-VXD uint64_t globalTimerNs() {
-    uint64_t t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
 }
 
 // Rewind pass over the candidate pairs as a dataflow. A candidate's
@@ -3439,6 +3441,7 @@ static int stepOnce(Context& c) {
     c.stats.rewindReplays = c.caWidenings;
     c.stats.rewindGapQueries = c.hostCounters.caGapQueries;
     c.stats.rewindCriticalMicros = c.hostCounters.caCritMicros;
+    c.stats.rewindSpeculateMicros = c.hostCounters.caSpecMicros;
     c.stats.warmStarted = c.hostCounters.warmStarted;
     c.stats.velocityIterations = (uint32_t)(2 * cfg.solver.velocityIterations * substeps);
     if (c.hostCounters.timeout) return fail(c, VXB_ERR_TIMEOUT, "a bounded device wait gave up");
