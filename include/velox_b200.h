@@ -55,6 +55,34 @@ typedef struct vxb_step_config {
     vx_solver_options solver;
 } vxb_step_config;
 
+/* Sleeping thresholds (velox::SleepConfig, include/velox/sleep.h:98-140;
+ * vxb_sleep_config_default gives the reference's defaults). */
+typedef struct vxb_sleep_config {
+    float linearVelocityThreshold;   /* 0.05 m/s */
+    float angularVelocityThreshold;  /* 0.05 rad/s */
+    float accelerationThreshold;     /* 0.01 m/s^2 */
+    float timeToSleep;               /* 0.5 s */
+    float timeToDrowsy;              /* 0.25 s */
+    float contactStabilityThreshold; /* 0.02 m/s */
+    int32_t contactStabilityFrames;  /* 10 */
+    uint8_t enableGradualSleep;      /* 1 */
+    uint8_t enableContactStability;  /* 1 */
+    uint8_t pad[2];
+} vxb_sleep_config;
+
+/* A contact or sensor event of the last step (velox::ContactEvent,
+ * include/velox/world.h:65-75, with dense body indices a < b instead of
+ * handles). type: 0 Begin, 1 Persist, 2 End. */
+typedef struct vxb_contact_event {
+    uint32_t a, b;
+    vx_vec3 point;
+    vx_vec3 normal;  /* from a towards b */
+    float impulse;
+    uint8_t type;
+    uint8_t sensor;
+    uint8_t pad[2];
+} vxb_contact_event;
+
 /* Counters of the last device step (subset of velox::StepStats,
  * include/velox/world.h:175-208, plus pipeline internals). */
 typedef struct vxb_step_stats {
@@ -180,6 +208,25 @@ int vxb_world_read_contacts(vxb_context* ctx, vx_contact* out, uint32_t cap, uin
  * fallback). m = 0 empties the cache. Ends an adjoint tape. */
 int vxb_world_write_contacts(vxb_context* ctx, const vx_contact* contacts, uint32_t m);
 int vxb_world_stats(vxb_context* ctx, vxb_step_stats* out);
+
+/* ---- sleeping and contact events of the device world -------------------------
+ * Every step runs the reference's wake pass (src/world.cpp:4106-4128, after
+ * detection, before warm starting), island sleeping (SleepManager::update,
+ * src/sleep.cpp:52-237: union-find islands over dynamic-dynamic contacts,
+ * contact stability, calm timers, the island minimum, drowsy / asleep
+ * transitions) and keeps the cached contacts of resting pairs for warm
+ * starting (src/world.cpp:4496-4521), whenever a loaded body may sleep
+ * (enableSleep) or is asleep. Body read-back carries `asleep` and
+ * `sleepTimer`. */
+void vxb_sleep_config_default(vxb_sleep_config* out);
+/* Replaces the sleeping thresholds (default: the reference's). */
+int vxb_world_configure_sleep(vxb_context* ctx, const vxb_sleep_config* config);
+/* Contact and sensor events (src/world.cpp:4398-4488): off by default (they
+ * cost a sort and two small read-backs per step); when on, every step
+ * records Begin / Persist / End events in the reference's order. */
+int vxb_world_enable_events(vxb_context* ctx, int enable);
+/* The last step's events; *count receives their number (out nullable). */
+int vxb_world_read_events(vxb_context* ctx, vxb_contact_event* out, uint32_t cap, uint32_t* count);
 
 /* ---- snapshots of the device world ------------------------------------------
  * World::saveSnapshot / restoreSnapshot (src/world.cpp:2038-2128) for the

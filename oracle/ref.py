@@ -74,6 +74,8 @@ def lib(strict=True):
         "ref_world_stats": ([vp, vp], None),
         "ref_world_contacts": ([vp, vp, u32], u32),
         "ref_world_prev_contacts": ([vp, vp, u32], u32),
+        "ref_world_events": ([vp, vp, u32], u32),
+        "ref_world_sleep_config": ([vp, f32, f32, f32, f32, f32, f32, i32, i32, i32], None),
         "ref_world_fix_tie_order": ([vp, i32], None),
         "ref_world_found_contacts": ([vp, vp, u32], u32),
         "ref_candidate_pairs": ([vp, u32, f32, vp, u32], u32),
@@ -202,6 +204,21 @@ class RefWorld:
         out = np.zeros(m, CONTACT)
         self.L.ref_world_found_contacts(self.h, _p(out), m)
         return out
+
+    def events(self):
+        """The last step's contact events (dense indices; velox_b200 EVENT layout)."""
+        from velox_b200.binding import EVENT
+        k = self.L.ref_world_events(self.h, None, 0)
+        out = np.zeros(k, EVENT)
+        self.L.ref_world_events(self.h, _p(out), k)
+        return out
+
+    def sleep_config(self, cfg):
+        """World::sleepConfig() from a velox_b200 SleepConfig."""
+        self.L.ref_world_sleep_config(self.h, cfg.linearVelocityThreshold, cfg.angularVelocityThreshold,
+                                      cfg.accelerationThreshold, cfg.timeToSleep, cfg.timeToDrowsy,
+                                      cfg.contactStabilityThreshold, cfg.contactStabilityFrames,
+                                      cfg.enableGradualSleep, cfg.enableContactStability)
 
     def prev_contacts(self):
         """The world's warm-start cache (World::prevContacts_) in its order."""

@@ -472,6 +472,62 @@ void ref_world_set_bodies(void* handle, const vx_body* in) {
         std::memcpy(&w->world->body(w->ids[i]), &in[i], sizeof(Body));
 }
 
+// The last step's contact events (World::contactEvents) with dense body
+// indices, in the record layout of vxb_contact_event (a, b, point, normal,
+// impulse, type, sensor, 2 pad bytes: 40 bytes). Returns the count.
+struct RefEvent {
+    uint32_t a, b;
+    float point[3], normal[3];
+    float impulse;
+    uint8_t type, sensor, pad[2];
+};
+static_assert(sizeof(RefEvent) == 40, "event record");
+
+uint32_t ref_world_events(void* handle, void* out, uint32_t cap) {
+    auto* w = static_cast<RefWorld*>(handle);
+    const std::vector<ContactEvent>& ev = w->world->contactEvents();
+    if (out) {
+        std::vector<std::pair<uint64_t, uint32_t>> index(w->ids.size());
+        for (size_t i = 0; i < w->ids.size(); ++i) index[i] = {w->ids[i].value, (uint32_t)i};
+        std::sort(index.begin(), index.end());
+        auto dense = [&](BodyId id) {
+            auto it = std::lower_bound(index.begin(), index.end(), std::make_pair(id.value, 0u));
+            return it != index.end() && it->first == id.value ? it->second : ~0u;
+        };
+        RefEvent* o = static_cast<RefEvent*>(out);
+        for (size_t k = 0; k < ev.size() && k < cap; ++k) {
+            RefEvent r;
+            std::memset(&r, 0, sizeof(r));
+            r.a = dense(ev[k].a);
+            r.b = dense(ev[k].b);
+            r.point[0] = ev[k].point.x; r.point[1] = ev[k].point.y; r.point[2] = ev[k].point.z;
+            r.normal[0] = ev[k].normal.x; r.normal[1] = ev[k].normal.y; r.normal[2] = ev[k].normal.z;
+            r.impulse = ev[k].impulse;
+            r.type = (uint8_t)ev[k].type;
+            r.sensor = ev[k].sensor ? 1 : 0;
+            o[k] = r;
+        }
+    }
+    return (uint32_t)ev.size();
+}
+
+// World::sleepConfig(): the thresholds the device library takes as
+// vxb_sleep_config, in its field order.
+void ref_world_sleep_config(void* handle, float linear, float angular, float acceleration, float timeToSleep,
+                            float timeToDrowsy, float stabilityThreshold, int stabilityFrames, int gradual,
+                            int stability) {
+    SleepConfig& c = static_cast<RefWorld*>(handle)->world->sleepConfig();
+    c.linearVelocityThreshold = linear;
+    c.angularVelocityThreshold = angular;
+    c.accelerationThreshold = acceleration;
+    c.timeToSleep = timeToSleep;
+    c.timeToDrowsy = timeToDrowsy;
+    c.contactStabilityThreshold = stabilityThreshold;
+    c.contactStabilityFrames = stabilityFrames;
+    c.enableGradualSleep = gradual != 0;
+    c.enableContactStability = stability != 0;
+}
+
 // Copies the hull soup; returns the number of points, writes the number of
 // face indices to *faceIndexCount. Pass null buffers to query sizes.
 uint32_t ref_world_soup(void* handle, vx_vec3* points, uint32_t* faces,

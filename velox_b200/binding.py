@@ -74,11 +74,35 @@ SPEC = np.dtype({
     "offsets": [0, 1, 4, 8, 12, 16, 20, 32, 44, 60, 72, 84, 88, 92, 104, 108, 112],
     "itemsize": 116})
 
+EVENT = np.dtype({
+    "names": ["a", "b", "point", "normal", "impulse", "type", "sensor"],
+    "formats": [np.uint32, np.uint32, _v3, _v3, np.float32, np.uint8, np.uint8],
+    "offsets": [0, 4, 8, 20, 32, 36, 37],
+    "itemsize": 40})
+EVENT_TYPES = {0: "begin", 1: "persist", 2: "end"}
+
 # Contact fields that carry physics (padding bytes excluded).
 CONTACT_FLOAT_FIELDS = ["normal", "point", "localAnchorA", "localAnchorB", "gap", "bias0", "vn0",
                         "restitution", "friction1", "friction2", "rollingFriction", "spinningFriction",
                         "normalImpulse", "tangentImpulse1", "tangentImpulse2", "rollingImpulse1",
                         "rollingImpulse2", "spinningImpulse"]
+
+
+class SleepConfig(ctypes.Structure):
+    """vxb_sleep_config (velox::SleepConfig's thresholds)."""
+    _fields_ = [("linearVelocityThreshold", ctypes.c_float), ("angularVelocityThreshold", ctypes.c_float),
+                ("accelerationThreshold", ctypes.c_float), ("timeToSleep", ctypes.c_float),
+                ("timeToDrowsy", ctypes.c_float), ("contactStabilityThreshold", ctypes.c_float),
+                ("contactStabilityFrames", ctypes.c_int32), ("enableGradualSleep", ctypes.c_uint8),
+                ("enableContactStability", ctypes.c_uint8), ("pad", ctypes.c_uint8 * 2)]
+
+    @classmethod
+    def default(cls, **kw):
+        c = cls()
+        lib().vxb_sleep_config_default(ctypes.byref(c))
+        for k, v in kw.items():
+            setattr(c, k, v)
+        return c
 
 
 class SolverOptions(ctypes.Structure):
@@ -179,6 +203,10 @@ def lib(path=LIB_PATH):
         "vxb_world_write_forces": ([vp, vp, u32], i32),
         "vxb_world_read_contacts": ([vp, vp, u32, p_u32], i32),
         "vxb_world_write_contacts": ([vp, vp, u32], i32),
+        "vxb_sleep_config_default": ([vp], None),
+        "vxb_world_configure_sleep": ([vp, vp], i32),
+        "vxb_world_enable_events": ([vp, i32], i32),
+        "vxb_world_read_events": ([vp, vp, u32, p_u32], i32),
         "vxb_world_stats": ([vp, ctypes.POINTER(StepStats)], i32),
         "vxb_stage_pairs": ([vp, vp, u32, f32, vp, u32, p_u32], i32),
         "vxb_stage_collide": ([vp, vp, u32, ctypes.POINTER(Soup), vp, u32, f32, vp, u32, vp, p_u32], i32),
@@ -334,6 +362,21 @@ class Context:
         self._check(self.L.vxb_world_read_contacts(self.h, None, 0, ctypes.byref(cnt)))
         out = np.zeros(cnt.value, CONTACT)
         self._check(self.L.vxb_world_read_contacts(self.h, ptr(out), cnt.value, ctypes.byref(cnt)))
+        return out
+
+    def configure_sleep(self, config=None, **kw):
+        """Sleeping thresholds (SleepConfig.default(**kw) when config is None)."""
+        config = config or SleepConfig.default(**kw)
+        self._check(self.L.vxb_world_configure_sleep(self.h, ctypes.byref(config)))
+
+    def enable_events(self, on=True):
+        self._check(self.L.vxb_world_enable_events(self.h, 1 if on else 0))
+
+    def read_events(self):
+        cnt = ctypes.c_uint32()
+        self._check(self.L.vxb_world_read_events(self.h, None, 0, ctypes.byref(cnt)))
+        out = np.zeros(cnt.value, EVENT)
+        self._check(self.L.vxb_world_read_events(self.h, ptr(out), cnt.value, ctypes.byref(cnt)))
         return out
 
     def write_contacts(self, contacts):

@@ -91,6 +91,7 @@ int vxb_context_create(int device, vxb_context** out) {
     if (!ctx) return VXB_ERR_OOM;
     Context& c = ctx->impl;
     c.device = device;
+    vxb::sleepConfigDefault(&c.sleep.config);
     if (const char* limit = std::getenv("VXB_WAIT_LIMIT")) {  // polls; 0 or unset = the default
         const unsigned long v = std::strtoul(limit, nullptr, 10);
         if (v > 0 && v <= vxb::kSpinLimit) c.waitLimit = (uint32_t)v;
@@ -336,6 +337,37 @@ int vxb_world_write_forces(vxb_context* ctx, const float* in, uint32_t n) {
 int vxb_world_read_contacts(vxb_context* ctx, vx_contact* out, uint32_t cap, uint32_t* count) {
     GUARD(ctx);
     return vxb::readContacts(ctx->impl, out, cap, count);
+}
+
+void vxb_sleep_config_default(vxb_sleep_config* out) {
+    if (out) vxb::sleepConfigDefault(out);
+}
+
+int vxb_world_configure_sleep(vxb_context* ctx, const vxb_sleep_config* config) {
+    GUARD(ctx);
+    if (!config) return VXB_ERR_INVALID;
+    const float v[] = {config->linearVelocityThreshold, config->angularVelocityThreshold,
+                       config->accelerationThreshold, config->timeToSleep, config->timeToDrowsy,
+                       config->contactStabilityThreshold};
+    for (float x : v)
+        if (!std::isfinite(x) || x < 0.0f)
+            return vxb::fail(ctx->impl, VXB_ERR_INVALID, "sleep thresholds and times must be finite and >= 0");
+    if (config->contactStabilityFrames < 0 || config->contactStabilityFrames > 65535)
+        return vxb::fail(ctx->impl, VXB_ERR_INVALID, "contactStabilityFrames must be in [0, 65535]");
+    ctx->impl.sleep.config = *config;
+    return VXB_OK;
+}
+
+int vxb_world_enable_events(vxb_context* ctx, int enable) {
+    GUARD(ctx);
+    ctx->impl.sleep.events = enable != 0;
+    if (!ctx->impl.sleep.events) ctx->impl.sleep.eventCount = 0;
+    return VXB_OK;
+}
+
+int vxb_world_read_events(vxb_context* ctx, vxb_contact_event* out, uint32_t cap, uint32_t* count) {
+    GUARD(ctx);
+    return vxb::readEvents(ctx->impl, out, cap, count);
 }
 
 int vxb_world_write_contacts(vxb_context* ctx, const vx_contact* contacts, uint32_t m) {

@@ -118,6 +118,20 @@ struct StageTimer {
     uint64_t calls[kStageCount] = {};
 };
 
+// Island sleeping and contact events of the device world (sleep.cu).
+struct SleepState {
+    vxb_sleep_config config{};
+    bool events = false;          // record contact events (vxb_world_enable_events)
+    uint32_t sleepable = 0;       // dynamic bodies loaded with enableSleep
+    uint32_t asleep = 0;          // bodies asleep after the last step (an upper bound between steps)
+    uint32_t pairCount = 0;       // pair keys of the last step (active and resting pairs)
+    uint32_t eventCount = 0;      // events of the last step
+    DevBuf state;                 // float4 per body: sleepTimer, stable frames, state (0/1/2), enableSleep
+    DevBuf pairs;                 // sorted unique pair keys of the last step
+    DevBuf pairsNext, eventBuf;   // this step's pair keys (unsorted) and events
+    DevBuf keys, vals, flags, ranks, small, list, parent, bodyBits, kept, merge;
+};
+
 struct Context {
     int device = 0;
     int smCount = 148;
@@ -175,6 +189,8 @@ struct Context {
     DevBuf contactBuf[2];  // key-sorted contacts: current / previous step
     int cur = 0;
     uint32_t prevCount = 0;     // contacts held in contactBuf[cur ^ 1]
+    uint32_t stepContacts = 0;  // of those, the last step's own (the rest: resting pairs kept for warm starting)
+    DevBuf stepPosBuf;          // positions of the last step's own contacts in the cache (when some are kept)
     DevBuf prevKeyBuf;          // (a<<32|b) of the previous contacts
     DevBuf pairKeyBuf;          // (a<<32|b) per record in sorted order (CA pairs)
     DevBuf recOffsetBuf;        // first contact of each sorted record
@@ -225,6 +241,7 @@ struct Context {
     StageTimer timer;
 
     Tape tape;
+    SleepState sleep;
     DeviceSnapshot snapshots[kSnapshotSlots];
 
     cudaError_t err = cudaSuccess;
@@ -265,6 +282,20 @@ int readPoses(Context& c, float* out, uint32_t n);
 int writeForces(Context& c, const float* in, uint32_t n);
 int readContacts(Context& c, vx_contact* out, uint32_t cap, uint32_t* count);
 int writeContacts(Context& c, const vx_contact* contacts, uint32_t m);
+// Island sleeping and contact events (sleep.cu).
+int sleepLoad(Context& c, const vx_body* host, uint32_t n);
+int sleepExport(Context& c, vx_body* aosDevice);
+bool sleepActive(const Context& c);
+int wakePass(Context& c, const vx_contact* cs, uint32_t m);
+int sleepAndEvents(Context& c, const vx_contact* cs, uint32_t m, float dt, uint32_t* kept);
+int mergeKeptContacts(Context& c, uint32_t m, uint32_t kept);
+int readEvents(Context& c, vxb_contact_event* out, uint32_t cap, uint32_t* count);
+int readStepContacts(Context& c, vx_contact* out, uint32_t m);
+void sleepConfigDefault(vxb_sleep_config* c);
+// Pipeline pieces the sleep pass shares (pipeline.cu).
+int sortPairs(Context& c, uint64_t* keys, uint32_t* vals, uint32_t n, int bits);
+int exclusiveScan(Context& c, const uint32_t* in, uint32_t* out, uint32_t n, uint32_t* grandTotal);
+int unionRoots(Context& c, const vx_contact* cs, uint32_t m, uint32_t* parent);
 
 // Snapshots of the device world (snapshot.cu).
 int snapshotSave(Context& c, uint32_t slot);

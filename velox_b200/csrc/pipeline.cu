@@ -682,7 +682,7 @@ __global__ void scanApplyKernel(const uint32_t* in, uint32_t n, const uint32_t* 
     if (grandTotal && blockIdx.x == gridDim.x - 1 && threadIdx.x == blockDim.x - 1) *grandTotal = ex;
 }
 
-static int exclusiveScan(Context& c, const uint32_t* in, uint32_t* out, uint32_t n, uint32_t* grandTotal) {
+int exclusiveScan(Context& c, const uint32_t* in, uint32_t* out, uint32_t n, uint32_t* grandTotal) {
     if (n == 0) return VXB_OK;
     const uint32_t blocks = (n + kScanTile - 1) / kScanTile;
     VXB_TRY(ensure(c, c.scanTmp, (size_t)blocks * 4 + 16));
@@ -2550,7 +2550,7 @@ __global__ void contactKeysKernel(const vx_contact* cs, uint32_t m, uint64_t* ke
 // host orchestration
 // ===========================================================================
 
-static int sortPairs(Context& c, uint64_t* keys, uint32_t* vals, uint32_t n, int bits) {
+int sortPairs(Context& c, uint64_t* keys, uint32_t* vals, uint32_t n, int bits) {
     if (n <= 1 || bits <= 0) return VXB_OK;
     const uint32_t tiles = (n + kSortTile - 1) / kSortTile;
     VXB_TRY(ensure(c, c.sortKeysAlt, (size_t)n * 8));
@@ -2562,6 +2562,18 @@ static int sortPairs(Context& c, uint64_t* keys, uint32_t* vals, uint32_t n, int
     cudaError_t e = cudaSuccess;
     c.launches += radixSortPairs(keys, vals, n, 0, bits, c.sortScratch, c.stream, &e);
     if (e != cudaSuccess) return cudaStatus(c, e, "radix sort");
+    return VXB_OK;
+}
+
+// Union-find roots (parent[i] = the root of i) over the dynamic-dynamic
+// contacts of `cs` that involve no sensor (the islands of SleepManager::update,
+// src/sleep.cpp:63-91, and of the solve).
+int unionRoots(Context& c, const vx_contact* cs, uint32_t m, uint32_t* parent) {
+    LAUNCH(c, iotaKernel, blocksFor(c.n, 256), 256, parent, c.n);
+    if (m) {
+        LAUNCH(c, unionKernel, blocksFor(m, 256), 256, cs, m, c.B, parent, c.dCounters);
+        LAUNCH(c, compressKernel, blocksFor(c.n, 256), 256, parent, c.n);
+    }
     return VXB_OK;
 }
 
@@ -2678,13 +2690,16 @@ int loadBodies(Context& c, const vx_body* bodies, uint32_t n, const uint32_t* wo
         VXB_TRY(ensure(c, *b, mcap * 8 + 64));
     VXB_TRY(ensure(c, c.sortValsAlt, std::max<size_t>(mcap, (size_t)c.pairCap) * 4 + 64));
     c.prevCount = 0;
+    c.stepContacts = 0;
     c.backendContacts = 0;
+    VXB_TRY(sleepLoad(c, bodies, n));
     return VXB_OK;
 }
 
 int readBodies(Context& c, vx_body* out, uint32_t n) {
     if (n != c.n) return fail(c, VXB_ERR_INVALID, "body count mismatch");
     LAUNCH(c, unpackBodiesKernel, blocksFor(n, 256), 256, P<vx_body>(c.aosBuf), n, c.B);
+    VXB_TRY(sleepExport(c, P<vx_body>(c.aosBuf)));
     VXB_CUDA(c, cudaMemcpyAsync(out, c.aosBuf.ptr, (size_t)n * sizeof(vx_body), cudaMemcpyDeviceToHost, c.stream));
     VXB_CUDA(c, cudaStreamSynchronize(c.stream));
     return VXB_OK;
@@ -3400,6 +3415,7 @@ static int stepOnce(Context& c) {
                         P<uint64_t>(c.pairBuf) + c.pairCap));
     vx_contact* cs = P<vx_contact>(c.contactBuf[c.cur]);
     stageBegin(c, kStageWarmStart);
+    VXB_TRY(wakePass(c, cs, m));  // src/world.cpp:4106-4128: after detection, before warm starting
     if (c.tape.active)
         VXB_TRY(tapeBeforeMatch(c, cs, m, P<vx_contact>(c.contactBuf[c.cur ^ 1]), P<uint64_t>(c.prevKeyBuf),
                                 c.prevCount));
@@ -3424,11 +3440,23 @@ static int stepOnce(Context& c) {
     stageBegin(c, kStagePositions);
     VXB_TRY(positionCorrection(c, cs, plan, cfg.solver, h));
     stageEnd(c, kStagePositions);
+    // events, sleeping and the resting pairs' cached contacts (before the
+    // forces are cleared: the calm test reads them)
+    uint32_t kept = 0;
+    VXB_TRY(sleepAndEvents(c, cs, m, dt, &kept));
     LAUNCH(c, clearForcesKernel, blocksFor(n, 256), 256, c.B, n);
-    // previous-contact cache: this step's contacts in (a, b, point) order
-    VXB_TRY(ensure(c, c.prevKeyBuf, (size_t)m * 8 + 16));
-    if (m) LAUNCH(c, contactKeysKernel, blocksFor(m, 256), 256, cs, m, P<uint64_t>(c.prevKeyBuf));
-    c.prevCount = m;
+    // previous-contact cache: this step's contacts in (a, b, point) order, and
+    // resting pairs' cached contacts merged in by pair
+    if (kept) {
+        VXB_TRY(mergeKeptContacts(c, m, kept));
+        cs = P<vx_contact>(c.contactBuf[c.cur]);
+    }
+    const uint32_t cacheCount = m + kept;
+    VXB_TRY(ensure(c, c.prevKeyBuf, (size_t)cacheCount * 8 + 16));
+    if (cacheCount)
+        LAUNCH(c, contactKeysKernel, blocksFor(cacheCount, 256), 256, cs, cacheCount, P<uint64_t>(c.prevKeyBuf));
+    c.prevCount = cacheCount;
+    c.stepContacts = m;
     c.cur ^= 1;
     if (c.tape.active) VXB_TRY(tapeStepEnd(c, m));
     VXB_TRY(readCounters(c));
@@ -3461,8 +3489,9 @@ int worldStep(Context& c, int steps) {
 }
 
 int readContacts(Context& c, vx_contact* out, uint32_t cap, uint32_t* count) {
-    const uint32_t m = c.prevCount;
+    const uint32_t m = c.stepContacts;
     if (count) *count = m;
+    if (out && m && c.prevCount != m) return readStepContacts(c, out, std::min(m, cap));
     if (out && m) {
         VXB_CUDA(c, cudaMemcpyAsync(out, c.contactBuf[c.cur ^ 1].ptr, (size_t)std::min(m, cap) * sizeof(vx_contact),
                                     cudaMemcpyDeviceToHost, c.stream));
@@ -3482,6 +3511,7 @@ int writeContacts(Context& c, const vx_contact* contacts, uint32_t m) {
                P<uint64_t>(c.prevKeyBuf));
     }
     c.prevCount = m;
+    c.stepContacts = m;
     VXB_CUDA(c, cudaStreamSynchronize(c.stream));
     return VXB_OK;
 }

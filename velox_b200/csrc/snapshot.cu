@@ -1,8 +1,9 @@
 // Snapshots of the device-resident world (World::saveSnapshot /
 // restoreSnapshot, src/world.cpp:2038-2128, for the state this library keeps
 // on the device): every body array, the previous step's contacts and their
-// keys (the warm-start cache), the step configuration and the last step's
-// statistics. Two forms:
+// keys (the warm-start cache, resting pairs' contacts included), the sleep
+// state of every body and the last step's pair keys, the step and sleep
+// configuration and the last step's statistics. Two forms:
 //   * device slots: copies stay in device memory (device-to-device copies, no
 //     host round trip) for rollback and replay;
 //   * a byte image in caller memory (for files or another context that
@@ -18,20 +19,23 @@ namespace vxb {
 namespace {
 
 constexpr uint32_t kSnapshotMagic = 0x53425856u;  // "VXBS"
-constexpr uint32_t kSnapshotVersion = 1;
+constexpr uint32_t kSnapshotVersion = 2;
 
 struct SnapshotHeader {
     uint32_t magic, version, n, worlds;
-    uint32_t prevCount, cur, configured, pad;
+    uint32_t prevCount, cur, configured, stepContacts;
+    uint32_t pairCount, sleepable, asleep, pad;
     uint64_t bodyBytes, totalBytes;
     vxb_step_config config;
+    vxb_sleep_config sleepConfig;
     vxb_step_stats stats;
 };
 
 size_t bodyBytesOf(const Context& c) { return (((size_t)c.n * 16 + 255) & ~(size_t)255) * 16; }
 
-size_t imageBytes(const Context& c, uint32_t prevCount) {
-    return sizeof(SnapshotHeader) + bodyBytesOf(c) + (size_t)prevCount * (sizeof(vx_contact) + 8);
+size_t imageBytes(const Context& c, uint32_t prevCount, uint32_t pairCount) {
+    return sizeof(SnapshotHeader) + bodyBytesOf(c) + (size_t)prevCount * (sizeof(vx_contact) + 8) +
+           (size_t)c.n * 16 + (size_t)pairCount * 8;
 }
 
 SnapshotHeader headerOf(const Context& c) {
@@ -44,9 +48,16 @@ SnapshotHeader headerOf(const Context& c) {
     h.prevCount = c.prevCount;
     h.cur = (uint32_t)c.cur;
     h.configured = c.configured ? 1u : 0u;
+    // a snapshot keeps the whole cache: after a restore, read-back of the last
+    // step's contacts returns the cache (resting pairs' contacts included)
+    h.stepContacts = c.prevCount;
+    h.pairCount = c.sleep.pairCount;
+    h.sleepable = c.sleep.sleepable;
+    h.asleep = c.sleep.asleep;
     h.bodyBytes = bodyBytesOf(c);
-    h.totalBytes = imageBytes(c, c.prevCount);
+    h.totalBytes = imageBytes(c, c.prevCount, c.sleep.pairCount);
     h.config = c.config;
+    h.sleepConfig = c.sleep.config;
     h.stats = c.stats;
     return h;
 }
@@ -68,12 +79,18 @@ SnapshotHeader headerOf(const Context& c) {
 int copyOut(Context& c, char* dst, cudaMemcpyKind kind) {
     const size_t bb = bodyBytesOf(c);
     SN_CUDA(c, cudaMemcpyAsync(dst, c.bodyBuf.ptr, bb, kind, c.stream));
+    char* at = dst + bb;
     if (c.prevCount) {
-        SN_CUDA(c, cudaMemcpyAsync(dst + bb, c.contactBuf[c.cur ^ 1].ptr, (size_t)c.prevCount * sizeof(vx_contact),
-                                   kind, c.stream));
-        SN_CUDA(c, cudaMemcpyAsync(dst + bb + (size_t)c.prevCount * sizeof(vx_contact), c.prevKeyBuf.ptr,
-                                   (size_t)c.prevCount * 8, kind, c.stream));
+        SN_CUDA(c, cudaMemcpyAsync(at, c.contactBuf[c.cur ^ 1].ptr, (size_t)c.prevCount * sizeof(vx_contact), kind,
+                                   c.stream));
+        at += (size_t)c.prevCount * sizeof(vx_contact);
+        SN_CUDA(c, cudaMemcpyAsync(at, c.prevKeyBuf.ptr, (size_t)c.prevCount * 8, kind, c.stream));
+        at += (size_t)c.prevCount * 8;
     }
+    SN_CUDA(c, cudaMemcpyAsync(at, c.sleep.state.ptr, (size_t)c.n * 16, kind, c.stream));
+    at += (size_t)c.n * 16;
+    if (c.sleep.pairCount)
+        SN_CUDA(c, cudaMemcpyAsync(at, c.sleep.pairs.ptr, (size_t)c.sleep.pairCount * 8, kind, c.stream));
     return VXB_OK;
 }
 
@@ -99,7 +116,21 @@ int copyIn(Context& c, const SnapshotHeader& h, const char* src, cudaMemcpyKind 
         SN_CUDA(c, cudaMemcpyAsync(c.prevKeyBuf.ptr, src + bb + (size_t)h.prevCount * sizeof(vx_contact),
                                    (size_t)h.prevCount * 8, kind, c.stream));
     }
+    const char* at = src + bb + (size_t)h.prevCount * (sizeof(vx_contact) + 8);
+    VXB_TRY_SN(c, ensure(c, c.sleep.state, (size_t)c.n * 16 + 16));
+    SN_CUDA(c, cudaMemcpyAsync(c.sleep.state.ptr, at, (size_t)c.n * 16, kind, c.stream));
+    at += (size_t)c.n * 16;
+    if (h.pairCount) {
+        VXB_TRY_SN(c, ensure(c, c.sleep.pairs, (size_t)h.pairCount * 8 + 64));
+        SN_CUDA(c, cudaMemcpyAsync(c.sleep.pairs.ptr, at, (size_t)h.pairCount * 8, kind, c.stream));
+    }
     c.prevCount = h.prevCount;
+    c.stepContacts = h.stepContacts;
+    c.sleep.pairCount = h.pairCount;
+    c.sleep.sleepable = h.sleepable;
+    c.sleep.asleep = h.asleep;
+    c.sleep.eventCount = 0;
+    c.sleep.config = h.sleepConfig;
     c.config = h.config;
     c.configured = h.configured != 0;
     c.stats = h.stats;
@@ -134,7 +165,7 @@ int snapshotRestore(Context& c, uint32_t slot) {
 
 int snapshotBytes(Context& c, size_t* bytes) {
     if (c.n == 0) return fail(c, VXB_ERR_INVALID, "snapshot: no bodies loaded");
-    *bytes = imageBytes(c, c.prevCount);
+    *bytes = imageBytes(c, c.prevCount, c.sleep.pairCount);
     return VXB_OK;
 }
 
