@@ -298,27 +298,39 @@ __global__ void activeEventsKernel(const uint64_t* keys, const uint32_t* vals, u
     }
 }
 
-// Pairs of the previous step without an active contact now (src/world.cpp:
-// 4458-4482): Persist when both bodies are static or asleep (the pair stays
-// a pair key), else End. Flags here, events written by rank.
-__global__ void endedFlagKernel(const uint64_t* prevPairs, uint32_t prevPairCount, const uint64_t* activePairs,
-                                const uint32_t* activeCount, uint32_t n, uint32_t* flags) {
-    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < prevPairCount; k += gridDim.x * blockDim.x) {
-        const uint64_t key = prevPairs[k];
-        const uint32_t lo = (uint32_t)(key >> 32), hi = (uint32_t)key;
-        flags[k] = (lo < n && hi < n && !inSorted(activePairs, *activeCount, key)) ? 1u : 0u;
+// Pairs of the previous step (src/world.cpp:4458-4482), in their order: a
+// pair found among this step's pair keys is skipped; otherwise Persist when
+// both bodies are static or asleep (the pair is appended to the pair keys),
+// else End. The reference looks pairs up with std::binary_search in a key
+// array it appends to as it goes, so after the first appended pair the array
+// is no longer sorted and the lookup can miss a pair that is present (which
+// then ends although active). This walk keeps that behaviour: one thread, the
+// same lower-bound bisection over the same growing array.
+VXD bool bisectFind(const uint64_t* keys, uint32_t count, uint64_t key) {
+    uint32_t first = 0, len = count;
+    while (len > 0) {
+        const uint32_t half = len >> 1, middle = first + half;
+        if (keys[middle] < key) {
+            first = middle + 1;
+            len = len - half - 1;
+        } else {
+            len = half;
+        }
     }
+    return first != count && !(key < keys[first]);
 }
 
-__global__ void endedEventsKernel(const uint64_t* prevPairs, uint32_t prevPairCount, const uint32_t* flags,
-                                  const uint32_t* rank, const uint32_t* activeCount, BodyArrays B,
-                                  const vx_contact* prevContacts, const uint64_t* prevKeys, uint32_t prevCount,
-                                  uint64_t sentinel, vxb_contact_event* events, uint64_t* pairsOut) {
-    const uint32_t base = *activeCount;
-    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < prevPairCount; k += gridDim.x * blockDim.x) {
-        if (!flags[k]) continue;
+__global__ void endedWalkKernel(const uint64_t* prevPairs, uint32_t prevPairCount, const uint32_t* activeCount,
+                                uint32_t n, BodyArrays B, const vx_contact* prevContacts, const uint64_t* prevKeys,
+                                uint32_t prevCount, vxb_contact_event* events, uint64_t* pairs, uint32_t* counts) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const uint32_t active = *activeCount;
+    uint32_t size = active, emitted = 0;
+    for (uint32_t k = 0; k < prevPairCount; ++k) {
         const uint64_t key = prevPairs[k];
+        if (bisectFind(pairs, size, key)) continue;
         const uint32_t lo = (uint32_t)(key >> 32), hi = (uint32_t)key;
+        if (lo >= n || hi >= n) continue;
         const uint32_t fl = B.filt[lo].x, fh = B.filt[hi].x;
         const bool resting = (isStaticBody(fl) || isAsleep(fl)) && (isStaticBody(fh) || isAsleep(fh));
         if (events) {
@@ -341,10 +353,13 @@ __global__ void endedEventsKernel(const uint64_t* prevPairs, uint32_t prevPairCo
                     e.impulse = c.normalImpulse;
                 }
             }
-            events[base + rank[k]] = e;
+            events[active + emitted] = e;
         }
-        pairsOut[base + rank[k]] = resting ? key : sentinel;  // ended pairs sort last and are dropped
+        ++emitted;
+        if (resting) pairs[size++] = key;
     }
+    counts[0] = emitted;
+    counts[1] = size - active;
 }
 
 __global__ void iotaU32Kernel(uint32_t* a, uint32_t n) {
@@ -505,7 +520,8 @@ int sleepAndEvents(Context& c, const vx_contact* cs, uint32_t m, float dt, uint3
     SL_TRY(ensure(c, S.ranks, cap * 4));
     SL_TRY(ensure(c, S.pairsNext, cap * 8));
     if (S.events) SL_TRY(ensure(c, S.eventBuf, cap * sizeof(vxb_contact_event)));
-    uint32_t* small = PT<uint32_t>(S.small);  // [0] active pairs, [1] ended, [2] pair keys, [3] asleep, [4] kept
+    uint32_t* small = PT<uint32_t>(S.small);  // [0] active pairs, [2] pair keys, [3] asleep, [4] kept,
+                                              // [5] other events, [6] resting pairs appended
     uint64_t* keys = PT<uint64_t>(S.keys);
     uint32_t* vals = PT<uint32_t>(S.vals);
     uint32_t* flags = PT<uint32_t>(S.flags);
@@ -523,18 +539,14 @@ int sleepAndEvents(Context& c, const vx_contact* cs, uint32_t m, float dt, uint3
         SL_LAUNCH(c, activeEventsKernel, gridFor(m, 256), 256, keys, vals, m, sentinel, ranks, cs, c.B, prevPairs,
                   prevPairCount, events, pairsNext);
     }
-    if (prevPairCount) {
-        SL_LAUNCH(c, endedFlagKernel, gridFor(prevPairCount, 256), 256, prevPairs, prevPairCount, pairsNext, small,
-                  n, flags);
-        SL_TRY(exclusiveScan(c, flags, ranks, prevPairCount, small + 1));
-        SL_LAUNCH(c, endedEventsKernel, gridFor(prevPairCount, 256), 256, prevPairs, prevPairCount, flags, ranks,
-                  small, c.B, prevContacts, prevKeys, prevCount, sentinel, events, pairsNext);
-    }
+    if (prevPairCount)
+        SL_LAUNCH(c, endedWalkKernel, 1, 32, prevPairs, prevPairCount, small, n, c.B, prevContacts, prevKeys,
+                  prevCount, events, pairsNext, small + 5);
     uint32_t host[8];
-    SL_CUDA(c, cudaMemcpyAsync(host, small, 8, cudaMemcpyDeviceToHost, c.stream));
+    SL_CUDA(c, cudaMemcpyAsync(host, small, 32, cudaMemcpyDeviceToHost, c.stream));
     SL_CUDA(c, cudaStreamSynchronize(c.stream));
-    const uint32_t total = host[0] + host[1];
-    S.eventCount = S.events ? total : 0;
+    const uint32_t total = host[0] + host[6];  // active pairs and the resting pairs appended
+    S.eventCount = S.events ? host[0] + host[5] : 0;
     // ---- this step's pair keys: active pairs and resting ones, sorted and unique
     uint32_t pairCount = 0;
     if (total) {
