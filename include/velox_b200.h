@@ -313,6 +313,11 @@ int vxb_tape_end(vxb_context* ctx);
  * and allPairsContactsKernel (src/backend_cuda.cu:174-299). */
 int vxb_stage_pairs(vxb_context* ctx, const vx_body* bodies, uint32_t n, float dt,
                     uint64_t* out, uint32_t cap, uint32_t* count);
+/* vxb_stage_pairs for scenes with static meshes, whose root bounds come from
+ * the soup (src/backend_cuda.cu:100-129: meshes pair with every body whose
+ * swept AABB overlaps those bounds). vxb_stage_pairs rejects mesh bodies. */
+int vxb_stage_pairs_soup(vxb_context* ctx, const vx_body* bodies, uint32_t n, const vx_soup* soup,
+                         float dt, uint64_t* out, uint32_t cap, uint32_t* count);
 /* collidePair (src/narrowphase.h:678-714) for each listed pair; contacts are
  * returned grouped in pair order, counts[p] per pair, *total overall. */
 int vxb_stage_collide(vxb_context* ctx, const vx_body* bodies, uint32_t n, const vx_soup* soup,
@@ -321,7 +326,8 @@ int vxb_stage_collide(vxb_context* ctx, const vx_body* bodies, uint32_t n, const
 /* gjkDistance(makeConvex(a), makeConvex(b)) (include/velox/gjk.h:751-777)
  * for each listed pair: out[11*p ..] = distance, normal xyz, pointA xyz,
  * pointB xyz, overlapping (1/0). path 0 = the rewind's query (register GJK,
- * general GJK/EPA on overlap), 1 = the general GJK/EPA only. */
+ * general GJK/EPA on overlap), 1 = the general GJK/EPA only. Convex bodies
+ * and planes only (VXB_ERR_UNSUPPORTED for meshes and compounds). */
 int vxb_stage_distance(vxb_context* ctx, const vx_body* bodies, uint32_t n, const vx_soup* soup,
                        const uint64_t* pairs, uint32_t npairs, int path, float* out);
 /* Greedy first-free-bit colouring (src/backend_cuda.cu:603-630) of contacts

@@ -153,15 +153,68 @@ typedef struct vx_solver_options {
     uint8_t reserved;
 } vx_solver_options;
 
-/* Static convex-hull geometry: the hull slice of velox::MeshSoup
- * (include/velox/backend.h:13-22). Bodies index it through
- * hullFirst/hullCount (points) and hullFaceFirst/hullFaceCount (triangles,
- * three point indices each, local to the body's point range). */
+/* velox::Mesh (include/velox/body.h:354-362, 52 B): one static triangle mesh
+ * in the soup. Vertices [firstVertex, +vertexCount), index triples
+ * [firstIndex, +indexCount) relative to firstVertex, BVH nodes
+ * [firstNode, +nodeCount) (absolute node indices; the root is firstNode),
+ * leaf triangle references from firstTriRef; aabb = root bounds. */
+typedef struct vx_mesh {
+    uint32_t firstVertex, vertexCount;
+    uint32_t firstIndex, indexCount;
+    uint32_t firstNode, nodeCount;
+    uint32_t firstTriRef;
+    vx_vec3 aabbMin, aabbMax;
+} vx_mesh;
+
+/* velox::BvhNode (body.h:370-374, 32 B). Inner node: triCount 0, children
+ * leftFirst and leftFirst + 1 (absolute node indices). Leaf: triCount > 0
+ * triangle references at bvhTriRefs[leftFirst ...], each a triangle number
+ * within its mesh. */
+typedef struct vx_bvh_node {
+    vx_vec3 aabbMin, aabbMax;
+    uint32_t leftFirst;
+    uint32_t triCount;
+} vx_bvh_node;
+
+/* velox::CompoundChild (body.h:105-114, 68 B): one convex child of a
+ * compound body, posed in the compound's frame (position relative to the
+ * compound's centre of mass). Hull children index the soup's hull arrays. */
+typedef struct vx_compound_child {
+    uint8_t shape;        /* a convex VX_SHAPE_* */
+    uint8_t pad[3];
+    vx_vec3 localPosition;
+    vx_quat localOrientation;
+    float radius;
+    vx_vec3 halfExtents;
+    float capsuleHalfHeight;
+    uint32_t hullFirst, hullCount;
+    uint32_t hullFaceFirst, hullFaceCount;
+} vx_compound_child;
+
+/* Static geometry of a scene: velox::MeshSoup (include/velox/backend.h:13-22).
+ * Hull bodies index hullPoints through hullFirst/hullCount and
+ * hullFaceIndices through hullFaceFirst/hullFaceCount (triangles, three point
+ * indices each, local to the body's point range). Mesh bodies index meshes
+ * through meshIndex; compound bodies index compoundChildren through
+ * compoundFirst/compoundCount. A caller without meshes or compounds leaves
+ * the fields after hullFaceIndexCount zero. */
 typedef struct vx_soup {
     const vx_vec3* hullPoints;
     uint32_t hullPointCount;
     const uint32_t* hullFaceIndices;
     uint32_t hullFaceIndexCount;
+    const vx_vec3* vertices;
+    uint32_t vertexCount;
+    const uint32_t* indices;
+    uint32_t indexCount;
+    const vx_mesh* meshes;
+    uint32_t meshCount;
+    const vx_bvh_node* bvhNodes;
+    uint32_t bvhNodeCount;
+    const uint32_t* bvhTriRefs;
+    uint32_t bvhTriRefCount;
+    const vx_compound_child* compoundChildren;
+    uint32_t compoundChildCount;
 } vx_soup;
 
 /* One body of a synthetic scene, described at the level of the reference's
@@ -206,5 +259,9 @@ VX_STATIC_ASSERT(offsetof(vx_body, compoundCount) == 296, "vx_body.compoundCount
 VX_STATIC_ASSERT(sizeof(vx_contact) == 128, "vx_contact must match velox::Contact (128 B)");
 VX_STATIC_ASSERT(offsetof(vx_contact, normalImpulse) == 96, "vx_contact.normalImpulse offset");
 VX_STATIC_ASSERT(sizeof(vx_solver_options) == 24, "vx_solver_options layout");
+VX_STATIC_ASSERT(sizeof(vx_mesh) == 52, "vx_mesh must match velox::Mesh (52 B)");
+VX_STATIC_ASSERT(sizeof(vx_bvh_node) == 32, "vx_bvh_node must match velox::BvhNode (32 B)");
+VX_STATIC_ASSERT(sizeof(vx_compound_child) == 68, "vx_compound_child must match velox::CompoundChild (68 B)");
+VX_STATIC_ASSERT(offsetof(vx_compound_child, hullFaceCount) == 64, "vx_compound_child.hullFaceCount offset");
 
 #endif /* VELOX_B200_TYPES_H */

@@ -78,7 +78,11 @@ def lib(strict=True):
         "ref_world_sleep_config": ([vp, f32, f32, f32, f32, f32, f32, i32, i32, i32], None),
         "ref_world_fix_tie_order": ([vp, i32], None),
         "ref_world_found_contacts": ([vp, vp, u32], u32),
-        "ref_candidate_pairs": ([vp, u32, f32, vp, u32], u32),
+        "ref_candidate_pairs": ([vp, u32, f32, vp, u32, vp], u32),
+        "ref_world_add_compound": ([vp, vp, vp, u32, vp], i32),
+        "ref_world_add_static_mesh": ([vp, vp, u32, vp, u32], i32),
+        "ref_world_add_heightfield": ([vp, u32, u32, f32, vp, vp], i32),
+        "ref_world_soup_part": ([vp, i32, vp, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64)], u32),
         "ref_body_aabb": ([vp, f32, vp], None),
         "ref_collide_pairs": ([vp, vp, vp, u32, f32, vp, u32, vp], u32),
         "ref_gjk": ([vp, vp, vp, vp], None),
@@ -171,6 +175,64 @@ class RefWorld:
         self.L.ref_world_soup(self.h, _p(pts), _p(faces), ctypes.byref(nf))
         return pts[:npts], faces[:nf.value]
 
+    def _added(self, index):
+        if index < 0:
+            raise RuntimeError(self.L.ref_last_error().decode())
+        self.n += 1
+        return index
+
+    def add_compound(self, spec, children, pool=None):
+        """World::addCompound at spec's position with spec's mass, then the
+        spec's orientation, velocities, friction, restitution and enableSleep.
+        children: velox_b200 COMPOUND_CHILD records (hull children index
+        `pool`). Returns the body's dense index."""
+        from velox_b200.binding import COMPOUND_CHILD, SPEC, records
+        spec = records(np.atleast_1d(spec), SPEC)
+        children = records(np.atleast_1d(children), COMPOUND_CHILD)
+        pool = np.ascontiguousarray(np.zeros((0, 3)) if pool is None else pool, np.float32)
+        return self._added(self.L.ref_world_add_compound(self.h, _p(spec), _p(children), len(children), _p(pool)))
+
+    def add_static_mesh(self, vertices, indices):
+        v = np.ascontiguousarray(vertices, np.float32).reshape(-1, 3)
+        i = np.ascontiguousarray(indices, np.uint32).reshape(-1)
+        return self._added(self.L.ref_world_add_static_mesh(self.h, _p(v), len(v), _p(i), len(i)))
+
+    def add_heightfield(self, heights, cell_size, origin=(0.0, 0.0, 0.0)):
+        """heights: (depth, width) samples (World::addStaticHeightfield)."""
+        h = np.ascontiguousarray(heights, np.float32)
+        o = np.asarray(origin, np.float32)
+        return self._added(self.L.ref_world_add_heightfield(self.h, h.shape[1], h.shape[0], cell_size, _p(h), _p(o)))
+
+    def mesh_soup(self):
+        """The world's whole MeshSoup: dict of numpy arrays (record layouts of
+        velox_b200.binding)."""
+        from velox_b200.binding import BVH_NODE, COMPOUND_CHILD, MESH
+        kinds = [("vertices", (np.float32, 3)), ("indices", np.uint32), ("meshes", MESH), ("nodes", BVH_NODE),
+                 ("tri_refs", np.uint32), ("hull", (np.float32, 3)), ("faces", np.uint32),
+                 ("children", COMPOUND_CHILD)]
+        out = {}
+        for part, (name, kind) in enumerate(kinds):
+            elem = ctypes.c_uint64()
+            n = self.L.ref_world_soup_part(self.h, part, None, 0, ctypes.byref(elem))
+            if n == 0xffffffff:
+                raise RuntimeError("the reference's snapshot layout did not parse")
+            if isinstance(kind, tuple):
+                arr = np.zeros((n, kind[1]), kind[0])
+            else:
+                arr = np.zeros(n, kind)
+            if n:
+                assert elem.value == arr.nbytes // n, (name, elem.value)
+                self.L.ref_world_soup_part(self.h, part, _p(arr), arr.nbytes, ctypes.byref(elem))
+            out[name] = arr
+        return out
+
+    def vx_soup(self):
+        """mesh_soup() as a velox_b200 Soup."""
+        from velox_b200.binding import make_soup
+        s = self.mesh_soup()
+        return make_soup(s["hull"], s["faces"], s["vertices"], s["indices"], s["meshes"], s["nodes"], s["tri_refs"],
+                         s["children"])
+
     def step(self, dt=1.0 / 60.0, steps=1):
         if self.L.ref_world_step(self.h, dt, steps) != 0:
             raise RuntimeError(self.L.ref_last_error().decode())
@@ -231,11 +293,13 @@ class RefWorld:
         return out
 
 
-def candidate_pairs(bodies, dt, strict=True):
+def candidate_pairs(bodies, dt, strict=True, soup=None):
+    """soup: a velox_b200 Soup (needed when the bodies include meshes)."""
     L = lib(strict)
-    n = L.ref_candidate_pairs(_p(bodies), len(bodies), dt, None, 0)
+    sp = ctypes.byref(soup) if soup is not None else None
+    n = L.ref_candidate_pairs(_p(bodies), len(bodies), dt, None, 0, sp)
     out = np.zeros(max(n, 1), np.uint64)
-    L.ref_candidate_pairs(_p(bodies), len(bodies), dt, _p(out), n)
+    L.ref_candidate_pairs(_p(bodies), len(bodies), dt, _p(out), n, sp)
     return out[:n]
 
 

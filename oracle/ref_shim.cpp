@@ -38,6 +38,13 @@ static_assert(offsetof(velox::Body, sleepTimer) == offsetof(vx_body, sleepTimer)
 static_assert(sizeof(velox::Contact) == sizeof(vx_contact), "Contact layout");
 static_assert(offsetof(velox::Contact, spinningImpulse) == offsetof(vx_contact, spinningImpulse), "Contact tail");
 static_assert(sizeof(velox::SolverOptions) == sizeof(vx_solver_options), "SolverOptions layout");
+static_assert(sizeof(velox::Mesh) == sizeof(vx_mesh), "Mesh layout");
+static_assert(sizeof(velox::BvhNode) == sizeof(vx_bvh_node), "BvhNode layout");
+static_assert(sizeof(velox::CompoundChild) == sizeof(vx_compound_child), "CompoundChild layout");
+static_assert(offsetof(velox::CompoundChild, localOrientation) == offsetof(vx_compound_child, localOrientation),
+              "CompoundChild.localOrientation");
+static_assert(offsetof(velox::CompoundChild, hullFaceCount) == offsetof(vx_compound_child, hullFaceCount),
+              "CompoundChild tail");
 
 namespace velox {
 namespace {
@@ -51,9 +58,9 @@ struct BoxLH { Vec3 lo, hi; };
 // Candidate pair set of the reference CUDA backend: allPairsContactsKernel
 // (backend_cuda.cu:272-299) below 4096 bodies, the grid (:174-250) above. Both
 // enumerate exactly the pairs i<j whose compact AABBs overlap (planes are
-// unbounded), that are not both inert and that pass canCollideWith. Returned
-// sorted ascending as (i<<32)|j.
-std::vector<uint64_t> candidatePairs(const std::vector<Body>& bodies, float dt) {
+// unbounded, meshes take their root bounds, :100-129), that are not both
+// inert and that pass canCollideWith. Returned sorted ascending as (i<<32)|j.
+std::vector<uint64_t> candidatePairs(const std::vector<Body>& bodies, float dt, const Mesh* meshes) {
     const size_t n = bodies.size();
     std::vector<BoxLH> boxes(n);
     std::vector<uint32_t> order;
@@ -63,6 +70,9 @@ std::vector<uint64_t> candidatePairs(const std::vector<Body>& bodies, float dt) 
         if (b.shape == ShapeType::Plane) {
             boxes[i] = {{-1e30f, -1e30f, -1e30f}, {1e30f, 1e30f, 1e30f}};
             planes.push_back(i);
+        } else if (b.shape == ShapeType::Mesh) {
+            boxes[i] = {meshes[b.meshIndex].aabbMin, meshes[b.meshIndex].aabbMax};
+            order.push_back(i);
         } else {
             bodyAabb(b, dt, boxes[i].lo, boxes[i].hi);
             order.push_back(i);
@@ -171,7 +181,7 @@ public:
         soupFaces = meshes.hullFaceIndices;
         if (bodies.size() < 2) return;
         const MeshSoupView soup = view(meshes);
-        lastPairs = candidatePairs(bodies, dt);
+        lastPairs = candidatePairs(bodies, dt, meshes.meshes.data());
         Contact buf[kMaxContactsPerPair];
         for (uint64_t p : lastPairs) {
             BodyIndex i = BodyIndex(p >> 32), j = BodyIndex(p);
@@ -368,6 +378,12 @@ MeshSoupView soupView(const vx_soup* s) {
     if (s) {
         v.hullPoints = reinterpret_cast<const Vec3*>(s->hullPoints);
         v.hullFaceIndices = s->hullFaceIndices;
+        v.vertices = reinterpret_cast<const Vec3*>(s->vertices);
+        v.indices = s->indices;
+        v.meshes = reinterpret_cast<const Mesh*>(s->meshes);
+        v.bvhNodes = reinterpret_cast<const BvhNode*>(s->bvhNodes);
+        v.bvhTriRefs = s->bvhTriRefs;
+        v.compoundChildren = reinterpret_cast<const CompoundChild*>(s->compoundChildren);
     }
     return v;
 }
@@ -452,6 +468,105 @@ int ref_world_build(void* handle, const vx_shape_spec* specs, uint32_t n,
         g_error = e.what();
         return -1;
     }
+}
+
+// The state a spec gives a body after World::add* (as ref_world_build does).
+static void applySpecState(RefWorld* w, BodyId id, const vx_shape_spec& s) {
+    Body& b = w->world->body(id);
+    b.orientation = Q(s.orientation);
+    b.velocity = V(s.velocity);
+    b.angularVelocity = V(s.angularVelocity);
+    b.friction = s.friction;
+    b.restitution = s.restitution;
+    b.enableSleep = s.enableSleep;
+}
+
+// World::addCompound (src/world.cpp:987-1301) at spec->position with
+// spec->mass; children as vx_compound_child records whose hull children give
+// their points as [hullFirst, +hullCount) of `pool`. Returns the dense index
+// or -1 (ref_last_error).
+int ref_world_add_compound(void* handle, const vx_shape_spec* spec, const vx_compound_child* children,
+                           uint32_t count, const vx_vec3* pool) {
+    auto* w = static_cast<RefWorld*>(handle);
+    try {
+        std::vector<CompoundShape> shapes(count);
+        for (uint32_t k = 0; k < count; ++k) {
+            const vx_compound_child& c = children[k];
+            CompoundShape& sh = shapes[k];
+            sh.shape = (ShapeType)c.shape;
+            sh.localPosition = V(c.localPosition);
+            sh.localOrientation = Q(c.localOrientation);
+            sh.radius = c.radius;
+            sh.halfExtents = V(c.halfExtents);
+            sh.capsuleHalfHeight = c.capsuleHalfHeight;
+            for (uint32_t i = 0; i < c.hullCount; ++i) sh.hullPoints.push_back(V(pool[c.hullFirst + i]));
+        }
+        BodyId id = w->world->addCompound(V(spec->position), shapes, spec->mass);
+        w->ids.push_back(id);
+        applySpecState(w, id, *spec);
+        return (int)w->ids.size() - 1;
+    } catch (const std::exception& e) {
+        g_error = e.what();
+        return -1;
+    }
+}
+
+// World::addStaticMesh (src/world.cpp:1379-1440). Returns the dense index or -1.
+int ref_world_add_static_mesh(void* handle, const vx_vec3* vertices, uint32_t vertexCount, const uint32_t* indices,
+                              uint32_t indexCount) {
+    auto* w = static_cast<RefWorld*>(handle);
+    try {
+        std::vector<Vec3> v(vertexCount);
+        for (uint32_t i = 0; i < vertexCount; ++i) v[i] = V(vertices[i]);
+        std::vector<uint32_t> ix(indices, indices + indexCount);
+        w->ids.push_back(w->world->addStaticMesh(v, ix));
+        return (int)w->ids.size() - 1;
+    } catch (const std::exception& e) {
+        g_error = e.what();
+        return -1;
+    }
+}
+
+// World::addStaticHeightfield (src/world.cpp:1442-1477). Returns the dense index or -1.
+int ref_world_add_heightfield(void* handle, uint32_t width, uint32_t depth, float cellSize, const float* heights,
+                              const vx_vec3* origin) {
+    auto* w = static_cast<RefWorld*>(handle);
+    try {
+        std::vector<float> h(heights, heights + (size_t)width * depth);
+        w->ids.push_back(w->world->addStaticHeightfield(width, depth, cellSize, h, V(*origin)));
+        return (int)w->ids.size() - 1;
+    } catch (const std::exception& e) {
+        g_error = e.what();
+        return -1;
+    }
+}
+
+// One array of the world's MeshSoup, read from its snapshot (the soup is
+// serialised after the 17 state vectors that follow the fixed header):
+// part 0 vertices, 1 indices, 2 meshes, 3 bvhNodes, 4 bvhTriRefs, 5 hullPoints,
+// 6 hullFaceIndices, 7 compoundChildren. Copies up to capBytes into out and
+// returns the element count (element size in *elemSize); ~0u on a layout error.
+uint32_t ref_world_soup_part(void* handle, int part, void* out, uint64_t capBytes, uint64_t* elemSize) {
+    auto* w = static_cast<RefWorld*>(handle);
+    SerializedScene scene = serializeWorld(*w->world);
+    const std::vector<uint8_t>& bytes = scene.data;
+    size_t at = sizeof(Vec3) + sizeof(int) + sizeof(WorldCcdDefaults) + sizeof(WorldMultiToiSettings) +
+                sizeof(SolverOptions);
+    for (int v = 0; v <= 17 + part; ++v) {
+        uint64_t elem = 0, n = 0;
+        if (at + 16 > bytes.size()) return ~0u;
+        std::memcpy(&elem, bytes.data() + at, 8);
+        std::memcpy(&n, bytes.data() + at + 8, 8);
+        at += 16;
+        if (at + elem * n > bytes.size()) return ~0u;
+        if (v == 17 + part) {
+            if (elemSize) *elemSize = elem;
+            if (out) std::memcpy(out, bytes.data() + at, std::min<uint64_t>(elem * n, capBytes));
+            return (uint32_t)n;
+        }
+        at += elem * n;
+    }
+    return ~0u;
 }
 
 uint32_t ref_world_body_count(void* handle) {
@@ -651,10 +766,10 @@ uint32_t ref_world_found_contacts(void* handle, vx_contact* out, uint32_t cap) {
 // ---- stage-level entry points over raw arrays ---------------------------
 
 uint32_t ref_candidate_pairs(const vx_body* bodies, uint32_t n, float dt, uint64_t* out,
-                             uint32_t cap) {
+                             uint32_t cap, const vx_soup* soup) {
     std::vector<Body> v(reinterpret_cast<const Body*>(bodies),
                         reinterpret_cast<const Body*>(bodies) + n);
-    std::vector<uint64_t> pairs = candidatePairs(v, dt);
+    std::vector<uint64_t> pairs = candidatePairs(v, dt, soup ? reinterpret_cast<const Mesh*>(soup->meshes) : nullptr);
     if (out) std::memcpy(out, pairs.data(), std::min<size_t>(pairs.size(), cap) * 8);
     return (uint32_t)pairs.size();
 }

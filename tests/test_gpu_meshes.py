@@ -1,0 +1,247 @@
+"""Compound bodies, static triangle meshes and heightfields on the device
+(src/narrowphase.h:609-714 meshConvex / collidePair's compound dispatch,
+src/backend_cuda.cu:100-129 mesh bounds in the broad phase, src/world.cpp:
+2916-2958 gapAt's compound and mesh cases in the rewind), against the
+reference engine built from its sources: pair sets bit-exact, narrow-phase
+contacts at the geometry tolerances, whole steps within 1e-4 relative of the
+reference CUDA backend's algorithm and of its own CUDA code on this GPU, the
+reference World stepping on this library, batched worlds, and the soup
+checks that keep the device's BVH walks inside their arrays."""
+import numpy as np
+import pytest
+
+import velox_b200
+import mesh_scenes as ms
+
+pytestmark = pytest.mark.gpu
+DT = 1.0 / 60.0
+POS_TOL = 1e-5
+ANGLE_TOL = 1e-4
+
+
+def _state(b):
+    return np.concatenate([b["position"], b["orientation"], b["velocity"], b["angularVelocity"]], 1)
+
+
+def _rel(mine, theirs):
+    return float((np.abs(_state(mine) - _state(theirs)) / np.maximum(1.0, np.abs(_state(theirs)))).max())
+
+
+def _compare_contacts(mine, theirs):
+    assert len(mine) == len(theirs)
+    assert np.array_equal(mine["a"], theirs["a"]) and np.array_equal(mine["b"], theirs["b"])
+    assert np.array_equal(mine["featureKey"], theirs["featureKey"])
+    for f in ("point", "localAnchorA", "localAnchorB", "gap", "bias0"):
+        assert np.abs(mine[f] - theirs[f]).max() <= POS_TOL, f
+    a, b = mine["normal"].astype(np.float64), theirs["normal"].astype(np.float64)
+    angle = np.arctan2(np.linalg.norm(np.cross(a, b), axis=1), np.sum(a * b, 1))
+    assert angle.max() <= ANGLE_TOL
+    for f in ("vn0", "restitution", "friction1", "friction2"):
+        assert np.allclose(mine[f], theirs[f], rtol=1e-5, atol=1e-5), f
+
+
+def _states(ref, steps=(0, 15, 40)):
+    """(bodies, soup) of the scene after each number of reference steps."""
+    w, bodies, soup = ms.load_pair(ref)
+    w.configure(substeps=4, workers=1)
+    out, done = [], 0
+    for s in steps:
+        w.step(DT, s - done)
+        done = s
+        out.append(w.bodies())
+    w.close()
+    return out, soup
+
+
+def test_pairs_bit_exact_with_meshes_and_compounds(ctx, ref):
+    states, soup = _states(ref)
+    for bodies in states:
+        theirs = ref.candidate_pairs(bodies, DT, soup=soup)
+        mine = ctx.pairs(bodies, DT, soup)
+        shapes = bodies["shape"]
+        kinds = {tuple(sorted((shapes[p >> 32], shapes[p & 0xffffffff]))) for p in theirs.tolist()}
+        assert (0, 4) in kinds or (2, 4) in kinds or (4, 6) in kinds  # mesh pairs present
+        assert any(6 in k for k in kinds)
+        assert np.array_equal(mine, theirs)
+
+
+def test_narrowphase_meshes_and_compounds_match_reference(ctx, ref):
+    states, soup = _states(ref)
+    seen = set()
+    for bodies in states:
+        pairs = ref.candidate_pairs(bodies, DT, soup=soup)
+        theirs, tcounts = ref.collide_pairs(bodies, soup, pairs, DT)
+        mine, mcounts = ctx.collide(bodies, soup, pairs, DT)
+        assert np.array_equal(mcounts, tcounts)
+        _compare_contacts(mine, theirs)
+        shapes = bodies["shape"]
+        seen |= {(int(shapes[c["a"]]), int(shapes[c["b"]])) for c in theirs}
+    # contacts of compounds with compounds, meshes, the plane and convex bodies
+    assert any(a == 6 and b == 4 for a, b in seen) or any(a == 4 and b == 6 for a, b in seen)
+    assert any(6 in (a, b) and 1 in (a, b) for a, b in seen) or any(6 == a == b for a, b in seen)
+    assert any(4 in (a, b) and {a, b} & {0, 2, 3, 5} for a, b in seen)
+
+
+def _order_free_steps(ref, steps, **kw):
+    a = ms.mesh_compound_world(ref, **kw)
+    b = ms.mesh_compound_world(ref, reverse_ties=True, **kw)
+    for w in (a, b):
+        w.configure(substeps=4, workers=1)
+    free = steps
+    for step in range(steps):
+        a.step(DT, 1)
+        b.step(DT, 1)
+        if not np.array_equal(_state(a.bodies()), _state(b.bodies())):
+            free = step
+            break
+    a.close()
+    b.close()
+    return free
+
+
+def test_world_steps_match_reference(ref):
+    steps = min(40, _order_free_steps(ref, 40))
+    assert steps >= 10
+    w, bodies, soup = ms.load_pair(ref)
+    w.configure(substeps=4, workers=1)
+    ctx = ms.device_world(bodies, soup)
+    rewinds = contacts = 0
+    for step in range(steps):
+        w.step(DT, 1)
+        ctx.step(1)
+        assert _rel(ctx.read_bodies(), w.bodies()) <= 1e-4, step
+        st = ctx.stats()
+        rewinds += st["rewinds"]
+        contacts = max(contacts, st["contacts"])
+    assert rewinds > 0 and contacts > 50
+    ctx.close()
+    w.close()
+
+
+def test_world_steps_match_the_reference_cuda_backend(ref):
+    if not ref.available("cuda"):
+        pytest.skip("reference CUDA build missing (make -C oracle cuda)")
+    steps = min(20, _order_free_steps(ref, 20))
+    assert steps >= 5
+    w, bodies, soup = ms.load_pair(ref, strict="cuda")
+    assert w.L.ref_world_backend_name(w.h) == b"cuda"
+    w.configure(substeps=4, workers=1)
+    ctx = ms.device_world(bodies, soup)
+    for step in range(steps):
+        w.step(DT, 1)
+        ctx.step(1)
+        assert _rel(ctx.read_bodies(), w.bodies()) <= 1e-4, step
+    assert w.stats()["deviceSubsteps"] == 1
+    ctx.close()
+    w.close()
+
+
+def test_reference_world_on_b200_backend_with_meshes(ref):
+    if not ref.available("dropin"):
+        pytest.skip("drop-in build missing")
+    steps = min(10, _order_free_steps(ref, 10))
+    emu = ms.mesh_compound_world(ref)
+    dev = ms.mesh_compound_world(ref, strict="dropin")
+    assert dev.L.ref_world_backend_name(dev.h) == b"cuda"
+    for w in (emu, dev):
+        w.configure(substeps=4, workers=1)
+    for step in range(steps):
+        emu.step(DT, 1)
+        dev.step(DT, 1)
+        assert _rel(dev.bodies(), emu.bodies()) <= 1e-4, step
+    assert dev.stats()["generated"] > 0
+    emu.close()
+    dev.close()
+
+
+def test_batched_mesh_worlds_equal_the_worlds_alone(ref):
+    parts = []
+    for seed in (0, 1, 2):
+        w = ms.mesh_compound_world(ref, seed=seed, compounds=10 + 4 * seed, convex=8)
+        parts.append((w.bodies(), w.mesh_soup()))
+        w.close()
+    bodies, world_of, soup = ms.merge_worlds(parts)
+    batch = velox_b200.Context(0)
+    batch.load(bodies, ms.make_soup(soup), world_of)
+    batch.configure(dt=DT, substeps=4)
+    alone = []
+    for b, s in parts:
+        c = velox_b200.Context(0)
+        c.load(b, ms.make_soup(s))
+        c.configure(dt=DT, substeps=4)
+        alone.append(c)
+    for _ in range(25):
+        batch.step(1)
+        for c in alone:
+            c.step(1)
+    got = batch.read_bodies()
+    start = 0
+    for c, (b, _) in zip(alone, parts):
+        mine = c.read_bodies()
+        assert np.array_equal(_state(got[start:start + len(b)]), _state(mine))
+        start += len(b)
+        c.close()
+    batch.close()
+
+
+def _load_status(bodies, soup_dict):
+    ctx = velox_b200.Context(0)
+    try:
+        ctx.load(bodies, ms.make_soup(soup_dict))
+        return 0, ""
+    except velox_b200.VeloxError as e:
+        return e.status, str(e)
+    finally:
+        ctx.close()
+
+
+def test_invalid_mesh_and_compound_references_are_rejected(ref):
+    w = ms.mesh_compound_world(ref, compounds=6, convex=4)
+    bodies, soup = w.bodies(), w.mesh_soup()
+    w.close()
+    assert _load_status(bodies, soup)[0] == 0
+    mesh = int(np.flatnonzero(bodies["shape"] == 4)[0])
+    comp = int(np.flatnonzero(bodies["shape"] == 6)[0])
+    cases = []
+    b = bodies.copy(); b["meshIndex"][mesh] = len(soup["meshes"]); cases.append((b, soup, "invalid mesh"))
+    b = bodies.copy(); b["compoundCount"][comp] = 0; cases.append((b, soup, "invalid child storage"))
+    b = bodies.copy(); b["compoundFirst"][comp] = len(soup["children"]); cases.append((b, soup, "invalid child storage"))
+    b = bodies.copy(); b["motionType"][mesh] = 2; cases.append((b, soup, "mesh bodies are static"))
+    s = dict(soup, nodes=soup["nodes"].copy())
+    inner = int(np.flatnonzero(s["nodes"]["triCount"] == 0)[1])
+    s["nodes"]["leftFirst"][inner] = inner  # a cycle: the walk would not end
+    cases.append((bodies, s, "invalid inner node"))
+    s = dict(soup, indices=soup["indices"].copy())
+    s["indices"][5] = 10 ** 6
+    cases.append((bodies, s, "outside the vertex array"))
+    s = dict(soup, tri_refs=soup["tri_refs"].copy())
+    s["tri_refs"][0] = 10 ** 6
+    cases.append((bodies, s, "invalid triangle"))
+    s = dict(soup, children=soup["children"].copy())
+    s["children"]["shape"][0] = 4  # a mesh child
+    cases.append((bodies, s, "compound child contains invalid state"))
+    for b, s, why in cases:
+        status, msg = _load_status(b, s)
+        assert status == velox_b200.binding.VXB_ERR_INVALID and why in msg, (why, status, msg)
+
+
+def test_snapshot_image_restores_mesh_worlds_and_rejects_other_geometry(ref):
+    w, bodies, soup = ms.load_pair(ref)
+    w.close()
+    a = ms.device_world(bodies, soup)
+    a.step(10)
+    image = a.snapshot_bytes()
+    a.step(10)
+    want = a.read_bodies()
+    b = ms.device_world(bodies, soup)
+    b.snapshot_load(image)
+    b.step(10)
+    assert np.array_equal(_state(b.read_bodies()), _state(want))
+    # the same bodies over a soup of another size: the image is refused
+    other = ms.mesh_compound_world(ref, mesh_rows=5)
+    c = ms.device_world(other.bodies(), other.vx_soup())
+    other.close()
+    with pytest.raises(velox_b200.VeloxError, match="other shapes or another soup"):
+        c.snapshot_load(image)
+    for x in (a, b, c):
+        x.close()

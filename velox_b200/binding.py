@@ -12,6 +12,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libvelox_b200.so")
 
 VXB_OK = 0
+VXB_ERR_INVALID = 1
 STATUS = {0: "ok", 1: "invalid", 2: "no device", 3: "out of memory", 4: "device lost",
           5: "capacity", 6: "unsupported", 7: "timeout"}
 
@@ -126,7 +127,28 @@ class Vec3(ctypes.Structure):
 
 class Soup(ctypes.Structure):
     _fields_ = [("hullPoints", ctypes.c_void_p), ("hullPointCount", ctypes.c_uint32),
-                ("hullFaceIndices", ctypes.c_void_p), ("hullFaceIndexCount", ctypes.c_uint32)]
+                ("hullFaceIndices", ctypes.c_void_p), ("hullFaceIndexCount", ctypes.c_uint32),
+                ("vertices", ctypes.c_void_p), ("vertexCount", ctypes.c_uint32),
+                ("indices", ctypes.c_void_p), ("indexCount", ctypes.c_uint32),
+                ("meshes", ctypes.c_void_p), ("meshCount", ctypes.c_uint32),
+                ("bvhNodes", ctypes.c_void_p), ("bvhNodeCount", ctypes.c_uint32),
+                ("bvhTriRefs", ctypes.c_void_p), ("bvhTriRefCount", ctypes.c_uint32),
+                ("compoundChildren", ctypes.c_void_p), ("compoundChildCount", ctypes.c_uint32)]
+
+
+# velox::Mesh, velox::BvhNode and velox::CompoundChild records (vx_mesh,
+# vx_bvh_node, vx_compound_child in include/velox_b200_types.h).
+MESH = np.dtype([("firstVertex", "<u4"), ("vertexCount", "<u4"), ("firstIndex", "<u4"), ("indexCount", "<u4"),
+                 ("firstNode", "<u4"), ("nodeCount", "<u4"), ("firstTriRef", "<u4"),
+                 ("aabbMin", "<f4", 3), ("aabbMax", "<f4", 3)])
+BVH_NODE = np.dtype([("aabbMin", "<f4", 3), ("aabbMax", "<f4", 3), ("leftFirst", "<u4"), ("triCount", "<u4")])
+COMPOUND_CHILD = np.dtype({"names": ["shape", "localPosition", "localOrientation", "radius", "halfExtents",
+                                     "capsuleHalfHeight", "hullFirst", "hullCount", "hullFaceFirst",
+                                     "hullFaceCount"],
+                           "formats": ["u1", ("<f4", 3), ("<f4", 4), "<f4", ("<f4", 3), "<f4", "<u4", "<u4",
+                                       "<u4", "<u4"],
+                           "offsets": [0, 4, 16, 32, 36, 48, 52, 56, 60, 64], "itemsize": 68})
+assert MESH.itemsize == 52 and BVH_NODE.itemsize == 32
 
 
 class StepConfig(ctypes.Structure):
@@ -210,6 +232,7 @@ def lib(path=LIB_PATH):
         "vxb_world_stats": ([vp, ctypes.POINTER(StepStats)], i32),
         "vxb_stage_pairs": ([vp, vp, u32, f32, vp, u32, p_u32], i32),
         "vxb_stage_collide": ([vp, vp, u32, ctypes.POINTER(Soup), vp, u32, f32, vp, u32, vp, p_u32], i32),
+        "vxb_stage_pairs_soup": ([vp, vp, u32, ctypes.POINTER(Soup), f32, vp, u32, p_u32], i32),
         "vxb_stage_distance": ([vp, vp, u32, ctypes.POINTER(Soup), vp, u32, i32, vp], i32),
         "vxb_stage_color": ([vp, vp, u32, vp, u32, vp, p_u32], i32),
         "vxb_stage_pairs_noalloc": ([vp, u32, f32, vp, u32, p_u32, vp], i32),
@@ -274,11 +297,19 @@ def bodies_from_specs(specs, pool):
     return bodies, hull[:hc.value], faces[:fc.value]
 
 
-def make_soup(hull, faces):
-    hull = np.ascontiguousarray(hull, np.float32)
-    faces = np.ascontiguousarray(faces, np.uint32)
-    s = Soup(ptr(hull), len(hull), ptr(faces), len(faces))
-    s._keep = (hull, faces)
+def make_soup(hull, faces, vertices=None, indices=None, meshes=None, nodes=None, tri_refs=None, children=None):
+    """A vx_soup over numpy arrays (kept alive by the returned object)."""
+    hull = np.ascontiguousarray(hull, np.float32).reshape(-1, 3)
+    faces = np.ascontiguousarray(faces, np.uint32).reshape(-1)
+    vertices = np.ascontiguousarray(np.zeros((0, 3)) if vertices is None else vertices, np.float32).reshape(-1, 3)
+    indices = np.ascontiguousarray(np.zeros(0) if indices is None else indices, np.uint32).reshape(-1)
+    meshes = records(np.zeros(0, MESH) if meshes is None else meshes, MESH)
+    nodes = records(np.zeros(0, BVH_NODE) if nodes is None else nodes, BVH_NODE)
+    tri_refs = np.ascontiguousarray(np.zeros(0) if tri_refs is None else tri_refs, np.uint32).reshape(-1)
+    children = records(np.zeros(0, COMPOUND_CHILD) if children is None else children, COMPOUND_CHILD)
+    keep = (hull, faces, vertices, indices, meshes, nodes, tri_refs, children)
+    s = Soup(*[x for a in keep for x in (ptr(a) if len(a) else None, len(a))])
+    s._keep = keep
     return s
 
 
@@ -477,13 +508,18 @@ class Context:
         self._check(self.L.vxb_tape_end(self.h))
 
     # ---- stages
-    def pairs(self, bodies, dt):
+    def pairs(self, bodies, dt, soup=None):
         bodies = records(bodies, BODY)
         cnt = ctypes.c_uint32()
-        self._check(self.L.vxb_stage_pairs(self.h, ptr(bodies), len(bodies), dt, None, 0, ctypes.byref(cnt)))
+        if soup is None:
+            call = lambda out, cap: self.L.vxb_stage_pairs(self.h, ptr(bodies), len(bodies), dt, out, cap,
+                                                           ctypes.byref(cnt))
+        else:
+            call = lambda out, cap: self.L.vxb_stage_pairs_soup(self.h, ptr(bodies), len(bodies),
+                                                                ctypes.byref(soup), dt, out, cap, ctypes.byref(cnt))
+        self._check(call(None, 0))
         out = np.zeros(max(cnt.value, 1), np.uint64)
-        self._check(self.L.vxb_stage_pairs(self.h, ptr(bodies), len(bodies), dt, ptr(out), cnt.value,
-                                           ctypes.byref(cnt)))
+        self._check(call(ptr(out), cnt.value))
         return out[:cnt.value]
 
     def collide(self, bodies, soup, pairs, dt, cap=None):

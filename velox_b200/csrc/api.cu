@@ -121,7 +121,8 @@ void vxb_context_destroy(vxb_context* ctx) {
     for (auto& snap : c.snapshots)
         if (snap.buf.ptr) cudaFree(snap.buf.ptr);
     vxb::DevBuf* bufs[] = {&c.bodyBuf, &c.aosBuf, &c.worldOfBuf, &c.planeStartBuf, &c.planeListBuf, &c.prevPoseBuf,
-                           &c.snapBuf, &c.hullPtsBuf, &c.facesBuf, &c.aabbBuf, &c.cellKeyBuf, &c.cellValBuf,
+                           &c.snapBuf, &c.hullPtsBuf, &c.facesBuf, &c.vertBuf, &c.indexBuf, &c.meshBuf, &c.nodeBuf,
+                           &c.triRefBuf, &c.childBuf, &c.aabbBuf, &c.cellKeyBuf, &c.cellValBuf,
                            &c.sortKeysAlt, &c.sortValsAlt, &c.sortHist, &c.hashKeyBuf, &c.hashValBuf, &c.pairBuf,
                            &c.contactTmpBuf, &c.recKeyBuf, &c.recValBuf, &c.recInfoBuf, &c.recCountBuf,
                            &c.contactBuf[0], &c.contactBuf[1], &c.prevKeyBuf, &c.pairKeyBuf, &c.recOffsetBuf,
@@ -197,6 +198,17 @@ int vxb_backend_integrate(vxb_context* ctx, vx_body* bodies, uint32_t n, vx_vec3
     return vxb::readBodies(c, bodies, n);
 }
 
+// The soup's structure and the mesh / compound bodies' references into it:
+// what device reads depend on (the reference World validated the rest).
+static int checkSoupRefs(Context& c, const vx_body* bodies, uint32_t n, const vx_soup* soup) {
+    std::string why;
+    if (!vxb::validSoup(soup, why)) return vxb::fail(c, VXB_ERR_INVALID, why);
+    for (uint32_t i = 0; i < n; ++i)
+        if (!vxb::validComplexRefs(bodies[i], soup, why))
+            return vxb::fail(c, VXB_ERR_INVALID, "body " + std::to_string(i) + ": " + why);
+    return VXB_OK;
+}
+
 int vxb_backend_find_contacts(vxb_context* ctx, const vx_body* bodies, uint32_t n, const vx_soup* soup, float dt,
                               uint32_t* count) {
     GUARD(ctx);
@@ -206,6 +218,7 @@ int vxb_backend_find_contacts(vxb_context* ctx, const vx_body* bodies, uint32_t 
     c.backendContacts = 0;
     if (n < 2) return VXB_OK;
     if (!bodies) return VXB_ERR_INVALID;
+    TRY(checkSoupRefs(c, bodies, n, soup));
     TRY(ensureCounters(c));
     TRY(vxb::loadBodies(c, bodies, n, nullptr));
     TRY(vxb::loadSoup(c, soup));
@@ -277,9 +290,9 @@ int vxb_world_load(vxb_context* ctx, const vx_body* bodies, uint32_t n, const vx
     Context& c = ctx->impl;
     {
         std::string why;
-        const size_t hp = soup ? soup->hullPointCount : 0, fi = soup ? soup->hullFaceIndexCount : 0;
+        if (!vxb::validSoup(soup, why)) return vxb::fail(c, VXB_ERR_INVALID, why);
         for (uint32_t i = 0; i < n; ++i)
-            if (!vxb::validBody(bodies[i], hp, fi, why))
+            if (!vxb::validBody(bodies[i], soup, why))
                 return vxb::fail(c, VXB_ERR_INVALID, "body " + std::to_string(i) + ": " + why);
     }
     TRY(ensureCounters(c));
@@ -477,8 +490,23 @@ int vxb_stage_pairs(vxb_context* ctx, const vx_body* bodies, uint32_t n, float d
     GUARD(ctx);
     if (!bodies || !count || n == 0) return VXB_ERR_INVALID;
     Context& c = ctx->impl;
+    for (uint32_t i = 0; i < n; ++i)
+        if (bodies[i].shape == VX_SHAPE_MESH)
+            return vxb::fail(c, VXB_ERR_INVALID, "mesh bodies need their soup: use vxb_stage_pairs_soup");
     TRY(ensureCounters(c));
     TRY(vxb::loadBodies(c, bodies, n, nullptr));
+    return vxb::stagePairs(c, dt, out, cap, count);
+}
+
+int vxb_stage_pairs_soup(vxb_context* ctx, const vx_body* bodies, uint32_t n, const vx_soup* soup, float dt,
+                         uint64_t* out, uint32_t cap, uint32_t* count) {
+    GUARD(ctx);
+    if (!bodies || !count || n == 0) return VXB_ERR_INVALID;
+    Context& c = ctx->impl;
+    TRY(checkSoupRefs(c, bodies, n, soup));
+    TRY(ensureCounters(c));
+    TRY(vxb::loadBodies(c, bodies, n, nullptr));
+    TRY(vxb::loadSoup(c, soup));
     return vxb::stagePairs(c, dt, out, cap, count);
 }
 
@@ -489,6 +517,9 @@ int vxb_stage_distance(vxb_context* ctx, const vx_body* bodies, uint32_t n, cons
     Context& c = ctx->impl;
     for (uint32_t p = 0; p < npairs; ++p)
         if ((uint32_t)(pairs[p] >> 32) >= n || (uint32_t)pairs[p] >= n) return VXB_ERR_INVALID;
+    for (uint32_t i = 0; i < n; ++i)
+        if (bodies[i].shape == VX_SHAPE_MESH || bodies[i].shape == VX_SHAPE_COMPOUND)
+            return vxb::fail(c, VXB_ERR_UNSUPPORTED, "the distance stage takes convex bodies and planes");
     TRY(ensureCounters(c));
     TRY(vxb::loadBodies(c, bodies, n, nullptr));
     TRY(vxb::loadSoup(c, soup));
@@ -503,6 +534,7 @@ int vxb_stage_collide(vxb_context* ctx, const vx_body* bodies, uint32_t n, const
     Context& c = ctx->impl;
     for (uint32_t p = 0; p < npairs; ++p)
         if ((uint32_t)(pairs[p] >> 32) >= n || (uint32_t)pairs[p] >= n) return VXB_ERR_INVALID;
+    TRY(checkSoupRefs(c, bodies, n, soup));
     TRY(ensureCounters(c));
     TRY(vxb::loadBodies(c, bodies, n, nullptr));
     TRY(vxb::loadSoup(c, soup));

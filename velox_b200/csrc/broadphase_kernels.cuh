@@ -8,7 +8,10 @@ namespace vxb {
 constexpr int kCellBitsPerAxis = 10;  // must equal pipeline.cu's kCellBits
 
 __global__ void packBodiesKernel(const vx_body* __restrict__ in, uint32_t n, BodyArrays B);
-__global__ void aabbKernel(BodyArrays B, uint32_t n, float dt, float4* lo, float4* hi, Counters* C);
+// meshes: the soup's mesh records (read for mesh bodies only; may be null
+// when no mesh body is loaded)
+__global__ void aabbKernel(BodyArrays B, uint32_t n, float dt, const vx_mesh* meshes, float4* lo, float4* hi,
+                           Counters* C);
 __global__ void keyKernel(BodyArrays B, uint32_t n, const uint32_t* worldOf, const float4* lo, const float4* hi,
                           const Counters* C, uint64_t* keys, uint32_t* vals, uint64_t planeKey);
 __global__ void cellTableKernel(const uint64_t* keys, uint32_t n, uint64_t planeKey, uint64_t* hk, uint32_t* hv,

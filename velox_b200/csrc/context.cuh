@@ -167,6 +167,13 @@ struct Context {
     // ---- soup ----
     DevBuf hullPtsBuf, facesBuf;
     size_t hullPointCount = 0, faceIndexCount = 0;
+    // triangle meshes and compound children of the soup (static geometry)
+    DevBuf vertBuf, indexBuf, meshBuf, nodeBuf, triRefBuf, childBuf;
+    std::vector<vx_mesh> hostMeshes;   // root bounds for the broad phase
+    bool complexShapes = false;        // any mesh or compound body loaded
+    // FNV-1a keys of the loaded bodies' shape references and of the soup's
+    // array sizes (a snapshot image restores only into the same geometry)
+    uint64_t bodyGeometryKey = 0, soupGeometryKey = 0;
 
     // ---- broad phase ----
     DevBuf aabbBuf;      // float4 lo[n], hi[n]
@@ -305,7 +312,9 @@ int snapshotRead(Context& c, void* out, size_t capacity);
 int snapshotWrite(Context& c, const void* in, size_t size);
 
 // Input validation (validate.cpp), the reference's per-step checks of public state.
-bool validBody(const vx_body& b, size_t hullPoints, size_t faceIndices, std::string& why);
+bool validBody(const vx_body& b, const vx_soup* soup, std::string& why);
+bool validComplexRefs(const vx_body& b, const vx_soup* soup, std::string& why);
+bool validSoup(const vx_soup* soup, std::string& why);
 bool validSolverOptions(const vx_solver_options& o, std::string& why);
 bool finiteValues(const float* v, size_t count);
 

@@ -20,6 +20,7 @@ constexpr int kMaxContactsPerPair = 12;
 constexpr uint32_t kNoFeature = 0xffffffffu;
 constexpr uint32_t kFaceFeature = 0x40000000u;
 constexpr uint32_t kImplicitFeature = 0x80000000u;
+constexpr uint32_t kTriangleFeature = 0xc0000000u;
 constexpr uint32_t kEdgeTag = 0x20000000u;
 constexpr uint32_t kFaceTag = 0x40000000u;
 
@@ -44,8 +45,14 @@ struct BodyArrays {
 };
 
 struct Soup {
-    const float* points;   // xyz triples
-    const uint32_t* faces; // index triples
+    const float* points;   // hull points, xyz triples
+    const uint32_t* faces; // hull faces, index triples local to a hull's points
+    const float* vertices;             // mesh vertices, xyz triples
+    const uint32_t* indices;           // mesh index triples, relative to a mesh's firstVertex
+    const vx_mesh* meshes;
+    const vx_bvh_node* nodes;          // all meshes' BVH nodes
+    const uint32_t* triRefs;           // leaf triangle numbers
+    const vx_compound_child* children; // compound children
 };
 
 // Everything the narrow phase reads of one body.
@@ -243,6 +250,13 @@ VXD V3 supportOffsetBody(const Convex& c, const V3& dir) {
         const V3 l = len > 1e-9f ? s * (1.0f / len) : V3{0.0f, 0.0f, 0.0f};
         return rotate(c.orientation, l);
     }
+    case cTriangle: {  // corners segA, segB and triC (kept in halfExtents)
+        V3 best = c.segA - c.position;
+        const V3 b = c.segB - c.position, t = c.halfExtents - c.position;
+        if (dot(dir, b) > dot(dir, best)) best = b;
+        if (dot(dir, t) > dot(dir, best)) best = t;
+        return best;
+    }
     default: return V3{0.0f, 0.0f, 0.0f};
     }
 }
@@ -309,6 +323,24 @@ VXD Convex makeConvex(const BodyView& b, const Soup& soup) {
     return c;
 }
 
+// makeTriangle (gjk.h:228-239): a triangle of a static mesh, centred on its
+// centroid, corners in world space (the third corner in halfExtents).
+VXD Convex makeTriangle(const V3& a, const V3& b, const V3& c) {
+    Convex t;
+    t.kind = cTriangle;
+    t.quality = 0;
+    t.position = a + ((b - a) + (c - a)) * (1.0f / 3.0f);
+    t.orientation = Q4{0.0f, 0.0f, 0.0f, 1.0f};
+    t.segA = a;
+    t.segB = b;
+    t.halfExtents = c;
+    t.hullPts = nullptr; t.hullCount = 0; t.hullFaces = nullptr; t.hullFaceCount = 0;
+    t.radius = 0.0f;
+    t.geomRadius = 0.0f;
+    t.boundingRadius = vmax(length(a - t.position), vmax(length(b - t.position), length(c - t.position)));
+    return t;
+}
+
 // ---- GJK / EPA (gjk.h:241-777) --------------------------------------------
 
 struct GjkResult {
@@ -328,6 +360,8 @@ VXD float convexScale(const Convex& c) {
     if (c.boundingRadius > 0.0f) return c.boundingRadius + c.radius;
     if (c.kind == cBox) return length(c.halfExtents) + c.radius;
     if (c.kind == cSegment) return 0.5f * length(c.segA - c.segB) + c.radius;
+    if (c.kind == cTriangle)
+        return vmax(length(c.segA - c.position), vmax(length(c.segB - c.position), length(c.halfExtents - c.position)));
     return c.radius;
 }
 VXD float pairScale(const Convex& A, const Convex& B) {
@@ -1393,16 +1427,142 @@ static __device__ __noinline__ void convexConvex(const BodyView& a, const BodyVi
     emitContact(a, b, ia, ib, r.normal, (r.pointA + r.pointB) * 0.5f, r.distance, dt, out, cap, n, 0);
 }
 
-// collideSimplePair (narrowphase.h:656-673) for the supported shapes
-// (meshes and compounds are rejected when the scene is loaded).
-VXD int collidePair(const BodyView& a, const BodyView& b, uint32_t ia, uint32_t ib, const Soup& soup,
-                    float dt, vx_contact* out, int cap) {
+// ---- static triangle meshes and compounds (narrowphase.h:609-714) ---------
+//
+// A mesh body keeps its mesh index in the hull word (hullFirst); a compound
+// keeps compoundFirst / compoundCount there (hullFirst / hullCount). Neither
+// shape has hull points of its own.
+
+VXD V3 v3(const vx_vec3& v) { return V3{v.x, v.y, v.z}; }
+
+VXD V3 meshVertex(const Soup& soup, uint32_t i) {
+    return V3{soup.vertices[3 * (size_t)i], soup.vertices[3 * (size_t)i + 1], soup.vertices[3 * (size_t)i + 2]};
+}
+
+// Triangle `tri` of mesh `m` as a convex (makeTriangle of its three corners).
+VXD Convex meshTriangle(const Soup& soup, const vx_mesh& m, uint32_t tri) {
+    const uint32_t base = m.firstIndex + tri * 3;
+    return makeTriangle(meshVertex(soup, m.firstVertex + soup.indices[base]),
+                        meshVertex(soup, m.firstVertex + soup.indices[base + 1]),
+                        meshVertex(soup, m.firstVertex + soup.indices[base + 2]));
+}
+
+// compoundChildBody (backend.h:42-57): child `ch` of `parent` posed in world
+// space, with the parent's motion, materials, filters and CCD tuning.
+VXD BodyView compoundChildView(const BodyView& parent, const vx_compound_child& ch) {
+    BodyView r = parent;
+    r.flags = (parent.flags & ~kShapeMask) | ((uint32_t)ch.shape & kShapeMask);
+    r.p = parent.p + rotate(parent.q, v3(ch.localPosition));
+    r.q = qmul(parent.q, Q4{ch.localOrientation.x, ch.localOrientation.y, ch.localOrientation.z,
+                            ch.localOrientation.w});
+    r.radius = ch.radius;
+    r.half = v3(ch.halfExtents);
+    r.hh = ch.capsuleHalfHeight;
+    r.hullFirst = ch.hullFirst;
+    r.hullCount = ch.hullCount;
+    r.faceFirst = ch.hullFaceFirst;
+    r.faceCount = ch.hullFaceCount;
+    return r;
+}
+
+// Bounding-volume descent of one mesh's BVH (the explicit 48-entry stack of
+// narrowphase.h:617-636: children that do not fit are dropped, as there),
+// calling visit(tri) for each triangle of a leaf whose box overlaps [lo, hi].
+// visit returns false to stop the walk early.
+template <class Visit>
+VXD void meshVisit(const Soup& soup, const vx_mesh& m, const V3& lo, const V3& hi, Visit visit) {
+    uint32_t stack[48];
+    int sp = 0;
+    stack[sp++] = m.firstNode;
+    while (sp > 0) {
+        const vx_bvh_node& node = soup.nodes[stack[--sp]];
+        if (!aabbOverlap(lo, hi, v3(node.aabbMin), v3(node.aabbMax))) continue;
+        if (node.triCount == 0) {
+            if (sp + 2 <= 48) {
+                stack[sp++] = node.leftFirst;
+                stack[sp++] = node.leftFirst + 1;
+            }
+            continue;
+        }
+        for (uint32_t k = 0; k < node.triCount; ++k)
+            if (!visit(soup.triRefs[node.leftFirst + k])) return;
+    }
+}
+
+// meshConvex (narrowphase.h:609-643): one GJK witness contact per triangle
+// whose BVH leaf overlaps the convex's swept AABB, feature key
+// (implicit, triangle | tri). Contacts: a = the convex, b = the mesh.
+static __device__ __noinline__ void meshConvex(const BodyView& conv, const BodyView& mesh, uint32_t ic, uint32_t im,
+                                               const Soup& soup, float dt, vx_contact* out, int cap, int& n) {
+    const vx_mesh& m = soup.meshes[mesh.hullFirst];
+    const float reach = aabbReach(conv.flags, conv.half, conv.radius, conv.hh, conv.margin, conv.v, conv.w, dt);
+    const V3 lo = conv.p - V3{reach, reach, reach}, hi = conv.p + V3{reach, reach, reach};
+    const Convex cc = makeConvex(conv, soup);
+    meshVisit(soup, m, lo, hi, [&](uint32_t tri) {
+        const GjkResult r = gjkDistanceQuick(cc, meshTriangle(soup, m, tri));  // gjkDistance's result
+        emitContact(conv, mesh, ic, im, r.normal, (r.pointA + r.pointB) * 0.5f, r.distance, dt, out, cap, n,
+                    contactFeatureKey(kImplicitFeature, kTriangleFeature | tri));
+        return n < cap;  // later triangles could emit nothing more
+    });
+}
+
+// collideSimplePair (narrowphase.h:656-673).
+VXD int collideSimplePair(const BodyView& a, const BodyView& b, uint32_t ia, uint32_t ib, const Soup& soup,
+                          float dt, vx_contact* out, int cap) {
     int n = 0;
     const uint32_t sa = shapeOf(a.flags), sb = shapeOf(b.flags);
     if (isConvexVolume(sa) && isConvexVolume(sb)) convexConvex(a, b, ia, ib, soup, dt, out, cap, n);
     else if (isConvexVolume(sa) && sb == kPlane) planeConvex(a, b, ia, ib, soup, dt, out, cap, n);
     else if (sa == kPlane && isConvexVolume(sb)) planeConvex(b, a, ib, ia, soup, dt, out, cap, n);
+    else if (isConvexVolume(sa) && sb == kMesh) meshConvex(a, b, ia, ib, soup, dt, out, cap, n);
+    else if (sa == kMesh && isConvexVolume(sb)) meshConvex(b, a, ib, ia, soup, dt, out, cap, n);
     return n;
+}
+
+VXD bool isComplexShape(uint32_t s) { return s == kMesh || s == kCompound; }
+
+// Compound dispatch of collidePair (narrowphase.h:678-714): every child pair
+// through collideSimplePair, contacts owned by the parents: anchors in the
+// parents' frames, vn0 from the parents' point velocities, feature keys
+// tagged with the child numbers.
+static __device__ __noinline__ int collideCompound(const BodyView& a, const BodyView& b, uint32_t ia, uint32_t ib,
+                                                   const Soup& soup, float dt, vx_contact* out, int cap) {
+    const bool ca = shapeOf(a.flags) == kCompound, cb = shapeOf(b.flags) == kCompound;
+    const int countA = ca ? (int)a.hullCount : 1;
+    const int countB = cb ? (int)b.hullCount : 1;
+    int total = 0;
+    for (int x = 0; x < countA && total < cap; ++x) {
+        const BodyView ga = ca ? compoundChildView(a, soup.children[a.hullFirst + x]) : a;
+        for (int y = 0; y < countB && total < cap; ++y) {
+            const BodyView gb = cb ? compoundChildView(b, soup.children[b.hullFirst + y]) : b;
+            const int added = collideSimplePair(ga, gb, ia, ib, soup, dt, out + total, cap - total);
+            const uint64_t tag = (uint64_t)(x + 1) * 0x9e3779b185ebca87ull ^ (uint64_t)(y + 1) * 0xc2b2ae3d27d4eb4full;
+            for (int k = 0; k < added; ++k) {
+                vx_contact& c = out[total + k];
+                const BodyView& ownerA = c.a == ia ? a : b;
+                const BodyView& ownerB = c.b == ib ? b : a;
+                const V3 point = v3(c.point), normal = v3(c.normal);
+                const V3 la = rotateInv(ownerA.q, point - ownerA.p);
+                const V3 lb = rotateInv(ownerB.q, point - ownerB.p);
+                c.localAnchorA = vx_vec3{la.x, la.y, la.z};
+                c.localAnchorB = vx_vec3{lb.x, lb.y, lb.z};
+                c.vn0 = dot(pointVelocity(ownerA.p, ownerA.v, ownerA.w, point) -
+                                pointVelocity(ownerB.p, ownerB.v, ownerB.w, point),
+                            normal);
+                c.featureKey ^= tag;
+            }
+            total += added;
+        }
+    }
+    return total;
+}
+
+// collidePair (narrowphase.h:678-714).
+VXD int collidePair(const BodyView& a, const BodyView& b, uint32_t ia, uint32_t ib, const Soup& soup,
+                    float dt, vx_contact* out, int cap) {
+    if (shapeOf(a.flags) == kCompound || shapeOf(b.flags) == kCompound)
+        return collideCompound(a, b, ia, ib, soup, dt, out, cap);
+    return collideSimplePair(a, b, ia, ib, soup, dt, out, cap);
 }
 
 // ---- solver rows (narrowphase.h:80-366) -----------------------------------

@@ -194,7 +194,7 @@ extern "C" int vxb_stage_pairs_noalloc(const vx_body* bodies, uint32_t n, float 
 
     const uint32_t blocks = (n + 255) / 256;
     packBodiesKernel<<<blocks, 256, 0, st>>>(aos, n, B);
-    aabbKernel<<<blocks, 256, 0, st>>>(B, n, dt, lo, hi, C);
+    aabbKernel<<<blocks, 256, 0, st>>>(B, n, dt, nullptr, lo, hi, C);  // mesh bodies are rejected above
     const uint64_t planeKey = 1ull << (3 * kCellBitsPerAxis);
     keyKernel<<<blocks, 256, 0, st>>>(B, n, nullptr, lo, hi, C, keys, vals, planeKey);
     cudaError_t e = cudaSuccess;

@@ -257,7 +257,10 @@ __global__ void packBodiesKernel(const vx_body* __restrict__ in, uint32_t n, Bod
                                   b.ccdTuning.speculativeDistance);
         B.ccd[i] = make_float4(b.ccdTuning.collisionMargin, b.ccdTuning.minVelocityForCCD, 0.0f, 0.0f);
         B.plane[i] = make_float4(b.planeNormal.x, b.planeNormal.y, b.planeNormal.z, b.planeOffset);
-        B.hull[i] = make_uint4(b.hullFirst, b.hullCount, b.hullFaceFirst, b.hullFaceCount);
+        // the hull word: a mesh keeps its mesh index there, a compound its child range
+        B.hull[i] = b.shape == VX_SHAPE_MESH       ? make_uint4(b.meshIndex, 0u, 0u, 0u)
+                    : b.shape == VX_SHAPE_COMPOUND ? make_uint4(b.compoundFirst, b.compoundCount, 0u, 0u)
+                                                   : make_uint4(b.hullFirst, b.hullCount, b.hullFaceFirst, b.hullFaceCount);
         const uint32_t flags = (uint32_t)(b.shape & 15u) | ((uint32_t)(b.motionType & 3u) << kMotionShift) |
                                ((uint32_t)(b.ccdTuning.quality & 3u) << kQualityShift) |
                                (b.ccdTuning.enableContinuous ? kContinuousBit : 0u) |
@@ -330,7 +333,11 @@ constexpr int kCellBits = 10;  // per axis; coordinates wrap modulo 1024 (exactn
 constexpr uint32_t kCellMask = (1u << kCellBits) - 1u;
 constexpr uint64_t kEmptySlot = ~0ull;
 
-__global__ void aabbKernel(BodyArrays B, uint32_t n, float dt, float4* lo, float4* hi, Counters* C) {
+// Swept AABBs (bodyAabb, narrowphase.h:369-398); planes unbounded, meshes
+// their root bounds (src/backend_cuda.cu:100-129). Neither enters the cell
+// size or the cell grid's extent.
+__global__ void aabbKernel(BodyArrays B, uint32_t n, float dt, const vx_mesh* meshes, float4* lo, float4* hi,
+                           Counters* C) {
     float ext = 0.0f;
     float mn[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, mx[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -338,6 +345,12 @@ __global__ void aabbKernel(BodyArrays B, uint32_t n, float dt, float4* lo, float
         if (shapeOf(flags) == kPlane) {
             lo[i] = make_float4(-1e30f, -1e30f, -1e30f, 0.0f);
             hi[i] = make_float4(1e30f, 1e30f, 1e30f, 0.0f);
+            continue;
+        }
+        if (shapeOf(flags) == kMesh) {
+            const vx_mesh& m = meshes[B.hull[i].x];
+            lo[i] = make_float4(m.aabbMin.x, m.aabbMin.y, m.aabbMin.z, 0.0f);
+            hi[i] = make_float4(m.aabbMax.x, m.aabbMax.y, m.aabbMax.z, 0.0f);
             continue;
         }
         const V3 p = f3(B.pos[i]);
@@ -388,7 +401,8 @@ __global__ void keyKernel(BodyArrays B, uint32_t n, const uint32_t* worldOf, con
                 m2 = fromOrdered(C->cellMinBits[2]);
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         vals[i] = i;
-        if (shapeOf(B.filt[i].x) == kPlane) { keys[i] = planeKey; continue; }
+        const uint32_t shape = shapeOf(B.filt[i].x);
+        if (shape == kPlane || shape == kMesh) { keys[i] = planeKey; continue; }
         const float4 L = lo[i], H = hi[i];
         const int cx = cellCoord((L.x + H.x) * 0.5f, inv, m0);
         const int cy = cellCoord((L.y + H.y) * 0.5f, inv, m1);
@@ -434,7 +448,10 @@ VXD void emitPair(uint64_t pair, uint64_t* pairs, uint32_t cap, uint32_t* counte
 
 // Candidate pairs (src/backend_cuda.cu:174-250): the 27 neighbouring cells of
 // each body's cell (same world), pairs i<j discovered from i's side, plus the
-// planes of the body's world.
+// planes and meshes of the body's world (the list `planeList`; a mesh pair
+// also needs overlapping AABBs). Plane pairs of simple convex bodies go to
+// `planePairs`; mesh pairs and a compound's plane pairs join the general
+// pairs, whose narrow phase handles every shape.
 __global__ void pairKernel(BodyArrays B, uint32_t n, const uint64_t* keys, const uint32_t* vals, const float4* lo,
                            const float4* hi, const uint64_t* hk, const uint32_t* hv, uint32_t mask, uint64_t planeKey,
                            const uint32_t* worldOf, const uint32_t* planeStart, const uint32_t* planeList,
@@ -468,14 +485,18 @@ __global__ void pairKernel(BodyArrays B, uint32_t n, const uint64_t* keys, const
                     }
                 }
         const uint32_t w = worldOf ? worldOf[i] : 0u;
+        const bool compound = shapeOf(fi.x) == kCompound;
         for (uint32_t k = planeStart[w]; k < planeStart[w + 1]; ++k) {
             const uint32_t p = planeList[k];
             const uint4 fp = B.filt[p];
+            const bool mesh = shapeOf(fp.x) == kMesh;
+            if (mesh && !aabbOverlap(Li, Hi, f3(lo[p]), f3(hi[p]))) continue;
             if (inert(fi.x) && inert(fp.x)) continue;
             const uint32_t a = i < p ? i : p, b = i < p ? p : i;
             const uint4 fa = a == i ? fi : fp, fb = a == i ? fp : fi;
             if (!canCollide(fa.y, fa.z, (int32_t)fa.w, fb.y, fb.z, (int32_t)fb.w)) continue;
-            emitPair(((uint64_t)a << 32) | b, planePairs, planeCap, &C->planePairs, C);
+            if (mesh || compound) emitPair(((uint64_t)a << 32) | b, pairs, cap, &C->pairs, C);
+            else emitPair(((uint64_t)a << 32) | b, planePairs, planeCap, &C->planePairs, C);
         }
     }
 }
@@ -496,7 +517,9 @@ VXD bool pointLess(const vx_contact& x, const vx_contact& y) {
 // mode 0: key = (a << bodyBits) | b; mode 1: key = pair index, emission order kept.
 // Which pair classes one instantiation handles: plane pairs compile to a
 // light kernel (high occupancy), convex pairs to the GJK/EPA kernel.
-enum PairClass : int { kAnyPairs = 0, kPlanePairs = 1, kConvexPairs = 2 };
+// Mesh and compound pairs (among the general pairs) take a third
+// instantiation, launched only when such bodies are loaded.
+enum PairClass : int { kAnyPairs = 0, kPlanePairs = 1, kConvexPairs = 2, kComplexPairs = 3 };
 
 // `order` (optional): the pairs in the order to process them (convex pairs
 // grouped by shape combination so that a warp runs one code path).
@@ -518,13 +541,16 @@ __global__ void __launch_bounds__(128) collideKernel(BodyArrays B, Soup soup, co
             const uint32_t i = (uint32_t)(pr >> 32), j = (uint32_t)pr;
             const BodyView a = loadView(B, i);
             const BodyView b = loadView(B, j);
+            const bool complex = isComplexShape(shapeOf(a.flags)) || isComplexShape(shapeOf(b.flags));
             if (Class == kAnyPairs) {
                 count = collidePair(a, b, i, j, soup, dt, buf, kMaxContactsPerPair);
             } else if (Class == kPlanePairs) {
                 if (shapeOf(b.flags) == kPlane) planeConvex(a, b, i, j, soup, dt, buf, kMaxContactsPerPair, count);
                 else planeConvex(b, a, j, i, soup, dt, buf, kMaxContactsPerPair, count);
-            } else {
-                convexConvex(a, b, i, j, soup, dt, buf, kMaxContactsPerPair, count);
+            } else if (Class == kConvexPairs) {
+                if (!complex) convexConvex(a, b, i, j, soup, dt, buf, kMaxContactsPerPair, count);
+            } else if (complex) {
+                count = collidePair(a, b, i, j, soup, dt, buf, kMaxContactsPerPair);
             }
             if (mode == 0)
                 for (int x = 1; x < count; ++x) {
@@ -2120,7 +2146,23 @@ VXD BodyView withPose(BodyView b, const V3& p, const Q4& q) {
 // Distance query of the rewind: gjkDistance's results, the common case in registers.
 VXD GjkResult distanceQuery(const Convex& ca, const Convex& cb) { return gjkDistanceQuick(ca, cb); }
 
-__device__ __noinline__ GapProbe gapAt(const BodyView& a, const BodyView& b, const Soup& soup) {
+// meshSimpleGapProbe (narrowphase.h:719-749): the smallest gap (strictly
+// smaller replaces) between `a` and the triangles of mesh `b` whose BVH
+// leaves overlap a cube of half width `search` around a's position.
+__device__ __noinline__ void meshGap(const BodyView& a, const BodyView& b, const Soup& soup, float search,
+                                     GapProbe& best) {
+    const vx_mesh& m = soup.meshes[b.hullFirst];
+    const V3 lo = a.p - V3{search, search, search}, hi = a.p + V3{search, search, search};
+    const Convex ca = makeConvex(a, soup);
+    meshVisit(soup, m, lo, hi, [&](uint32_t tri) {
+        const GjkResult g = distanceQuery(ca, meshTriangle(soup, m, tri));
+        if (g.distance < best.gap) best = GapProbe{g.distance, g.normal};
+        return true;
+    });
+}
+
+// gapAt (world.cpp:2916-2958) for two non-compound bodies, b not a mesh.
+VXD GapProbe gapConvex(const BodyView& a, const BodyView& b, const Soup& soup) {
     if (shapeOf(b.flags) == kPlane) {
         const Convex c = makeConvex(a, soup);
         const V3 deep = c.position + supportOffsetBody(c, -b.planeN);
@@ -2128,6 +2170,49 @@ __device__ __noinline__ GapProbe gapAt(const BodyView& a, const BodyView& b, con
     }
     const GjkResult r = distanceQuery(makeConvex(a, soup), makeConvex(b, soup));
     return GapProbe{r.distance, r.normal};
+}
+
+// gapAt's compound and mesh cases: the minimum over every child pair (A's
+// children outer, B's inner) and every searched triangle, the first minimum
+// kept, starting from (1e30, +y) as the reference's recursion does.
+__device__ __noinline__ GapProbe gapComplex(const BodyView& a, const BodyView& b, const Soup& soup, float search) {
+    GapProbe best{1e30f, V3{0.0f, 1.0f, 0.0f}};
+    const bool ca = shapeOf(a.flags) == kCompound, cb = shapeOf(b.flags) == kCompound;
+    const uint32_t countA = ca ? a.hullCount : 1u, countB = cb ? b.hullCount : 1u;
+    for (uint32_t x = 0; x < countA; ++x) {
+        const BodyView ga = ca ? compoundChildView(a, soup.children[a.hullFirst + x]) : a;
+        for (uint32_t y = 0; y < countB; ++y) {
+            const BodyView gb = cb ? compoundChildView(b, soup.children[b.hullFirst + y]) : b;
+            if (shapeOf(gb.flags) == kMesh) {
+                meshGap(ga, gb, soup, search, best);
+            } else {
+                const GapProbe g = gapConvex(ga, gb, soup);
+                if (g.gap < best.gap) best = g;
+            }
+        }
+    }
+    return best;
+}
+
+// Signed gap and normal (from b towards a) of the rewind's distance oracle;
+// `dt` sizes the mesh search cube as the rewind loop does (world.cpp:4272-4273).
+__device__ __noinline__ GapProbe gapAt(const BodyView& a, const BodyView& b, const Soup& soup, float dt) {
+    if (isComplexShape(shapeOf(a.flags)) || isComplexShape(shapeOf(b.flags))) {
+        const float search = maxPointSpeed(a) * dt + a.radius + length(a.half) + a.hh + 0.1f;
+        return gapComplex(a, b, soup, search);
+    }
+    return gapConvex(a, b, soup);
+}
+
+// Bounding spheres more than 1 mm apart give a positive end gap, so the
+// rewind's `gap >= -8 mm` test skips the pair (planes and meshes have no
+// bounding sphere).
+VXD bool spheresApart(const BodyView& a, const BodyView& b) {
+    const uint32_t sb = shapeOf(b.flags);
+    if (sb == kPlane || sb == kMesh) return false;
+    const float reach = coreExtent(shapeOf(a.flags), a.half, a.radius, a.hh) +
+                        coreExtent(sb, b.half, b.radius, b.hh) + 1e-3f;
+    return lengthSq(a.p - b.p) > reach * reach;
 }
 
 VXD Mass massOfView(const BodyArrays& B, uint32_t i) { return loadMass(B, i); }
@@ -2149,23 +2234,15 @@ VXD void orientPair(const BodyArrays& B, uint64_t key, uint32_t& i, uint32_t& j)
     if (!isDynamic(B.filt[i].x) && isDynamic(B.filt[j].x)) { const uint32_t t = i; i = j; j = t; }
 }
 
-__global__ void caProbeKernel(BodyArrays B, Soup soup, const uint64_t* pairKeys, uint32_t npairs,
+__global__ void caProbeKernel(BodyArrays B, Soup soup, const uint64_t* pairKeys, uint32_t npairs, float dt,
                               uint32_t* flags, uint32_t* bodyMark, float4* endGap) {
     for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < npairs; r += gridDim.x * blockDim.x) {
         uint32_t i, j;
         orientPair(B, pairKeys[r], i, j);
         const BodyView a = loadView(B, i), b = loadView(B, j);
         uint32_t flag = 0;
-        bool separated = false;
-        if (shapeOf(b.flags) != kPlane) {
-            // Bounding spheres apart by more than 1 mm: the end gap is positive,
-            // so the reference's `gap >= -8 mm` test skips the pair.
-            const float reach = coreExtent(shapeOf(a.flags), a.half, a.radius, a.hh) +
-                                coreExtent(shapeOf(b.flags), b.half, b.radius, b.hh) + 1e-3f;
-            separated = lengthSq(a.p - b.p) > reach * reach;
-        }
-        if (!separated && caEligible(a, b, B, i)) {
-            const GapProbe end = gapAt(a, b, soup);
+        if (!spheresApart(a, b) && caEligible(a, b, B, i)) {
+            const GapProbe end = gapAt(a, b, soup, dt);
             if (end.gap < -8e-3f) {
                 flag = 1;
                 endGap[r] = make_float4(end.gap, end.normal.x, end.normal.y, end.normal.z);
@@ -2203,18 +2280,13 @@ __device__ __noinline__ bool caRewind(BodyArrays& B, const Soup& soup, uint32_t 
                                       const float4* cached, float4* spec = nullptr) {
     BodyView a = loadViewCoherent(B, i), b = loadViewCoherent(B, j);
     if (!caEligible(a, b, B, i)) return false;
-    if (shapeOf(b.flags) != kPlane) {
-        // bounding spheres more than 1 mm apart: positive end gap, no rewind (the probe's test)
-        const float reach = coreExtent(shapeOf(a.flags), a.half, a.radius, a.hh) +
-                            coreExtent(shapeOf(b.flags), b.half, b.radius, b.hh) + 1e-3f;
-        if (lengthSq(a.p - b.p) > reach * reach) return false;
-    }
+    if (spheresApart(a, b)) return false;  // positive end gap, no rewind (the probe's test)
     GapProbe end;
     if (cached) {
         const float4 g = *cached;
         end = GapProbe{g.x, V3{g.y, g.z, g.w}};
     } else {
-        end = gapAt(a, b, soup);
+        end = gapAt(a, b, soup, dt);
     }
     if (end.gap >= -8e-3f) return false;
     const bool bStatic = isStaticBody(b.flags), bDyn = isDynamic(b.flags);
@@ -2235,7 +2307,7 @@ __device__ __noinline__ bool caRewind(BodyArrays& B, const Soup& soup, uint32_t 
         ++queries;
         const Q4 qa = orientationAt(ma, qa0, La, dt * t);
         const Q4 qb = bStatic ? qb0 : orientationAt(mb, qb0, Lb, dt * t);
-        const GapProbe g = gapAt(withPose(a, pa0 + da * t, qa), withPose(b, pb0 + db * t, qb), soup);
+        const GapProbe g = gapAt(withPose(a, pa0 + da * t, qa), withPose(b, pb0 + db * t, qb), soup, dt);
         n = g.normal;
         if (g.gap < 1e-3f) break;
         t = vmin(1.0f, t + g.gap / bound);
@@ -2599,6 +2671,12 @@ static int resetCounters(Context& c) {
     return VXB_OK;
 }
 
+static uint64_t fnv1a(uint64_t h, const void* data, size_t bytes) {
+    const unsigned char* p = static_cast<const unsigned char*>(data);
+    for (size_t k = 0; k < bytes; ++k) h = (h ^ p[k]) * 0x100000001b3ull;
+    return h;
+}
+
 int loadSoup(Context& c, const vx_soup* soup) {
     c.hullPointCount = soup ? soup->hullPointCount : 0;
     c.faceIndexCount = soup ? soup->hullFaceIndexCount : 0;
@@ -2610,17 +2688,51 @@ int loadSoup(Context& c, const vx_soup* soup) {
     if (c.faceIndexCount)
         VXB_CUDA(c, cudaMemcpyAsync(c.facesBuf.ptr, soup->hullFaceIndices, c.faceIndexCount * 4,
                                     cudaMemcpyHostToDevice, c.stream));
+    // triangle meshes, their BVHs and compound children
+    struct Part { DevBuf* buf; const void* src; size_t bytes; };
+    const Part parts[] = {
+        {&c.vertBuf, soup ? soup->vertices : nullptr, soup ? (size_t)soup->vertexCount * 12 : 0},
+        {&c.indexBuf, soup ? soup->indices : nullptr, soup ? (size_t)soup->indexCount * 4 : 0},
+        {&c.meshBuf, soup ? soup->meshes : nullptr, soup ? (size_t)soup->meshCount * sizeof(vx_mesh) : 0},
+        {&c.nodeBuf, soup ? soup->bvhNodes : nullptr, soup ? (size_t)soup->bvhNodeCount * sizeof(vx_bvh_node) : 0},
+        {&c.triRefBuf, soup ? soup->bvhTriRefs : nullptr, soup ? (size_t)soup->bvhTriRefCount * 4 : 0},
+        {&c.childBuf, soup ? soup->compoundChildren : nullptr,
+         soup ? (size_t)soup->compoundChildCount * sizeof(vx_compound_child) : 0}};
+    for (const Part& part : parts) {
+        VXB_TRY(ensure(c, *part.buf, part.bytes + 16));
+        if (part.bytes)
+            VXB_CUDA(c, cudaMemcpyAsync(part.buf->ptr, part.src, part.bytes, cudaMemcpyHostToDevice, c.stream));
+    }
+    if (soup && soup->meshCount) VXB_CUDA(c, cudaStreamSynchronize(c.stream));  // copies read the caller's arrays
+    uint64_t key = 0xcbf29ce484222325ull;
+    for (const Part& part : parts) key = fnv1a(key, &part.bytes, sizeof(part.bytes));
+    const size_t hull[2] = {c.hullPointCount, c.faceIndexCount};
+    c.soupGeometryKey = fnv1a(key, hull, sizeof(hull));
     return VXB_OK;
 }
 
-static Soup soupOf(Context& c) { return Soup{P<float>(c.hullPtsBuf), P<uint32_t>(c.facesBuf)}; }
+static Soup soupOf(Context& c) {
+    return Soup{P<float>(c.hullPtsBuf), P<uint32_t>(c.facesBuf),  P<float>(c.vertBuf),
+                P<uint32_t>(c.indexBuf), P<vx_mesh>(c.meshBuf),    P<vx_bvh_node>(c.nodeBuf),
+                P<uint32_t>(c.triRefBuf), P<vx_compound_child>(c.childBuf)};
+}
 
 int loadBodies(Context& c, const vx_body* bodies, uint32_t n, const uint32_t* worldOf) {
     if (n == 0) return fail(c, VXB_ERR_INVALID, "no bodies");
+    c.complexShapes = false;
+    uint64_t key = 0xcbf29ce484222325ull;
+    for (uint32_t i = 0; i < n; ++i) {
+        const vx_body& b = bodies[i];
+        const uint32_t refs[6] = {b.shape, b.meshIndex, b.hullFirst, b.hullCount, b.compoundFirst, b.compoundCount};
+        key = fnv1a(key, refs, sizeof(refs));
+        key = fnv1a(key, &b.hullFaceFirst, 8);  // hullFaceFirst, hullFaceCount
+    }
+    c.bodyGeometryKey = key;
     for (uint32_t i = 0; i < n; ++i) {
         const uint8_t s = bodies[i].shape;
-        if (s == VX_SHAPE_MESH || s == VX_SHAPE_COMPOUND)
-            return fail(c, VXB_ERR_UNSUPPORTED, "mesh and compound bodies are not supported by the device pipeline");
+        if (s == VX_SHAPE_MESH || s == VX_SHAPE_COMPOUND) c.complexShapes = true;
+        if (s == VX_SHAPE_MESH && bodies[i].motionType != VX_MOTION_STATIC)
+            return fail(c, VXB_ERR_INVALID, "mesh bodies are static");
         if (bodies[i].motionType == VX_MOTION_KINEMATIC)
             return fail(c, VXB_ERR_UNSUPPORTED, "kinematic bodies are not supported by the device pipeline");
     }
@@ -2638,7 +2750,7 @@ int loadBodies(Context& c, const vx_body* bodies, uint32_t n, const uint32_t* wo
     VXB_TRY(ensure(c, c.aosBuf, (size_t)n * sizeof(vx_body)));
     VXB_CUDA(c, cudaMemcpyAsync(c.aosBuf.ptr, bodies, (size_t)n * sizeof(vx_body), cudaMemcpyHostToDevice, c.stream));
     LAUNCH(c, packBodiesKernel, blocksFor(n, 256), 256, P<vx_body>(c.aosBuf), n, c.B);
-    // worlds and per-world plane lists
+    // worlds and per-world lists of planes and meshes (paired with every body of their world)
     c.hostWorldOf.assign(n, 0u);
     uint32_t worlds = 1;
     if (worldOf) {
@@ -2651,14 +2763,15 @@ int loadBodies(Context& c, const vx_body* bodies, uint32_t n, const uint32_t* wo
     }
     c.worlds = worlds;
     std::vector<uint32_t> planeStart(worlds + 1, 0), planeList;
+    auto boundless = [&](uint32_t i) { return bodies[i].shape == VX_SHAPE_PLANE || bodies[i].shape == VX_SHAPE_MESH; };
     for (uint32_t i = 0; i < n; ++i)
-        if (bodies[i].shape == VX_SHAPE_PLANE) ++planeStart[c.hostWorldOf[i] + 1];
+        if (boundless(i)) ++planeStart[c.hostWorldOf[i] + 1];
     for (uint32_t w = 0; w < worlds; ++w) planeStart[w + 1] += planeStart[w];
     planeList.resize(planeStart[worlds]);
     {
         std::vector<uint32_t> fill(planeStart.begin(), planeStart.end() - 1);
         for (uint32_t i = 0; i < n; ++i)
-            if (bodies[i].shape == VX_SHAPE_PLANE) planeList[fill[c.hostWorldOf[i]]++] = i;
+            if (boundless(i)) planeList[fill[c.hostWorldOf[i]]++] = i;
     }
     VXB_TRY(ensure(c, c.worldOfBuf, (size_t)n * 4));
     VXB_TRY(ensure(c, c.planeStartBuf, planeStart.size() * 4));
@@ -2730,8 +2843,8 @@ static int broadPhase(Context& c, float dt, uint32_t* pairCount) {
     float4* lo = P<float4>(c.aabbBuf);
     float4* hi = lo + n;
     stageBegin(c, kStageBroadphase);
-    LAUNCH(c, aabbKernel, std::min<uint32_t>(blocksFor(n, 256), (uint32_t)c.smCount * 8), 256, c.B, n, dt, lo, hi,
-           c.dCounters);
+    LAUNCH(c, aabbKernel, std::min<uint32_t>(blocksFor(n, 256), (uint32_t)c.smCount * 8), 256, c.B, n, dt,
+           (const vx_mesh*)P<vx_mesh>(c.meshBuf), lo, hi, c.dCounters);
     const int worldBits = bitsFor(c.worlds > 1 ? c.worlds - 1 : 0);
     const int keyBitsTotal = 3 * kCellBits + worldBits + 1;
     const uint64_t planeKey = 1ull << (3 * kCellBits + worldBits);
@@ -2820,6 +2933,12 @@ static int narrowPhase(Context& c, const uint64_t* pairs, uint32_t npairs, float
                        128, c.B, soupOf(c), pairs, (const uint32_t*)P<uint32_t>(c.classValBuf), convexSplit, dt, mode,
                        bodyBits, P<vx_contact>(c.contactTmpBuf), c.contactCap, P<uint64_t>(c.recKeyBuf),
                        P<uint32_t>(c.recValBuf), P<uint2>(c.recInfoBuf), c.recCap, c.dCounters);
+                if (c.complexShapes)
+                    LAUNCH(c, collideKernel<kComplexPairs>,
+                           std::min<uint32_t>(blocksFor(convexSplit, 128), (uint32_t)c.smCount * 16), 128, c.B,
+                           soupOf(c), pairs, (const uint32_t*)P<uint32_t>(c.classValBuf), convexSplit, dt, mode,
+                           bodyBits, P<vx_contact>(c.contactTmpBuf), c.contactCap, P<uint64_t>(c.recKeyBuf),
+                           P<uint32_t>(c.recValBuf), P<uint2>(c.recInfoBuf), c.recCap, c.dCounters);
             }
             if (np)
                 LAUNCH(c, collideKernel<kPlanePairs>, std::min<uint32_t>(blocksFor(np, 128), (uint32_t)c.smCount * 16),
@@ -3286,7 +3405,7 @@ static int conservativeAdvancement(Context& c, uint32_t npairs, float dt) {
     const float4* prevPos = P<float4>(c.prevPoseBuf);
     const float4* prevRot = prevPos + n;
     LAUNCH(c, caProbeKernel, std::min<uint32_t>(blocksFor(npairs, 128), (uint32_t)c.smCount * 16), 128, c.B, soupOf(c),
-           pk, npairs, flags, bodyMark, endGap);
+           pk, npairs, dt, flags, bodyMark, endGap);
     // speculative outcomes of the flagged pairs on the probe's state
     VXB_TRY(exclusiveScan(c, flags, flagRank, npairs, &c.dCounters->caFlagged));
     VXB_TRY(readCounters(c));

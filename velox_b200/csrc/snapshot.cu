@@ -8,8 +8,10 @@
 //     host round trip) for rollback and replay;
 //   * a byte image in caller memory (for files or another context that
 //     loaded the same bodies).
-// A snapshot restores only into a world with the same body count and world
-// partition; restoring ends an active adjoint tape.
+// A snapshot restores only into a world with the same body count, world
+// partition and geometry (shapes and their references into the soup, and the
+// soup's array sizes: the image's body words index the destination's soup);
+// restoring ends an active adjoint tape.
 #include <cstring>
 
 #include "context.cuh"
@@ -19,17 +21,21 @@ namespace vxb {
 namespace {
 
 constexpr uint32_t kSnapshotMagic = 0x53425856u;  // "VXBS"
-constexpr uint32_t kSnapshotVersion = 2;
+constexpr uint32_t kSnapshotVersion = 3;
 
 struct SnapshotHeader {
     uint32_t magic, version, n, worlds;
     uint32_t prevCount, cur, configured, stepContacts;
     uint32_t pairCount, sleepable, asleep, pad;
     uint64_t bodyBytes, totalBytes;
+    uint64_t geometry;  // geometryKey of the world the image was taken from
     vxb_step_config config;
     vxb_sleep_config sleepConfig;
     vxb_step_stats stats;
 };
+
+// The loaded bodies' shape references and the soup's sizes in one key.
+uint64_t geometryKey(const Context& c) { return c.bodyGeometryKey * 0x9e3779b97f4a7c15ull ^ c.soupGeometryKey; }
 
 size_t bodyBytesOf(const Context& c) { return (((size_t)c.n * 16 + 255) & ~(size_t)255) * 16; }
 
@@ -56,6 +62,7 @@ SnapshotHeader headerOf(const Context& c) {
     h.asleep = c.sleep.asleep;
     h.bodyBytes = bodyBytesOf(c);
     h.totalBytes = imageBytes(c, c.prevCount, c.sleep.pairCount);
+    h.geometry = geometryKey(c);
     h.config = c.config;
     h.sleepConfig = c.sleep.config;
     h.stats = c.stats;
@@ -99,6 +106,8 @@ int checkCompatible(Context& c, const SnapshotHeader& h) {
         return fail(c, VXB_ERR_INVALID, "snapshot: not a snapshot image of this library version");
     if (h.n != c.n || h.worlds != c.worlds || h.bodyBytes != bodyBytesOf(c))
         return fail(c, VXB_ERR_INVALID, "snapshot: the world has another body count or world partition");
+    if (h.geometry != geometryKey(c))
+        return fail(c, VXB_ERR_INVALID, "snapshot: the world has other shapes or another soup");
     return VXB_OK;
 }
 

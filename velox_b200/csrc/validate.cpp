@@ -28,7 +28,74 @@ bool bad(std::string& why, const char* what) {
 
 }  // namespace
 
-bool validBody(const vx_body& b, size_t hullPoints, size_t faceIndices, std::string& why) {
+bool convexShape(uint8_t s) {
+    return s == VX_SHAPE_SPHERE || s == VX_SHAPE_BOX || s == VX_SHAPE_CAPSULE || s == VX_SHAPE_HULL ||
+           s == VX_SHAPE_CYLINDER || s == VX_SHAPE_CONE || s == VX_SHAPE_ROUNDED_BOX || s == VX_SHAPE_ELLIPSOID;
+}
+
+// References of a mesh or compound body into the soup (src/world.cpp:3901-3927).
+bool validComplexRefs(const vx_body& b, const vx_soup* soup, std::string& why) {
+    if (b.shape == VX_SHAPE_MESH) {
+        if (!soup || b.meshIndex >= soup->meshCount) return bad(why, "mesh body references an invalid mesh");
+    } else if (b.shape == VX_SHAPE_COMPOUND) {
+        if (!soup || b.compoundCount == 0 || (size_t)b.compoundFirst + b.compoundCount > soup->compoundChildCount)
+            return bad(why, "compound body references invalid child storage");
+    }
+    return true;
+}
+
+// Structure of the soup's meshes, BVHs and compound children, checked once
+// when it is loaded so that the device walks stay inside their arrays and
+// every BVH descent ends (an inner node's children follow it).
+bool validSoup(const vx_soup* soup, std::string& why) {
+    if (!soup) return true;
+    const vx_soup& s = *soup;
+    if ((s.hullPointCount && !s.hullPoints) || (s.hullFaceIndexCount && !s.hullFaceIndices) ||
+        (s.vertexCount && !s.vertices) || (s.indexCount && !s.indices) || (s.meshCount && !s.meshes) ||
+        (s.bvhNodeCount && !s.bvhNodes) || (s.bvhTriRefCount && !s.bvhTriRefs) ||
+        (s.compoundChildCount && !s.compoundChildren))
+        return bad(why, "mesh soup has a null array with a non-zero count");
+    for (uint32_t k = 0; k < s.meshCount; ++k) {
+        const vx_mesh& m = s.meshes[k];
+        const size_t tris = m.indexCount / 3;
+        if ((size_t)m.firstVertex + m.vertexCount > s.vertexCount || (size_t)m.firstIndex + m.indexCount > s.indexCount ||
+            m.indexCount % 3 != 0 || m.nodeCount == 0 || (size_t)m.firstNode + m.nodeCount > s.bvhNodeCount)
+            return bad(why, "mesh references invalid vertex, index or node storage");
+        for (uint32_t x = 0; x < m.indexCount; ++x)
+            if (s.indices[m.firstIndex + x] >= m.vertexCount) return bad(why, "mesh index is outside the vertex array");
+        const size_t nodeEnd = (size_t)m.firstNode + m.nodeCount;
+        for (size_t v = m.firstNode; v < nodeEnd; ++v) {
+            const vx_bvh_node& node = s.bvhNodes[v];
+            if (node.triCount == 0) {
+                if (node.leftFirst <= v || (size_t)node.leftFirst + 1 >= nodeEnd)
+                    return bad(why, "mesh BVH has an invalid inner node");
+            } else {
+                if ((size_t)node.leftFirst + node.triCount > s.bvhTriRefCount)
+                    return bad(why, "mesh BVH leaf references invalid triangle storage");
+                for (uint32_t t = 0; t < node.triCount; ++t)
+                    if (s.bvhTriRefs[node.leftFirst + t] >= tris)
+                        return bad(why, "mesh BVH leaf references an invalid triangle");
+            }
+        }
+    }
+    for (uint32_t k = 0; k < s.compoundChildCount; ++k) {
+        const vx_compound_child& c = s.compoundChildren[k];
+        if (!fin3(c.localPosition) || !finq(c.localOrientation) || !convexShape(c.shape))
+            return bad(why, "compound child contains invalid state");
+        if (c.shape == VX_SHAPE_HULL) {
+            if (c.hullCount == 0 || (size_t)c.hullFirst + c.hullCount > s.hullPointCount ||
+                (size_t)c.hullFaceFirst + (size_t)c.hullFaceCount * 3 > s.hullFaceIndexCount)
+                return bad(why, "compound child references invalid hull storage");
+            for (size_t f = 0; f < (size_t)c.hullFaceCount * 3; ++f)
+                if (s.hullFaceIndices[c.hullFaceFirst + f] >= c.hullCount)
+                    return bad(why, "compound child references invalid hull storage");
+        }
+    }
+    return true;
+}
+
+bool validBody(const vx_body& b, const vx_soup* soup, std::string& why) {
+    const size_t hullPoints = soup ? soup->hullPointCount : 0, faceIndices = soup ? soup->hullFaceIndexCount : 0;
     if (!fin3(b.position) || !finq(b.orientation) || !finq(b.inertiaOrientation) || !fin3(b.velocity) ||
         !fin3(b.angularVelocity) || !fin3(b.force) || !fin3(b.torque) || !nonNegative(b.invMass) ||
         !fin3(b.invInertia) || b.invInertia.x < 0.0f || b.invInertia.y < 0.0f || b.invInertia.z < 0.0f ||
@@ -83,7 +150,8 @@ bool validBody(const vx_body& b, size_t hullPoints, size_t faceIndices, std::str
         break;
     case VX_SHAPE_MESH:
     case VX_SHAPE_COMPOUND:
-        break;  // rejected by the device pipeline with VXB_ERR_UNSUPPORTED
+        if (!validComplexRefs(b, soup, why)) return false;
+        break;
     default:
         return bad(why, "body has an unknown shape");
     }

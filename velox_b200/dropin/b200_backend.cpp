@@ -13,6 +13,7 @@
 #include "velox/backend.h"
 #include "velox/error.h"
 
+#include <cstddef>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -22,6 +23,11 @@
 static_assert(sizeof(velox::Body) == sizeof(vx_body), "velox::Body and vx_body must share one layout");
 static_assert(sizeof(velox::Contact) == sizeof(vx_contact), "velox::Contact and vx_contact must share one layout");
 static_assert(sizeof(velox::SolverOptions) == sizeof(vx_solver_options), "SolverOptions layout");
+static_assert(sizeof(velox::Mesh) == sizeof(vx_mesh), "Mesh layout");
+static_assert(sizeof(velox::BvhNode) == sizeof(vx_bvh_node), "BvhNode layout");
+static_assert(sizeof(velox::CompoundChild) == sizeof(vx_compound_child), "CompoundChild layout");
+static_assert(offsetof(velox::CompoundChild, hullFaceCount) == offsetof(vx_compound_child, hullFaceCount),
+              "CompoundChild tail");
 
 namespace velox {
 namespace {
@@ -43,8 +49,21 @@ public:
                       std::vector<Contact>& out) override {
         out.clear();
         vx_soup soup{reinterpret_cast<const vx_vec3*>(meshes.hullPoints.data()),
-                     (uint32_t)meshes.hullPoints.size(), meshes.hullFaceIndices.data(),
-                     (uint32_t)meshes.hullFaceIndices.size()};
+                     (uint32_t)meshes.hullPoints.size(),
+                     meshes.hullFaceIndices.data(),
+                     (uint32_t)meshes.hullFaceIndices.size(),
+                     reinterpret_cast<const vx_vec3*>(meshes.vertices.data()),
+                     (uint32_t)meshes.vertices.size(),
+                     meshes.indices.data(),
+                     (uint32_t)meshes.indices.size(),
+                     reinterpret_cast<const vx_mesh*>(meshes.meshes.data()),
+                     (uint32_t)meshes.meshes.size(),
+                     reinterpret_cast<const vx_bvh_node*>(meshes.bvhNodes.data()),
+                     (uint32_t)meshes.bvhNodes.size(),
+                     meshes.bvhTriRefs.data(),
+                     (uint32_t)meshes.bvhTriRefs.size(),
+                     reinterpret_cast<const vx_compound_child*>(meshes.compoundChildren.data()),
+                     (uint32_t)meshes.compoundChildren.size()};
         uint32_t count = 0;
         check(vxb_backend_find_contacts(ctx_, reinterpret_cast<const vx_body*>(bodies.data()),
                                         (uint32_t)bodies.size(), &soup, dt, &count));
