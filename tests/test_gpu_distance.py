@@ -37,3 +37,31 @@ def test_distance_paths_match_reference_gjk(ctx, ref, kind, size, spread):
     assert np.array_equal(fast.view(np.uint32), general.view(np.uint32))
     assert np.array_equal(general[:, 10], theirs[:, 10])
     assert np.allclose(general[:, :10], theirs[:, :10], rtol=0.0, atol=1e-5)
+
+
+def test_curved_and_rounded_shapes_match_reference_gjk(ctx, ref):
+    # cones, rounded boxes and ellipsoids (absent from the generated scenes)
+    # against every other convex shape, separated and overlapping
+    w, specs, pool, bodies, soup = reference_scene(ref, "dense", 600)
+    w.close()
+    rng = np.random.default_rng(3)
+    bodies = bodies.copy()
+    dyn = np.flatnonzero(bodies["shape"] != 1)
+    pick = rng.choice(dyn, len(dyn) // 2, replace=False)
+    kinds = rng.choice([8, 9, 10], len(pick))
+    bodies["shape"][pick] = kinds
+    bodies["halfExtents"][pick] = rng.uniform(0.08, 0.3, (len(pick), 3))
+    bodies["radius"][pick] = rng.uniform(0.03, 0.2, len(pick))
+    bodies["capsuleHalfHeight"][pick] = rng.uniform(0.08, 0.3, len(pick))
+    pairs = _pairs(bodies, rng, 4000)
+    theirs = ref.gjk_distances(bodies, soup, pairs)
+    fast = ctx.distance(bodies, soup, pairs, path=0)
+    general = ctx.distance(bodies, soup, pairs, path=1)
+    a = bodies["shape"][(pairs >> np.uint64(32)).astype(np.int64)]
+    b = bodies["shape"][(pairs & np.uint64(0xffffffff)).astype(np.int64)]
+    curved = np.isin(a, [8, 9, 10]) | np.isin(b, [8, 9, 10])
+    assert curved.sum() > 1000 and (theirs[curved, 10] == 1).any() and (theirs[curved, 10] == 0).any()
+    assert np.array_equal(fast.view(np.uint32), general.view(np.uint32))
+    assert np.array_equal(general[:, 10], theirs[:, 10])
+    bad = np.flatnonzero(np.abs(general[:, :10] - theirs[:, :10]).max(1) > 1e-5)
+    assert len(bad) == 0, [(int(a[k]), int(b[k]), general[k].tolist(), theirs[k].tolist()) for k in bad[:3]]

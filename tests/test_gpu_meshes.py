@@ -100,8 +100,10 @@ def _order_free_steps(ref, steps, **kw):
 
 
 def test_world_steps_match_reference(ref):
-    steps = min(40, _order_free_steps(ref, 40))
-    assert steps >= 10
+    # The oracle's emulated backend keeps contacts that tie on (a, b, point)
+    # (a convex on an edge two triangles share, box children on box children)
+    # in emission order, as the device does, so no step is excluded here.
+    steps = 40
     w, bodies, soup = ms.load_pair(ref)
     w.configure(substeps=4, workers=1)
     ctx = ms.device_world(bodies, soup)
@@ -119,10 +121,13 @@ def test_world_steps_match_reference(ref):
 
 
 def test_world_steps_match_the_reference_cuda_backend(ref):
+    # The reference's own CUDA backend leaves the order of tied contacts to an
+    # unstable sort, so it is compared up to the first step whose result can
+    # depend on that order (the emulation with ties reversed departs there).
     if not ref.available("cuda"):
         pytest.skip("reference CUDA build missing (make -C oracle cuda)")
     steps = min(20, _order_free_steps(ref, 20))
-    assert steps >= 5
+    assert steps >= 2
     w, bodies, soup = ms.load_pair(ref, strict="cuda")
     assert w.L.ref_world_backend_name(w.h) == b"cuda"
     w.configure(substeps=4, workers=1)
@@ -139,7 +144,10 @@ def test_world_steps_match_the_reference_cuda_backend(ref):
 def test_reference_world_on_b200_backend_with_meshes(ref):
     if not ref.available("dropin"):
         pytest.skip("drop-in build missing")
+    # the reference World's own warm-start cache sort leaves tied contacts'
+    # order unspecified on this path: compared up to the first order-dependent step
     steps = min(10, _order_free_steps(ref, 10))
+    assert steps >= 2
     emu = ms.mesh_compound_world(ref)
     dev = ms.mesh_compound_world(ref, strict="dropin")
     assert dev.L.ref_world_backend_name(dev.h) == b"cuda"
@@ -245,3 +253,54 @@ def test_snapshot_image_restores_mesh_worlds_and_rejects_other_geometry(ref):
         c.snapshot_load(image)
     for x in (a, b, c):
         x.close()
+
+
+def _fast_sphere_world(ref, x0, target, family=None):
+    """A sphere at 55 m/s onto one body (a box spec re-shaped to `target`, or
+    a compound of family `family`): a collision the solver cannot stop in one
+    step, so the rewind decides the outcome."""
+    from velox_b200 import binding
+    specs = np.zeros(2 if family is not None else 3, binding.SPEC)
+    specs["orientation"] = ms.IDENTITY
+    specs["friction"] = 0.5
+    specs[0]["shape"] = 1
+    specs[0]["planeNormal"] = (0, 1, 0)
+    specs[0]["planeOffset"] = -3.0
+    s = specs[1]
+    s["shape"], s["mass"], s["radius"] = 0, 0.5, 0.15
+    s["position"], s["velocity"] = (x0, 1.2, 0.02), (0.0, -55.0, 0.0)
+    if family is None:
+        specs[2]["shape"], specs[2]["mass"], specs[2]["halfExtents"] = 2, 2.0, (0.2, 0.12, 0.15)
+    w = ref.RefWorld(specs, np.zeros((0, 3), np.float32))
+    if family is None:
+        b = w.bodies()
+        b["shape"][2], b["radius"][2], b["capsuleHalfHeight"][2] = target, 0.05, 0.15
+        w.set_bodies(b)
+    else:
+        rng = np.random.default_rng(1)
+        pool = []
+        kinds = ms.compound_kinds(rng, pool)
+        c = np.zeros(1, binding.SPEC)
+        c["mass"], c["friction"], c["orientation"] = 2.0, 0.6, ms.IDENTITY
+        w.add_compound(c, kinds[family], np.concatenate(pool))
+    return w
+
+
+@pytest.mark.parametrize("target,family", [(2, None), (8, None), (9, None), (10, None)] +
+                         [(6, f) for f in range(6)])
+def test_fast_sphere_rewinds_match_reference(ref, target, family):
+    # cones, rounded boxes and ellipsoids, alone and as compound children: the
+    # rewind must examine every pair the reference's distance query finds
+    # penetrating (its ellipsoid and rounded-box queries reach past the
+    # shapes' nominal extents)
+    for x0 in (-0.2, 0.05, 0.25):
+        w = _fast_sphere_world(ref, x0, target, family)
+        bodies = w.bodies()
+        w.configure(substeps=4, workers=1)
+        ctx = ms.device_world(bodies, w.vx_soup())
+        for step in range(3):
+            w.step(DT, 1)
+            ctx.step(1)
+            assert _rel(ctx.read_bodies(), w.bodies()) <= 1e-4, (x0, step)
+        ctx.close()
+        w.close()

@@ -116,18 +116,24 @@ VXD float maxPointSpeed(const BodyView& b) {
     return maxPointSpeedOf(shapeOf(b.flags), b.half, b.radius, b.hh, b.v, b.w);
 }
 
-// Bound on the distance from a body's position to any point of its shape
-// (the `ext` term of bodyAabb, narrowphase.h:371-390).
+// Bound on the distance from a body's position to any point of the surface
+// that gjkDistance measures for it (support point plus inflation radius).
+// This is the `ext` term of bodyAabb (narrowphase.h:371-390) except where the
+// distance query's shape reaches further: a rounded box's support already
+// adds its radius and the query inflates by it again (gjk.h:112-127, :208-213),
+// and an ellipsoid's support points have unit length (gjk.h:128-143 divides
+// by |(a^2 d.x, b^2 d.y, c^2 d.z)|). Compounds return a negative value: no
+// bound (their aggregate radius inherits the children's nominal extents).
 VXD float coreExtent(uint32_t shape, const V3& half, float radius, float hh) {
     switch (shape) {
     case kBox: return length(half);
-    case kRoundedBox: return length(half) + radius;
-    case kEllipsoid: return vmax(half.x, vmax(half.y, half.z));
+    case kRoundedBox: return length(half) + 2.0f * radius;
+    case kEllipsoid: return vmax(1.0f, vmax(half.x, vmax(half.y, half.z)));
     case kCapsule: return hh + radius;
-    case kSphere: case kHull: case kCompound: return radius;
+    case kSphere: case kHull: return radius;
     case kCylinder: return sqrtf(radius * radius + hh * hh);
     case kCone: return vmax(1.5f * hh, sqrtf(radius * radius + 0.25f * hh * hh));
-    default: return 0.0f;
+    default: return -1.0f;
     }
 }
 

@@ -2205,13 +2205,13 @@ __device__ __noinline__ GapProbe gapAt(const BodyView& a, const BodyView& b, con
 }
 
 // Bounding spheres more than 1 mm apart give a positive end gap, so the
-// rewind's `gap >= -8 mm` test skips the pair (planes and meshes have no
-// bounding sphere).
+// rewind's `gap >= -8 mm` test skips the pair (planes, meshes and compounds
+// have no bounding sphere here).
 VXD bool spheresApart(const BodyView& a, const BodyView& b) {
-    const uint32_t sb = shapeOf(b.flags);
-    if (sb == kPlane || sb == kMesh) return false;
-    const float reach = coreExtent(shapeOf(a.flags), a.half, a.radius, a.hh) +
-                        coreExtent(sb, b.half, b.radius, b.hh) + 1e-3f;
+    const float ea = coreExtent(shapeOf(a.flags), a.half, a.radius, a.hh);
+    const float eb = coreExtent(shapeOf(b.flags), b.half, b.radius, b.hh);
+    if (ea < 0.0f || eb < 0.0f) return false;
+    const float reach = ea + eb + 1e-3f;
     return lengthSq(a.p - b.p) > reach * reach;
 }
 
