@@ -217,6 +217,66 @@ typedef struct vx_soup {
     uint32_t compoundChildCount;
 } vx_soup;
 
+/* velox::JointType (include/velox/joint.h:46-60) */
+enum {
+    VX_JOINT_BALL = 0, VX_JOINT_DISTANCE = 1, VX_JOINT_HINGE = 2, VX_JOINT_CONE_TWIST = 3,
+    VX_JOINT_FIXED = 4, VX_JOINT_PRISMATIC = 5, VX_JOINT_SIX_DOF = 6, VX_JOINT_MOTOR = 7,
+    VX_JOINT_WELD = 8, VX_JOINT_WHEEL = 9, VX_JOINT_ROPE = 10, VX_JOINT_PULLEY = 11,
+    VX_JOINT_GEAR = 12
+};
+
+/* velox::Joint (include/velox/joint.h:92-188): a two-body constraint with
+ * its configuration and the solver's per-substep scratch (the impulses after
+ * gearRatio, reset every substep) and the broken flag. a, b are dense body
+ * indices. Byte-identical to the reference record (asserted by the
+ * reference-side adapter). */
+typedef struct vx_joint {
+    uint8_t type;
+    uint8_t pad0[3];
+    uint32_t a, b;
+    vx_vec3 localAnchorA, localAnchorB;
+    vx_vec3 localAxisA, localAxisB;
+    vx_vec3 localRefA, localRefB;
+    float restLength;
+    uint8_t collideConnected;
+    uint8_t enableSpring;
+    uint8_t pad1[2];
+    float springFrequencyHz, springDampingRatio;
+    float breakForce, breakTorque;
+    uint8_t enableMotor;
+    uint8_t pad2[3];
+    float motorSpeed, maxMotorTorque, maxMotorForce;
+    uint8_t enableLimit;
+    uint8_t pad3[3];
+    float lowerLimit, upperLimit;
+    uint8_t enableSwingLimit;
+    uint8_t pad4[3];
+    float swingLimit;
+    uint8_t enableTwistLimit;
+    uint8_t pad5[3];
+    float lowerTwistLimit, upperTwistLimit;
+    uint8_t linearLimitMask, angularLimitMask, linearMotorMask, angularMotorMask;
+    vx_vec3 lowerLinearLimit, upperLinearLimit;
+    vx_vec3 lowerAngularLimit, upperAngularLimit;
+    vx_vec3 linearMotorSpeed, angularMotorSpeed;
+    vx_vec3 maxLinearMotorForce, maxAngularMotorTorque;
+    float weldFrequencyHz, weldDampingRatio;
+    float suspensionFrequencyHz, suspensionDampingRatio, wheelRadius;
+    uint8_t enableSteering;
+    uint8_t pad6[3];
+    float steeringAngle, maxSteeringAngle;
+    float maxLength;
+    vx_vec3 pulleyAnchorA, pulleyAnchorB;
+    float pulleyRatio;
+    float gearRatio;
+    float motorImpulse, limitImpulse, swingImpulse, twistImpulse, springImpulse;
+    vx_vec3 linearMotorImpulse, angularMotorImpulse;
+    vx_vec3 linearLimitImpulse, angularLimitImpulse;
+    vx_vec3 reactionLinearImpulse, reactionAngularImpulse;
+    uint8_t broken;
+    uint8_t pad7[3];
+} vx_joint;
+
 /* One body of a synthetic scene, described at the level of the reference's
  * World::add* calls (include/velox/world.h:459-470: addSphere, addBox,
  * addCapsule, addCylinder, addConvexHull, addStaticPlane). Mass properties,
@@ -263,5 +323,7 @@ VX_STATIC_ASSERT(sizeof(vx_mesh) == 52, "vx_mesh must match velox::Mesh (52 B)")
 VX_STATIC_ASSERT(sizeof(vx_bvh_node) == 32, "vx_bvh_node must match velox::BvhNode (32 B)");
 VX_STATIC_ASSERT(sizeof(vx_compound_child) == 68, "vx_compound_child must match velox::CompoundChild (68 B)");
 VX_STATIC_ASSERT(offsetof(vx_compound_child, hullFaceCount) == 64, "vx_compound_child.hullFaceCount offset");
+VX_STATIC_ASSERT(offsetof(vx_joint, gearRatio) == 320, "vx_joint.gearRatio offset");
+VX_STATIC_ASSERT(sizeof(vx_joint) == 420, "vx_joint must match velox::Joint (420 B)");
 
 #endif /* VELOX_B200_TYPES_H */

@@ -17,7 +17,11 @@
 
 namespace vxb {
 
+// A host-side parity check of code written on this header may define VXD as
+// __host__ __device__ before including it.
+#ifndef VXD
 #define VXD __device__ __forceinline__
+#endif
 
 struct V3 { float x, y, z; };
 struct Q4 { float x, y, z, w; };
