@@ -172,6 +172,19 @@ int vxb_backend_advance_substeps(vxb_context* ctx, vx_body* bodies, uint32_t n,
                                  vx_contact* contacts, uint32_t m, vx_vec3 gravity, float h,
                                  int substeps, const vx_solver_options* options, int* advanced,
                                  uint32_t* iterations);
+/* Backend::advanceSubsteps with joints (src/backend_cuda.cu:691-760): with
+ * 64 or more joints, all of types up to VX_JOINT_GEAR, every substep runs
+ * the contact sweeps (the first warm-started), the joints' reset, 8 sweeps
+ * colour by colour and break test, and the position integration of every
+ * body; joints (their scratch impulses and broken flags) and bodies are
+ * written back. A joint whose endpoints differ in `asleep` wakes both first
+ * (also when the call declines). *advanced = 0 (the host path) for fewer
+ * joints, an unsupported type or the Adaptive iteration policy. */
+int vxb_backend_advance_substeps_joints(vxb_context* ctx, vx_body* bodies, uint32_t n,
+                                        vx_contact* contacts, uint32_t m, vx_joint* joints,
+                                        uint32_t njoints, vx_vec3 gravity, float h, int substeps,
+                                        const vx_solver_options* options, int* advanced,
+                                        uint32_t* iterations);
 /* Backend::fetchImpulses (backend.h:148; src/backend_cuda.cu:763-768). */
 int vxb_backend_fetch_impulses(vxb_context* ctx, vx_contact* contacts, uint32_t m);
 /* Backend::invalidateCaches (backend.h:150; src/backend_cuda.cu:770-784). */

@@ -76,6 +76,15 @@ int vxb_backend_advance_substeps(vxb_context* ctx, vx_body* bodies, uint32_t n, 
     return VXB_ERR_INVALID;
 }
 
+int vxb_backend_advance_substeps_joints(vxb_context* ctx, vx_body* bodies, uint32_t n, vx_contact* contacts,
+                                        uint32_t m, vx_joint* joints, uint32_t njoints, vx_vec3 gravity, float h,
+                                        int substeps, const vx_solver_options* options, int* advanced,
+                                        uint32_t* iterations) {
+    (void)ctx; (void)bodies; (void)n; (void)contacts; (void)m; (void)joints; (void)njoints; (void)gravity; (void)h;
+    (void)substeps; (void)options; (void)advanced; (void)iterations;
+    return VXB_ERR_INVALID;
+}
+
 int vxb_backend_fetch_impulses(vxb_context* ctx, vx_contact* contacts, uint32_t m) {
     (void)ctx; (void)contacts; (void)m;
     return VXB_ERR_INVALID;

@@ -83,6 +83,11 @@ def lib(strict=True):
         "ref_world_add_static_mesh": ([vp, vp, u32, vp, u32], i32),
         "ref_world_add_heightfield": ([vp, u32, u32, f32, vp, vp], i32),
         "ref_world_soup_part": ([vp, i32, vp, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64)], u32),
+        "ref_world_add_joint": ([vp, i32, u32, u32, vp, vp], i32),
+        "ref_world_joint_count": ([vp], u32),
+        "ref_world_joint_get": ([vp, u32, vp], None),
+        "ref_world_joint_set": ([vp, u32, vp], None),
+        "ref_world_joints": ([vp, vp, u32], u32),
         "ref_body_aabb": ([vp, f32, vp], None),
         "ref_collide_pairs": ([vp, vp, vp, u32, f32, vp, u32, vp], u32),
         "ref_gjk": ([vp, vp, vp, vp], None),
@@ -202,6 +207,38 @@ class RefWorld:
         h = np.ascontiguousarray(heights, np.float32)
         o = np.asarray(origin, np.float32)
         return self._added(self.L.ref_world_add_heightfield(self.h, h.shape[1], h.shape[0], cell_size, _p(h), _p(o)))
+
+    def add_joint(self, kind, a, b, p0=(0, 0, 0), p1=(0, 0, 0), axis0=(0, 1, 0), axis1=(0, 1, 0),
+                  ground0=(0, 0, 0), ground1=(0, 0, 0), x=(0.0, 0.0, 0.0)):
+        """A joint of `kind` (velox_b200.binding JOINT_* / VX_JOINT_*) between
+        dense bodies a and b through the World's typed adder; returns its
+        creation index. Which arguments a kind reads: ref_shim.cpp."""
+        v = np.array([*p0, *p1, *axis0, *axis1, *ground0, *ground1], np.float32)
+        xs = np.array(x, np.float32)
+        k = self.L.ref_world_add_joint(self.h, kind, a, b, _p(v), _p(xs))
+        if k < 0:
+            raise RuntimeError(self.L.ref_last_error().decode())
+        return k
+
+    def joint(self, k):
+        from velox_b200.binding import JOINT
+        out = np.zeros(1, JOINT)
+        self.L.ref_world_joint_get(self.h, k, _p(out))
+        return out
+
+    def set_joint(self, k, record):
+        from velox_b200.binding import JOINT, records
+        self.L.ref_world_joint_set(self.h, k, _p(records(np.atleast_1d(record), JOINT)))
+
+    def joints(self):
+        """World::joints_ in dense order (what the backend receives)."""
+        from velox_b200.binding import JOINT
+        n = self.L.ref_world_joints(self.h, None, 0)
+        if n == 0xffffffff:
+            raise RuntimeError("the reference's snapshot layout did not parse")
+        out = np.zeros(n, JOINT)
+        self.L.ref_world_joints(self.h, _p(out), n)
+        return out
 
     def mesh_soup(self):
         """The world's whole MeshSoup: dict of numpy arrays (record layouts of

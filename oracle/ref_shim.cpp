@@ -18,6 +18,7 @@
 #include "velox/sleep.h"
 #include "velox/serialization.h"
 #include "narrowphase.h"
+#include "joint_solver.h"
 #include "mass_properties.h"
 #include "velox_b200_types.h"
 
@@ -39,6 +40,8 @@ static_assert(sizeof(velox::Contact) == sizeof(vx_contact), "Contact layout");
 static_assert(offsetof(velox::Contact, spinningImpulse) == offsetof(vx_contact, spinningImpulse), "Contact tail");
 static_assert(sizeof(velox::SolverOptions) == sizeof(vx_solver_options), "SolverOptions layout");
 static_assert(sizeof(velox::Mesh) == sizeof(vx_mesh), "Mesh layout");
+static_assert(sizeof(velox::Joint) == sizeof(vx_joint), "Joint layout");
+static_assert(offsetof(velox::Joint, broken) == offsetof(vx_joint, broken), "Joint tail");
 static_assert(sizeof(velox::BvhNode) == sizeof(vx_bvh_node), "BvhNode layout");
 static_assert(sizeof(velox::CompoundChild) == sizeof(vx_compound_child), "CompoundChild layout");
 static_assert(offsetof(velox::CompoundChild, localOrientation) == offsetof(vx_compound_child, localOrientation),
@@ -223,22 +226,95 @@ public:
         runSweeps(bodies, dt, options);
     }
 
+    // The joint path (backend_cuda.cu:691-760, prepareJoints :800-880): 64 or
+    // more supported joints are coloured greedily over their dynamic
+    // endpoints and, every substep after the contact sweeps, reset (broken
+    // ones kept from the second substep on), swept kIterations times colour
+    // by colour and break-tested. Solving a colour's joints one after another
+    // equals the device's parallel pass: they share no dynamic body.
     bool advanceSubsteps(std::vector<Body>& bodies, std::vector<Contact>& contacts,
                          std::vector<Joint>& joints, const Vec3& gravity, float dt,
                          int substeps, const SolverOptions& options) override {
-        if (!joints.empty()) return false;
+        if (!joints.empty() && joints.size() < 64) return false;
+        for (const Joint& joint : joints)
+            if (!joint_solver::supported(joint)) return false;
+        for (const Joint& joint : joints) {
+            if (bodies[joint.a].asleep == bodies[joint.b].asleep) continue;
+            bodies[joint.a].asleep = bodies[joint.b].asleep = 0;
+            bodies[joint.a].sleepTimer = bodies[joint.b].sleepTimer = 0.0f;
+        }
         if (options.iterationPolicy == IterationPolicy::Adaptive) return false;
         const bool hasContacts = !contacts.empty();
         solveVelocities(bodies, contacts, dt, true, options);
+        std::vector<int> colorStart, order;
+        std::vector<Joint> sorted;
+        if (!joints.empty()) colorJoints(bodies, joints, colorStart, order, sorted);
         for (int s = 0; s < substeps; ++s) {
             if (s > 0) {
                 integrateVelocities(bodies, gravity, dt);
                 if (hasContacts) runSweeps(bodies, dt, options);
             }
+            if (!sorted.empty()) {
+                for (Joint& joint : sorted)
+                    if (!(s > 0 && joint.broken)) joint_solver::reset(joint);
+                for (int it = 0; it < joint_solver::kIterations; ++it)
+                    for (size_t c = 0; c + 1 < colorStart.size(); ++c)
+                        for (int k = colorStart[c]; k < colorStart[c + 1]; ++k) {
+                            Joint& joint = sorted[k];
+                            if (joint.broken) continue;
+                            joint_solver::solve(joint, bodies[joint.a], bodies[joint.b], dt);
+                        }
+                for (Joint& joint : sorted) {
+                    if (joint.broken) continue;
+                    float force = length(joint.reactionLinearImpulse) / dt;
+                    float torque = length(joint.reactionAngularImpulse) / dt;
+                    joint.broken = force > joint.breakForce || torque > joint.breakTorque;
+                }
+            }
             integrateTransforms(bodies, dt);
         }
+        for (size_t k = 0; k < sorted.size(); ++k) joints[order[k]] = sorted[k];
         lastIterations_ *= (uint32_t)substeps;
         return true;
+    }
+
+    static void colorJoints(const std::vector<Body>& bodies, const std::vector<Joint>& joints,
+                            std::vector<int>& colorStart, std::vector<int>& order, std::vector<Joint>& sorted) {
+        const size_t count = joints.size();
+        std::vector<uint64_t> mask(bodies.size(), 0);
+        std::vector<int> next(bodies.size(), 64), colorOf(count);
+        int colors = 0;
+        for (size_t k = 0; k < count; ++k) {
+            const Joint& joint = joints[k];
+            const bool staticA = !bodies[joint.a].isDynamic(), staticB = !bodies[joint.b].isDynamic();
+            const uint64_t used = (staticA ? 0 : mask[joint.a]) | (staticB ? 0 : mask[joint.b]);
+            int color;
+            if (~used) {
+                color = 0;
+                while (used & (1ull << color)) ++color;
+            } else {
+                color = std::max(staticA ? 64 : next[joint.a], staticB ? 64 : next[joint.b]);
+                if (!staticA) next[joint.a] = color + 1;
+                if (!staticB) next[joint.b] = color + 1;
+            }
+            if (color < 64) {
+                if (!staticA) mask[joint.a] |= 1ull << color;
+                if (!staticB) mask[joint.b] |= 1ull << color;
+            }
+            colorOf[k] = color;
+            colors = std::max(colors, color + 1);
+        }
+        colorStart.assign(colors + 1, 0);
+        for (int color : colorOf) ++colorStart[color + 1];
+        for (int c = 0; c < colors; ++c) colorStart[c + 1] += colorStart[c];
+        std::vector<int> fill(colorStart.begin(), colorStart.end() - 1);
+        order.assign(count, 0);
+        sorted.resize(count);
+        for (size_t k = 0; k < count; ++k) {
+            const int at = fill[colorOf[k]]++;
+            order[at] = (int)k;
+            sorted[at] = joints[k];
+        }
     }
 
     void fetchImpulses(std::vector<Contact>& contacts) override {
@@ -293,6 +369,7 @@ struct RefWorld {
     std::unique_ptr<World> world;
     ColoredCpuBackend* emulated = nullptr;
     std::vector<BodyId> ids;
+    std::vector<JointId> jointIds;
     std::vector<Vec3> soupPoints;
     std::vector<uint32_t> soupFaces;
     double lastStepMs = 0.0;
@@ -567,6 +644,89 @@ uint32_t ref_world_soup_part(void* handle, int part, void* out, uint64_t capByte
         at += elem * n;
     }
     return ~0u;
+}
+
+// A joint between dense bodies a and b through the World's typed adder for
+// `type` (include/velox/world.h:617-670). v: six points / axes (p0, p1, axis0,
+// axis1, ground0, ground1), x: three scalars; which ones a type reads:
+//   Ball, Fixed, SixDof: p0            Distance: p0, p1 (x0 > 0: a spring of
+//   x0 Hz and damping x1)              Hinge, ConeTwist, Prismatic, Wheel: p0, axis0
+//   Motor: p0, p1, x0 force, x1 torque Weld: p0, x0 / x1 break force / torque
+//   Rope: p0, p1, x0 length            Pulley: p0, p1, ground0, ground1, x0 ratio
+//   Gear: axis0, axis1, x0 ratio
+// Returns the joint's index (creation order) or -1 (ref_last_error).
+int ref_world_add_joint(void* handle, int type, uint32_t a, uint32_t b, const float* v, const float* x) {
+    auto* w = static_cast<RefWorld*>(handle);
+    try {
+        World& W = *w->world;
+        const BodyId A = w->ids.at(a), B = w->ids.at(b);
+        const Vec3 p0{v[0], v[1], v[2]}, p1{v[3], v[4], v[5]}, ax0{v[6], v[7], v[8]}, ax1{v[9], v[10], v[11]};
+        const Vec3 g0{v[12], v[13], v[14]}, g1{v[15], v[16], v[17]};
+        JointId id;
+        switch ((JointType)type) {
+        case JointType::Ball: id = W.addBallJoint(A, B, p0); break;
+        case JointType::Distance:
+            id = x[0] > 0.0f ? W.addSpringJoint(A, B, p0, p1, x[0], x[1]) : W.addDistanceJoint(A, B, p0, p1);
+            break;
+        case JointType::Hinge: id = W.addHingeJoint(A, B, p0, ax0); break;
+        case JointType::ConeTwist: id = W.addConeTwistJoint(A, B, p0, ax0); break;
+        case JointType::Fixed: id = W.addFixedJoint(A, B, p0); break;
+        case JointType::Prismatic: id = W.addPrismaticJoint(A, B, p0, ax0); break;
+        case JointType::SixDof: id = W.addSixDofJoint(A, B, p0); break;
+        case JointType::Motor: id = W.addMotorJoint(A, B, p0, p1, x[0], x[1]); break;
+        case JointType::Weld: id = W.addWeldJoint(A, B, p0, x[0], x[1]); break;
+        case JointType::Wheel: id = W.addWheelJoint(A, B, p0, ax0); break;
+        case JointType::Rope: id = W.addRopeJoint(A, B, p0, p1, x[0]); break;
+        case JointType::Pulley: id = W.addPulleyJoint(A, B, p0, p1, g0, g1, x[0]); break;
+        case JointType::Gear: id = W.addGearJoint(A, B, ax0, ax1, x[0]); break;
+        default: g_error = "unknown joint type"; return -1;
+        }
+        w->jointIds.push_back(id);
+        return (int)w->jointIds.size() - 1;
+    } catch (const std::exception& e) {
+        g_error = e.what();
+        return -1;
+    }
+}
+
+// The world's joints in dense order (World::joints_, the sixth state vector
+// of its snapshot after prevContacts_), as the backend receives them; broken
+// joints are removed by the World after a step. Returns the count (~0u on a
+// layout error).
+uint32_t ref_world_joints(void* handle, vx_joint* out, uint32_t cap) {
+    auto* w = static_cast<RefWorld*>(handle);
+    SerializedScene scene = serializeWorld(*w->world);
+    const std::vector<uint8_t>& bytes = scene.data;
+    size_t at = sizeof(Vec3) + sizeof(int) + sizeof(WorldCcdDefaults) + sizeof(WorldMultiToiSettings) +
+                sizeof(SolverOptions);
+    for (int v = 0; v <= 6; ++v) {
+        uint64_t elem = 0, n = 0;
+        if (at + 16 > bytes.size()) return ~0u;
+        std::memcpy(&elem, bytes.data() + at, 8);
+        std::memcpy(&n, bytes.data() + at + 8, 8);
+        at += 16;
+        if (at + elem * n > bytes.size()) return ~0u;
+        if (v == 6) {
+            if (elem != sizeof(Joint)) return ~0u;
+            if (out) std::memcpy(out, bytes.data() + at, std::min<uint64_t>(n, cap) * sizeof(Joint));
+            return (uint32_t)n;
+        }
+        at += elem * n;
+    }
+    return ~0u;
+}
+
+// Reads / overwrites joint k (creation order) as the vx_joint record.
+uint32_t ref_world_joint_count(void* handle) { return (uint32_t)static_cast<RefWorld*>(handle)->jointIds.size(); }
+void ref_world_joint_get(void* handle, uint32_t k, vx_joint* out) {
+    auto* w = static_cast<RefWorld*>(handle);
+    const Joint& j = w->world->joint(w->jointIds.at(k));
+    std::memcpy(out, &j, sizeof(Joint));
+}
+void ref_world_joint_set(void* handle, uint32_t k, const vx_joint* in) {
+    auto* w = static_cast<RefWorld*>(handle);
+    Joint& j = w->world->joint(w->jointIds.at(k));
+    std::memcpy(&j, in, sizeof(Joint));
 }
 
 uint32_t ref_world_body_count(void* handle) {

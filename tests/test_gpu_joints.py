@@ -1,0 +1,96 @@
+"""Joints on the device: the reference World (src/world.cpp:4196-4207) stepping
+on this library through its Backend interface, whose advanceSubsteps takes
+64 or more joints to the device joint pass (velox_b200/csrc/joints.cu; the
+reference CUDA backend's algorithm, src/backend_cuda.cu:691-760), against
+the same World on the oracle's CPU emulation of that backend, and against
+the reference's own CUDA backend on this GPU. The joint rows themselves are
+pinned bit for bit on the CPU (tests/test_joint_rows.py)."""
+import numpy as np
+import pytest
+
+import joint_scenes as js
+
+pytestmark = pytest.mark.gpu
+DT = 1.0 / 60.0
+
+
+def _state(b):
+    return np.concatenate([b["position"], b["orientation"], b["velocity"], b["angularVelocity"]], 1)
+
+
+def _rel(mine, theirs):
+    return float((np.abs(_state(mine) - _state(theirs)) / np.maximum(1.0, np.abs(_state(theirs)))).max())
+
+
+def _need(ref, build):
+    if not ref.available(build):
+        pytest.skip(f"{build} build missing")
+
+
+def test_jointed_world_on_b200_backend_matches_the_emulated_reference(ref):
+    _need(ref, "dropin")
+    emu = js.jointed_world(ref)
+    dev = js.jointed_world(ref, strict="dropin")
+    assert dev.L.ref_world_backend_name(dev.h) == b"cuda" and len(dev.joints()) == 80
+    for w in (emu, dev):
+        w.configure(substeps=4, workers=1)
+    contacts = 0
+    for step in range(30):
+        emu.step(DT, 1)
+        dev.step(DT, 1)
+        assert dev.stats()["deviceSubsteps"] == 1 and emu.stats()["deviceSubsteps"] == 1
+        assert _rel(dev.bodies(), emu.bodies()) <= 1e-4, step
+        contacts = max(contacts, dev.stats()["generated"])
+        je, jd = emu.joints(), dev.joints()
+        for f in ("reactionLinearImpulse", "reactionAngularImpulse", "motorImpulse", "limitImpulse"):
+            assert np.allclose(jd[f], je[f], rtol=1e-3, atol=1e-4), (step, f)
+    assert contacts > 0  # contacts and joints share bodies
+    emu.close()
+    dev.close()
+
+
+def test_jointed_world_matches_the_reference_cuda_backend(ref):
+    _need(ref, "dropin")
+    _need(ref, "cuda")
+    theirs = js.jointed_world(ref, strict="cuda")
+    mine = js.jointed_world(ref, strict="dropin")
+    for w in (theirs, mine):
+        w.configure(substeps=4, workers=1)
+    for step in range(20):
+        theirs.step(DT, 1)
+        mine.step(DT, 1)
+        assert theirs.stats()["deviceSubsteps"] == 1 and mine.stats()["deviceSubsteps"] == 1
+        assert _rel(mine.bodies(), theirs.bodies()) <= 1e-4, step
+    theirs.close()
+    mine.close()
+
+
+def test_breaking_joints_match_the_emulated_reference(ref):
+    _need(ref, "dropin")
+    emu = js.jointed_world(ref, break_force=60.0)
+    dev = js.jointed_world(ref, strict="dropin", break_force=60.0)
+    for w in (emu, dev):
+        w.configure(substeps=4, workers=1)
+    for step in range(20):
+        emu.step(DT, 1)
+        dev.step(DT, 1)
+        assert len(dev.joints()) == len(emu.joints()), step
+        assert _rel(dev.bodies(), emu.bodies()) <= 1e-4, step
+    assert len(emu.joints()) < 80  # some joints broke and the World removed them
+    emu.close()
+    dev.close()
+
+
+def test_fewer_than_64_joints_stay_on_the_host_path(ref):
+    _need(ref, "dropin")
+    emu = js.jointed_world(ref, chains=4)
+    dev = js.jointed_world(ref, chains=4, strict="dropin")
+    for w in (emu, dev):
+        w.configure(substeps=4, workers=1)
+    for step in range(10):
+        emu.step(DT, 1)
+        dev.step(DT, 1)
+        assert dev.stats()["deviceSubsteps"] == 0
+        assert _rel(dev.bodies(), emu.bodies()) <= 1e-4, step
+    emu.close()
+    dev.close()

@@ -16,29 +16,7 @@ from velox_b200 import binding
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 LIB = os.path.join(ROOT, "oracle", "_ref", "libjoint_check.so")
 
-JOINT = np.dtype({
-    "names": ["type", "a", "b", "localAnchorA", "localAnchorB", "localAxisA", "localAxisB", "localRefA",
-              "localRefB", "restLength", "collideConnected", "enableSpring", "springFrequencyHz",
-              "springDampingRatio", "breakForce", "breakTorque", "enableMotor", "motorSpeed", "maxMotorTorque",
-              "maxMotorForce", "enableLimit", "lowerLimit", "upperLimit", "enableSwingLimit", "swingLimit",
-              "enableTwistLimit", "lowerTwistLimit", "upperTwistLimit", "linearLimitMask", "angularLimitMask",
-              "linearMotorMask", "angularMotorMask", "lowerLinearLimit", "upperLinearLimit", "lowerAngularLimit",
-              "upperAngularLimit", "linearMotorSpeed", "angularMotorSpeed", "maxLinearMotorForce",
-              "maxAngularMotorTorque", "weldFrequencyHz", "weldDampingRatio", "suspensionFrequencyHz",
-              "suspensionDampingRatio", "wheelRadius", "enableSteering", "steeringAngle", "maxSteeringAngle",
-              "maxLength", "pulleyAnchorA", "pulleyAnchorB", "pulleyRatio", "gearRatio", "motorImpulse",
-              "limitImpulse", "swingImpulse", "twistImpulse", "springImpulse", "linearMotorImpulse",
-              "angularMotorImpulse", "linearLimitImpulse", "angularLimitImpulse", "reactionLinearImpulse",
-              "reactionAngularImpulse", "broken"],
-    "formats": ["u1", "<u4", "<u4"] + [("<f4", 3)] * 6 + ["<f4", "u1", "u1", "<f4", "<f4", "<f4", "<f4", "u1",
-                "<f4", "<f4", "<f4", "u1", "<f4", "<f4", "u1", "<f4", "u1", "<f4", "<f4", "u1", "u1", "u1", "u1"]
-               + [("<f4", 3)] * 8 + ["<f4"] * 5 + ["u1", "<f4", "<f4", "<f4", ("<f4", 3), ("<f4", 3), "<f4", "<f4",
-                "<f4", "<f4", "<f4", "<f4", "<f4"] + [("<f4", 3)] * 6 + ["u1"],
-    "offsets": [0, 4, 8, 12, 24, 36, 48, 60, 72, 84, 88, 89, 92, 96, 100, 104, 108, 112, 116, 120, 124, 128, 132,
-                136, 140, 144, 148, 152, 156, 157, 158, 159, 160, 172, 184, 196, 208, 220, 232, 244, 256, 260, 264,
-                268, 272, 276, 280, 284, 288, 292, 304, 316, 320, 324, 328, 332, 336, 340, 344, 356, 368, 380, 392,
-                404, 416],
-    "itemsize": 420})
+JOINT = binding.JOINT
 
 
 @pytest.fixture(scope="module")

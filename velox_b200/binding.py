@@ -150,6 +150,31 @@ COMPOUND_CHILD = np.dtype({"names": ["shape", "localPosition", "localOrientation
                            "offsets": [0, 4, 16, 32, 36, 48, 52, 56, 60, 64], "itemsize": 68})
 assert MESH.itemsize == 52 and BVH_NODE.itemsize == 32
 
+# velox::Joint (vx_joint in include/velox_b200_types.h, 420 bytes).
+JOINT = np.dtype({
+    "names": ["type", "a", "b", "localAnchorA", "localAnchorB", "localAxisA", "localAxisB", "localRefA",
+              "localRefB", "restLength", "collideConnected", "enableSpring", "springFrequencyHz",
+              "springDampingRatio", "breakForce", "breakTorque", "enableMotor", "motorSpeed", "maxMotorTorque",
+              "maxMotorForce", "enableLimit", "lowerLimit", "upperLimit", "enableSwingLimit", "swingLimit",
+              "enableTwistLimit", "lowerTwistLimit", "upperTwistLimit", "linearLimitMask", "angularLimitMask",
+              "linearMotorMask", "angularMotorMask", "lowerLinearLimit", "upperLinearLimit", "lowerAngularLimit",
+              "upperAngularLimit", "linearMotorSpeed", "angularMotorSpeed", "maxLinearMotorForce",
+              "maxAngularMotorTorque", "weldFrequencyHz", "weldDampingRatio", "suspensionFrequencyHz",
+              "suspensionDampingRatio", "wheelRadius", "enableSteering", "steeringAngle", "maxSteeringAngle",
+              "maxLength", "pulleyAnchorA", "pulleyAnchorB", "pulleyRatio", "gearRatio", "motorImpulse",
+              "limitImpulse", "swingImpulse", "twistImpulse", "springImpulse", "linearMotorImpulse",
+              "angularMotorImpulse", "linearLimitImpulse", "angularLimitImpulse", "reactionLinearImpulse",
+              "reactionAngularImpulse", "broken"],
+    "formats": ["u1", "<u4", "<u4"] + [("<f4", 3)] * 6 + ["<f4", "u1", "u1", "<f4", "<f4", "<f4", "<f4", "u1",
+                "<f4", "<f4", "<f4", "u1", "<f4", "<f4", "u1", "<f4", "u1", "<f4", "<f4", "u1", "u1", "u1", "u1"]
+               + [("<f4", 3)] * 8 + ["<f4"] * 5 + ["u1", "<f4", "<f4", "<f4", ("<f4", 3), ("<f4", 3), "<f4", "<f4",
+                "<f4", "<f4", "<f4", "<f4", "<f4"] + [("<f4", 3)] * 6 + ["u1"],
+    "offsets": [0, 4, 8, 12, 24, 36, 48, 60, 72, 84, 88, 89, 92, 96, 100, 104, 108, 112, 116, 120, 124, 128, 132,
+                136, 140, 144, 148, 152, 156, 157, 158, 159, 160, 172, 184, 196, 208, 220, 232, 244, 256, 260, 264,
+                268, 272, 276, 280, 284, 288, 292, 304, 316, 320, 324, 328, 332, 336, 340, 344, 356, 368, 380, 392,
+                404, 416],
+    "itemsize": 420})
+
 
 class StepConfig(ctypes.Structure):
     _fields_ = [("dt", ctypes.c_float), ("gravity", Vec3), ("substeps", ctypes.c_int32),

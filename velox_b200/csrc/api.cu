@@ -122,7 +122,7 @@ void vxb_context_destroy(vxb_context* ctx) {
         if (snap.buf.ptr) cudaFree(snap.buf.ptr);
     vxb::DevBuf* bufs[] = {&c.bodyBuf, &c.aosBuf, &c.worldOfBuf, &c.planeStartBuf, &c.planeListBuf, &c.prevPoseBuf,
                            &c.snapBuf, &c.hullPtsBuf, &c.facesBuf, &c.vertBuf, &c.indexBuf, &c.meshBuf, &c.nodeBuf,
-                           &c.triRefBuf, &c.childBuf, &c.aabbBuf, &c.cellKeyBuf, &c.cellValBuf,
+                           &c.triRefBuf, &c.childBuf, &c.jointBuf, &c.aabbBuf, &c.cellKeyBuf, &c.cellValBuf,
                            &c.sortKeysAlt, &c.sortValsAlt, &c.sortHist, &c.hashKeyBuf, &c.hashValBuf, &c.pairBuf,
                            &c.contactTmpBuf, &c.recKeyBuf, &c.recValBuf, &c.recInfoBuf, &c.recCountBuf,
                            &c.contactBuf[0], &c.contactBuf[1], &c.prevKeyBuf, &c.pairKeyBuf, &c.recOffsetBuf,
@@ -265,6 +265,24 @@ int vxb_backend_advance_substeps(vxb_context* ctx, vx_body* bodies, uint32_t n, 
     *advanced = 1;
     if (iterations) *iterations = m ? (uint32_t)(2 * options->velocityIterations * substeps) : 0u;
     return VXB_OK;
+}
+
+int vxb_backend_advance_substeps_joints(vxb_context* ctx, vx_body* bodies, uint32_t n, vx_contact* contacts,
+                                        uint32_t m, vx_joint* joints, uint32_t njoints, vx_vec3 gravity, float h,
+                                        int substeps, const vx_solver_options* options, int* advanced,
+                                        uint32_t* iterations) {
+    GUARD(ctx);
+    if (!advanced || !options) return VXB_ERR_INVALID;
+    *advanced = 0;
+    if (iterations) *iterations = 0;
+    if (njoints == 0)
+        return vxb_backend_advance_substeps(ctx, bodies, n, contacts, m, gravity, h, substeps, options, advanced,
+                                            iterations);
+    if (!bodies || !joints || n == 0 || (m && !contacts) || substeps <= 0) return VXB_ERR_INVALID;
+    Context& c = ctx->impl;
+    TRY(ensureCounters(c));
+    return vxb::backendAdvanceJoints(c, bodies, n, contacts, m, joints, njoints, gravity, h, substeps, *options,
+                                     advanced, iterations);
 }
 
 int vxb_backend_fetch_impulses(vxb_context* ctx, vx_contact* contacts, uint32_t m) {

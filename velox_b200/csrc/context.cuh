@@ -169,6 +169,7 @@ struct Context {
     size_t hullPointCount = 0, faceIndexCount = 0;
     // triangle meshes and compound children of the soup (static geometry)
     DevBuf vertBuf, indexBuf, meshBuf, nodeBuf, triRefBuf, childBuf;
+    DevBuf jointBuf;  // joints of the Backend path, in colour order
     std::vector<vx_mesh> hostMeshes;   // root bounds for the broad phase
     bool complexShapes = false;        // any mesh or compound body loaded
     // FNV-1a keys of the loaded bodies' shape references and of the soup's
@@ -280,6 +281,11 @@ int stageCollide(Context& c, const uint64_t* pairs, uint32_t npairs, float dt, v
 int stageColor(Context& c, const vx_contact* contacts, uint32_t m, int32_t* colorOf, uint32_t* numColors);
 int stageDistance(Context& c, const uint64_t* pairs, uint32_t npairs, int path, float* out);
 int backendIntegrate(Context& c, vx_vec3 gravity, float dt);
+int backendIntegrateTransforms(Context& c, float dt);
+// The reference CUDA backend's joint path of advanceSubsteps (joints.cu).
+int backendAdvanceJoints(Context& c, vx_body* bodies, uint32_t n, vx_contact* contacts, uint32_t m,
+                         vx_joint* joints, uint32_t njoints, vx_vec3 gravity, float h, int substeps,
+                         const vx_solver_options& o, int* advanced, uint32_t* iterations);
 int backendFindContacts(Context& c, float dt, uint32_t* count);
 int backendCopyContacts(Context& c, vx_contact* out, uint32_t cap);
 int backendSolve(Context& c, vx_contact* contacts, uint32_t m, float h, bool warmStart,

@@ -325,6 +325,11 @@ __global__ void integrateKernel(BodyArrays B, uint32_t n, V3 g, float h) {
         integrateVelocity(B, i, g, h);
 }
 
+__global__ void transformsKernel(BodyArrays B, uint32_t n, float h) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        integrateTransform(B, i, h);
+}
+
 // ---------------------------------------------------------------------------
 // broad phase
 // ---------------------------------------------------------------------------
@@ -3733,6 +3738,11 @@ int stageDistance(Context& c, const uint64_t* pairs, uint32_t npairs, int path, 
 
 int backendIntegrate(Context& c, vx_vec3 gravity, float dt) {
     LAUNCH(c, integrateKernel, blocksFor(c.n, 256), 256, c.B, c.n, V3{gravity.x, gravity.y, gravity.z}, dt);
+    return VXB_OK;
+}
+
+int backendIntegrateTransforms(Context& c, float dt) {
+    LAUNCH(c, transformsKernel, blocksFor(c.n, 256), 256, c.B, c.n, dt);
     return VXB_OK;
 }
 

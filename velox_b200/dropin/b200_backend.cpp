@@ -24,6 +24,9 @@ static_assert(sizeof(velox::Body) == sizeof(vx_body), "velox::Body and vx_body m
 static_assert(sizeof(velox::Contact) == sizeof(vx_contact), "velox::Contact and vx_contact must share one layout");
 static_assert(sizeof(velox::SolverOptions) == sizeof(vx_solver_options), "SolverOptions layout");
 static_assert(sizeof(velox::Mesh) == sizeof(vx_mesh), "Mesh layout");
+static_assert(sizeof(velox::Joint) == sizeof(vx_joint), "Joint layout");
+static_assert(offsetof(velox::Joint, gearRatio) == offsetof(vx_joint, gearRatio), "Joint.gearRatio");
+static_assert(offsetof(velox::Joint, broken) == offsetof(vx_joint, broken), "Joint tail");
 static_assert(sizeof(velox::BvhNode) == sizeof(vx_bvh_node), "BvhNode layout");
 static_assert(sizeof(velox::CompoundChild) == sizeof(vx_compound_child), "CompoundChild layout");
 static_assert(offsetof(velox::CompoundChild, hullFaceCount) == offsetof(vx_compound_child, hullFaceCount),
@@ -81,13 +84,13 @@ public:
 
     bool advanceSubsteps(std::vector<Body>& bodies, std::vector<Contact>& contacts, std::vector<Joint>& joints,
                          const Vec3& gravity, float h, int substeps, const SolverOptions& options) override {
-        if (!joints.empty()) return false;  // joint rows stay on the host path
         vx_solver_options o;
         std::memcpy(&o, &options, sizeof(o));
         int advanced = 0;
-        check(vxb_backend_advance_substeps(ctx_, asBodies(bodies), (uint32_t)bodies.size(), asContacts(contacts),
-                                           (uint32_t)contacts.size(), vec(gravity), h, substeps, &o, &advanced,
-                                           &lastIterations_));
+        check(vxb_backend_advance_substeps_joints(
+            ctx_, asBodies(bodies), (uint32_t)bodies.size(), asContacts(contacts), (uint32_t)contacts.size(),
+            reinterpret_cast<vx_joint*>(joints.data()), (uint32_t)joints.size(), vec(gravity), h, substeps, &o,
+            &advanced, &lastIterations_));
         return advanced != 0;
     }
 
