@@ -315,6 +315,8 @@ int vxb_world_load(vxb_context* ctx, const vx_body* bodies, uint32_t n, const vx
     }
     TRY(ensureCounters(c));
     vxb::tapeEnd(c);  // a tape belongs to the world it recorded
+    c.backendContacts = 0;  // a new world: no coloured Backend contacts
+    c.backendColored = false;
     TRY(vxb::loadBodies(c, bodies, n, worldOfBody));
     TRY(vxb::loadSoup(c, soup));
     cudaError_t e = cudaStreamSynchronize(c.stream);

@@ -2724,6 +2724,13 @@ static Soup soupOf(Context& c) {
 
 int loadBodies(Context& c, const vx_body* bodies, uint32_t n, const uint32_t* worldOf) {
     if (n == 0) return fail(c, VXB_ERR_INVALID, "no bodies");
+    // The Backend path reloads the same bodies between its calls of one step
+    // (integrate between substeps' solves): the coloured contacts stay valid
+    // unless the body set changed.
+    if (n != c.n) {
+        c.backendContacts = 0;
+        c.backendColored = false;
+    }
     c.complexShapes = false;
     uint64_t key = 0xcbf29ce484222325ull;
     for (uint32_t i = 0; i < n; ++i) {
@@ -2809,7 +2816,6 @@ int loadBodies(Context& c, const vx_body* bodies, uint32_t n, const uint32_t* wo
     VXB_TRY(ensure(c, c.sortValsAlt, std::max<size_t>(mcap, (size_t)c.pairCap) * 4 + 64));
     c.prevCount = 0;
     c.stepContacts = 0;
-    c.backendContacts = 0;
     VXB_TRY(sleepLoad(c, bodies, n));
     return VXB_OK;
 }
