@@ -97,3 +97,49 @@ def test_fewer_than_64_joints_stay_on_the_host_path(ref):
         assert _rel(dev.bodies(), emu.bodies()) <= 1e-4, step
     emu.close()
     dev.close()
+
+
+def _kinematic_world(ref, strict):
+    """Spheres on a plane swept by a kinematic box paddle (moving and
+    spinning at a set velocity) and resting on a kinematic platform."""
+    from velox_b200 import binding
+    specs = np.zeros(2 + 2 + 40, binding.SPEC)
+    specs["orientation"] = (0, 0, 0, 1)
+    specs["friction"] = 0.5
+    specs[0]["shape"], specs[0]["planeNormal"] = 1, (0, 1, 0)
+    specs[1]["shape"], specs[1]["mass"], specs[1]["halfExtents"] = 2, 1.0, (0.2, 0.4, 1.5)
+    specs[1]["position"] = (-2.0, 0.45, 0.0)
+    specs[2]["shape"], specs[2]["mass"], specs[2]["halfExtents"] = 2, 1.0, (1.0, 0.1, 1.0)
+    specs[2]["position"] = (3.0, 1.0, 0.0)
+    specs[3]["shape"], specs[3]["mass"], specs[3]["radius"] = 0, 1.0, 0.2
+    specs[3]["position"] = (3.0, 1.35, 0.0)
+    rng = np.random.default_rng(3)
+    for k in range(4, len(specs)):
+        specs[k]["shape"], specs[k]["mass"], specs[k]["radius"] = 0, 0.5, 0.18
+        specs[k]["position"] = (rng.uniform(-1.0, 2.0), 0.2 + 0.4 * (k % 3), rng.uniform(-1.2, 1.2))
+    w = ref.RefWorld(specs, np.zeros((0, 3), np.float32), strict=strict)
+    b = w.bodies()
+    for k, v, om in ((1, (2.0, 0.0, 0.0), (0.0, 1.0, 0.0)), (2, (0.0, 0.5, 0.0), (0.0, 0.0, 0.0))):
+        b["motionType"][k] = 1  # Kinematic
+        b["invMass"][k] = 0.0
+        b["invInertia"][k] = (0.0, 0.0, 0.0)
+        b["velocity"][k], b["angularVelocity"][k] = v, om
+    w.set_bodies(b)
+    return w
+
+
+def test_kinematic_bodies_on_the_b200_backend_match_the_emulated_reference(ref):
+    _need(ref, "dropin")
+    emu, dev = _kinematic_world(ref, True), _kinematic_world(ref, "dropin")
+    for w in (emu, dev):
+        w.configure(substeps=4, workers=1)
+    for step in range(30):
+        emu.step(DT, 1)
+        dev.step(DT, 1)
+        assert dev.stats()["deviceSubsteps"] == 1
+        assert _rel(dev.bodies(), emu.bodies()) <= 1e-4, step
+    b = dev.bodies()
+    assert abs(b["position"][1][0] - (-2.0 + 2.0 * 30 * DT)) < 1e-3  # the paddle moved at its set speed
+    assert dev.stats()["generated"] > 0
+    emu.close()
+    dev.close()

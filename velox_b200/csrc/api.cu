@@ -260,6 +260,13 @@ int vxb_backend_advance_substeps(vxb_context* ctx, vx_body* bodies, uint32_t n, 
     Context& c = ctx->impl;
     TRY(ensureCounters(c));
     TRY(vxb::loadBodies(c, bodies, n, nullptr));
+    if (c.kinematic) {
+        // kinematic bodies move every substep: the substep-wise order keeps
+        // their poses current for the contact rows of every island
+        TRY(vxb::backendStepwise(c, bodies, n, contacts, m, nullptr, 0, gravity, h, substeps, *options, iterations));
+        *advanced = 1;
+        return VXB_OK;
+    }
     TRY(vxb::backendSolve(c, contacts, m, h, true, *options, gravity, substeps, true));
     TRY(vxb::readBodies(c, bodies, n));
     *advanced = 1;
@@ -317,7 +324,7 @@ int vxb_world_load(vxb_context* ctx, const vx_body* bodies, uint32_t n, const vx
     vxb::tapeEnd(c);  // a tape belongs to the world it recorded
     c.backendContacts = 0;  // a new world: no coloured Backend contacts
     c.backendColored = false;
-    TRY(vxb::loadBodies(c, bodies, n, worldOfBody));
+    TRY(vxb::loadBodies(c, bodies, n, worldOfBody, true));
     TRY(vxb::loadSoup(c, soup));
     cudaError_t e = cudaStreamSynchronize(c.stream);
     return vxb::cudaStatus(c, e, "world load");

@@ -172,6 +172,7 @@ struct Context {
     DevBuf jointBuf;  // joints of the Backend path, in colour order
     std::vector<vx_mesh> hostMeshes;   // root bounds for the broad phase
     bool complexShapes = false;        // any mesh or compound body loaded
+    bool kinematic = false;            // any kinematic body loaded (Backend path)
     // FNV-1a keys of the loaded bodies' shape references and of the soup's
     // array sizes (a snapshot image restores only into the same geometry)
     uint64_t bodyGeometryKey = 0, soupGeometryKey = 0;
@@ -271,7 +272,9 @@ int resetCoop(Context& c, CoopState* st);
 int ensure(Context& c, DevBuf& b, size_t bytes);
 
 // Pipeline entry points (pipeline.cu).
-int loadBodies(Context& c, const vx_body* bodies, uint32_t n, const uint32_t* worldOf);
+// deviceWorld: the device-resident world (vxb_world_load), which does not take
+// kinematic bodies; the Backend and stage paths do.
+int loadBodies(Context& c, const vx_body* bodies, uint32_t n, const uint32_t* worldOf, bool deviceWorld = false);
 int loadSoup(Context& c, const vx_soup* soup);
 int readBodies(Context& c, vx_body* out, uint32_t n);
 int worldStep(Context& c, int steps);
@@ -282,6 +285,12 @@ int stageColor(Context& c, const vx_contact* contacts, uint32_t m, int32_t* colo
 int stageDistance(Context& c, const uint64_t* pairs, uint32_t npairs, int path, float* out);
 int backendIntegrate(Context& c, vx_vec3 gravity, float dt);
 int backendIntegrateTransforms(Context& c, float dt);
+// advanceSubsteps one substep at a time, as the reference CUDA backend runs
+// it (joints.cu): contact sweeps, optional joint sweeps, then the integration
+// of every body (kinematic ones too) each substep. Bodies must be loaded.
+int backendStepwise(Context& c, vx_body* bodies, uint32_t n, vx_contact* contacts, uint32_t m, vx_joint* joints,
+                    uint32_t njoints, vx_vec3 gravity, float h, int substeps, const vx_solver_options& o,
+                    uint32_t* iterations);
 // The reference CUDA backend's joint path of advanceSubsteps (joints.cu).
 int backendAdvanceJoints(Context& c, vx_body* bodies, uint32_t n, vx_contact* contacts, uint32_t m,
                          vx_joint* joints, uint32_t njoints, vx_vec3 gravity, float h, int substeps,

@@ -1,4 +1,4 @@
-// The joint path of advanceSubsteps on the device (the reference CUDA
+// The substep-wise path of advanceSubsteps on the device (the reference CUDA
 // backend's, src/backend_cuda.cu:691-760 and :800-880): with 64 or more
 // joints of supported types, every substep runs the contact sweeps, then
 // reset + 8 sweeps of the joints colour by colour + the break test, then the
@@ -142,35 +142,47 @@ int backendAdvanceJoints(Context& c, vx_body* bodies, uint32_t n, vx_contact* co
     }
     if (o.iterationPolicy != 0) return VXB_OK;  // Adaptive: the host path, like the reference
     JT_TRY(loadBodies(c, bodies, n, nullptr));
+    JT_TRY(backendStepwise(c, bodies, n, contacts, m, joints, njoints, gravity, h, substeps, o, iterations));
+    *advanced = 1;
+    return VXB_OK;
+}
 
-    std::vector<uint32_t> order, colourStart;
-    colourJoints(bodies, n, joints, njoints, order, colourStart);
-    std::vector<vx_joint> sorted(njoints);
-    for (uint32_t s = 0; s < njoints; ++s) sorted[s] = joints[order[s]];
-    JT_TRY(ensure(c, c.jointBuf, (size_t)njoints * sizeof(vx_joint)));
-    vx_joint* dj = reinterpret_cast<vx_joint*>(c.jointBuf.ptr);
-    JT_CUDA(c, cudaMemcpyAsync(dj, sorted.data(), (size_t)njoints * sizeof(vx_joint), cudaMemcpyHostToDevice,
-                                c.stream));
-
+int backendStepwise(Context& c, vx_body* bodies, uint32_t n, vx_contact* contacts, uint32_t m, vx_joint* joints,
+                    uint32_t njoints, vx_vec3 gravity, float h, int substeps, const vx_solver_options& o,
+                    uint32_t* iterations) {
+    std::vector<uint32_t> order, colourStart(1, 0);
+    std::vector<vx_joint> sorted;
+    vx_joint* dj = nullptr;
+    if (njoints) {
+        colourJoints(bodies, n, joints, njoints, order, colourStart);
+        sorted.resize(njoints);
+        for (uint32_t s = 0; s < njoints; ++s) sorted[s] = joints[order[s]];
+        JT_TRY(ensure(c, c.jointBuf, (size_t)njoints * sizeof(vx_joint)));
+        dj = reinterpret_cast<vx_joint*>(c.jointBuf.ptr);
+        JT_CUDA(c, cudaMemcpyAsync(dj, sorted.data(), (size_t)njoints * sizeof(vx_joint), cudaMemcpyHostToDevice,
+                                    c.stream));
+    }
     const uint32_t colours = (uint32_t)colourStart.size() - 1;
     for (int s = 0; s < substeps; ++s) {
         if (s > 0) JT_TRY(backendIntegrate(c, gravity, h));
         // contact sweeps (the first substep warm-starts and colours the contacts)
         if (m) JT_TRY(backendSolve(c, contacts, m, h, s == 0, o, gravity, 1, false));
-        JT_LAUNCH(c, jointResetKernel, gridFor(njoints, 128), 128, dj, njoints, s > 0 ? 1 : 0);
-        for (int it = 0; it < joint::kIterations; ++it)
-            for (uint32_t col = 0; col < colours; ++col) {
-                const uint32_t first = colourStart[col], count = colourStart[col + 1] - first;
-                JT_LAUNCH(c, jointColorKernel, gridFor(count, 128), 128, c.B, dj, first, count, h);
-            }
-        JT_LAUNCH(c, jointBreakKernel, gridFor(njoints, 128), 128, dj, njoints, h);
+        if (njoints) {
+            JT_LAUNCH(c, jointResetKernel, gridFor(njoints, 128), 128, dj, njoints, s > 0 ? 1 : 0);
+            for (int it = 0; it < joint::kIterations; ++it)
+                for (uint32_t col = 0; col < colours; ++col) {
+                    const uint32_t first = colourStart[col], count = colourStart[col + 1] - first;
+                    JT_LAUNCH(c, jointColorKernel, gridFor(count, 128), 128, c.B, dj, first, count, h);
+                }
+            JT_LAUNCH(c, jointBreakKernel, gridFor(njoints, 128), 128, dj, njoints, h);
+        }
         JT_TRY(backendIntegrateTransforms(c, h));
     }
-    JT_CUDA(c, cudaMemcpyAsync(sorted.data(), dj, (size_t)njoints * sizeof(vx_joint), cudaMemcpyDeviceToHost,
-                                c.stream));
+    if (njoints)
+        JT_CUDA(c, cudaMemcpyAsync(sorted.data(), dj, (size_t)njoints * sizeof(vx_joint), cudaMemcpyDeviceToHost,
+                                    c.stream));
     JT_TRY(readBodies(c, bodies, n));  // synchronises the stream
     for (uint32_t s = 0; s < njoints; ++s) joints[order[s]] = sorted[s];
-    *advanced = 1;
     if (iterations) *iterations = m ? (uint32_t)(2 * o.velocityIterations * substeps) : 0u;
     return VXB_OK;
 }

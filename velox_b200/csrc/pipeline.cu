@@ -2722,7 +2722,7 @@ static Soup soupOf(Context& c) {
                 P<uint32_t>(c.triRefBuf), P<vx_compound_child>(c.childBuf)};
 }
 
-int loadBodies(Context& c, const vx_body* bodies, uint32_t n, const uint32_t* worldOf) {
+int loadBodies(Context& c, const vx_body* bodies, uint32_t n, const uint32_t* worldOf, bool deviceWorld) {
     if (n == 0) return fail(c, VXB_ERR_INVALID, "no bodies");
     // The Backend path reloads the same bodies between its calls of one step
     // (integrate between substeps' solves): the coloured contacts stay valid
@@ -2732,6 +2732,7 @@ int loadBodies(Context& c, const vx_body* bodies, uint32_t n, const uint32_t* wo
         c.backendColored = false;
     }
     c.complexShapes = false;
+    c.kinematic = false;
     uint64_t key = 0xcbf29ce484222325ull;
     for (uint32_t i = 0; i < n; ++i) {
         const vx_body& b = bodies[i];
@@ -2745,8 +2746,9 @@ int loadBodies(Context& c, const vx_body* bodies, uint32_t n, const uint32_t* wo
         if (s == VX_SHAPE_MESH || s == VX_SHAPE_COMPOUND) c.complexShapes = true;
         if (s == VX_SHAPE_MESH && bodies[i].motionType != VX_MOTION_STATIC)
             return fail(c, VXB_ERR_INVALID, "mesh bodies are static");
-        if (bodies[i].motionType == VX_MOTION_KINEMATIC)
-            return fail(c, VXB_ERR_UNSUPPORTED, "kinematic bodies are not supported by the device pipeline");
+        if (deviceWorld && bodies[i].motionType == VX_MOTION_KINEMATIC)
+            return fail(c, VXB_ERR_UNSUPPORTED, "kinematic bodies are not supported by the device world");
+        if (bodies[i].motionType == VX_MOTION_KINEMATIC) c.kinematic = true;
     }
     c.n = n;
     // SoA arrays in one allocation (16 arrays of 16-byte elements).
