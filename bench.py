@@ -284,6 +284,7 @@ def run_batched(args):
     sampler.start()
     barrier()
     launches0 = ctx.launches
+    syncs0 = ctx.host_syncs
     ctx.enable_timing(True)
     if args.profile:
         torch.cuda.cudart().cudaProfilerStart()
@@ -293,6 +294,7 @@ def run_batched(args):
     barrier()
     clocks = sampler.stop()
     launches = ctx.launches - launches0
+    host_syncs = ctx.host_syncs - syncs0
     stage = ctx.stage_times()
     last = ctx.stats()
     ctx.close()
@@ -361,7 +363,7 @@ def run_batched(args):
             "cpu_baseline": cpu,
             "e2e": {"value": nworlds * args.steps / (e2e_ms / 1e3), "unit": "world-steps/s",
                     "h2d_bytes_per_step": int(forces.numel() * 4), "d2h_bytes_per_step": int(poses.numel() * 4)},
-            "clocks": clocks, "gpu_launches": int(launches)}
+            "clocks": clocks, "gpu_launches": int(launches), "host_syncs_per_step": host_syncs / args.steps}
     print(json.dumps(line))
     return 0
 
@@ -464,6 +466,7 @@ def main():
     sampler.start()
     barrier()
     launches0 = ctx.launches
+    syncs0 = ctx.host_syncs
     ctx.enable_timing(True)
     events = []
     contacts_total = 0
@@ -495,6 +498,7 @@ def main():
     barrier()
     clocks = sampler.stop()
     launches = ctx.launches - launches0
+    host_syncs = ctx.host_syncs - syncs0
     stage = ctx.stage_times()
     ctx.enable_timing(False)
     ms = sum(a.elapsed_time(b) for a, b in events)
@@ -593,6 +597,9 @@ def main():
             plain_gpu = {"error": str(exc)}
 
     stats = ctx.stats()
+    # launch shapes the tuner settled on (or is still exploring) at the last step's pair count
+    autotune = {site: dict(zip(("threads", "blocks_per_sm", "decided"), ctx.tuned_shape(site, stats["candidatePairs"])))
+                for site in ("collide_convex", "collide_plane", "rewind_probe")}
     ctx.close()
     if dist:
         dist.destroy_process_group()
@@ -610,7 +617,8 @@ def main():
             "roofline": roofline, "solve_roofline": solve_roofline, "rewind_roofline": rewind_roofline,
             "memory_rooflines": memory_rooflines,
             "cpu_baseline": baseline, "e2e": e2e, "clocks": clocks,
-            "gpu_launches": int(launches), "plain_gpu": plain_gpu}
+            "gpu_launches": int(launches), "host_syncs_per_step": host_syncs / args.steps,
+            "autotune": autotune, "plain_gpu": plain_gpu}
     line.update(extra)
     print(json.dumps(line))
     return 0
@@ -683,9 +691,9 @@ def measure_batched(local, stream, nworlds, steps, warmup, plain_sample=PLAIN_SA
     ctx.configure(dt=DT, substeps=SUBSTEPS)
     ctx.step(max(warmup, 3))
     torch.cuda.synchronize()
-    launches0 = ctx.launches
+    launches0, syncs0 = ctx.launches, ctx.host_syncs
     ms = _timed_blocks(ctx, stream, flush, steps)
-    launches = ctx.launches - launches0
+    launches, syncs = ctx.launches - launches0, ctx.host_syncs - syncs0
     ctx.close()
     value = nworlds * steps / (ms / 1e3)
     counts = np.bincount(specs["world"], minlength=nworlds)
@@ -732,7 +740,7 @@ def measure_batched(local, stream, nworlds, steps, warmup, plain_sample=PLAIN_SA
             "plain": {"value": plain, "unit": "world-steps/s",
                       "sample": f"{len(sample)} worlds over the body-count distribution, one context per world, "
                                 f"one world at a time, {steps} device-timed steps each"},
-            "vs_plain": value / plain, "gpu_launches": int(launches),
+            "vs_plain": value / plain, "gpu_launches": int(launches), "host_syncs_per_step": syncs / steps,
             "plain_reference_gpu": plain_ref,
             "vs_plain_reference_gpu": value / plain_ref["value"] if plain_ref else None}
 

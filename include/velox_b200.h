@@ -133,6 +133,41 @@ uint64_t vxb_context_launch_count(const vxb_context* ctx);
  * src/world.cpp:3807-3828. */
 int vxb_context_set_wait_limit(vxb_context* ctx, uint32_t polls);
 
+/* Blocking host reads of device counts this context made since it was
+ * created (each drains the stream: a step sizes its later launches from the
+ * counts of earlier kernels). No counterpart in the reference. */
+uint64_t vxb_context_host_syncs(const vxb_context* ctx);
+
+/* Launch-shape autotuning of the throughput kernels: the narrow phase's
+ * per-pair kernels and the rewind's per-pair probe. Per site and size bucket
+ * (floor(log2(items))) the first calls try six shapes (block size 32/64/128
+ * threads x grid cap of 2,048 threads per SM or one resident wave), timed with
+ * CUDA events on the context's stream; the fastest is kept and written to a
+ * cache file that later contexts on the same device model read at creation.
+ * Shapes change timing only: every result is identical under any shape.
+ * mode 1 (the default; VXB_TUNE=0 in the environment makes it 0 for new
+ * contexts) tunes; mode 0 launches the fixed default shape (128 threads,
+ * 16 blocks per SM). The cache file is VXB_TUNE_CACHE, else
+ * $XDG_CACHE_HOME/velox_b200/launch_shapes.txt, else
+ * $HOME/.cache/velox_b200/launch_shapes.txt; VXB_TUNE_CACHE="" keeps the
+ * decisions in memory. No counterpart in the reference, whose narrow phase
+ * launches a fixed 256-thread block per 256 pairs (src/backend_cuda.cu:459,
+ * :556-561). */
+#define VXB_TUNE_COLLIDE_CONVEX 0
+#define VXB_TUNE_COLLIDE_COMPLEX 1
+#define VXB_TUNE_COLLIDE_PLANE 2
+#define VXB_TUNE_COLLIDE_ANY 3
+#define VXB_TUNE_REWIND_PROBE 4
+int vxb_context_set_tuning(vxb_context* ctx, int mode);
+/* The shape the next launch of `site` over `items` items would use, and
+ * whether its size bucket is decided (1) or still being explored (0). */
+int vxb_context_tuned_shape(const vxb_context* ctx, int site, uint32_t items, uint32_t* threads,
+                            uint32_t* blocksPerSm, int* decided);
+/* Writes this context's decisions to the cache file now (also done when a
+ * bucket is decided and when the context is destroyed). VXB_ERR_INVALID when
+ * no cache file is configured or it cannot be written. */
+int vxb_context_tuning_save(vxb_context* ctx);
+
 /* Per-stage device timing with CUDA events recorded on the context's stream
  * (stages: 0 prepare, 1 broad phase, 2 cell-key sort, 3 narrow phase,
  * 4 contact placement, 5 warm start, 6 islands + colouring, 7 substep solve,

@@ -230,6 +230,10 @@ def lib(path=LIB_PATH):
         "vxb_context_set_stream": ([vp, vp], i32),
         "vxb_context_launch_count": ([vp], ctypes.c_uint64),
         "vxb_context_set_wait_limit": ([vp, u32], i32),
+        "vxb_context_host_syncs": ([vp], ctypes.c_uint64),
+        "vxb_context_set_tuning": ([vp, i32], i32),
+        "vxb_context_tuned_shape": ([vp, i32, u32, p_u32, p_u32, ctypes.POINTER(ctypes.c_int)], i32),
+        "vxb_context_tuning_save": ([vp], i32),
         "vxb_context_enable_timing": ([vp, i32], i32),
         "vxb_context_stage_times": ([vp, vp, vp, u32], i32),
         "vxb_backend_integrate": ([vp, vp, u32, Vec3, f32], i32),
@@ -368,6 +372,29 @@ class Context:
     @property
     def launches(self):
         return int(self.L.vxb_context_launch_count(self.h))
+
+    @property
+    def host_syncs(self):
+        """Blocking reads of device counts since the context was created."""
+        return int(self.L.vxb_context_host_syncs(self.h))
+
+    TUNE_SITES = {"collide_convex": 0, "collide_complex": 1, "collide_plane": 2, "collide_any": 3,
+                  "rewind_probe": 4}
+
+    def set_tuning(self, on=True):
+        """Launch-shape autotuning on (the default) or the fixed default shapes."""
+        self._check(self.L.vxb_context_set_tuning(self.h, 1 if on else 0))
+
+    def tuned_shape(self, site, items):
+        """(threads, blocks per SM, decided) the next launch of `site` over
+        `items` items would use."""
+        t, b, d = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_int()
+        self._check(self.L.vxb_context_tuned_shape(self.h, self.TUNE_SITES.get(site, site), items, ctypes.byref(t),
+                                                   ctypes.byref(b), ctypes.byref(d)))
+        return t.value, b.value, bool(d.value)
+
+    def tuning_save(self):
+        self._check(self.L.vxb_context_tuning_save(self.h))
 
     STAGES = ["prepare", "broadphase", "cell_sort", "narrowphase", "placement", "warm_start",
               "islands", "solve", "rewind", "positions"]

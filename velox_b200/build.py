@@ -18,7 +18,7 @@ OBJ = os.path.join(HERE, "_obj")
 LIB = os.path.join(HERE, "libvelox_b200.so")
 
 SOURCES = ["api.cu", "pipeline.cu", "adjoint.cu", "snapshot.cu", "sleep.cu", "joints.cu", "radix_sort.cu", "noalloc.cu",
-           "scene.cpp", "validate.cpp"]
+           "scene.cpp", "validate.cpp", "tuner.cpp"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -108,6 +108,7 @@ int vxb_context_create(int device, vxb_context** out) {
         delete ctx;
         return VXB_ERR_OOM;
     }
+    c.tuner.init(device, c.smCount);
     *out = ctx;
     return VXB_OK;
 }
@@ -117,6 +118,7 @@ void vxb_context_destroy(vxb_context* ctx) {
     Context& c = ctx->impl;
     cudaSetDevice(c.device);
     if (c.stream) cudaStreamSynchronize(c.stream);
+    c.tuner.release();  // after the drain: its last samples have completed
     vxb::tapeEnd(c);
     for (auto& snap : c.snapshots)
         if (snap.buf.ptr) cudaFree(snap.buf.ptr);
@@ -153,6 +155,31 @@ int vxb_context_set_stream(vxb_context* ctx, void* stream) {
 }
 
 uint64_t vxb_context_launch_count(const vxb_context* ctx) { return ctx ? ctx->impl.launches : 0; }
+
+uint64_t vxb_context_host_syncs(const vxb_context* ctx) { return ctx ? ctx->impl.hostSyncs : 0; }
+
+int vxb_context_set_tuning(vxb_context* ctx, int mode) {
+    GUARD(ctx);
+    if (mode != 0 && mode != 1) return VXB_ERR_INVALID;
+    ctx->impl.tuner.setMode(mode);
+    return VXB_OK;
+}
+
+int vxb_context_tuned_shape(const vxb_context* ctx, int site, uint32_t items, uint32_t* threads,
+                            uint32_t* blocksPerSm, int* decided) {
+    if (!ctx || site < 0 || site >= vxb::kTuneSiteCount || !threads || !blocksPerSm) return VXB_ERR_INVALID;
+    bool d = false;
+    const vxb::LaunchShape s = ctx->impl.tuner.shapeFor(site, items, &d);
+    *threads = s.threads;
+    *blocksPerSm = s.blocksPerSm;
+    if (decided) *decided = d ? 1 : 0;
+    return VXB_OK;
+}
+
+int vxb_context_tuning_save(vxb_context* ctx) {
+    GUARD(ctx);
+    return ctx->impl.tuner.save() ? VXB_OK : VXB_ERR_INVALID;
+}
 
 int vxb_context_set_wait_limit(vxb_context* ctx, uint32_t polls) {
     if (!ctx || polls > vxb::kSpinLimit) return VXB_ERR_INVALID;

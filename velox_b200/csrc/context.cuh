@@ -11,6 +11,7 @@
 #include "coop.cuh"
 #include "geom.cuh"
 #include "radix_sort.cuh"
+#include "tuner.h"
 #include "velox_b200.h"
 
 namespace vxb {
@@ -150,6 +151,8 @@ struct Context {
     cudaStream_t stream = nullptr;
     std::string lastError;
     uint64_t launches = 0;
+    uint64_t hostSyncs = 0;  // blocking reads of device counts (the stream drains)
+    Tuner tuner;             // launch shapes of the narrow phase and the rewind probe
 
     // ---- bodies ----
     uint32_t n = 0;

@@ -135,6 +135,16 @@ static inline int bitsFor(uint64_t maxValue) { return keyBits(maxValue); }
         ++(c).launches;                                                      \
     } while (0)
 
+// Launch at a tuned site: block size and grid cap come from the context's
+// launch-shape tuner (tuner.h) for this item count.
+#define TUNED_LAUNCH(c, site, items, kernel, ...)                                                        \
+    do {                                                                                                 \
+        const TunedLaunch tl_ = (c).tuner.begin((site), (items), (c).stream);                           \
+        kernel<<<tl_.shape.grid((items), (c).smCount), tl_.shape.threads, 0, (c).stream>>>(__VA_ARGS__); \
+        ++(c).launches;                                                                                  \
+        (c).tuner.end(tl_, (c).stream);                                                                  \
+    } while (0)
+
 // ---------------------------------------------------------------------------
 // device helpers
 // ---------------------------------------------------------------------------
@@ -2664,6 +2674,7 @@ int resetCoop(Context& c, CoopState* st) {
 
 static int readCounters(Context& c) {
     VXB_CUDA(c, cudaMemcpyAsync(&c.hostCounters, c.dCounters, sizeof(Counters), cudaMemcpyDeviceToHost, c.stream));
+    ++c.hostSyncs;
     VXB_CUDA(c, cudaStreamSynchronize(c.stream));
     return VXB_OK;
 }
@@ -2942,27 +2953,26 @@ static int narrowPhase(Context& c, const uint64_t* pairs, uint32_t npairs, float
                            P<uint64_t>(c.classKeyBuf), P<uint32_t>(c.classValBuf));
                     VXB_TRY(sortPairs(c, P<uint64_t>(c.classKeyBuf), P<uint32_t>(c.classValBuf), convexSplit, 8));
                 }
-                LAUNCH(c, collideKernel<kConvexPairs>, std::min<uint32_t>(blocksFor(convexSplit, 128), (uint32_t)c.smCount * 16),
-                       128, c.B, soupOf(c), pairs, (const uint32_t*)P<uint32_t>(c.classValBuf), convexSplit, dt, mode,
-                       bodyBits, P<vx_contact>(c.contactTmpBuf), c.contactCap, P<uint64_t>(c.recKeyBuf),
-                       P<uint32_t>(c.recValBuf), P<uint2>(c.recInfoBuf), c.recCap, c.dCounters);
+                TUNED_LAUNCH(c, kTuneCollideConvex, convexSplit, collideKernel<kConvexPairs>, c.B, soupOf(c), pairs,
+                             (const uint32_t*)P<uint32_t>(c.classValBuf), convexSplit, dt, mode, bodyBits,
+                             P<vx_contact>(c.contactTmpBuf), c.contactCap, P<uint64_t>(c.recKeyBuf),
+                             P<uint32_t>(c.recValBuf), P<uint2>(c.recInfoBuf), c.recCap, c.dCounters);
                 if (c.complexShapes)
-                    LAUNCH(c, collideKernel<kComplexPairs>,
-                           std::min<uint32_t>(blocksFor(convexSplit, 128), (uint32_t)c.smCount * 16), 128, c.B,
-                           soupOf(c), pairs, (const uint32_t*)P<uint32_t>(c.classValBuf), convexSplit, dt, mode,
-                           bodyBits, P<vx_contact>(c.contactTmpBuf), c.contactCap, P<uint64_t>(c.recKeyBuf),
-                           P<uint32_t>(c.recValBuf), P<uint2>(c.recInfoBuf), c.recCap, c.dCounters);
+                    TUNED_LAUNCH(c, kTuneCollideComplex, convexSplit, collideKernel<kComplexPairs>, c.B, soupOf(c),
+                                 pairs, (const uint32_t*)P<uint32_t>(c.classValBuf), convexSplit, dt, mode, bodyBits,
+                                 P<vx_contact>(c.contactTmpBuf), c.contactCap, P<uint64_t>(c.recKeyBuf),
+                                 P<uint32_t>(c.recValBuf), P<uint2>(c.recInfoBuf), c.recCap, c.dCounters);
             }
             if (np)
-                LAUNCH(c, collideKernel<kPlanePairs>, std::min<uint32_t>(blocksFor(np, 128), (uint32_t)c.smCount * 16),
-                       128, c.B, soupOf(c), planePairs, (const uint32_t*)nullptr, np, dt, mode, bodyBits,
-                       P<vx_contact>(c.contactTmpBuf), c.contactCap, P<uint64_t>(c.recKeyBuf),
-                       P<uint32_t>(c.recValBuf), P<uint2>(c.recInfoBuf), c.recCap, c.dCounters);
+                TUNED_LAUNCH(c, kTuneCollidePlane, np, collideKernel<kPlanePairs>, c.B, soupOf(c), planePairs,
+                             (const uint32_t*)nullptr, np, dt, mode, bodyBits, P<vx_contact>(c.contactTmpBuf),
+                             c.contactCap, P<uint64_t>(c.recKeyBuf), P<uint32_t>(c.recValBuf),
+                             P<uint2>(c.recInfoBuf), c.recCap, c.dCounters);
         } else if (npairs) {
-            LAUNCH(c, collideKernel<kAnyPairs>, std::min<uint32_t>(blocksFor(npairs, 128), (uint32_t)c.smCount * 16), 128,
-                   c.B, soupOf(c), pairs, (const uint32_t*)nullptr, npairs, dt, mode, bodyBits,
-                   P<vx_contact>(c.contactTmpBuf), c.contactCap, P<uint64_t>(c.recKeyBuf), P<uint32_t>(c.recValBuf),
-                   P<uint2>(c.recInfoBuf), c.recCap, c.dCounters);
+            TUNED_LAUNCH(c, kTuneCollideAny, npairs, collideKernel<kAnyPairs>, c.B, soupOf(c), pairs,
+                         (const uint32_t*)nullptr, npairs, dt, mode, bodyBits, P<vx_contact>(c.contactTmpBuf),
+                         c.contactCap, P<uint64_t>(c.recKeyBuf), P<uint32_t>(c.recValBuf), P<uint2>(c.recInfoBuf),
+                         c.recCap, c.dCounters);
         }
         stageEnd(c, kStageNarrowphase);
         VXB_TRY(readCounters(c));
@@ -3049,6 +3059,7 @@ static int parallelColor(Context& c, const vx_contact* cs, const uint32_t* order
     if (rc != VXB_OK) return rc;
     CoopState host;
     VXB_CUDA(c, cudaMemcpyAsync(&host, st, sizeof(host), cudaMemcpyDeviceToHost, c.stream));
+    ++c.hostSyncs;
     VXB_CUDA(c, cudaStreamSynchronize(c.stream));
     c.stats.colorRounds = host.rounds;
     if (host.timeout || (host.spill & 2u)) return VXB_ERR_TIMEOUT;
@@ -3417,8 +3428,7 @@ static int conservativeAdvancement(Context& c, uint32_t npairs, float dt) {
     const uint64_t* pk = P<uint64_t>(c.pairKeyBuf);
     const float4* prevPos = P<float4>(c.prevPoseBuf);
     const float4* prevRot = prevPos + n;
-    LAUNCH(c, caProbeKernel, std::min<uint32_t>(blocksFor(npairs, 128), (uint32_t)c.smCount * 16), 128, c.B, soupOf(c),
-           pk, npairs, dt, flags, bodyMark, endGap);
+    TUNED_LAUNCH(c, kTuneProbe, npairs, caProbeKernel, c.B, soupOf(c), pk, npairs, dt, flags, bodyMark, endGap);
     // speculative outcomes of the flagged pairs on the probe's state
     VXB_TRY(exclusiveScan(c, flags, flagRank, npairs, &c.dCounters->caFlagged));
     VXB_TRY(readCounters(c));

@@ -544,6 +544,7 @@ int sleepAndEvents(Context& c, const vx_contact* cs, uint32_t m, float dt, uint3
                   prevCount, events, pairsNext, small + 5);
     uint32_t host[8];
     SL_CUDA(c, cudaMemcpyAsync(host, small, 32, cudaMemcpyDeviceToHost, c.stream));
+    ++c.hostSyncs;
     SL_CUDA(c, cudaStreamSynchronize(c.stream));
     const uint32_t total = host[0] + host[6];  // active pairs and the resting pairs appended
     S.eventCount = S.events ? host[0] + host[5] : 0;
@@ -559,6 +560,7 @@ int sleepAndEvents(Context& c, const vx_contact* cs, uint32_t m, float dt, uint3
         SL_LAUNCH(c, compactKeysKernel, gridFor(total, 256), 256, pairsNext, flags, ranks, total,
                   PT<uint64_t>(S.pairs));
         SL_CUDA(c, cudaMemcpyAsync(host + 2, small + 2, 4, cudaMemcpyDeviceToHost, c.stream));
+        ++c.hostSyncs;
         SL_CUDA(c, cudaStreamSynchronize(c.stream));
         pairCount = host[2];
     }
@@ -594,6 +596,7 @@ int sleepAndEvents(Context& c, const vx_contact* cs, uint32_t m, float dt, uint3
                   PT<vx_contact>(S.kept));
     }
     SL_CUDA(c, cudaMemcpyAsync(host + 3, small + 3, 8, cudaMemcpyDeviceToHost, c.stream));
+    ++c.hostSyncs;
     SL_CUDA(c, cudaStreamSynchronize(c.stream));
     S.asleep = host[3];
     *keptOut = prevCount && pairCount ? host[4] : 0;

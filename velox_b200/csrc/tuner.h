@@ -1,0 +1,112 @@
+// Launch-shape autotuner of the throughput kernels (narrow phase, rewind probe).
+//
+// Each tuned launch site picks its block size and its grid cap (blocks per SM,
+// which sets how many pairs a thread walks in the grid-stride loop) per size
+// bucket (floor(log2(items))). While a bucket is undecided, successive calls
+// try the candidate shapes round-robin, each timed with CUDA events on the
+// launching stream and normalised per item; once every candidate has been
+// timed twice the fastest is kept. Decisions are cached per device in a text
+// file (one line per site and bucket) and read back by later contexts, which
+// then launch the cached shape from their first call.
+//
+// The tuned kernels compute one pair per thread with no cross-thread state:
+// their outputs are keyed by pair (records sorted by body pair afterwards), so
+// the launch shape changes timing only, never a result.
+//
+// Environment: VXB_TUNE=0 launches the fixed default shapes (no timing, no
+// cache); VXB_TUNE_CACHE=<file> names the cache file (empty: keep decisions in
+// memory only); default $XDG_CACHE_HOME/velox_b200/launch_shapes.txt, else
+// $HOME/.cache/velox_b200/launch_shapes.txt.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <string>
+
+namespace vxb {
+
+enum TuneSite : int {
+    kTuneCollideConvex = 0,  // collideKernel over convex-convex pairs (GJK / EPA, clipping)
+    kTuneCollideComplex,     // collideKernel over pairs with a mesh, heightfield or compound
+    kTuneCollidePlane,       // collideKernel over body-plane pairs
+    kTuneCollideAny,         // collideKernel over unclassified pairs (stage entry points)
+    kTuneProbe,              // caProbeKernel: the rewind's end-of-step distance query per pair
+    kTuneSiteCount
+};
+
+constexpr int kTuneBuckets = 33;     // floor(log2(items)) for items in [1, 2^32)
+constexpr int kTuneCandidates = 6;   // shapes per site
+constexpr int kTuneSamples = 2;      // timings per candidate before a decision
+
+struct LaunchShape {
+    uint32_t threads = 128;
+    uint32_t blocksPerSm = 16;
+    uint32_t grid(uint32_t items, int smCount) const {
+        const uint64_t need = ((uint64_t)items + threads - 1) / threads;
+        const uint64_t cap = (uint64_t)blocksPerSm * (uint64_t)smCount;
+        const uint64_t g = need < cap ? need : cap;
+        return (uint32_t)(g > 0 ? g : 1);
+    }
+};
+
+// One tuned launch: the shape to use and, while exploring, the timing slot.
+struct TunedLaunch {
+    LaunchShape shape;
+    int site = -1;
+    bool timed = false;
+};
+
+class Tuner {
+public:
+    // Reads the environment and the cache entries of this device.
+    void init(int device, int smCount);
+    // Destroys the events; writes pending decisions to the cache file.
+    void release();
+    // 0: fixed default shapes; 1: tune and use the cache.
+    void setMode(int mode);
+    int mode() const { return mode_; }
+
+    // Shape for `items` work items at `site`; records the start event when the
+    // call is an exploration sample.
+    TunedLaunch begin(int site, uint32_t items, cudaStream_t stream);
+    // Records the stop event of an exploration sample.
+    void end(const TunedLaunch& t, cudaStream_t stream);
+
+    // What `begin` would launch for `items` at `site`, and whether that bucket
+    // is decided (no exploration left).
+    LaunchShape shapeFor(int site, uint32_t items, bool* decided) const;
+    // Writes this device's decisions into the cache file (merged with the
+    // other devices' lines already there). Returns false when the file cannot
+    // be written.
+    bool save();
+    const std::string& cachePath() const { return path_; }
+
+    static const char* siteName(int site);
+    static LaunchShape defaultShape(int site);
+    static LaunchShape candidate(int site, int k);
+
+private:
+    struct Bucket {
+        int decided = -1;                    // chosen candidate, -1 while exploring
+        int next = 0;                        // next candidate to sample
+        int samples[kTuneCandidates] = {};
+        float bestPerItem[kTuneCandidates] = {};  // ms per item, best sample
+    };
+    struct Pending {
+        bool active = false;
+        int bucket = 0, cand = 0;
+        uint32_t items = 0;
+    };
+    void harvest(int site);
+    static int bucketOf(uint32_t items);
+
+    int mode_ = 1;
+    int smCount_ = 148;
+    bool ready_ = false;
+    bool dirty_ = false;
+    std::string path_, deviceKey_;
+    Bucket buckets_[kTuneSiteCount][kTuneBuckets];
+    Pending pending_[kTuneSiteCount];
+    cudaEvent_t start_[kTuneSiteCount] = {}, stop_[kTuneSiteCount] = {};
+};
+
+}  // namespace vxb
