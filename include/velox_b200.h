@@ -140,10 +140,11 @@ uint64_t vxb_context_host_syncs(const vxb_context* ctx);
 
 /* Launch-shape autotuning of the throughput kernels: the narrow phase's
  * per-pair kernels and the rewind's per-pair probe. Per site and size bucket
- * (floor(log2(items))) the first calls try six shapes (block size 32/64/128
- * threads x grid cap of 2,048 threads per SM or one resident wave), timed with
- * CUDA events on the context's stream; the fastest is kept and written to a
- * cache file that later contexts on the same device model read at creation.
+ * (floor(log2(items))) the first launch runs six shapes (block size 32/64/128
+ * threads x grid cap of 2,048 threads per SM or one resident wave) twice each
+ * on the same inputs, timed with CUDA events on the context's stream (a
+ * one-time cost that waits for each trial); the fastest is kept and written to
+ * a cache file that later contexts on the same device model read at creation.
  * Shapes change timing only: every result is identical under any shape.
  * mode 1 (the default; VXB_TUNE=0 in the environment makes it 0 for new
  * contexts) tunes; mode 0 launches the fixed default shape (128 threads,
@@ -160,7 +161,7 @@ uint64_t vxb_context_host_syncs(const vxb_context* ctx);
 #define VXB_TUNE_REWIND_PROBE 4
 int vxb_context_set_tuning(vxb_context* ctx, int mode);
 /* The shape the next launch of `site` over `items` items would use, and
- * whether its size bucket is decided (1) or still being explored (0). */
+ * whether its size bucket is decided (1) or still has its trials ahead (0). */
 int vxb_context_tuned_shape(const vxb_context* ctx, int site, uint32_t items, uint32_t* threads,
                             uint32_t* blocksPerSm, int* decided);
 /* Writes this context's decisions to the cache file now (also done when a

@@ -136,7 +136,7 @@ void vxb_context_destroy(vxb_context* ctx) {
                            &c.fpSlotBuf, &c.fpColorBuf, &c.fpRunStartBuf, &c.fpIslandBuf, &c.coopBuf,
                            &c.giantBuf, &c.classKeyBuf, &c.classValBuf, &c.rowBodyBuf, &c.tinyBuf, &c.tinyKeyBuf, &c.clusterInfoBuf, &c.clusterKeyBuf,
                            &c.clusterValBuf, &c.clusterOfBuf, &c.clusterCountBuf, &c.clusterStartBuf,
-                           &c.clusterRowsBuf, &c.clusterLinkBuf, &c.caInfoBuf,
+                           &c.clusterRowsBuf, &c.clusterLinkBuf, &c.caInfoBuf, &c.tuneSaveBuf,
                            &c.countersBuf};
     for (vxb::DevBuf* b : bufs)
         if (b->ptr) cudaFree(b->ptr);

@@ -231,6 +231,7 @@ struct Context {
         clusterRowsBuf;                 // spatial clusters of a giant island
     DevBuf clusterLinkBuf;              // cross-cluster predecessor links + remote-successor flags
     DevBuf caInfoBuf;                   // rewind pass: one record per candidate
+    DevBuf tuneSaveBuf;                 // launch-shape trials: device copy of the counters
 
     DevBuf countersBuf;
     Counters* dCounters = nullptr;

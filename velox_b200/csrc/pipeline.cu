@@ -135,15 +135,6 @@ static inline int bitsFor(uint64_t maxValue) { return keyBits(maxValue); }
         ++(c).launches;                                                      \
     } while (0)
 
-// Launch at a tuned site: block size and grid cap come from the context's
-// launch-shape tuner (tuner.h) for this item count.
-#define TUNED_LAUNCH(c, site, items, kernel, ...)                                                        \
-    do {                                                                                                 \
-        const TunedLaunch tl_ = (c).tuner.begin((site), (items), (c).stream);                           \
-        kernel<<<tl_.shape.grid((items), (c).smCount), tl_.shape.threads, 0, (c).stream>>>(__VA_ARGS__); \
-        ++(c).launches;                                                                                  \
-        (c).tuner.end(tl_, (c).stream);                                                                  \
-    } while (0)
 
 // ---------------------------------------------------------------------------
 // device helpers
@@ -2000,15 +1991,43 @@ __global__ void clusterScatterKernel(SolveArgs A, const uint32_t* rowList, uint3
     }
 }
 
+// Shared-memory index of a block's cluster: the start of each of its G colour
+// cells relative to the block's first row (G + 1 words, padded to 16 bytes),
+// then per row its solve position, contact index and two bodies. A step then
+// reads its rows' indices from shared memory instead of three dependent global
+// loads (cell start, row, contact index and bodies). A block whose rows do not
+// fit reads them from global memory.
+constexpr uint32_t kClusterSmemBytes = 64u * 1024u;
+
+VXD uint32_t clusterHeadWords(uint32_t G) { return (G + 1u + 3u) & ~3u; }
+
+VXD bool clusterIndexFits(uint32_t G, uint32_t rowsInBlock) {
+    return (uint64_t)clusterHeadWords(G) * 4u + (uint64_t)rowsInBlock * 16u <= (uint64_t)kClusterSmemBytes;
+}
+
 // One unit (sweep) step of block c's cluster for colour slot gl; false = abort.
 // `pred`: the cross-cluster links (clusterLinkKernel); `remote`: rows that
-// publish their sweep counter.
-VXD bool clusterStep(const SolveArgs& A, const uint32_t* start, const uint32_t* rows, uint32_t cell, int u, int op,
+// publish their sweep counter. `resident`: the block's index is in shared
+// memory (cellStart, info); else the rows come from start/rows in global memory.
+VXD bool clusterStep(const SolveArgs& A, const uint32_t* start, const uint32_t* rows, bool resident,
+                     const uint32_t* cellStart, const uint4* info, uint32_t base, uint32_t gl, int u, int op,
                      const uint32_t* pred, const uint32_t* remote, uint32_t* done, CoopState* st, int* abortFlag) {
-    for (uint32_t idx = start[cell] + threadIdx.x; idx < start[cell + 1]; idx += blockDim.x) {
-        const uint32_t k = rows[idx];
+    const uint32_t i0 = resident ? cellStart[gl] : start[base + gl];
+    const uint32_t i1 = resident ? cellStart[gl + 1] : start[base + gl + 1];
+    for (uint32_t idx = i0 + threadIdx.x; idx < i1; idx += blockDim.x) {
+        uint32_t k;
         GiantRowIn in;
-        giantRowFetch(A, k, op, in);
+        if (resident) {
+            const uint4 r = info[idx];
+            k = r.x;
+            in.ab = make_uint2(r.z, r.w);
+            in.cp = A.contacts + r.y;
+            loadContactCoherent(in.cp, in.cc);
+            if (op == 0 || op == 1) coherentPrep(A.prep + k, in.P);
+        } else {
+            k = rows[idx];
+            giantRowFetch(A, k, op, in);
+        }
         const uint32_t p0 = pred[2 * k], p1 = pred[2 * k + 1];
         if (p0 != kNoPred || p1 != kNoPred) {
             const uint32_t need0 = (p0 & kWrap) ? (uint32_t)u : (uint32_t)u + 1u;
@@ -2040,17 +2059,32 @@ __global__ void __launch_bounds__(256) solveClusterKernel(SolveArgs A, uint32_t 
                                                           const uint32_t* rows, const uint32_t* rowList, uint32_t R,
                                                           const uint32_t* bodyIds, uint32_t NB, const uint32_t* pred,
                                                           const uint32_t* remote, uint32_t* done, CoopState* st) {
+    extern __shared__ uint4 clusterSmem[];  // kClusterSmemBytes: the block's cluster index
     __shared__ int abortFlag;
-    if (threadIdx.x == 0) abortFlag = 0;
-    __syncthreads();
     const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
     const uint32_t base = blockIdx.x * G;
+    const uint32_t s0 = start[base], s1 = start[base + G];
+    const bool resident = G > 0 && clusterIndexFits(G, s1 - s0);
+    uint32_t* cellStart = reinterpret_cast<uint32_t*>(clusterSmem);
+    uint4* info = clusterSmem + clusterHeadWords(G) / 4u;
+    if (resident) {
+        for (uint32_t t = threadIdx.x; t <= G; t += blockDim.x) cellStart[t] = start[base + t] - s0;
+        for (uint32_t i = threadIdx.x; i < s1 - s0; i += blockDim.x) {
+            const uint32_t k = rows[s0 + i];
+            const uint2 ab = A.rowBodies[k];
+            info[i] = make_uint4(k, A.order[k], ab.x, ab.y);
+        }
+    }
+    if (threadIdx.x == 0) abortFlag = 0;
+    __syncthreads();
     if (A.positionIterations > 0) {
         for (uint32_t t = tid; t < R; t += stride) __stcg(done + rowList[t], 0u);
         if (!gridSync(&st->bar, &st->timeout, st->spinLimit)) return;
         for (int u = 0; u < A.positionIterations; ++u)
             for (uint32_t gl = 0; gl < G; ++gl)
-                if (!clusterStep(A, start, rows, base + gl, u, 2, pred, remote, done, st, &abortFlag)) return;
+                if (!clusterStep(A, start, rows, resident, cellStart, info, base, gl, u, 2, pred, remote, done, st,
+                                 &abortFlag))
+                    return;
         gridSync(&st->bar, &st->timeout, st->spinLimit);
         return;
     }
@@ -2070,8 +2104,8 @@ __global__ void __launch_bounds__(256) solveClusterKernel(SolveArgs A, uint32_t 
         const int warmUnits = A.warmStart && s == 0 ? 1 : 0;
         for (int u = 0; u < warmUnits + A.sweeps; ++u)
             for (uint32_t gl = 0; gl < G; ++gl)
-                if (!clusterStep(A, start, rows, base + gl, u, u < warmUnits ? 0 : 1, pred, remote, done, st,
-                                 &abortFlag))
+                if (!clusterStep(A, start, rows, resident, cellStart, info, base, gl, u, u < warmUnits ? 0 : 1, pred,
+                                 remote, done, st, &abortFlag))
                     return;
         if (!gridSync(&st->bar, &st->timeout, st->spinLimit)) return;
         if (A.integrate) {
@@ -2249,9 +2283,13 @@ VXD void orientPair(const BodyArrays& B, uint64_t key, uint32_t& i, uint32_t& j)
     if (!isDynamic(B.filt[i].x) && isDynamic(B.filt[j].x)) { const uint32_t t = i; i = j; j = t; }
 }
 
-__global__ void caProbeKernel(BodyArrays B, Soup soup, const uint64_t* pairKeys, uint32_t npairs, float dt,
-                              uint32_t* flags, uint32_t* bodyMark, float4* endGap) {
-    for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < npairs; r += gridDim.x * blockDim.x) {
+// `order` (optional): the pairs grouped by shape combination, so that a warp's
+// lanes mostly take the same distance-query path; every outcome is written at
+// the pair's own index.
+__global__ void caProbeKernel(BodyArrays B, Soup soup, const uint64_t* pairKeys, const uint32_t* order,
+                              uint32_t npairs, float dt, uint32_t* flags, uint32_t* bodyMark, float4* endGap) {
+    for (uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x; slot < npairs; slot += gridDim.x * blockDim.x) {
+        const uint32_t r = order ? order[slot] : slot;
         uint32_t i, j;
         orientPair(B, pairKeys[r], i, j);
         const BodyView a = loadView(B, i), b = loadView(B, j);
@@ -2408,6 +2446,7 @@ __global__ void caSpeculateKernel(BodyArrays B, Soup soup, const uint64_t* pairK
 // candidates from a queue, so independent chains never wait for one another.
 // Cooperative launch (all workers resident); every wait is bounded.
 constexpr int kCaWidenLimit = 8;  // replays with a widened marked set before the serial loop
+constexpr uint32_t kProbeGroupMin = 8192;  // pairs from which the probe groups them by shape combination
 constexpr int kCaWidenHops = 8;   // hops of widening per replay
 constexpr int kCaInitialHops = 8; // hops of widening before the first pass
 // Workers of the rewind pass: one block of kCaFlowThreads threads per SM, one
@@ -2679,6 +2718,50 @@ static int readCounters(Context& c) {
     return VXB_OK;
 }
 
+// Launch at a tuned site (tuner.h): `launch(shape)` issues the kernel with
+// that block size and grid cap. While the size bucket of `items` has no shape,
+// every candidate first runs on the same inputs, `restore()` putting back what
+// a launch consumes before each trial and before the real launch.
+template <class Launch, class Restore>
+static int tunedLaunch(Context& c, int site, uint32_t items, Launch launch, Restore restore) {
+    if (c.tuner.undecided(site, items)) {
+        c.tuner.beginTrials();
+        for (int round = 0; round < kTuneSamples; ++round)
+            for (int k = 0; k < kTuneCandidates; ++k) {
+                VXB_TRY(restore());
+                c.tuner.trialStart(c.stream);
+                launch(Tuner::candidate(site, k));
+                ++c.hostSyncs;
+                const cudaError_t e = c.tuner.trialStop(k, c.stream);
+                if (e != cudaSuccess) return cudaStatus(c, e, "launch-shape trial");
+            }
+        c.tuner.decide(site, items);
+        VXB_TRY(restore());
+    }
+    launch(c.tuner.shapeFor(site, items, nullptr));
+    return VXB_OK;
+}
+
+// Restores the device counters a narrow-phase launch appends to (contacts,
+// records, overflow flags): the first call keeps a device copy, later calls
+// put it back.
+struct CounterRestore {
+    Context& c;
+    bool saved = false;
+    int operator()() {
+        if (!saved) {
+            VXB_TRY(ensure(c, c.tuneSaveBuf, sizeof(Counters)));
+            VXB_CUDA(c, cudaMemcpyAsync(c.tuneSaveBuf.ptr, c.dCounters, sizeof(Counters), cudaMemcpyDeviceToDevice,
+                                        c.stream));
+            saved = true;
+            return VXB_OK;
+        }
+        VXB_CUDA(c, cudaMemcpyAsync(c.dCounters, c.tuneSaveBuf.ptr, sizeof(Counters), cudaMemcpyDeviceToDevice,
+                                    c.stream));
+        return VXB_OK;
+    }
+};
+
 static int resetCounters(Context& c) {
     Counters z;
     std::memset(&z, 0, sizeof(z));
@@ -2941,6 +3024,10 @@ static int narrowPhase(Context& c, const uint64_t* pairs, uint32_t npairs, float
         VXB_CUDA(c, cudaMemsetAsync(&c.dCounters->contactsTmp, 0, 8, c.stream));  // contactsTmp + records
         VXB_CUDA(c, cudaMemsetAsync(&c.dCounters->overflow, 0, 4, c.stream));
         stageBegin(c, kStageNarrowphase);
+        vx_contact* tmp = P<vx_contact>(c.contactTmpBuf);
+        uint64_t* recKeys = P<uint64_t>(c.recKeyBuf);
+        uint32_t* recVals = P<uint32_t>(c.recValBuf);
+        uint2* recInfo = P<uint2>(c.recInfoBuf);
         if (npairs && convexSplit <= npairs) {
             const uint32_t np = npairs - convexSplit;
             if (convexSplit) {
@@ -2953,26 +3040,31 @@ static int narrowPhase(Context& c, const uint64_t* pairs, uint32_t npairs, float
                            P<uint64_t>(c.classKeyBuf), P<uint32_t>(c.classValBuf));
                     VXB_TRY(sortPairs(c, P<uint64_t>(c.classKeyBuf), P<uint32_t>(c.classValBuf), convexSplit, 8));
                 }
-                TUNED_LAUNCH(c, kTuneCollideConvex, convexSplit, collideKernel<kConvexPairs>, c.B, soupOf(c), pairs,
-                             (const uint32_t*)P<uint32_t>(c.classValBuf), convexSplit, dt, mode, bodyBits,
-                             P<vx_contact>(c.contactTmpBuf), c.contactCap, P<uint64_t>(c.recKeyBuf),
-                             P<uint32_t>(c.recValBuf), P<uint2>(c.recInfoBuf), c.recCap, c.dCounters);
+                const uint32_t* order = P<uint32_t>(c.classValBuf);
+                VXB_TRY(tunedLaunch(c, kTuneCollideConvex, convexSplit, [&](LaunchShape sh) {
+                    LAUNCH(c, collideKernel<kConvexPairs>, sh.grid(convexSplit, c.smCount), sh.threads, c.B, soupOf(c),
+                           pairs, order, convexSplit, dt, mode, bodyBits, tmp, c.contactCap, recKeys, recVals, recInfo,
+                           c.recCap, c.dCounters);
+                }, CounterRestore{c}));
                 if (c.complexShapes)
-                    TUNED_LAUNCH(c, kTuneCollideComplex, convexSplit, collideKernel<kComplexPairs>, c.B, soupOf(c),
-                                 pairs, (const uint32_t*)P<uint32_t>(c.classValBuf), convexSplit, dt, mode, bodyBits,
-                                 P<vx_contact>(c.contactTmpBuf), c.contactCap, P<uint64_t>(c.recKeyBuf),
-                                 P<uint32_t>(c.recValBuf), P<uint2>(c.recInfoBuf), c.recCap, c.dCounters);
+                    VXB_TRY(tunedLaunch(c, kTuneCollideComplex, convexSplit, [&](LaunchShape sh) {
+                        LAUNCH(c, collideKernel<kComplexPairs>, sh.grid(convexSplit, c.smCount), sh.threads, c.B,
+                               soupOf(c), pairs, order, convexSplit, dt, mode, bodyBits, tmp, c.contactCap, recKeys,
+                               recVals, recInfo, c.recCap, c.dCounters);
+                    }, CounterRestore{c}));
             }
             if (np)
-                TUNED_LAUNCH(c, kTuneCollidePlane, np, collideKernel<kPlanePairs>, c.B, soupOf(c), planePairs,
-                             (const uint32_t*)nullptr, np, dt, mode, bodyBits, P<vx_contact>(c.contactTmpBuf),
-                             c.contactCap, P<uint64_t>(c.recKeyBuf), P<uint32_t>(c.recValBuf),
-                             P<uint2>(c.recInfoBuf), c.recCap, c.dCounters);
+                VXB_TRY(tunedLaunch(c, kTuneCollidePlane, np, [&](LaunchShape sh) {
+                    LAUNCH(c, collideKernel<kPlanePairs>, sh.grid(np, c.smCount), sh.threads, c.B, soupOf(c), planePairs,
+                           (const uint32_t*)nullptr, np, dt, mode, bodyBits, tmp, c.contactCap, recKeys, recVals,
+                           recInfo, c.recCap, c.dCounters);
+                }, CounterRestore{c}));
         } else if (npairs) {
-            TUNED_LAUNCH(c, kTuneCollideAny, npairs, collideKernel<kAnyPairs>, c.B, soupOf(c), pairs,
-                         (const uint32_t*)nullptr, npairs, dt, mode, bodyBits, P<vx_contact>(c.contactTmpBuf),
-                         c.contactCap, P<uint64_t>(c.recKeyBuf), P<uint32_t>(c.recValBuf), P<uint2>(c.recInfoBuf),
-                         c.recCap, c.dCounters);
+            VXB_TRY(tunedLaunch(c, kTuneCollideAny, npairs, [&](LaunchShape sh) {
+                LAUNCH(c, collideKernel<kAnyPairs>, sh.grid(npairs, c.smCount), sh.threads, c.B, soupOf(c), pairs,
+                       (const uint32_t*)nullptr, npairs, dt, mode, bodyBits, tmp, c.contactCap, recKeys, recVals,
+                       recInfo, c.recCap, c.dCounters);
+            }, CounterRestore{c}));
         }
         stageEnd(c, kStageNarrowphase);
         VXB_TRY(readCounters(c));
@@ -3012,21 +3104,27 @@ static int narrowPhase(Context& c, const uint64_t* pairs, uint32_t npairs, float
 // (nothing recorded) when the device cannot run it: callers then take their
 // serial path.
 template <class Kernel, class... Args>
-static int launchCooperativeCapped(Context& c, int maxPerSm, Kernel kernel, int threads, Args... args) {
+static int launchCooperativeSmem(Context& c, int maxPerSm, size_t smem, Kernel kernel, int threads, Args... args) {
     int perSm = 0;
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kernel, threads, 0);
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kernel, threads, smem);
     if (e != cudaSuccess) return cudaStatus(c, e, "cooperative occupancy");
     if (perSm <= 0 || !c.cooperative) return VXB_ERR_UNSUPPORTED;
     if (maxPerSm > 0 && perSm > maxPerSm) perSm = maxPerSm;
     void* params[] = {&args...};
-    e = cudaLaunchCooperativeKernel((const void*)kernel, dim3(perSm * c.smCount), dim3(threads), params, 0, c.stream);
+    e = cudaLaunchCooperativeKernel((const void*)kernel, dim3(perSm * c.smCount), dim3(threads), params, smem,
+                                    c.stream);
     ++c.launches;
     return cudaStatus(c, e, "cudaLaunchCooperativeKernel");
 }
 
 template <class Kernel, class... Args>
+static int launchCooperativeCapped(Context& c, int maxPerSm, Kernel kernel, int threads, Args... args) {
+    return launchCooperativeSmem(c, maxPerSm, 0, kernel, threads, args...);
+}
+
+template <class Kernel, class... Args>
 static int launchCooperative(Context& c, Kernel kernel, int threads, Args... args) {
-    return launchCooperativeCapped(c, 0, kernel, threads, args...);
+    return launchCooperativeSmem(c, 0, 0, kernel, threads, args...);
 }
 
 // Colours of the islands above kSerialColorLimit contacts (colorOf, colour
@@ -3291,7 +3389,9 @@ static int launchSolve(Context& c, const SolveArgs& A) {
     if (c.cooperative) {
         // the giant islands in spatial clusters, one per block of the cooperative grid
         int perSm = 0;
-        VXB_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, solveClusterKernel, 256, 0));
+        VXB_CUDA(c, cudaFuncSetAttribute(solveClusterKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)kClusterSmemBytes));
+        VXB_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, solveClusterKernel, 256, kClusterSmemBytes));
         const uint32_t clusters = (uint32_t)(perSm * c.smCount);
         const uint32_t n = c.n;
         VXB_TRY(ensure(c, c.clusterInfoBuf, ((size_t)n * 3 + (size_t)m * 3 + 64) * 4));
@@ -3348,7 +3448,7 @@ static int launchSolve(Context& c, const SolveArgs& A) {
         }
         if (clusters > 0 && c.clusterBuilt) {
             VXB_TRY(resetCoop(c, st));
-            const int rcc = launchCooperative(c, solveClusterKernel, 256, G, c.clusterG,
+            const int rcc = launchCooperativeSmem(c, 0, kClusterSmemBytes, solveClusterKernel, 256, G, c.clusterG,
                                               (const uint32_t*)P<uint32_t>(c.clusterStartBuf),
                                               (const uint32_t*)P<uint32_t>(c.clusterRowsBuf), (const uint32_t*)rowList,
                                               c.clusterR, (const uint32_t*)P<uint32_t>(c.clusterValBuf), c.clusterNB,
@@ -3428,7 +3528,22 @@ static int conservativeAdvancement(Context& c, uint32_t npairs, float dt) {
     const uint64_t* pk = P<uint64_t>(c.pairKeyBuf);
     const float4* prevPos = P<float4>(c.prevPoseBuf);
     const float4* prevRot = prevPos + n;
-    TUNED_LAUNCH(c, kTuneProbe, npairs, caProbeKernel, c.B, soupOf(c), pk, npairs, dt, flags, bodyMark, endGap);
+    // group the pairs by shape combination for the probe (the narrow phase's
+    // grouping buffers are free again at this point of the step)
+    const uint32_t* probeOrder = nullptr;
+    if (npairs >= kProbeGroupMin) {
+        VXB_TRY(ensure(c, c.classKeyBuf, (size_t)npairs * 8 + 64));
+        VXB_TRY(ensure(c, c.classValBuf, (size_t)npairs * 4 + 64));
+        LAUNCH(c, pairClassKernel, blocksFor(npairs, 256), 256, c.B, pk, npairs, P<uint64_t>(c.classKeyBuf),
+               P<uint32_t>(c.classValBuf));
+        VXB_TRY(sortPairs(c, P<uint64_t>(c.classKeyBuf), P<uint32_t>(c.classValBuf), npairs, 8));
+        probeOrder = P<uint32_t>(c.classValBuf);
+    }
+    // the probe writes each pair's outcome at its own index and only sets marks: trials need no restore
+    VXB_TRY(tunedLaunch(c, kTuneProbe, npairs, [&](LaunchShape sh) {
+        LAUNCH(c, caProbeKernel, sh.grid(npairs, c.smCount), sh.threads, c.B, soupOf(c), pk, probeOrder, npairs, dt,
+               flags, bodyMark, endGap);
+    }, [] { return (int)VXB_OK; }));
     // speculative outcomes of the flagged pairs on the probe's state
     VXB_TRY(exclusiveScan(c, flags, flagRank, npairs, &c.dCounters->caFlagged));
     VXB_TRY(readCounters(c));

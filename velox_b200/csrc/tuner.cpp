@@ -63,6 +63,8 @@ int Tuner::bucketOf(uint32_t items) {
 
 void Tuner::init(int device, int smCount) {
     smCount_ = smCount;
+    for (auto& site : decided_)
+        for (int& d : site) d = -1;
     if (const char* m = std::getenv("VXB_TUNE")) mode_ = std::atoi(m) != 0 ? 1 : 0;
     cudaDeviceProp prop;
     std::memset(&prop, 0, sizeof(prop));
@@ -79,9 +81,9 @@ void Tuner::init(int device, int smCount) {
     } else if (const char* h = std::getenv("HOME"); h && *h) {
         path_ = std::string(h) + "/.cache/velox_b200/launch_shapes.txt";
     }
-    for (int s = 0; s < kTuneSiteCount; ++s) {
-        cudaEventCreate(&start_[s]);
-        cudaEventCreate(&stop_[s]);
+    if (cudaEventCreate(&start_) != cudaSuccess || cudaEventCreate(&stop_) != cudaSuccess) {
+        cudaGetLastError();
+        mode_ = 0;  // no events: fixed shapes
     }
     ready_ = true;
     if (path_.empty()) return;
@@ -97,50 +99,47 @@ void Tuner::init(int device, int smCount) {
         for (int s = 0; s < kTuneSiteCount; ++s) {
             if (site != kSiteNames[s]) continue;
             for (int k = 0; k < kTuneCandidates; ++k)
-                if (kCandidates[k].threads == threads && kCandidates[k].blocksPerSm == bps)
-                    buckets_[s][bucket].decided = k;
+                if (kCandidates[k].threads == threads && kCandidates[k].blocksPerSm == bps) decided_[s][bucket] = k;
         }
     }
 }
 
 void Tuner::release() {
     if (!ready_) return;
-    for (int s = 0; s < kTuneSiteCount; ++s) harvest(s);
     if (dirty_) save();
-    for (int s = 0; s < kTuneSiteCount; ++s) {
-        if (start_[s]) cudaEventDestroy(start_[s]);
-        if (stop_[s]) cudaEventDestroy(stop_[s]);
-        start_[s] = stop_[s] = nullptr;
-    }
+    if (start_) cudaEventDestroy(start_);
+    if (stop_) cudaEventDestroy(stop_);
+    start_ = stop_ = nullptr;
     ready_ = false;
 }
 
-void Tuner::setMode(int mode) { mode_ = mode != 0 ? 1 : 0; }
+void Tuner::setMode(int mode) { mode_ = mode != 0 && start_ && stop_ ? 1 : 0; }
 
-// Folds a finished exploration sample of `site` into its bucket (non-blocking:
-// a sample whose stop event has not completed stays pending).
-void Tuner::harvest(int site) {
-    Pending& p = pending_[site];
-    if (!p.active) return;
-    const cudaError_t q = cudaEventQuery(stop_[site]);
-    if (q == cudaErrorNotReady) return;
-    p.active = false;
+bool Tuner::undecided(int site, uint32_t items) const {
+    return ready_ && mode_ == 1 && site >= 0 && site < kTuneSiteCount && decided_[site][bucketOf(items)] < 0;
+}
+
+void Tuner::beginTrials() {
+    for (float& t : trialMs_) t = -1.0f;
+}
+
+void Tuner::trialStart(cudaStream_t stream) { cudaEventRecord(start_, stream); }
+
+cudaError_t Tuner::trialStop(int k, cudaStream_t stream) {
     float ms = 0.0f;
-    if (q != cudaSuccess || cudaEventElapsedTime(&ms, start_[site], stop_[site]) != cudaSuccess) {
-        cudaGetLastError();  // a failed sample is dropped; the step's own status reports real errors
-        return;
-    }
-    Bucket& b = buckets_[site][p.bucket];
-    if (b.decided >= 0) return;
-    const float perItem = ms / (float)(p.items ? p.items : 1);
-    if (b.samples[p.cand] == 0 || perItem < b.bestPerItem[p.cand]) b.bestPerItem[p.cand] = perItem;
-    ++b.samples[p.cand];
-    for (int k = 0; k < kTuneCandidates; ++k)
-        if (b.samples[k] < kTuneSamples) return;
+    cudaError_t e = cudaEventRecord(stop_, stream);
+    if (e == cudaSuccess) e = cudaEventSynchronize(stop_);
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, start_, stop_);
+    if (e != cudaSuccess) return e;
+    if (trialMs_[k] < 0.0f || ms < trialMs_[k]) trialMs_[k] = ms;
+    return cudaSuccess;
+}
+
+void Tuner::decide(int site, uint32_t items) {
     int best = 0;
     for (int k = 1; k < kTuneCandidates; ++k)
-        if (b.bestPerItem[k] < b.bestPerItem[best]) best = k;
-    b.decided = best;
+        if (trialMs_[k] >= 0.0f && (trialMs_[best] < 0.0f || trialMs_[k] < trialMs_[best])) best = k;
+    decided_[site][bucketOf(items)] = best;
     dirty_ = true;
     save();
 }
@@ -152,50 +151,12 @@ LaunchShape Tuner::shapeFor(int site, uint32_t items, bool* decided) const {
         if (decided) *decided = true;
         return defaultShape(site);
     }
-    const Bucket& b = buckets_[site][bucketOf(items)];
-    if (b.decided >= 0) {
+    const int d = decided_[site][bucketOf(items)];
+    if (d >= 0) {
         if (decided) *decided = true;
-        return kCandidates[b.decided];
+        return kCandidates[d];
     }
-    return kCandidates[b.next];
-}
-
-TunedLaunch Tuner::begin(int site, uint32_t items, cudaStream_t stream) {
-    TunedLaunch t;
-    t.site = site;
-    t.shape = defaultShape(site);
-    if (!ready_ || mode_ == 0 || site < 0 || site >= kTuneSiteCount) return t;
-    harvest(site);
-    Bucket& b = buckets_[site][bucketOf(items)];
-    if (b.decided >= 0) {
-        t.shape = kCandidates[b.decided];
-        return t;
-    }
-    if (pending_[site].active) return t;  // the previous sample is still in flight: launch the default, untimed
-    // round-robin over the candidates that still need samples
-    int k = b.next;
-    for (int tries = 0; tries < kTuneCandidates && b.samples[k] >= kTuneSamples; ++tries) k = (k + 1) % kTuneCandidates;
-    b.next = (k + 1) % kTuneCandidates;
-    t.shape = kCandidates[k];
-    if (cudaEventRecord(start_[site], stream) != cudaSuccess) {
-        cudaGetLastError();
-        return t;
-    }
-    t.timed = true;
-    Pending& p = pending_[site];
-    p.active = true;
-    p.bucket = bucketOf(items);
-    p.cand = k;
-    p.items = items;
-    return t;
-}
-
-void Tuner::end(const TunedLaunch& t, cudaStream_t stream) {
-    if (!t.timed) return;
-    if (cudaEventRecord(stop_[t.site], stream) != cudaSuccess) {
-        cudaGetLastError();
-        pending_[t.site].active = false;
-    }
+    return defaultShape(site);
 }
 
 bool Tuner::save() {
@@ -212,7 +173,7 @@ bool Tuner::save() {
     }
     for (int s = 0; s < kTuneSiteCount; ++s)
         for (int bkt = 0; bkt < kTuneBuckets; ++bkt) {
-            const int d = buckets_[s][bkt].decided;
+            const int d = decided_[s][bkt];
             if (d < 0) continue;
             keep.push_back(deviceKey_ + " " + kSiteNames[s] + " " + std::to_string(bkt) + " " +
                            std::to_string(kCandidates[d].threads) + " " + std::to_string(kCandidates[d].blocksPerSm));

@@ -2,18 +2,19 @@
 //
 // Each tuned launch site picks its block size and its grid cap (blocks per SM,
 // which sets how many pairs a thread walks in the grid-stride loop) per size
-// bucket (floor(log2(items))). While a bucket is undecided, successive calls
-// try the candidate shapes round-robin, each timed with CUDA events on the
-// launching stream and normalised per item; once every candidate has been
-// timed twice the fastest is kept. Decisions are cached per device in a text
-// file (one line per site and bucket) and read back by later contexts, which
-// then launch the cached shape from their first call.
+// bucket (floor(log2(items))). The first launch in an undecided bucket runs
+// every candidate shape on the same inputs, twice, timed with CUDA events on
+// the launching stream (the caller restores what a launch consumes before each
+// trial), keeps the fastest, and then makes the real launch with it. Decisions
+// are cached per device in a text file (one line per site and bucket) and read
+// back by later contexts, which then launch the cached shape from their first
+// call.
 //
 // The tuned kernels compute one pair per thread with no cross-thread state:
 // their outputs are keyed by pair (records sorted by body pair afterwards), so
 // the launch shape changes timing only, never a result.
 //
-// Environment: VXB_TUNE=0 launches the fixed default shapes (no timing, no
+// Environment: VXB_TUNE=0 launches the fixed default shapes (no trials, no
 // cache); VXB_TUNE_CACHE=<file> names the cache file (empty: keep decisions in
 // memory only); default $XDG_CACHE_HOME/velox_b200/launch_shapes.txt, else
 // $HOME/.cache/velox_b200/launch_shapes.txt.
@@ -35,7 +36,7 @@ enum TuneSite : int {
 
 constexpr int kTuneBuckets = 33;     // floor(log2(items)) for items in [1, 2^32)
 constexpr int kTuneCandidates = 6;   // shapes per site
-constexpr int kTuneSamples = 2;      // timings per candidate before a decision
+constexpr int kTuneSamples = 2;      // trials per candidate before a decision
 
 struct LaunchShape {
     uint32_t threads = 128;
@@ -48,13 +49,6 @@ struct LaunchShape {
     }
 };
 
-// One tuned launch: the shape to use and, while exploring, the timing slot.
-struct TunedLaunch {
-    LaunchShape shape;
-    int site = -1;
-    bool timed = false;
-};
-
 class Tuner {
 public:
     // Reads the environment and the cache entries of this device.
@@ -65,14 +59,21 @@ public:
     void setMode(int mode);
     int mode() const { return mode_; }
 
-    // Shape for `items` work items at `site`; records the start event when the
-    // call is an exploration sample.
-    TunedLaunch begin(int site, uint32_t items, cudaStream_t stream);
-    // Records the stop event of an exploration sample.
-    void end(const TunedLaunch& t, cudaStream_t stream);
+    // True when the size bucket of `items` at `site` has no shape yet: the
+    // caller then times every candidate (trialStart / trialStop around each
+    // launch) before its real launch.
+    bool undecided(int site, uint32_t items) const;
+    // Forgets the trial times of the previous bucket.
+    void beginTrials();
+    void trialStart(cudaStream_t stream);
+    // Records the end of candidate k's trial and waits for it.
+    cudaError_t trialStop(int k, cudaStream_t stream);
+    // Keeps the candidate with the fastest trial for the bucket and writes
+    // the cache file.
+    void decide(int site, uint32_t items);
 
-    // What `begin` would launch for `items` at `site`, and whether that bucket
-    // is decided (no exploration left).
+    // The shape the next launch of `site` over `items` uses, and whether that
+    // bucket is decided (no trials left).
     LaunchShape shapeFor(int site, uint32_t items, bool* decided) const;
     // Writes this device's decisions into the cache file (merged with the
     // other devices' lines already there). Returns false when the file cannot
@@ -85,18 +86,6 @@ public:
     static LaunchShape candidate(int site, int k);
 
 private:
-    struct Bucket {
-        int decided = -1;                    // chosen candidate, -1 while exploring
-        int next = 0;                        // next candidate to sample
-        int samples[kTuneCandidates] = {};
-        float bestPerItem[kTuneCandidates] = {};  // ms per item, best sample
-    };
-    struct Pending {
-        bool active = false;
-        int bucket = 0, cand = 0;
-        uint32_t items = 0;
-    };
-    void harvest(int site);
     static int bucketOf(uint32_t items);
 
     int mode_ = 1;
@@ -104,9 +93,9 @@ private:
     bool ready_ = false;
     bool dirty_ = false;
     std::string path_, deviceKey_;
-    Bucket buckets_[kTuneSiteCount][kTuneBuckets];
-    Pending pending_[kTuneSiteCount];
-    cudaEvent_t start_[kTuneSiteCount] = {}, stop_[kTuneSiteCount] = {};
+    int decided_[kTuneSiteCount][kTuneBuckets];  // chosen candidate, -1 while undecided
+    float trialMs_[kTuneCandidates] = {};        // best trial of each candidate (current bucket)
+    cudaEvent_t start_ = nullptr, stop_ = nullptr;
 };
 
 }  // namespace vxb
