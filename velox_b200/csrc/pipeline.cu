@@ -1739,11 +1739,30 @@ VXD void storeContactCoherent(vx_contact* p, const vx_contact& c) {
     for (int i = 0; i < (int)(sizeof(vx_contact) / 16); ++i) __stcg(dst + i, src[i]);
 }
 
+// A row's prepared terms through L2 as 16-byte words: one sector per word and
+// lane, where word-sized loads would fetch each sector four times (the rows of
+// a warp lie 176 bytes apart, and L2-only loads do not keep sectors in L1).
+static_assert(sizeof(RowPrep) % 16 == 0, "prepared rows must be whole 16-byte words");
+
 VXD void coherentPrep(const RowPrep* p, RowPrep& P) {
-    const float* s = reinterpret_cast<const float*>(p);
+    const float4* s = reinterpret_cast<const float4*>(p);
     float* d = reinterpret_cast<float*>(&P);
 #pragma unroll
-    for (int i = 0; i < (int)(sizeof(RowPrep) / 4); ++i) d[i] = __ldcg(s + i);
+    for (int i = 0; i < (int)(sizeof(RowPrep) / 16); ++i) {
+        const float4 v = __ldcg(s + i);
+        d[4 * i + 0] = v.x;
+        d[4 * i + 1] = v.y;
+        d[4 * i + 2] = v.z;
+        d[4 * i + 3] = v.w;
+    }
+}
+
+VXD void storePrepCoherent(RowPrep* p, const RowPrep& P) {
+    float4* dst = reinterpret_cast<float4*>(p);
+    const float* src = reinterpret_cast<const float*>(&P);
+#pragma unroll
+    for (int i = 0; i < (int)(sizeof(RowPrep) / 16); ++i)
+        __stcg(dst + i, make_float4(src[4 * i + 0], src[4 * i + 1], src[4 * i + 2], src[4 * i + 3]));
 }
 
 // Inputs of one giant row that only the row itself writes (its contact
@@ -1793,10 +1812,7 @@ VXD void giantRowRun(const SolveArgs& A, uint32_t pos, int op, GiantRowIn& in) {
     RowPrep& P = in.P;
     if (op == 3) {
         prepRow(a, b, r, A.h, A.coneBlock != 0, P);
-        const float* src = reinterpret_cast<const float*>(&P);
-        float* dst = reinterpret_cast<float*>(A.prep + pos);
-#pragma unroll
-        for (int i = 0; i < (int)(sizeof(RowPrep) / 4); ++i) __stcg(dst + i, src[i]);
+        storePrepCoherent(A.prep + pos, P);
         return;
     }
     if (op == 0) warmPrepRow(a, b, r, P);
@@ -1997,7 +2013,8 @@ __global__ void clusterScatterKernel(SolveArgs A, const uint32_t* rowList, uint3
 // reads its rows' indices from shared memory instead of three dependent global
 // loads (cell start, row, contact index and bodies). A block whose rows do not
 // fit reads them from global memory.
-constexpr uint32_t kClusterSmemBytes = 64u * 1024u;
+constexpr int kClusterThreads = 256;               // threads of a cluster block
+constexpr uint32_t kClusterSmemBytes = 64u * 1024u;  // its shared-memory index
 
 VXD uint32_t clusterHeadWords(uint32_t G) { return (G + 1u + 3u) & ~3u; }
 
@@ -2055,7 +2072,7 @@ VXD bool clusterStep(const SolveArgs& A, const uint32_t* start, const uint32_t* 
     return *abortFlag == 0;
 }
 
-__global__ void __launch_bounds__(256) solveClusterKernel(SolveArgs A, uint32_t G, const uint32_t* start,
+__global__ void __launch_bounds__(kClusterThreads) solveClusterKernel(SolveArgs A, uint32_t G, const uint32_t* start,
                                                           const uint32_t* rows, const uint32_t* rowList, uint32_t R,
                                                           const uint32_t* bodyIds, uint32_t NB, const uint32_t* pred,
                                                           const uint32_t* remote, uint32_t* done, CoopState* st) {
@@ -3391,7 +3408,8 @@ static int launchSolve(Context& c, const SolveArgs& A) {
         int perSm = 0;
         VXB_CUDA(c, cudaFuncSetAttribute(solveClusterKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           (int)kClusterSmemBytes));
-        VXB_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, solveClusterKernel, 256, kClusterSmemBytes));
+        VXB_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, solveClusterKernel, kClusterThreads,
+                                                                  kClusterSmemBytes));
         const uint32_t clusters = (uint32_t)(perSm * c.smCount);
         const uint32_t n = c.n;
         VXB_TRY(ensure(c, c.clusterInfoBuf, ((size_t)n * 3 + (size_t)m * 3 + 64) * 4));
@@ -3448,7 +3466,8 @@ static int launchSolve(Context& c, const SolveArgs& A) {
         }
         if (clusters > 0 && c.clusterBuilt) {
             VXB_TRY(resetCoop(c, st));
-            const int rcc = launchCooperativeSmem(c, 0, kClusterSmemBytes, solveClusterKernel, 256, G, c.clusterG,
+            const int rcc = launchCooperativeSmem(c, 0, kClusterSmemBytes, solveClusterKernel, kClusterThreads, G,
+                                                  c.clusterG,
                                               (const uint32_t*)P<uint32_t>(c.clusterStartBuf),
                                               (const uint32_t*)P<uint32_t>(c.clusterRowsBuf), (const uint32_t*)rowList,
                                               c.clusterR, (const uint32_t*)P<uint32_t>(c.clusterValBuf), c.clusterNB,
