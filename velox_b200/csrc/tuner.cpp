@@ -163,12 +163,20 @@ bool Tuner::save() {
     if (path_.empty() || deviceKey_.empty()) return false;
     std::vector<std::string> keep;
     {
+        // keep every line this context does not replace: other devices' lines,
+        // and this device's buckets decided by other contexts
         std::ifstream in(path_);
         std::string line;
         while (std::getline(in, line)) {
             std::istringstream ls(line);
-            std::string key;
-            if ((ls >> key) && key != deviceKey_) keep.push_back(line);
+            std::string key, site;
+            int bucket = -1;
+            if (!(ls >> key)) continue;
+            bool replaced = false;
+            if (key == deviceKey_ && (ls >> site >> bucket) && bucket >= 0 && bucket < kTuneBuckets)
+                for (int s = 0; s < kTuneSiteCount; ++s)
+                    if (site == kSiteNames[s] && decided_[s][bucket] >= 0) replaced = true;
+            if (!replaced) keep.push_back(line);
         }
     }
     for (int s = 0; s < kTuneSiteCount; ++s)

@@ -51,6 +51,10 @@ struct LaunchShape {
 
 class Tuner {
 public:
+    Tuner() {
+        for (auto& site : decided_)
+            for (int& d : site) d = -1;
+    }
     // Reads the environment and the cache entries of this device.
     void init(int device, int smCount);
     // Destroys the events; writes pending decisions to the cache file.
@@ -75,9 +79,9 @@ public:
     // The shape the next launch of `site` over `items` uses, and whether that
     // bucket is decided (no trials left).
     LaunchShape shapeFor(int site, uint32_t items, bool* decided) const;
-    // Writes this device's decisions into the cache file (merged with the
-    // other devices' lines already there). Returns false when the file cannot
-    // be written.
+    // Writes this context's decisions into the cache file, merged with the
+    // lines already there (other devices, and this device's buckets that this
+    // context did not decide). Returns false when the file cannot be written.
     bool save();
     const std::string& cachePath() const { return path_; }
 
