@@ -597,9 +597,7 @@ def main():
             plain_gpu = {"error": str(exc)}
 
     stats = ctx.stats()
-    # launch shapes the tuner settled on (or is still exploring) at the last step's pair count
-    autotune = {site: dict(zip(("threads", "blocks_per_sm", "decided"), ctx.tuned_shape(site, stats["candidatePairs"])))
-                for site in ("collide_convex", "collide_plane", "rewind_probe")}
+    autotune = tuned_shapes(ctx)
     ctx.close()
     if dist:
         dist.destroy_process_group()
@@ -622,6 +620,20 @@ def main():
     line.update(extra)
     print(json.dumps(line))
     return 0
+
+
+def tuned_shapes(ctx):
+    """Launch shapes the tuner decided, per site and size bucket
+    (floor(log2(items)) -> [threads, blocks per SM])."""
+    out = {}
+    for site in ("collide_convex", "collide_plane", "rewind_probe"):
+        decided = {}
+        for bucket in range(4, 25):
+            threads, per_sm, done = ctx.tuned_shape(site, 1 << bucket)
+            if done:
+                decided[str(bucket)] = [threads, per_sm]
+        out[site] = decided
+    return out
 
 
 def reference_gpu(specs, pool, n, steps, warmup, budget_s=60.0):
